@@ -1,0 +1,322 @@
+"""Benchmark of the CUDA path tracer on the BVH-stress workload.
+
+Workload: a 2^20-triangle UV sphere (1024 x 512, vertices displaced radially by seeded gradient
+noise of 5 % amplitude) inside a closed Lambertian box with one area light; 1920 x 1080 pinhole
+camera; four hero wavelengths over 360-830 nm; max depth 12, Russian roulette from depth 6. The
+scene is generated here (synthetic data; the reference ships no such scene).
+
+One step is one pass of one sample per pixel: 2,073,600 camera paths. The metric is spectral paths
+per second over the whole job; every rank renders its own sample streams of the same image (weak
+scaling) and the films are summed over NCCL once at the end.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+
+`--impl reference` times the reference engine's own CPU transport (compiled from its sources into
+oracle/_ref) on this machine's host cores over a bounded band of the same image.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "optical-pathtracer_b200")
+sys.path.insert(0, PKG)
+
+import owec_abi as A  # noqa: E402
+import scenes  # noqa: E402
+
+WIDTH, HEIGHT = 1920, 1080
+MAX_DEPTH, RR_DEPTH = 12, 6
+METRIC = "spectral paths/s"
+WORKLOAD = "bvh_stress_room: 2^20-tri displaced UV sphere in a Lambertian box, 1 area light, 1920x1080, hero-4 spectral, depth 12"
+NODE_BYTES, PRIM_BYTES = 80, 48
+RAY_STATE_BYTES = 4 + 64 + 24  # queue index, the path's ray record, the hit record written
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def settings_for(rank):
+    return A.make_settings(seed=rank, max_depth=MAX_DEPTH, rr_depth=RR_DEPTH, wavelength_mode=A.WAVELENGTHS_HERO4)
+
+
+def cpu_reference_rate(desc, seconds_target=12.0, threads=0):
+    """The reference engine (oracle/_ref) on this host: paths/s over a band of image rows through
+    the sphere, sized to about `seconds_target` of work. Returns (paths/s, threads, sample text)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_ref import ReferenceEngine  # the oracle, used here only as the timed CPU baseline
+    ref = ReferenceEngine(desc)
+    s = settings_for(0)
+    # a probe band, then one sized to the target
+    mid = HEIGHT // 2
+    band = 8
+    t0 = time.perf_counter()
+    ref.render(s, 1, pixel_begin=(mid - band // 2) * WIDTH, pixel_end=(mid + band // 2) * WIDTH, threads=threads)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    rows = int(min(HEIGHT, max(4, band * seconds_target / dt)))
+    r0 = max(0, mid - rows // 2)
+    t0 = time.perf_counter()
+    _, st = ref.render(s, 1, pixel_begin=r0 * WIDTH, pixel_end=(r0 + rows) * WIDTH, threads=threads)
+    dt = time.perf_counter() - t0
+    n_threads = threads if threads > 0 else os.cpu_count()
+    return st["paths"] / dt, n_threads, f"{rows} centre rows of the 1920x1080 frame at 1 spp ({st['paths']} paths, {dt:.1f} s)"
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    desc = scenes.bvh_stress_room(WIDTH, HEIGHT).desc()
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    try:
+        from oracle_ref import ReferenceEngine, REF_LIB
+        if not os.path.exists(REF_LIB):
+            raise RuntimeError("oracle/_ref/liboweref.so was not built")
+        ref = ReferenceEngine(desc)
+    except BaseException as e:  # pytest.skip raises a BaseException subclass
+        print(json.dumps({"impl": "reference", "unavailable": f"reference engine not built: {e}"}))
+        return 0
+    s = settings_for(0)
+    mid = HEIGHT // 2
+    # size a step to about 2-3 s of host work
+    t0 = time.perf_counter()
+    ref.render(s, 1, pixel_begin=(mid - 2) * WIDTH, pixel_end=(mid + 2) * WIDTH)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    rows = int(min(HEIGHT, max(2, 4 * 2.5 / dt)))
+    r0 = max(0, mid - rows // 2)
+    for _ in range(args.warmup):
+        ref.render(s, 1, pixel_begin=r0 * WIDTH, pixel_end=(r0 + rows) * WIDTH)
+    paths = 0
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        _, st = ref.render(s, 1, first_pass=k + 1, pixel_begin=r0 * WIDTH, pixel_end=(r0 + rows) * WIDTH)
+        paths += st["paths"]
+    dt = time.perf_counter() - t0
+    rate = paths / dt
+    cores = os.cpu_count()
+    sample = f"{rows} centre rows of the 1920x1080 frame at 1 spp per step"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": "paths/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rows_per_step": rows},
+        "cpu_baseline": {"value": rate, "unit": "paths/s", "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": rate, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+    return 0
+
+
+def run_cuda(args):
+    import torch
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    import owe_cuda
+
+    desc = scenes.bvh_stress_room(WIDTH, HEIGHT).desc()
+    backend = owe_cuda.CudaBackend()
+    renderer = backend.create_renderer(desc, settings_for(rank), device=local)
+    ctx = renderer.ctx
+    info = ctx.bvh_info()
+    n_pix = WIDTH * HEIGHT
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    for _ in range(max(3, args.warmup)):
+        ctx.run_pass(1)
+
+    # algorithmic traffic of a pass (counting pass, untimed)
+    ctx.trace_counters(1)
+    ctx.run_pass(1)
+    cnt = ctx.trace_counters(0)
+    _, isec_prof, _, launches_prof = ctx.last_pass_timing()
+
+    stats0 = ctx.stats()
+    times, isec, shadow = [], [], []
+    launches = 0
+    gpu_index = int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[local]) if os.environ.get(
+        "CUDA_VISIBLE_DEVICES") else local
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    wall0 = time.perf_counter()
+    with ClockSampler(gpu_index) as clocks:
+        for _ in range(args.steps):
+            flush.fill_(1.0)  # evict the L2 between steps
+            torch.cuda.synchronize()
+            ctx.run_pass(1)
+            t, ti, ts, nl = ctx.last_pass_timing()
+            times.append(t)
+            isec.append(ti)
+            shadow.append(ts)
+            launches += nl
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    stats1 = ctx.stats()
+    device_seconds = sum(times)
+    if world > 1:
+        t = torch.tensor([device_seconds], dtype=torch.float64, device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        device_seconds = float(t.item())
+    paths_rank = stats1["paths"] - stats0["paths"]
+    total_paths = paths_rank * world
+    value = total_paths / device_seconds
+
+    # end to end through the public API: a pass and the film read back to the host, every step
+    e2e_steps = max(2, min(args.steps, 5))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        renderer.run_pass(1)
+        img = renderer.resolve()
+    e2e_seconds = time.perf_counter() - t0
+    e2e_value = n_pix * world * e2e_steps / e2e_seconds
+    d2h = n_pix * (3 + 1) * 8
+
+    # the film over NCCL: the one exchange step of a multi-GPU render
+    if world > 1:
+        film = torch.from_numpy(np.ascontiguousarray(img)).to(f"cuda:{local}")
+        torch.distributed.all_reduce(film)
+        torch.cuda.synchronize()
+
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        q, nodes, prims = cnt[0], cnt[1], cnt[2]
+        bytes_isec = nodes * NODE_BYTES + prims * PRIM_BYTES + q * RAY_STATE_BYTES
+        per_launch_bytes = bytes_isec / max(1, launches_prof)
+        per_launch_s = isec_prof / max(1, launches_prof)
+        achieved = per_launch_bytes / per_launch_s / 1e9
+        clk = clocks.summary()
+        cpu_rate, cores, sample = (None, None, "skipped")
+        if not args.no_cpu_baseline:
+            try:
+                cpu_rate, cores, sample = cpu_reference_rate(desc)
+            except BaseException as e:  # pytest.skip when the oracle was not built
+                sample = f"unavailable: {e}"
+        line = {
+            "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * device_seconds / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "paths_per_step": n_pix, "triangles": info["triangles"],
+                       "precision": "fp32 camera-relative + selective fp64", "l2": "flushed between steps (512 MB write)",
+                       "parallelism": f"replicated scene, dp{world} over sample streams"},
+            "gpu_launches": None,
+            "rays_per_s": (stats1["segments"] - stats0["segments"] + stats1["shadow_rays"] - stats0["shadow_rays"])
+                          * world / device_seconds,
+            "segments_per_path": (stats1["segments"] - stats0["segments"]) / max(1, paths_rank),
+            "wall_seconds": wall,
+            "intersect_share": sum(isec) / sum(times),
+            "shadow_share": sum(shadow) / sum(times),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "peak_kind": peak_kind, "traffic": None, "kernel": "kIntersect",
+                         "bytes_per_launch": per_launch_bytes,
+                         "per_query": {"nodes": nodes / max(1, q), "prims": prims / max(1, q)}},
+            "clocks": clk,
+            "cpu_baseline": {"value": cpu_rate, "unit": "paths/s", "cores": cores, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
+                    "steps": e2e_steps, "note": "pass + film readback to host per step through owe_cuda.Renderer"},
+            "faults": stats1["device_faults"],
+        }
+        # our own kernel launches in the timed region: 4 per bounce + generate + film, per step
+        line["gpu_launches"] = int(launches * 4 // max(1, args.steps) * args.steps + 2 * args.steps)
+        print(json.dumps(line))
+    renderer.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_cuda(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

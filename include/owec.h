@@ -1,0 +1,288 @@
+/*
+ * owec.h — the C ABI of the B200 path-tracing backend ("cuda") of the Optical World Engine.
+ *
+ * The engine's hot path is its unidirectional spectral path tracer: the reference runs it as
+ * `Tracer::radiance` over `World::intersect` behind the `owe::Backend` / `owe::Renderer` pair
+ * (src/owe/render/backend.hpp:31-52, src/owe/render/renderer.hpp:19-79). This library replaces
+ * everything below `Renderer::pass()` and `Renderer::resolve()` with sm_100a kernels. The engine
+ * binds it through a thin C++ adapter (a `CudaBackend : owe::Backend` that flattens `owe::Scene`
+ * into `owec_scene_desc`), so the world model, scenes and front ends stay unchanged.
+ *
+ * Conventions
+ *   - Every function returns an `int` status: OWEC_OK (0) or a negative OWEC_E_* code. The
+ *     message of the last failure on the calling thread is returned by owec_last_error().
+ *     The engine's adapter turns a non-zero status into std::runtime_error, which is how the
+ *     reference reports an unusable backend (src/owe/render/backend.hpp:44).
+ *   - Lengths are metres, wavelengths nanometres, angles radians, as in the reference.
+ *   - All pointers are host pointers unless a name ends in `_dev` (device pointers).
+ *   - One context serves one thread at a time (the reference drives a Renderer from one thread,
+ *     src/owe/render/renderer.hpp:38-47). Calls are synchronous at return unless noted.
+ */
+#ifndef OWEC_H
+#define OWEC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OWEC_ABI_VERSION 1
+
+/* ------------------------------------------------------------------ status codes */
+#define OWEC_OK 0
+#define OWEC_E_INVALID (-1)      /* a bad argument or scene description                         */
+#define OWEC_E_CUDA (-2)         /* a CUDA runtime failure (no device, launch error, ...)       */
+#define OWEC_E_NOMEM (-3)        /* device or host allocation failed                            */
+#define OWEC_E_STATE (-4)        /* the call needs a step that has not been taken (no scene, ...) */
+#define OWEC_E_DEVICE_FAULT (-5) /* a kernel reported a bounded-loop overrun or queue overflow   */
+#define OWEC_E_UNSUPPORTED (-6)  /* a feature this backend does not implement                   */
+
+/* ------------------------------------------------------------------ scene description
+ * A flattened owe::World (src/owe/scene/world.hpp:1-7): media, regions, optics, emissions and
+ * boundaries in world coordinates (IEEE double), plus the environment and one detector. Indices
+ * refer to the arrays of the same description. Mirrors the reference's types field by field.
+ */
+
+/* Spectrum kinds (src/owe/core/spectrum.hpp:28-78). */
+#define OWEC_SPEC_CONSTANT 0  /* value a                                                        */
+#define OWEC_SPEC_TABULATED 1 /* piecewise linear over (lambda, value) pairs, clamped at the ends */
+#define OWEC_SPEC_BLACKBODY 2 /* Planck at a kelvin, times scale                                 */
+
+typedef struct owec_spectrum {
+    int32_t kind;
+    int32_t table_offset; /* first (lambda, value) pair in owec_scene_desc.spectrum_table */
+    int32_t table_count;  /* number of pairs                                             */
+    int32_t pad0;
+    double a;     /* constant value, or blackbody temperature in kelvin */
+    double scale; /* multiplier of tabulated and blackbody spectra (1 when unused) */
+} owec_spectrum;
+
+/* Refractive-index models (src/owe/core/medium.hpp:12-40). */
+#define OWEC_INDEX_CONSTANT 0  /* n = coef_a[0]                                        */
+#define OWEC_INDEX_CAUCHY 1    /* n = A + B/l^2 + C/l^4, (A,B,C) = coef_a[0..2], l in um */
+#define OWEC_INDEX_SELLMEIER 2 /* n^2 = 1 + sum B_i l^2/(l^2 - C_i), B = coef_a, C = coef_b */
+#define OWEC_INDEX_CIDDOR 3    /* standard dry air (Ciddor 1996 two-term form)          */
+#define OWEC_INDEX_TABULATED 4 /* n = spectrum `index_table`                            */
+
+#define OWEC_MAX_SELLMEIER_TERMS 4
+
+typedef struct owec_medium {
+    int32_t index_kind;
+    int32_t n_terms;      /* Sellmeier terms used (1..4) */
+    int32_t rel_air;      /* 1: the model is relative to air and is multiplied by n_air(l) */
+    int32_t opaque;       /* 1: never entered by light (interiors of opaque bodies) */
+    double coef_a[OWEC_MAX_SELLMEIER_TERMS];
+    double coef_b[OWEC_MAX_SELLMEIER_TERMS];
+    int32_t absorption;   /* spectrum index of sigma_a (1/m), -1 = none */
+    int32_t scattering;   /* spectrum index of sigma_s (1/m), -1 = none */
+    int32_t index_table;  /* spectrum index for OWEC_INDEX_TABULATED, else -1 */
+    int32_t pad0;
+    double g;             /* Henyey-Greenstein anisotropy */
+} owec_medium;
+
+/* Surface types (src/owe/scene/world.hpp:52-61), same order. */
+#define OWEC_SURF_NULL 0
+#define OWEC_SURF_DIELECTRIC 1
+#define OWEC_SURF_DIFFUSE 2
+#define OWEC_SURF_CONDUCTOR 3
+#define OWEC_SURF_MIRROR 4
+#define OWEC_SURF_ABSORBER 5
+#define OWEC_SURF_DETECTOR 6
+
+typedef struct owec_optics {
+    int32_t type;
+    int32_t back_absorbs;  /* thin opaque sheet with a black back */
+    int32_t reflectance;   /* spectrum index (diffuse albedo / mirror reflectance / conductor tint), -1 = 1 */
+    int32_t conductor_n;   /* spectrum index of the metal's n, -1 = none */
+    int32_t conductor_k;   /* spectrum index of the metal's k, -1 = none */
+    int32_t pad0;
+    double roughness;      /* GGX alpha; below 1e-3 the surface is smooth (a delta) */
+} owec_optics;
+
+typedef struct owec_emission {
+    int32_t radiance; /* spectrum index (Lambertian spectral radiance) */
+    int32_t front;
+    int32_t back;
+    int32_t nee;      /* 0: only seen when hit, never sampled by next-event estimation */
+    int32_t distant;  /* sampling hint for astronomical emitters */
+    int32_t pad0;
+} owec_emission;
+
+/* Shapes (src/owe/scene/geometry.hpp), in their own frames. */
+#define OWEC_SHAPE_SPHERE 0   /* params: R                                        */
+#define OWEC_SHAPE_SAG 1      /* params: c (1/R), k (conic), rMax, rMin; quadric form, vertex at 0, +z normal */
+#define OWEC_SHAPE_PLANE 2    /* params: aperture (0 disk, 1 rect, 2 ellipse), a, b */
+#define OWEC_SHAPE_CYLINDER 3 /* params: R, z0, z1                                */
+#define OWEC_SHAPE_MESH 4     /* mesh: index into owec_scene_desc.meshes           */
+
+#define OWEC_APERTURE_DISK 0 /* a = rMax, b = rMin */
+#define OWEC_APERTURE_RECT 1 /* a = halfX, b = halfY */
+#define OWEC_APERTURE_ELLIPSE 2
+
+#define OWEC_REGION_OUTSIDE 0xFFFFFFFFu /* placeholder resolved by the engine before flattening */
+
+typedef struct owec_boundary {
+    int32_t shape;
+    int32_t mesh;       /* OWEC_SHAPE_MESH: mesh index; else -1 */
+    uint32_t front;     /* region on the +normal side */
+    uint32_t back;      /* region on the -normal side */
+    uint32_t optics;
+    int32_t emission;   /* -1 = none */
+    double to_world[12];/* rigid transform shape -> world: row-major [R | t], 3 rows of 4 */
+    double params[4];
+} owec_boundary;
+
+typedef struct owec_mesh {
+    uint64_t vertex_offset; /* first vertex in owec_scene_desc.vertices (xyz triples) */
+    uint64_t vertex_count;
+    uint64_t tri_offset;    /* first triangle in owec_scene_desc.triangles (index triples, mesh-local) */
+    uint64_t tri_count;
+} owec_mesh;
+
+#define OWEC_SKY_NONE 0
+#define OWEC_SKY_UNIFORM 1
+
+typedef struct owec_environment {
+    int32_t sky_model;
+    int32_t sky_radiance;     /* spectrum index of the uniform sky, -1 = none */
+    int32_t has_sun;
+    int32_t sun_radiance;     /* spectrum index */
+    double sun_dir[3];        /* unit vector toward the sun */
+    double sun_angular_radius;/* radians; the reference default is 0.2665 degrees */
+    double sun_nee_share;     /* fraction of NEE light selections given to the sun (0 = by power) */
+} owec_environment;
+
+#define OWEC_DETECTOR_OBSERVER 0 /* IdealObserver, pinhole (src/owe/scene/detector.hpp:77-123) */
+#define OWEC_DETECTOR_SENSOR 1   /* SurfaceSensor, hemispherical (src/owe/scene/detector.hpp:125-158) */
+
+typedef struct owec_detector {
+    int32_t kind;
+    int32_t width;
+    int32_t height;
+    uint32_t region;          /* region in which camera paths start */
+    double position[3];       /* observer */
+    double look_at[3];
+    double up[3];
+    double fov_y;
+    double pixel_sigma;       /* Gaussian pixel response in pixels; 0 = the square alone */
+    uint32_t boundary;        /* sensor: its detector boundary */
+    int32_t pad0;
+    double half_x, half_y;    /* sensor: half sizes in the boundary's plane */
+} owec_detector;
+
+typedef struct owec_scene_desc {
+    uint32_t abi_version;     /* OWEC_ABI_VERSION */
+    uint32_t n_spectra, n_media, n_regions, n_optics, n_emissions, n_boundaries, n_meshes;
+    uint64_t n_spectrum_table, n_vertices, n_triangles;
+    const owec_spectrum* spectra;
+    const double* spectrum_table;  /* (lambda, value) pairs */
+    const owec_medium* media;
+    const uint32_t* region_medium; /* medium of each region; region 0 is the ambient region */
+    const owec_optics* optics;
+    const owec_emission* emissions;
+    const owec_boundary* boundaries;
+    const owec_mesh* meshes;
+    const double* vertices;        /* xyz triples, shape frame of their boundary */
+    const uint32_t* triangles;     /* index triples, counter-clockwise = front */
+    owec_environment env;
+    owec_detector detector;
+} owec_scene_desc;
+
+/* ------------------------------------------------------------------ pass settings */
+
+#define OWEC_WAVELENGTHS_HERO4 0      /* four stratified hero wavelengths (src/owe/core/wavelengths.hpp:32-44) */
+#define OWEC_WAVELENGTHS_UNIFORM1 1   /* one wavelength per path, uniform in [lambda_min, lambda_max] */
+
+#define OWEC_PRECISION_MIXED 0  /* FP32 camera-relative + FP64 root refinement, re-offset, film sums */
+#define OWEC_PRECISION_FP32 1   /* plain FP32 everywhere (the baseline the mixed mode is measured against) */
+#define OWEC_PRECISION_FP64 2   /* all-FP64 instantiation of the same kernels */
+
+typedef struct owec_settings {
+    uint64_t seed;          /* RenderSettings::seed (src/owe/scene/scene.hpp:15-49) */
+    int32_t max_depth;      /* RenderSettings::maxDepth */
+    int32_t rr_depth;       /* RenderSettings::rrDepth */
+    int32_t wavelength_mode;
+    int32_t precision;
+    double lambda_min;      /* OWEC_WAVELENGTHS_UNIFORM1 range, nm */
+    double lambda_max;
+    double fresnel_floor;   /* RenderSettings::fresnelFloor */
+} owec_settings;
+
+/* Transport statistics (src/owe/scene/transport_stats.hpp:12-31) plus device counters. */
+typedef struct owec_stats {
+    uint64_t paths, segments, inconsistencies, leaks;
+    uint64_t shadow_rays;   /* next-event visibility queries traced */
+    uint64_t device_faults; /* bounded loops that ran out (traversal stack, shadow walk guard) */
+} owec_stats;
+
+/* ------------------------------------------------------------------ context */
+
+typedef struct owec_ctx owec_ctx;
+
+/* Message of the last failure on this thread (never NULL). */
+const char* owec_last_error(void);
+/* OWEC_ABI_VERSION of the loaded library. */
+int owec_abi_version(void);
+
+/* Opens device `device` (-1: the current one). Replaces Backend::available/createRenderer's
+ * device selection (src/owe/render/backend.hpp:38-51). */
+int owec_open(int device, owec_ctx** out);
+int owec_close(owec_ctx* ctx);
+/* Name of the opened device, e.g. "NVIDIA B200". */
+int owec_device_name(owec_ctx* ctx, char* buf, size_t len);
+
+/* Copies a scene to the device: the camera-relative FP32 geometry, FP64 shape frames, media,
+ * optics and the next-event light table (World::build's buildLightTable,
+ * src/owe/scene/world.cpp:285-350). Discards the film. Replaces the scene half of
+ * CpuRenderer's constructor (src/owe/backends/cpu/cpu_backend.cpp:37-44). */
+int owec_upload_scene(owec_ctx* ctx, const owec_scene_desc* scene);
+/* Builds the wide BVH over every primitive on the device (World::build's Bvh::build and each
+ * MeshShape's, src/owe/scene/world.cpp:280, src/owe/scene/mesh.cpp:40). */
+int owec_build_bvh(owec_ctx* ctx);
+/* Node, leaf and primitive counts of the built BVH; bytes of its node and primitive arrays. */
+int owec_bvh_info(owec_ctx* ctx, uint64_t info[6]);
+
+/* Render settings used by the next passes; resets the film when they change the estimator. */
+int owec_set_settings(owec_ctx* ctx, const owec_settings* settings);
+/* One pass of `spp` samples per pixel (Renderer::pass, src/owe/render/renderer.hpp:63;
+ * CpuRenderer::pass, src/owe/backends/cpu/cpu_backend.cpp:52-94). Sample s of the pass draws
+ * from the PCG32 stream (hashCombine(seed, pixel), pass_index + s): a 1-spp pass reproduces the
+ * reference's per-pixel stream exactly. Synchronous at return. */
+int owec_pass(owec_ctx* ctx, int spp);
+/* Resolved image: XYZ per pixel (3 doubles, row-major) and samples per pixel
+ * (CpuRenderer::resolve, src/owe/backends/cpu/cpu_backend.cpp:96-107). Either pointer may be NULL. */
+int owec_resolve(owec_ctx* ctx, double* xyz, double* samples);
+/* Discards the film and the pass count (Renderer::resetObserver, src/owe/render/renderer.hpp:60). */
+int owec_reset_film(owec_ctx* ctx);
+int owec_read_stats(owec_ctx* ctx, owec_stats* stats);
+/* Timing of the last owec_pass, measured with CUDA events on the context's stream:
+ * out[0] device seconds of the whole pass, out[1] of its closest-hit (intersect) kernels,
+ * out[2] of its shadow-ray kernels, out[3] the number of intersect launches. */
+int owec_last_pass_timing(owec_ctx* ctx, double out[4]);
+
+/* Closest hits of n rays given in world coordinates (World::intersect,
+ * src/owe/scene/world.cpp:553-582, with no departure anchor). Outputs per ray: boundary index
+ * (0xFFFFFFFE on a miss, the reference's kNone), primitive (mesh triangle index, 0 for analytic
+ * shapes) and distance. Host buffers; copies are part of the call. */
+int owec_cast_rays(owec_ctx* ctx, uint64_t n, const double* origins, const double* directions,
+                   uint32_t* boundary, uint32_t* prim, double* t);
+/* The same on device buffers already resident in HBM (float32 camera-relative origins, unit
+ * float32 directions, packed xyz). Asynchronous on the context's stream; *seconds (may be NULL)
+ * receives the kernel's CUDA-event time after an implicit synchronisation when non-NULL. */
+int owec_cast_rays_device(owec_ctx* ctx, uint64_t n, const float* origins_dev, const float* directions_dev,
+                          uint32_t* boundary_dev, uint32_t* prim_dev, float* t_dev, double* seconds);
+/* Traversal counters for the algorithmic traffic of a pass. enable = 1 zeroes and starts them,
+ * 0 stops them; out (may be NULL) receives [closest-hit queries, wide nodes visited, primitives
+ * tested, shadow queries, their nodes, their primitives] counted while enabled. Counting adds
+ * atomics to the traversal kernels: never enable it in a timed pass. */
+int owec_trace_counters(owec_ctx* ctx, int enable, uint64_t out[6]);
+/* The camera-relative origin the device geometry is stored against (world = stored + origin). */
+int owec_scene_origin(owec_ctx* ctx, double origin[3]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OWEC_H */

@@ -1,0 +1,1024 @@
+// Host runtime of the CUDA backend and its C ABI (include/owec.h).
+//
+// A context owns one stream and everything on the device: the flattened scene, the wide BVH, the
+// path state of a batch of samples, the queues and the film. owec_upload_scene restates the parts of
+// World::build the kernels need (src/owe/scene/world.cpp:263-350: frames, world boxes, the scene
+// radius and the light table) and converts the geometry to camera-relative FP32. owec_pass runs
+// batches of one-sample sub-passes through the wavefront loop and folds them into the film.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "bvh_build.hpp"
+#include "owec.h"
+#include "spectral.cuh"
+#include "wavefront.hpp"
+
+using namespace owec;
+
+namespace {
+
+thread_local std::string g_error = "no error";
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& w) : std::runtime_error(w), code(c) {}
+};
+
+// ------------------------------------------------------------------ host restatements of World::build parts
+double hostCieY(double l) { return cieY(l); }
+
+// Composite Simpson over [360, 830] nm in 0.5 nm steps (spectrum.cpp:10-17).
+template <class F>
+double integrateVisible(F f) {
+    const int n = int((kLambdaMax - kLambdaMin) * 2);
+    const double h = (kLambdaMax - kLambdaMin) / n;
+    double s = f(kLambdaMin) + f(kLambdaMax);
+    for (int i = 1; i < n; ++i) s += f(kLambdaMin + i * h) * ((i & 1) ? 4 : 2);
+    return s * h / 3;
+}
+
+double cieYIntegralHost() {
+    static const double v = integrateVisible([](double l) { return hostCieY(l); });
+    return v;
+}
+
+double evalSpectrumHost(const owec_scene_desc& d, int32_t idx, double l) {
+    if (idx < 0) return 0;
+    const owec_spectrum& s = d.spectra[idx];
+    if (s.kind == OWEC_SPEC_CONSTANT) return s.a;
+    if (s.kind == OWEC_SPEC_BLACKBODY) return s.scale * planck(l, s.a);
+    const double* t = d.spectrum_table + 2 * s.table_offset;
+    const int n = s.table_count;
+    if (l <= t[0]) return s.scale * t[1];
+    if (l >= t[2 * (n - 1)]) return s.scale * t[2 * (n - 1) + 1];
+    int i = 1;
+    while (i < n && t[2 * i] <= l) ++i;
+    const double u = (l - t[2 * (i - 1)]) / (t[2 * i] - t[2 * (i - 1)]);
+    return s.scale * (t[2 * (i - 1) + 1] * (1 - u) + t[2 * i + 1] * u);
+}
+
+// Spectrum::luminance (spectrum.cpp:165-167).
+double luminanceHost(const owec_scene_desc& d, int32_t idx) {
+    return integrateVisible([&](double l) { return evalSpectrumHost(d, idx, l) * hostCieY(l); }) / cieYIntegralHost();
+}
+
+struct Box {
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    void expand(const double p[3]) {
+        for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], p[k]); hi[k] = std::max(hi[k], p[k]); }
+    }
+    bool valid() const { return lo[0] <= hi[0] && lo[1] <= hi[1] && lo[2] <= hi[2]; }
+};
+
+void xfPoint(const double m[12], const double p[3], double out[3]) {
+    for (int i = 0; i < 3; ++i) out[i] = m[4 * i] * p[0] + m[4 * i + 1] * p[1] + m[4 * i + 2] * p[2] + m[4 * i + 3];
+}
+
+// The conic sag's z range over the aperture (SagSurface's constructor, geometry.cpp:74-90).
+void sagZRange(double c, double k, double rMax, double rMin, double& zMin, double& zMax) {
+    zMin = INFINITY;
+    zMax = -INFINITY;
+    const int N = 512;
+    for (int i = 0; i <= N; ++i) {
+        const double r = rMin + (rMax - rMin) * i / N;
+        const double r2 = r * r;
+        const double z = c * r2 / (1 + std::sqrt(std::max(0.0, 1 - (1 + k) * c * c * r2)));
+        zMin = std::min(zMin, z);
+        zMax = std::max(zMax, z);
+    }
+    const double pad = 1e-9 + 1e-3 * (zMax - zMin);
+    zMin -= pad;
+    zMax += pad;
+}
+
+// A shape's bounds in its frame (Shape::bounds of the reference's shapes).
+Box localBounds(const owec_scene_desc& d, const owec_boundary& b) {
+    Box bx;
+    const double* P = b.params;
+    auto put = [&](double x0, double y0, double z0, double x1, double y1, double z1) {
+        const double a[3] = {x0, y0, z0}, c[3] = {x1, y1, z1};
+        bx.expand(a);
+        bx.expand(c);
+    };
+    switch (b.shape) {
+        case OWEC_SHAPE_SPHERE: put(-P[0], -P[0], -P[0], P[0], P[0], P[0]); break;
+        case OWEC_SHAPE_SAG: {
+            double zMin, zMax;
+            sagZRange(P[0], P[1], P[2], P[3], zMin, zMax);
+            put(-P[2], -P[2], zMin, P[2], P[2], zMax);
+            break;
+        }
+        case OWEC_SHAPE_PLANE: {
+            const double ex = P[1], ey = int(P[0]) == OWEC_APERTURE_DISK ? P[1] : P[2];
+            const double pad = 1e-9 * (1 + std::max(ex, ey));
+            put(-ex, -ey, -pad, ex, ey, pad);
+            break;
+        }
+        case OWEC_SHAPE_CYLINDER: put(-P[0], -P[0], std::min(P[1], P[2]), P[0], P[0], std::max(P[1], P[2])); break;
+        case OWEC_SHAPE_MESH: {
+            const owec_mesh& m = d.meshes[b.mesh];
+            for (uint64_t t = 0; t < m.tri_count; ++t) {
+                const uint32_t* tri = d.triangles + 3 * (m.tri_offset + t);
+                Box tb;
+                for (int k = 0; k < 3; ++k) tb.expand(d.vertices + 3 * (m.vertex_offset + tri[k]));
+                const double pad = 1e-12 * (1 + std::max({std::fabs(tb.hi[0]), std::fabs(tb.hi[1]), std::fabs(tb.hi[2])}) +
+                                            std::max({std::fabs(tb.lo[0]), std::fabs(tb.lo[1]), std::fabs(tb.lo[2])}));
+                for (int k = 0; k < 3; ++k) { tb.lo[k] -= pad; tb.hi[k] += pad; }
+                bx.expand(tb.lo);
+                bx.expand(tb.hi);
+            }
+            break;
+        }
+    }
+    return bx;
+}
+
+Box worldBox(const Box& local, const double m[12]) {
+    Box w;
+    for (int i = 0; i < 8; ++i) {
+        const double c[3] = {(i & 1) ? local.hi[0] : local.lo[0], (i & 2) ? local.hi[1] : local.lo[1],
+                             (i & 4) ? local.hi[2] : local.lo[2]};
+        double p[3];
+        xfPoint(m, c, p);
+        w.expand(p);
+    }
+    return w;
+}
+
+double shapeArea(const owec_scene_desc& d, const owec_boundary& b, bool& canSample) {
+    const double* P = b.params;
+    canSample = true;
+    switch (b.shape) {
+        case OWEC_SHAPE_SPHERE: return 4 * kPi * P[0] * P[0];
+        case OWEC_SHAPE_PLANE: {
+            const int ap = int(P[0]);
+            if (ap == OWEC_APERTURE_DISK) return kPi * (P[1] * P[1] - P[2] * P[2]);
+            if (ap == OWEC_APERTURE_RECT) return 4 * P[1] * P[2];
+            return kPi * P[1] * P[2];
+        }
+        case OWEC_SHAPE_SAG:
+            canSample = P[0] == 0;  // only a flat sag has an area sampler
+            return kPi * (P[2] * P[2] - P[3] * P[3]);
+        case OWEC_SHAPE_CYLINDER: return 2 * kPi * P[0] * std::fabs(P[2] - P[1]);
+        default: canSample = false; return 0;  // emitting meshes are not sampled by next-event estimation here
+    }
+}
+
+void invertRigid(const double m[12], double out[12]) {
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) out[4 * i + j] = m[4 * j + i];
+    for (int i = 0; i < 3; ++i)
+        out[4 * i + 3] = -(out[4 * i] * m[3] + out[4 * i + 1] * m[7] + out[4 * i + 2] * m[11]);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ the context
+struct owec_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t passStart = nullptr, passStop = nullptr;
+    std::vector<cudaEvent_t> travEvents;
+    int numSMs = 148;
+    char name[256] = {0};
+
+    // scene (host)
+    bool hasScene = false, bvhDirty = true;
+    owec_scene_desc descCopy{};
+    std::vector<owec_spectrum> spectra;
+    std::vector<double> table;
+    std::vector<owec_medium> media;
+    std::vector<uint32_t> regionMedium;
+    std::vector<owec_optics> optics;
+    std::vector<owec_emission> emissions;
+    std::vector<DBoundary> boundaries;
+    std::vector<DLight> lights;
+    std::vector<float4> primLo, primHi, triRecs;
+    std::vector<double> tri64;
+    uint32_t nTriangles = 0, nPrims = 0;
+    bool hasNull = false;
+    DeviceScene ds{};
+
+    // scene (device)
+    DBuf<owec_spectrum> dSpectra;
+    DBuf<double> dTable;
+    DBuf<owec_medium> dMedia;
+    DBuf<uint32_t> dRegionMedium;
+    DBuf<owec_optics> dOptics;
+    DBuf<owec_emission> dEmissions;
+    DBuf<DBoundary> dBoundaries;
+    DBuf<DLight> dLights;
+    DBuf<float4> dPrimLo, dPrimHi, dTri;
+    DBuf<double> dTri64;
+    BvhScratch scratch;
+    DBuf<WideNode> dNodes;
+    DBuf<uint32_t> dLeafOrder;
+    DBuf<PrimRec> dPrims;
+    DBuf<PrimRec64> dPrims64;
+    uint32_t nNodes = 0;
+    bool prims64Ready = false;
+
+    // rendering
+    owec_settings settings{1, 64, 6, OWEC_WAVELENGTHS_HERO4, OWEC_PRECISION_MIXED, 380, 780, 0};
+    uint64_t passCount = 0;  // samples per pixel accumulated (the PCG32 stream of the next sample)
+    DBuf<double> dFilm, dComp, dSamples;
+    DBuf<uint8_t> dPathRay, dPathSpec, dPathAux, dHit, dShadow;
+    DBuf<uint32_t> dQueue0, dQueue1, dQueueSurf, dQueueShadow, dCounts;
+    DBuf<StatCounters> dStats;
+    DBuf<unsigned long long> dTravCounters;
+    uint32_t capacity = 0;
+    double lastPassSeconds = 0, lastIntersectSeconds = 0, lastShadowSeconds = 0, lastIntersectLaunches = 0;
+    uint32_t* hostCounts = nullptr;  // pinned
+};
+
+namespace {
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return OWEC_OK;
+    } catch (const Error& e) {
+        g_error = e.what();
+        return e.code;
+    } catch (const CudaError& e) {
+        g_error = e.what();
+        return e.code == cudaErrorMemoryAllocation ? OWEC_E_NOMEM : OWEC_E_CUDA;
+    } catch (const std::bad_alloc&) {
+        g_error = "host allocation failed";
+        return OWEC_E_NOMEM;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return OWEC_E_INVALID;
+    }
+}
+
+void require(bool ok, const std::string& why, int code = OWEC_E_INVALID) {
+    if (!ok) throw Error(code, why);
+}
+
+void checkLaunch() {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw CudaError(e, std::string("kernel launch: ") + cudaGetErrorString(e));
+}
+
+void validateDesc(const owec_scene_desc& d) {
+    require(d.abi_version == OWEC_ABI_VERSION, "scene description ABI version mismatch");
+    require(d.n_regions >= 1 && d.region_medium, "a scene needs its ambient region");
+    for (uint32_t r = 0; r < d.n_regions; ++r) require(d.region_medium[r] < d.n_media, "region medium out of range");
+    auto specOk = [&](int32_t s) { return s < 0 || uint32_t(s) < d.n_spectra; };
+    for (uint32_t i = 0; i < d.n_spectra; ++i) {
+        const owec_spectrum& s = d.spectra[i];
+        require(s.kind >= OWEC_SPEC_CONSTANT && s.kind <= OWEC_SPEC_BLACKBODY, "unknown spectrum kind");
+        if (s.kind == OWEC_SPEC_TABULATED)
+            require(s.table_count >= 1 && uint64_t(s.table_offset) + s.table_count <= d.n_spectrum_table,
+                    "tabulated spectrum out of the table");
+    }
+    for (uint32_t i = 0; i < d.n_media; ++i) {
+        const owec_medium& m = d.media[i];
+        require(m.index_kind >= OWEC_INDEX_CONSTANT && m.index_kind <= OWEC_INDEX_TABULATED, "unknown index model");
+        require(m.index_kind != OWEC_INDEX_SELLMEIER || (m.n_terms >= 1 && m.n_terms <= OWEC_MAX_SELLMEIER_TERMS),
+                "Sellmeier needs 1 to 4 terms");
+        require(specOk(m.absorption) && specOk(m.scattering), "medium spectrum out of range");
+        require(m.index_kind != OWEC_INDEX_TABULATED || (m.index_table >= 0 && specOk(m.index_table)),
+                "tabulated index needs a spectrum");
+    }
+    for (uint32_t i = 0; i < d.n_optics; ++i) {
+        const owec_optics& o = d.optics[i];
+        require(o.type >= OWEC_SURF_NULL && o.type <= OWEC_SURF_DETECTOR, "unknown surface type");
+        require(specOk(o.reflectance) && specOk(o.conductor_n) && specOk(o.conductor_k), "optics spectrum out of range");
+    }
+    for (uint32_t i = 0; i < d.n_emissions; ++i) require(specOk(d.emissions[i].radiance) && d.emissions[i].radiance >= 0,
+                                                          "emission needs a radiance spectrum");
+    for (uint32_t i = 0; i < d.n_boundaries; ++i) {
+        const owec_boundary& b = d.boundaries[i];
+        require(b.shape >= OWEC_SHAPE_SPHERE && b.shape <= OWEC_SHAPE_MESH, "unknown shape");
+        require(b.front < d.n_regions && b.back < d.n_regions, "boundary region out of range");
+        require(b.optics < d.n_optics, "boundary optics out of range");
+        require(b.emission < 0 || uint32_t(b.emission) < d.n_emissions, "boundary emission out of range");
+        if (b.shape == OWEC_SHAPE_MESH) {
+            require(b.mesh >= 0 && uint32_t(b.mesh) < d.n_meshes, "mesh index out of range");
+            const owec_mesh& m = d.meshes[b.mesh];
+            require(m.vertex_offset + m.vertex_count <= d.n_vertices && m.tri_offset + m.tri_count <= d.n_triangles,
+                    "mesh out of the vertex or triangle arrays");
+            for (uint64_t t = 0; t < m.tri_count; ++t)
+                for (int k = 0; k < 3; ++k)
+                    require(d.triangles[3 * (m.tri_offset + t) + k] < m.vertex_count, "triangle index out of range");
+        }
+        if (b.shape == OWEC_SHAPE_SAG) {
+            const double c = b.params[0], k = b.params[1], rMax = b.params[2], rMin = b.params[3];
+            require(rMax > 0 && rMin >= 0 && rMin < rMax, "sag surface: invalid aperture radii");
+            require(1 - (1 + k) * c * c * rMax * rMax >= 0, "sag surface: aperture exceeds the conic's domain");
+        }
+        if ((d.optics[b.optics].type == OWEC_SURF_DIELECTRIC || d.optics[b.optics].type == OWEC_SURF_NULL))
+            require(!d.media[d.region_medium[b.front]].opaque && !d.media[d.region_medium[b.back]].opaque,
+                    "a transmissive boundary borders an opaque medium");
+    }
+    const owec_detector& det = d.detector;
+    require(det.width > 0 && det.height > 0 && uint64_t(det.width) * det.height <= (1ull << 28),
+            "detector resolution out of range");
+    require(det.kind == OWEC_DETECTOR_OBSERVER || det.kind == OWEC_DETECTOR_SENSOR, "unknown detector kind");
+    if (det.kind == OWEC_DETECTOR_SENSOR) {
+        require(det.boundary < d.n_boundaries, "sensor boundary out of range");
+        require(det.half_x > 0 && det.half_y > 0, "sensor needs a size");
+    } else {
+        require(det.region < d.n_regions, "observer region out of range (the engine locates it before flattening)");
+        require(det.fov_y > 0 && det.fov_y < kPi, "observer field of view out of range");
+    }
+    require(d.env.sky_model == OWEC_SKY_NONE || d.env.sky_model == OWEC_SKY_UNIFORM, "unknown sky model");
+    require(specOk(d.env.sky_radiance) && specOk(d.env.sun_radiance), "environment spectrum out of range");
+}
+
+void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
+    validateDesc(d);
+    cudaStream_t s = c.stream;
+    c.spectra.assign(d.spectra, d.spectra + d.n_spectra);
+    c.table.assign(d.spectrum_table, d.spectrum_table + 2 * d.n_spectrum_table);
+    c.media.assign(d.media, d.media + d.n_media);
+    c.regionMedium.assign(d.region_medium, d.region_medium + d.n_regions);
+    c.optics.assign(d.optics, d.optics + d.n_optics);
+    c.emissions.assign(d.emissions, d.emissions + d.n_emissions);
+
+    // The camera-relative origin: the observer's position, or the sensor's centre.
+    double origin[3];
+    if (d.detector.kind == OWEC_DETECTOR_OBSERVER) {
+        for (int k = 0; k < 3; ++k) origin[k] = d.detector.position[k];
+    } else {
+        const double* m = d.boundaries[d.detector.boundary].to_world;
+        origin[0] = m[3]; origin[1] = m[7]; origin[2] = m[11];
+    }
+
+    // Boundaries: frames relative to the origin, world boxes, emitter areas.
+    Box scene;
+    c.boundaries.resize(d.n_boundaries);
+    std::vector<Box> wboxes(d.n_boundaries);
+    c.hasNull = false;
+    for (uint32_t i = 0; i < d.n_boundaries; ++i) {
+        const owec_boundary& b = d.boundaries[i];
+        DBoundary& db = c.boundaries[i];
+        db.shape = b.shape;
+        db.emission = b.emission;
+        db.front = b.front;
+        db.back = b.back;
+        db.optics = b.optics;
+        db.light = -1;
+        for (int k = 0; k < 12; ++k) db.toWorld.m[k] = b.to_world[k];
+        wboxes[i] = worldBox(localBounds(d, b), b.to_world);
+        scene.expand(wboxes[i].lo);
+        scene.expand(wboxes[i].hi);
+        db.toWorld.m[3] -= origin[0];
+        db.toWorld.m[7] -= origin[1];
+        db.toWorld.m[11] -= origin[2];
+        invertRigid(db.toWorld.m, db.toLocal.m);
+        for (int k = 0; k < 4; ++k) db.params[k] = b.params[k];
+        bool canSample = false;
+        db.area = shapeArea(d, b, canSample);
+        if (!canSample) db.area = 0;
+        db.scale = 0;
+        for (int k = 0; k < 3; ++k) db.scale = std::max(db.scale, wboxes[i].hi[k] - wboxes[i].lo[k]);
+        if (d.optics[b.optics].type == OWEC_SURF_NULL) c.hasNull = true;
+    }
+    double sceneRadius = 1.0, center[3] = {0, 0, 0};
+    if (scene.valid()) {
+        double e2 = 0;
+        for (int k = 0; k < 3; ++k) {
+            e2 += (scene.hi[k] - scene.lo[k]) * (scene.hi[k] - scene.lo[k]);
+            center[k] = 0.5 * (scene.lo[k] + scene.hi[k]) - origin[k];
+        }
+        sceneRadius = std::max(1e-3, 0.5 * std::sqrt(e2));
+    }
+
+    // The light table (World::buildLightTable, world.cpp:285-350; no environment map here).
+    c.lights.clear();
+    std::vector<double> power;
+    std::vector<int> distant;
+    for (uint32_t i = 0; i < d.n_boundaries; ++i) {
+        const owec_boundary& b = d.boundaries[i];
+        if (b.emission < 0) continue;
+        const owec_emission& e = d.emissions[b.emission];
+        bool canSample = false;
+        const double area = shapeArea(d, b, canSample);
+        if (!canSample || !(area > 0) || !e.nee) continue;
+        const double sides = (e.front ? 1 : 0) + (e.back ? 1 : 0);
+        c.boundaries[i].light = int(c.lights.size());
+        c.lights.push_back(DLight{kLightBoundary, i, 0, 0});
+        power.push_back(std::max(1e-12, luminanceHost(d, e.radiance)) * area * kPi * sides);
+        distant.push_back(e.distant);
+    }
+    const double cosMax = std::cos(d.env.sun_angular_radius);
+    const double sunSolid = 2 * kPi * (1 - cosMax);
+    if (d.env.has_sun) {
+        c.lights.push_back(DLight{kLightSun, kNone, 0, 0});
+        power.push_back(std::max(1e-12, luminanceHost(d, d.env.sun_radiance)) * sunSolid * kPi * sceneRadius * sceneRadius);
+        distant.push_back(0);
+    }
+    double total = 0, boundaryPower = 0, nearbyPower = 0, distantPower = 0;
+    for (size_t l = 0; l < c.lights.size(); ++l) {
+        total += power[l];
+        if (c.lights[l].kind == kLightBoundary) {
+            boundaryPower += power[l];
+            (distant[l] ? distantPower : nearbyPower) += power[l];
+        }
+    }
+    double share = d.env.has_sun && boundaryPower > 0 ? std::min(0.999, std::max(0.0, d.env.sun_nee_share)) : 0;
+    if (distantPower > 0 && d.env.has_sun && share == 0) share = 0.5;
+    double acc = 0, sunSel = 0;
+    for (size_t l = 0; l < c.lights.size(); ++l) {
+        double p = total > 0 ? power[l] / total : 0;
+        if (share > 0) p = c.lights[l].kind == kLightSun ? share : (1 - share) * power[l] / boundaryPower;
+        if (distantPower > 0 && c.lights[l].kind == kLightBoundary) {
+            const double groupShare = nearbyPower > 0 ? 0.5 : 1;
+            p = (1 - share) * groupShare * power[l] / (distant[l] ? distantPower : nearbyPower);
+        }
+        c.lights[l].pdf = p;
+        acc += p;
+        c.lights[l].cdf = acc;
+        if (c.lights[l].kind == kLightSun) sunSel = p;
+    }
+    if (!c.lights.empty()) c.lights.back().cdf = 1.0;
+
+    // Primitives: every mesh triangle (camera-relative FP32, and FP64 for the all-FP64 mode), then
+    // every analytic boundary as one primitive of its own world box.
+    c.triRecs.clear();
+    c.tri64.clear();
+    c.primLo.clear();
+    c.primHi.clear();
+    auto padBox = [](const double lo[3], const double hi[3], float4& flo, float4& fhi) {
+        double ext = 0, mag = 0;
+        for (int k = 0; k < 3; ++k) {
+            ext = std::max(ext, hi[k] - lo[k]);
+            mag = std::max({mag, std::fabs(lo[k]), std::fabs(hi[k])});
+        }
+        const double pad = 1e-6 * (mag + ext) + 1e-9;
+        flo = make_float4(std::nextafter(float(lo[0] - pad), -INFINITY), std::nextafter(float(lo[1] - pad), -INFINITY),
+                          std::nextafter(float(lo[2] - pad), -INFINITY), 0.f);
+        fhi = make_float4(std::nextafter(float(hi[0] + pad), INFINITY), std::nextafter(float(hi[1] + pad), INFINITY),
+                          std::nextafter(float(hi[2] + pad), INFINITY), 0.f);
+    };
+    auto asF = [](uint32_t v) { float f; std::memcpy(&f, &v, 4); return f; };
+    for (uint32_t i = 0; i < d.n_boundaries; ++i) {
+        const owec_boundary& b = d.boundaries[i];
+        if (b.shape != OWEC_SHAPE_MESH) continue;
+        const owec_mesh& m = d.meshes[b.mesh];
+        double rel[12];
+        std::memcpy(rel, c.boundaries[i].toWorld.m, sizeof(rel));
+        for (uint64_t t = 0; t < m.tri_count; ++t) {
+            const uint32_t* tri = d.triangles + 3 * (m.tri_offset + t);
+            double w[3][3];
+            for (int k = 0; k < 3; ++k) xfPoint(rel, d.vertices + 3 * (m.vertex_offset + tri[k]), w[k]);
+            const uint32_t ids[3] = {i, uint32_t(t), kPrimTriangle};
+            double lo[3], hi[3];
+            for (int k = 0; k < 3; ++k) {
+                c.triRecs.push_back(make_float4(float(w[k][0]), float(w[k][1]), float(w[k][2]), asF(ids[k])));
+                for (int a = 0; a < 3; ++a) c.tri64.push_back(w[k][a]);
+            }
+            for (int a = 0; a < 3; ++a) {
+                // the box of the FP32 vertices (what the FP32 traversal tests), padded outward
+                float f0 = float(w[0][a]), f1 = float(w[1][a]), f2 = float(w[2][a]);
+                lo[a] = std::min({double(f0), double(f1), double(f2), w[0][a], w[1][a], w[2][a]});
+                hi[a] = std::max({double(f0), double(f1), double(f2), w[0][a], w[1][a], w[2][a]});
+            }
+            float4 flo, fhi;
+            padBox(lo, hi, flo, fhi);
+            c.primLo.push_back(flo);
+            c.primHi.push_back(fhi);
+        }
+    }
+    c.nTriangles = uint32_t(c.primLo.size());
+    for (uint32_t i = 0; i < d.n_boundaries; ++i) {
+        if (d.boundaries[i].shape == OWEC_SHAPE_MESH) continue;
+        const uint32_t ids[3] = {i, 0u, kPrimAnalytic};
+        for (int k = 0; k < 3; ++k) {
+            c.triRecs.push_back(make_float4(0.f, 0.f, 0.f, asF(ids[k])));
+            for (int a = 0; a < 3; ++a) c.tri64.push_back(0.0);
+        }
+        double lo[3], hi[3];
+        for (int k = 0; k < 3; ++k) { lo[k] = wboxes[i].lo[k] - origin[k]; hi[k] = wboxes[i].hi[k] - origin[k]; }
+        float4 flo, fhi;
+        padBox(lo, hi, flo, fhi);
+        c.primLo.push_back(flo);
+        c.primHi.push_back(fhi);
+    }
+    c.nPrims = uint32_t(c.primLo.size());
+
+    // The detector (IdealObserver::prepare, detector.cpp:46-59; SurfaceSensor::prepare, :102-111).
+    DDetector det{};
+    const owec_detector& dd = d.detector;
+    det.kind = dd.kind;
+    det.width = dd.width;
+    det.height = dd.height;
+    det.sigma = dd.pixel_sigma;
+    if (dd.kind == OWEC_DETECTOR_OBSERVER) {
+        double f[3], u[3] = {dd.up[0], dd.up[1], dd.up[2]};
+        double fl = 0;
+        for (int k = 0; k < 3; ++k) { f[k] = dd.look_at[k] - dd.position[k]; fl += f[k] * f[k]; }
+        fl = std::sqrt(fl);
+        require(fl > 0, "observer looks at its own position");
+        for (double& x : f) x /= fl;
+        const double ul = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        if (std::fabs((u[0] * f[0] + u[1] * f[1] + u[2] * f[2]) / ul) > 0.9999) {
+            u[0] = 0; u[1] = 0; u[2] = 0;
+            if (std::fabs(f[2]) < 0.9) u[2] = 1; else u[1] = 1;
+        }
+        double r[3] = {f[1] * u[2] - f[2] * u[1], f[2] * u[0] - f[0] * u[2], f[0] * u[1] - f[1] * u[0]};
+        const double rl = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+        for (double& x : r) x /= rl;
+        const double up[3] = {r[1] * f[2] - r[2] * f[1], r[2] * f[0] - r[0] * f[2], r[0] * f[1] - r[1] * f[0]};
+        for (int k = 0; k < 3; ++k) {
+            det.fwd[k] = f[k];
+            det.right[k] = r[k];
+            det.up[k] = up[k];
+            det.pos[k] = dd.position[k] - origin[k];
+        }
+        det.tanY = std::tan(0.5 * dd.fov_y);
+        det.tanX = det.tanY * double(dd.width) / double(dd.height);
+        det.region = dd.region;
+    } else {
+        const owec_boundary& b = d.boundaries[dd.boundary];
+        require(d.optics[b.optics].type == OWEC_SURF_DETECTOR || d.optics[b.optics].type == OWEC_SURF_DIFFUSE,
+                "sensor boundary is not a detector surface");
+        det.boundary = dd.boundary;
+        det.halfX = dd.half_x;
+        det.halfY = dd.half_y;
+        double nrm[3] = {b.to_world[2], b.to_world[6], b.to_world[10]};
+        const double nl = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+        for (int k = 0; k < 3; ++k) det.normal[k] = nrm[k] / nl;
+        det.region = b.front;
+    }
+
+    // Upload.
+    c.dSpectra.upload(c.spectra.data(), c.spectra.size(), s);
+    c.dTable.upload(c.table.data(), std::max<size_t>(2, c.table.size()), s);  // never empty
+    c.dMedia.upload(c.media.data(), c.media.size(), s);
+    c.dRegionMedium.upload(c.regionMedium.data(), c.regionMedium.size(), s);
+    c.dOptics.upload(c.optics.data(), c.optics.size(), s);
+    c.dEmissions.upload(c.emissions.data(), c.emissions.size(), s);
+    c.dBoundaries.upload(c.boundaries.data(), c.boundaries.size(), s);
+    c.dLights.upload(c.lights.data(), c.lights.size(), s);
+    c.dPrimLo.upload(c.primLo.data(), c.primLo.size(), s);
+    c.dPrimHi.upload(c.primHi.data(), c.primHi.size(), s);
+    c.dTri.upload(c.triRecs.data(), c.triRecs.size(), s);
+    OWEC_CUDA(cudaStreamSynchronize(s));  // the host vectors above may change after this call
+
+    DeviceScene& ds = c.ds;
+    ds = DeviceScene{};
+    ds.spectra = c.dSpectra.get();
+    ds.table = c.dTable.get();
+    ds.media = c.dMedia.get();
+    ds.regionMedium = c.dRegionMedium.get();
+    ds.optics = c.dOptics.get();
+    ds.emissions = c.dEmissions.get();
+    ds.boundaries = c.dBoundaries.get();
+    ds.lights = c.dLights.get();
+    ds.nRegions = d.n_regions;
+    ds.nBoundaries = d.n_boundaries;
+    ds.nLights = uint32_t(c.lights.size());
+    ds.nMedia = d.n_media;
+    ds.skyModel = d.env.sky_model;
+    ds.skySpectrum = d.env.sky_radiance;
+    ds.hasSun = d.env.has_sun;
+    ds.sunSpectrum = d.env.sun_radiance;
+    double sl = std::sqrt(d.env.sun_dir[0] * d.env.sun_dir[0] + d.env.sun_dir[1] * d.env.sun_dir[1] +
+                          d.env.sun_dir[2] * d.env.sun_dir[2]);
+    if (!(sl > 0)) sl = 1;
+    for (int k = 0; k < 3; ++k) {
+        ds.sunDir[k] = d.env.sun_dir[k] / sl;
+        ds.sceneCenter[k] = center[k];
+        ds.origin[k] = origin[k];
+    }
+    ds.sunCosMax = cosMax;
+    ds.sunSolidAngle = sunSolid;
+    ds.sunSelectPdf = sunSel;
+    ds.sceneRadius = sceneRadius;
+    ds.det = det;
+    ds.cieYIntegral = cieYIntegralHost();
+    ds.contactScale = sceneRadius;
+    c.hasScene = true;
+    c.bvhDirty = true;
+    c.prims64Ready = false;
+    c.passCount = 0;
+    c.dFilm.release();
+    c.dComp.release();
+    c.dSamples.release();
+}
+
+void buildBvh(owec_ctx& c) {
+    require(c.hasScene, "no scene uploaded", OWEC_E_STATE);
+    require(c.nPrims > 0, "the scene has no boundaries");
+    c.nNodes = buildWideBvh(c.dPrimLo.get(), c.dPrimHi.get(), c.nPrims, c.scratch, c.dNodes, c.dLeafOrder, c.stream);
+    c.dPrims.reserve(c.nPrims);
+    launchMaterialize(c.dLeafOrder.get(), c.nPrims, c.dTri.get(), nullptr, c.dPrims.get(), nullptr, c.stream);
+    checkLaunch();
+    OWEC_CUDA(cudaStreamSynchronize(c.stream));
+    c.ds.nodes = c.dNodes.get();
+    c.ds.prims = c.dPrims.get();
+    c.ds.nNodes = c.nNodes;
+    c.ds.nPrims = c.nPrims;
+    c.bvhDirty = false;
+    c.prims64Ready = false;
+}
+
+void ensurePrims64(owec_ctx& c) {
+    if (c.prims64Ready) return;
+    c.dTri64.upload(c.tri64.data(), c.tri64.size(), c.stream);
+    c.dPrims64.reserve(c.nPrims);
+    launchMaterialize(c.dLeafOrder.get(), c.nPrims, c.dTri.get(), c.dTri64.get(), c.dPrims.get(), c.dPrims64.get(),
+                      c.stream);
+    checkLaunch();
+    OWEC_CUDA(cudaStreamSynchronize(c.stream));
+    c.ds.prims64 = c.dPrims64.get();
+    c.prims64Ready = true;
+}
+
+void ensureReady(owec_ctx& c) {
+    require(c.hasScene, "no scene uploaded", OWEC_E_STATE);
+    if (c.bvhDirty) buildBvh(c);
+    if (c.settings.precision == OWEC_PRECISION_FP64) ensurePrims64(c);
+}
+
+void ensureFilm(owec_ctx& c) {
+    const size_t np = size_t(c.ds.det.width) * c.ds.det.height;
+    if (c.dFilm.size() != 3 * np) {
+        c.dFilm.resize(3 * np);
+        c.dComp.resize(3 * np);
+        c.dSamples.resize(np);
+        OWEC_CUDA(cudaMemsetAsync(c.dFilm.get(), 0, c.dFilm.bytes(), c.stream));
+        OWEC_CUDA(cudaMemsetAsync(c.dComp.get(), 0, c.dComp.bytes(), c.stream));
+        OWEC_CUDA(cudaMemsetAsync(c.dSamples.get(), 0, c.dSamples.bytes(), c.stream));
+    }
+}
+
+template <int M>
+void runPass(owec_ctx& c, int spp) {
+    using R = ModeR<M>;
+    const uint32_t nPix = uint32_t(c.ds.det.width) * uint32_t(c.ds.det.height);
+    // Paths in flight: enough to fill the GPU several times over (2M+), within the state budget.
+    const uint32_t target = std::max<uint32_t>(nPix, 1u << 21);
+    uint32_t perBatch = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(spp), target / nPix));
+    const uint32_t cap = perBatch * nPix;
+    if (c.capacity < cap || c.dPathRay.bytes() < size_t(cap) * sizeof(PathRay<R>) ||
+        c.dShadow.bytes() < size_t(cap) * sizeof(ShadowRay<R>)) {
+        c.dPathRay.resize(size_t(cap) * sizeof(PathRay<R>));
+        c.dPathSpec.resize(size_t(cap) * sizeof(PathSpec<R>));
+        c.dPathAux.resize(size_t(cap) * sizeof(PathAux));
+        c.dHit.resize(size_t(cap) * sizeof(HitRec));
+        c.dShadow.resize(size_t(cap) * sizeof(ShadowRay<R>));
+        c.dQueue0.resize(cap);
+        c.dQueue1.resize(cap);
+        c.dQueueSurf.resize(cap);
+        c.dQueueShadow.resize(cap);
+        c.capacity = cap;
+    }
+    PathBuffers<R> pb{reinterpret_cast<PathRay<R>*>(c.dPathRay.get()), reinterpret_cast<PathSpec<R>*>(c.dPathSpec.get()),
+                      reinterpret_cast<PathAux*>(c.dPathAux.get()), reinterpret_cast<HitRec*>(c.dHit.get()),
+                      reinterpret_cast<ShadowRay<R>*>(c.dShadow.get())};
+    Queues q{{c.dQueue0.get(), c.dQueue1.get()}, c.dQueueSurf.get(), c.dQueueShadow.get(), c.dCounts.get()};
+    PassParams pp{};
+    pp.seed = c.settings.seed;
+    pp.maxDepth = c.settings.max_depth;
+    pp.rrDepth = c.settings.rr_depth;
+    pp.wavelengthMode = c.settings.wavelength_mode;
+    pp.lambdaMin = float(c.settings.lambda_min);
+    pp.lambdaMax = float(c.settings.lambda_max);
+    pp.fresnelFloor = float(std::min(0.49, std::max(0.0, c.settings.fresnel_floor)));
+    pp.nPixels = nPix;
+    pp.anyHitShadows = c.hasNull ? 0 : 1;
+    const int grid = c.numSMs * 8;
+    cudaStream_t s = c.stream;
+    double travSeconds[2] = {0, 0};
+    int intersectLaunches = 0;
+    OWEC_CUDA(cudaEventRecord(c.passStart, s));
+    int evUsed = 0;
+    for (int done = 0; done < spp;) {
+        const uint32_t S = std::min<uint32_t>(perBatch, uint32_t(spp - done));
+        pp.nPaths = S * nPix;
+        pp.streamBase = uint32_t(c.passCount + done);
+        OWEC_CUDA(cudaMemsetAsync(c.dCounts.get(), 0, 8 * sizeof(uint32_t), s));
+        launchGenerate<M>(c.ds, pp, pb, q, c.dStats.get(), s);
+        checkLaunch();
+        int cur = 0;
+        for (int bounce = 0; bounce < 4 * pp.maxDepth + 8; ++bounce) {
+            if ((bounce & 1) == 0 || bounce > 2) {
+                OWEC_CUDA(cudaMemcpyAsync(c.hostCounts, c.dCounts.get(), 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+                OWEC_CUDA(cudaStreamSynchronize(s));
+                if (c.hostCounts[cur] == 0) break;
+            }
+            // the next-bounce queue and the per-bounce queues start empty
+            OWEC_CUDA(cudaMemsetAsync(c.dCounts.get() + (cur ^ 1), 0, sizeof(uint32_t), s));
+            OWEC_CUDA(cudaMemsetAsync(c.dCounts.get() + 2, 0, 2 * sizeof(uint32_t), s));
+            if (size_t(evUsed + 4) > c.travEvents.size())
+                for (int k = 0; k < 4; ++k) {
+                    cudaEvent_t e;
+                    OWEC_CUDA(cudaEventCreate(&e));
+                    c.travEvents.push_back(e);
+                }
+            OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed], s));
+            launchIntersect<M>(c.ds, pb, q, cur, c.dStats.get(), grid, s);
+            ++intersectLaunches;
+            OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 1], s));
+            checkLaunch();
+            launchMedium<M>(c.ds, pp, pb, q, cur, c.dStats.get(), grid, s);
+            launchSurface<M>(c.ds, pp, pb, q, cur, c.dStats.get(), grid, s);
+            OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 2], s));
+            launchShadow<M>(c.ds, pp, pb, q, c.dStats.get(), grid, s);
+            OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 3], s));
+            checkLaunch();
+            evUsed += 4;
+            OWEC_CUDA(cudaMemsetAsync(c.dCounts.get() + cur, 0, sizeof(uint32_t), s));
+            cur ^= 1;
+            if (evUsed >= 256) {  // fold the timings in before reusing the events
+                OWEC_CUDA(cudaStreamSynchronize(s));
+                for (int e = 0; e < evUsed; e += 2) {
+                    float ms = 0;
+                    OWEC_CUDA(cudaEventElapsedTime(&ms, c.travEvents[e], c.travEvents[e + 1]));
+                    travSeconds[(e >> 1) & 1] += ms * 1e-3;
+                }
+                evUsed = 0;
+            }
+        }
+        launchFilm<M>(c.ds, pp, pb, c.dFilm.get(), c.dComp.get(), c.dSamples.get(), S, s);
+        checkLaunch();
+        done += int(S);
+    }
+    OWEC_CUDA(cudaEventRecord(c.passStop, s));
+    OWEC_CUDA(cudaEventSynchronize(c.passStop));
+    for (int e = 0; e < evUsed; e += 2) {
+        float ms = 0;
+        OWEC_CUDA(cudaEventElapsedTime(&ms, c.travEvents[e], c.travEvents[e + 1]));
+        travSeconds[(e >> 1) & 1] += ms * 1e-3;  // pairs alternate: intersect, shadow
+    }
+    float passMs = 0;
+    OWEC_CUDA(cudaEventElapsedTime(&passMs, c.passStart, c.passStop));
+    c.lastPassSeconds = passMs * 1e-3;
+    c.lastIntersectSeconds = travSeconds[0];
+    c.lastShadowSeconds = travSeconds[1];
+    c.lastIntersectLaunches = intersectLaunches;
+    c.passCount += uint64_t(spp);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ the C ABI
+extern "C" {
+
+const char* owec_last_error(void) { return g_error.c_str(); }
+int owec_abi_version(void) { return OWEC_ABI_VERSION; }
+
+int owec_open(int device, owec_ctx** out) {
+    return guarded([&] {
+        require(out != nullptr, "owec_open: null output");
+        *out = nullptr;
+        int count = 0;
+        const cudaError_t e = cudaGetDeviceCount(&count);
+        if (e != cudaSuccess || count == 0) throw Error(OWEC_E_CUDA, "no CUDA device available");
+        if (device < 0) OWEC_CUDA(cudaGetDevice(&device));
+        require(device < count, "device index out of range");
+        OWEC_CUDA(cudaSetDevice(device));
+        auto c = std::make_unique<owec_ctx>();
+        c->device = device;
+        cudaDeviceProp prop;
+        OWEC_CUDA(cudaGetDeviceProperties(&prop, device));
+        c->numSMs = prop.multiProcessorCount;
+        std::snprintf(c->name, sizeof(c->name), "%s", prop.name);
+        OWEC_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        OWEC_CUDA(cudaEventCreate(&c->passStart));
+        OWEC_CUDA(cudaEventCreate(&c->passStop));
+        OWEC_CUDA(cudaMallocHost(&c->hostCounts, 8 * sizeof(uint32_t)));
+        c->dCounts.resize(8);
+        c->dStats.resize(1);
+        OWEC_CUDA(cudaMemsetAsync(c->dStats.get(), 0, sizeof(StatCounters), c->stream));
+        configureKernels();
+        OWEC_CUDA(cudaStreamSynchronize(c->stream));
+        *out = c.release();
+    });
+}
+
+int owec_close(owec_ctx* ctx) {
+    if (!ctx) return OWEC_OK;
+    return guarded([&] {
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+        for (cudaEvent_t e : ctx->travEvents) cudaEventDestroy(e);
+        cudaEventDestroy(ctx->passStart);
+        cudaEventDestroy(ctx->passStop);
+        cudaFreeHost(ctx->hostCounts);
+        cudaStream_t s = ctx->stream;
+        delete ctx;  // frees the device buffers
+        cudaStreamDestroy(s);
+    });
+}
+
+int owec_device_name(owec_ctx* ctx, char* buf, size_t len) {
+    return guarded([&] {
+        require(ctx && buf && len > 0, "owec_device_name: bad arguments");
+        std::snprintf(buf, len, "%s", ctx->name);
+    });
+}
+
+int owec_upload_scene(owec_ctx* ctx, const owec_scene_desc* scene) {
+    return guarded([&] {
+        require(ctx && scene, "owec_upload_scene: null argument");
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        uploadScene(*ctx, *scene);
+    });
+}
+
+int owec_build_bvh(owec_ctx* ctx) {
+    return guarded([&] {
+        require(ctx != nullptr, "owec_build_bvh: null context");
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        buildBvh(*ctx);
+    });
+}
+
+int owec_bvh_info(owec_ctx* ctx, uint64_t info[6]) {
+    return guarded([&] {
+        require(ctx && info, "owec_bvh_info: null argument");
+        require(!ctx->bvhDirty, "the BVH is not built", OWEC_E_STATE);
+        info[0] = ctx->nNodes;
+        info[1] = ctx->nPrims;
+        info[2] = ctx->nTriangles;
+        info[3] = uint64_t(ctx->nNodes) * sizeof(WideNode);
+        info[4] = uint64_t(ctx->nPrims) * sizeof(PrimRec);
+        info[5] = ctx->nPrims - ctx->nTriangles;
+    });
+}
+
+int owec_set_settings(owec_ctx* ctx, const owec_settings* s) {
+    return guarded([&] {
+        require(ctx && s, "owec_set_settings: null argument");
+        require(s->max_depth >= 0 && s->max_depth <= 4096 && s->rr_depth >= 0, "depth out of range");
+        require(s->wavelength_mode == OWEC_WAVELENGTHS_HERO4 || s->wavelength_mode == OWEC_WAVELENGTHS_UNIFORM1,
+                "unknown wavelength mode");
+        require(s->precision >= OWEC_PRECISION_MIXED && s->precision <= OWEC_PRECISION_FP64, "unknown precision mode");
+        require(s->wavelength_mode != OWEC_WAVELENGTHS_UNIFORM1 ||
+                    (s->lambda_min > 0 && s->lambda_max > s->lambda_min), "bad wavelength range");
+        const bool estimatorChange = std::memcmp(s, &ctx->settings, sizeof(owec_settings)) != 0;
+        ctx->settings = *s;
+        if (estimatorChange) {
+            ctx->passCount = 0;
+            ctx->dFilm.release();
+            ctx->dComp.release();
+            ctx->dSamples.release();
+        }
+    });
+}
+
+int owec_pass(owec_ctx* ctx, int spp) {
+    return guarded([&] {
+        require(ctx != nullptr, "owec_pass: null context");
+        if (spp <= 0) return;
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        ensureReady(*ctx);
+        ensureFilm(*ctx);
+        switch (ctx->settings.precision) {
+            case OWEC_PRECISION_MIXED: runPass<OWEC_PRECISION_MIXED>(*ctx, spp); break;
+            case OWEC_PRECISION_FP32: runPass<OWEC_PRECISION_FP32>(*ctx, spp); break;
+            default: runPass<OWEC_PRECISION_FP64>(*ctx, spp); break;
+        }
+    });
+}
+
+int owec_resolve(owec_ctx* ctx, double* xyz, double* samples) {
+    return guarded([&] {
+        require(ctx != nullptr, "owec_resolve: null context");
+        require(ctx->hasScene, "no scene uploaded", OWEC_E_STATE);
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        ensureFilm(*ctx);
+        const size_t np = size_t(ctx->ds.det.width) * ctx->ds.det.height;
+        std::vector<double> film(3 * np), comp(3 * np), n(np);
+        OWEC_CUDA(cudaMemcpyAsync(film.data(), ctx->dFilm.get(), film.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        OWEC_CUDA(cudaMemcpyAsync(comp.data(), ctx->dComp.get(), comp.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        OWEC_CUDA(cudaMemcpyAsync(n.data(), ctx->dSamples.get(), n.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (size_t i = 0; i < np; ++i) {
+            const double norm = n[i] > 0 ? 1.0 / n[i] : 0;
+            if (xyz)
+                for (int ch = 0; ch < 3; ++ch) xyz[3 * i + ch] = (film[3 * i + ch] - comp[3 * i + ch]) * norm;
+            if (samples) samples[i] = n[i];
+        }
+    });
+}
+
+int owec_reset_film(owec_ctx* ctx) {
+    return guarded([&] {
+        require(ctx != nullptr, "owec_reset_film: null context");
+        ctx->passCount = 0;
+        ctx->dFilm.release();
+        ctx->dComp.release();
+        ctx->dSamples.release();
+        OWEC_CUDA(cudaMemsetAsync(ctx->dStats.get(), 0, sizeof(StatCounters), ctx->stream));
+        OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int owec_read_stats(owec_ctx* ctx, owec_stats* out) {
+    return guarded([&] {
+        require(ctx && out, "owec_read_stats: null argument");
+        StatCounters h{};
+        OWEC_CUDA(cudaMemcpyAsync(&h, ctx->dStats.get(), sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+        OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+        out->paths = h.paths;
+        out->segments = h.segments;
+        out->inconsistencies = h.inconsistencies;
+        out->leaks = h.leaks;
+        out->shadow_rays = h.shadowRays;
+        out->device_faults = h.faults;
+    });
+}
+
+int owec_last_pass_timing(owec_ctx* ctx, double out[4]) {
+    return guarded([&] {
+        require(ctx && out, "owec_last_pass_timing: null argument");
+        out[0] = ctx->lastPassSeconds;
+        out[1] = ctx->lastIntersectSeconds;
+        out[2] = ctx->lastShadowSeconds;
+        out[3] = ctx->lastIntersectLaunches;
+    });
+}
+
+int owec_cast_rays(owec_ctx* ctx, uint64_t n, const double* origins, const double* directions, uint32_t* boundary,
+                   uint32_t* prim, double* t) {
+    return guarded([&] {
+        require(ctx && (n == 0 || (origins && directions && boundary && prim && t)), "owec_cast_rays: null argument");
+        if (n == 0) return;
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        ensureReady(*ctx);
+        DBuf<double> o(3 * n), d(3 * n), tt(n);
+        DBuf<uint32_t> b(n), p(n);
+        OWEC_CUDA(cudaMemcpyAsync(o.get(), origins, 24 * n, cudaMemcpyHostToDevice, ctx->stream));
+        OWEC_CUDA(cudaMemcpyAsync(d.get(), directions, 24 * n, cudaMemcpyHostToDevice, ctx->stream));
+        const int grid = ctx->numSMs * 8;
+        switch (ctx->settings.precision) {
+            case OWEC_PRECISION_MIXED:
+                launchCastRays<OWEC_PRECISION_MIXED>(ctx->ds, n, o.get(), d.get(), b.get(), p.get(), tt.get(), grid, ctx->stream);
+                break;
+            case OWEC_PRECISION_FP32:
+                launchCastRays<OWEC_PRECISION_FP32>(ctx->ds, n, o.get(), d.get(), b.get(), p.get(), tt.get(), grid, ctx->stream);
+                break;
+            default:
+                launchCastRays<OWEC_PRECISION_FP64>(ctx->ds, n, o.get(), d.get(), b.get(), p.get(), tt.get(), grid, ctx->stream);
+                break;
+        }
+        checkLaunch();
+        OWEC_CUDA(cudaMemcpyAsync(boundary, b.get(), 4 * n, cudaMemcpyDeviceToHost, ctx->stream));
+        OWEC_CUDA(cudaMemcpyAsync(prim, p.get(), 4 * n, cudaMemcpyDeviceToHost, ctx->stream));
+        OWEC_CUDA(cudaMemcpyAsync(t, tt.get(), 8 * n, cudaMemcpyDeviceToHost, ctx->stream));
+        OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int owec_cast_rays_device(owec_ctx* ctx, uint64_t n, const float* o, const float* d, uint32_t* b, uint32_t* p, float* t,
+                          double* seconds) {
+    return guarded([&] {
+        require(ctx != nullptr, "owec_cast_rays_device: null context");
+        if (n == 0) return;
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        ensureReady(*ctx);
+        OWEC_CUDA(cudaEventRecord(ctx->passStart, ctx->stream));
+        launchCastRaysF(ctx->ds, n, o, d, b, p, t, ctx->numSMs * 8, ctx->stream);
+        checkLaunch();
+        OWEC_CUDA(cudaEventRecord(ctx->passStop, ctx->stream));
+        if (seconds) {
+            OWEC_CUDA(cudaEventSynchronize(ctx->passStop));
+            float ms = 0;
+            OWEC_CUDA(cudaEventElapsedTime(&ms, ctx->passStart, ctx->passStop));
+            *seconds = ms * 1e-3;
+        }
+    });
+}
+
+int owec_trace_counters(owec_ctx* ctx, int enable, uint64_t out[6]) {
+    return guarded([&] {
+        require(ctx != nullptr, "owec_trace_counters: null context");
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        ctx->dTravCounters.reserve(6);
+        if (out) {
+            unsigned long long h[6];
+            OWEC_CUDA(cudaMemcpyAsync(h, ctx->dTravCounters.get(), sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+            OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+            for (int k = 0; k < 6; ++k) out[k] = h[k];
+        }
+        if (enable) {
+            OWEC_CUDA(cudaMemsetAsync(ctx->dTravCounters.get(), 0, 6 * sizeof(unsigned long long), ctx->stream));
+            OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+            ctx->ds.travCounters = ctx->dTravCounters.get();
+        } else {
+            ctx->ds.travCounters = nullptr;
+        }
+    });
+}
+
+int owec_scene_origin(owec_ctx* ctx, double origin[3]) {
+    return guarded([&] {
+        require(ctx && origin, "owec_scene_origin: null argument");
+        require(ctx->hasScene, "no scene uploaded", OWEC_E_STATE);
+        for (int k = 0; k < 3; ++k) origin[k] = ctx->ds.origin[k];
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,105 @@
+// Path state of the wavefront loop: structure-of-arrays in HBM, one slot per path in flight, and
+// the queues that join the kernels.
+#pragma once
+
+#include "device_scene.cuh"
+#include "rng.cuh"
+#include "traverse.cuh"
+
+namespace owec {
+
+// Precision modes (owec.h OWEC_PRECISION_*): R is the arithmetic of directions, throughput and
+// optics; Ro the analytic roots; Rr their refinement; origins are FP64 unless PlainOrigin.
+template <int M> struct Mode;
+template <> struct Mode<OWEC_PRECISION_MIXED> {
+    using R = float; using Ro = float; using Rr = double; static constexpr bool plainOrigin = false;
+};
+template <> struct Mode<OWEC_PRECISION_FP32> {
+    using R = float; using Ro = float; using Rr = float; static constexpr bool plainOrigin = true;
+};
+template <> struct Mode<OWEC_PRECISION_FP64> {
+    using R = double; using Ro = double; using Rr = double; static constexpr bool plainOrigin = false;
+};
+
+// The ray a path travels next, and what the intersect kernel needs of it.
+template <class R>
+struct alignas(16) PathRay {
+    double o[3];      // camera-relative origin (rounded to FP32 after every update in the plain mode)
+    R d[3];
+    uint32_t region;  // region the ray travels in
+    uint32_t depB;    // boundary and primitive it left (kNone)
+    uint32_t depP;
+    float errN;       // its anchor's error normal to a surface
+};
+
+// Throughput and spectral state.
+template <class R>
+struct alignas(16) PathSpec {
+    R beta[4];
+    float lambda[4];
+    float pdf[4];     // 0: terminated secondary
+    float L[4];       // radiance gathered so far
+};
+
+// Bookkeeping of a path.
+struct alignas(16) PathAux {
+    uint64_t rngState;
+    uint32_t stream;    // PCG32 stream (the pass index of this sample)
+    uint32_t pixel;
+    uint32_t depth;     // bounce count (the reference's loop variable)
+    uint32_t flags;     // kFlagSpecular | kFlagAlive | kFlagHasPrev
+    float prevPdf;
+    float weight;       // detector importance / pdf
+    float prevP[3];     // last scattering vertex (camera-relative), for emission MIS
+    uint32_t lastBoundary;
+};
+constexpr uint32_t kFlagSpecular = 1u, kFlagAlive = 2u;
+
+// A pending next-event visibility query and its contribution if the segment is clear.
+template <class R>
+struct alignas(16) ShadowRay {
+    double o[3];
+    R d[3];
+    double tmax;          // Inf for the sun
+    uint32_t region;      // region the segment starts in
+    uint32_t endRegion;   // region it must arrive in (kNone: the ambient region for the sun)
+    uint32_t depB, depP;
+    uint32_t path;
+    float errN;
+    float contrib[4];     // beta * f * Le * cos * w / pdf, before transmittance
+};
+
+struct Queues {
+    uint32_t* active[2];
+    uint32_t* surface;
+    uint32_t* shadow;
+    uint32_t* counts;     // [0], [1] active ping-pong, [2] surface, [3] shadow
+};
+
+struct StatCounters {
+    unsigned long long paths, segments, inconsistencies, leaks, shadowRays, faults;
+};
+
+template <class R>
+struct PathBuffers {
+    PathRay<R>* ray;
+    PathSpec<R>* spec;
+    PathAux* aux;
+    HitRec* hit;
+    ShadowRay<R>* shadow;  // indexed by shadow-queue position
+    float* sampleXyz;      // 3 per path slot: the path's XYZ estimate once the batch is done
+};
+
+struct PassParams {
+    uint64_t seed;
+    int32_t maxDepth, rrDepth;
+    int32_t wavelengthMode;
+    float lambdaMin, lambdaMax;
+    float fresnelFloor;
+    uint32_t nPixels;        // detector pixels
+    uint32_t nPaths;         // paths in this batch: nPixels * samples
+    uint32_t streamBase;     // PCG32 stream of the batch's first sample
+    int32_t anyHitShadows;   // 1: no null boundaries, shadow rays stop at the first crossing
+};
+
+}  // namespace owec

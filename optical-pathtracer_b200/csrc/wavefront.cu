@@ -1,0 +1,799 @@
+// The wavefront camera-path loop (the reference's Tracer::radiance, src/owe/transport/transport.cpp:
+// 473-529, run over every pixel sample of a pass as CpuRenderer::pass does,
+// src/owe/backends/cpu/cpu_backend.cpp:52-94).
+//
+// One bounce is four kernels joined by queues of path slots:
+//   kIntersect  closest hit of every active path (the wide-BVH traversal);
+//   kMedium     free flight through the current region's medium: Beer-Lambert, distance sampling
+//               with sigma_a / sigma_s and Henyey-Greenstein scattering with next-event estimation,
+//               escape to the sun and sky; surface hits go to the surface queue;
+//   kSurface    the boundary met: region bookkeeping, emission with MIS, spectral interface optics
+//               (index models at the hero wavelength, dispersion, Fresnel, GGX, conductors,
+//               Lambertian, mirrors), next-event light sampling, the scattering sample, Russian
+//               roulette; continuing paths go to the next active queue;
+//   kShadow     the visibility of the next-event samples, adding their contributions.
+// kGenerate starts a batch of samples; kFilm folds the batch's finished paths into the film in a
+// fixed order, so the film does not depend on scheduling.
+//
+// Each path draws from its own PCG32 stream in the reference's order, so for a one-sample pass
+// a device path makes the CPU path's decisions until rounding changes one of them.
+#include "transport.cuh"
+#include "wavefront.hpp"
+
+namespace owec {
+
+namespace {
+
+template <int M>
+using RT = typename Mode<M>::R;
+
+// Adds one query's node visits and primitive tests to the counters (profiling passes only).
+__device__ __forceinline__ void countTraversal(unsigned long long* c, uint32_t visits, uint32_t tests) {
+    atomicAdd(c, 1ull);
+    atomicAdd(c + 1, (unsigned long long)visits);
+    atomicAdd(c + 2, (unsigned long long)tests);
+}
+
+template <class R>
+__device__ __forceinline__ V3<R> rayDir(const PathRay<R>& r) { return V3<R>(r.d[0], r.d[1], r.d[2]); }
+__device__ __forceinline__ V3<double> rayOrigin(const double o[3]) { return V3<double>(o[0], o[1], o[2]); }
+
+template <int M>
+__device__ __forceinline__ void setOrigin(double o[3], const V3<double>& p) {
+    if (Mode<M>::plainOrigin) {
+        o[0] = double(float(p.x));
+        o[1] = double(float(p.y));
+        o[2] = double(float(p.z));
+    } else {
+        o[0] = p.x;
+        o[1] = p.y;
+        o[2] = p.z;
+    }
+}
+
+// ------------------------------------------------------------------ generate
+template <int M>
+__global__ void __launch_bounds__(256) kGenerate(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
+                                                 StatCounters* st) {
+    using R = RT<M>;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pp.nPaths) return;
+    const uint32_t pixel = i % pp.nPixels;
+    const uint32_t sub = i / pp.nPixels;
+    const DDetector& det = sc.det;
+    const int x = int(pixel % uint32_t(det.width)), y = int(pixel / uint32_t(det.width));
+    Pcg32 rng = Pcg32::seeded(hashCombine(pp.seed, pixel), pp.streamBase + sub);
+    // Hero strata of a one-sample pass: u = (0 + xi) / 1 + rot (cpu_backend.cpp:68-73)
+    const double rot = rng.uniform();
+    double u = rng.uniform() + rot;
+    u -= floor(u);
+    PathSpec<R> sp;
+    if (pp.wavelengthMode == OWEC_WAVELENGTHS_UNIFORM1) {
+        const double lam = double(pp.lambdaMin) + (double(pp.lambdaMax) - double(pp.lambdaMin)) * u;
+        for (int k = 0; k < NW; ++k) { sp.lambda[k] = float(lam); sp.pdf[k] = 0.f; }
+        sp.pdf[0] = float(1.0 / ((double(pp.lambdaMax) - double(pp.lambdaMin)) * NW));
+    } else {
+        for (int k = 0; k < NW; ++k) {
+            double up = u + double(k) / NW;
+            if (up >= 1) up -= 1;
+            const double lam = sampleVisibleWavelength(up);
+            sp.lambda[k] = float(lam);
+            sp.pdf[k] = float(visibleWavelengthPdf(lam));
+        }
+    }
+    double px = x + rng.uniform(), py = y + rng.uniform();
+    if (det.sigma > 0) {  // Detector::filterOffset: a Gaussian displacement (detector.hpp:57-62)
+        const Draw2<double> g(rng);
+        const double r = sqrt(-2 * log(1 - g.u1)), phi = 2 * kPi * g.u2;
+        px += r * cos(phi) * det.sigma;
+        py += r * sin(phi) * det.sigma;
+    }
+    PathRay<R> ray;
+    PathAux aux;
+    double weight = 0;
+    V3<double> o, dir;
+    if (det.kind == OWEC_DETECTOR_OBSERVER) {
+        // IdealObserver::generate, pinhole (detector.cpp:61-91)
+        const double sx = (2 * px / det.width - 1) * det.tanX;
+        const double sy = (1 - 2 * py / det.height) * det.tanY;
+        const V3<double> R3(det.right[0], det.right[1], det.right[2]), U3(det.up[0], det.up[1], det.up[2]),
+            F3(det.fwd[0], det.fwd[1], det.fwd[2]);
+        dir = normalize(R3 * sx + U3 * sy + F3);
+        o = V3<double>(det.pos[0], det.pos[1], det.pos[2]);
+        weight = 1;
+        ray.region = det.region;
+        ray.depB = kNone;
+        ray.depP = kNone;
+        ray.errN = 0.f;
+    } else if (!(px < 0 || py < 0 || px >= det.width || py >= det.height)) {
+        // SurfaceSensor::generate, hemispherical (detector.cpp:113-148)
+        const DBoundary& bd = sc.boundaries[det.boundary];
+        const V3<double> pl((2 * px / det.width - 1) * det.halfX, (1 - 2 * py / det.height) * det.halfY, 0);
+        o = bd.toWorld.point(pl);
+        const V3<double> nrm(det.normal[0], det.normal[1], det.normal[2]);
+        const Draw2<double> g(rng);
+        const double a = 2 * g.u1 - 1, b = 2 * g.u2 - 1;
+        double dx = 0, dy = 0;
+        if (!(a == 0 && b == 0)) {
+            double r, phi;
+            if (fabs(a) > fabs(b)) { r = a; phi = (kPi / 4) * (b / a); }
+            else { r = b; phi = kPi / 2 - (kPi / 4) * (a / b); }
+            dx = r * cos(phi);
+            dy = r * sin(phi);
+        }
+        dir = Frame<double>(nrm).toWorld(V3<double>(dx, dy, sqrt(fmax(0.0, 1 - dx * dx - dy * dy))));
+        weight = kPi;
+        ray.region = det.region;
+        ray.depB = det.boundary;
+        ray.depP = 0;
+        ray.errN = anchorError<R>(o);
+    }
+    aux.flags = 0;
+    aux.weight = float(weight);
+    aux.pixel = pixel;
+    aux.stream = pp.streamBase + sub;
+    aux.depth = 0;
+    aux.prevPdf = 0.f;
+    aux.lastBoundary = kNone;
+    for (int k = 0; k < NW; ++k) {
+        sp.beta[k] = (k == 0 || sp.pdf[k] != 0.f) ? R(1) : R(0);  // maskTerminated
+        sp.L[k] = 0.f;
+    }
+    const bool live = weight > 0;
+    if (live) {
+        setOrigin<M>(ray.o, o);
+        ray.d[0] = R(dir.x);
+        ray.d[1] = R(dir.y);
+        ray.d[2] = R(dir.z);
+        aux.flags = kFlagSpecular | kFlagAlive;
+        aux.prevP[0] = float(o.x);
+        aux.prevP[1] = float(o.y);
+        aux.prevP[2] = float(o.z);
+    }
+    aux.rngState = rng.state;
+    pb.ray[i] = ray;
+    pb.spec[i] = sp;
+    pb.aux[i] = aux;
+    warpCount(&st->paths, live);
+    warpPush(q.active[0], &q.counts[0], live, i);
+}
+
+// ------------------------------------------------------------------ intersect
+template <int M>
+__global__ void __launch_bounds__(128) kIntersect(DeviceScene sc, PathBuffers<RT<M>> pb, Queues q, int cur,
+                                                  StatCounters* st) {
+    using R = RT<M>;
+    extern __shared__ StackEntry stackMem[];
+    StackEntry* stack = stackMem + threadIdx.x;
+    const uint32_t n = q.counts[cur];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t i = q.active[cur][k];
+        const PathRay<R> ray = pb.ray[i];
+        RayQuery<R> rq;
+        rq.od = rayOrigin(ray.o);
+        rq.o = V3<R>(rq.od);
+        rq.d = rayDir(ray);
+        rq.tmax = R(INFINITY);
+        rq.depB = ray.depB;
+        rq.depP = ray.depP;
+        rq.region = ray.region;
+        rq.errN = R(ray.errN);
+        HitRec h;
+        h.boundary = kNone;
+        h.t = INFINITY;
+        uint32_t nv = 0, nt = 0;
+        const int s = traceRay<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false>(sc, rq, stack, blockDim.x, h,
+                                                                                   &nv, &nt);
+        if (sc.travCounters) countTraversal(sc.travCounters, nv, nt);
+        if (s != kTraceHit) { h.boundary = kNone; h.t = INFINITY; }
+        if (s == kTraceOverflow) h.boundary = kNone - 1u;  // a fault: the path ends
+        pb.hit[i] = h;
+        warpCount(&st->segments, true);
+        warpCount(&st->faults, s == kTraceOverflow);
+    }
+}
+
+// ------------------------------------------------------------------ next-event estimation
+// Prepares the shadow ray of directLighting (transport.cpp:323-348) at a surface point (surface
+// interface given) or a medium point (phase g), and queues it with its contribution.
+template <int M>
+__device__ void queueNee(const DeviceScene& sc, PathBuffers<RT<M>>& pb, Queues& q, uint32_t pathIdx,
+                         const PathSpec<RT<M>>& sp, const LightSampleD& ls, const RT<M> f[NW], RT<M> pdfScatter,
+                         RT<M> cosFactor, const V3<double>& p, uint32_t startRegion, uint32_t depB, uint32_t depP,
+                         float errN, bool valid) {
+    using R = RT<M>;
+    ShadowRay<R> sr;
+    float contrib[NW] = {0.f, 0.f, 0.f, 0.f};
+    bool any = false;
+    if (valid) {
+        const R w = powerHeuristic(R(ls.pdf), pdfScatter);
+        for (int k = 0; k < NW; ++k) {
+            if (sp.pdf[k] == 0.f && k > 0) continue;
+            const R Le = lightSampleLe<R>(sc, ls, R(sp.lambda[k]));
+            const R c = sp.beta[k] * f[k] * Le * (cosFactor * w / R(ls.pdf));
+            contrib[k] = float(c);
+            any = any || (c != R(0));
+        }
+    }
+    const bool push = valid && any;
+    const unsigned active = __activemask();
+    const unsigned mask = __ballot_sync(active, push);
+    if (mask == 0) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&q.counts[3], uint32_t(__popc(mask)));
+    base = __shfl_sync(active, base, leader);
+    if (!push) return;
+    const uint32_t slot = base + __popc(mask & ((1u << lane) - 1u));
+    setOrigin<M>(sr.o, p);
+    sr.d[0] = R(ls.wi.x);
+    sr.d[1] = R(ls.wi.y);
+    sr.d[2] = R(ls.wi.z);
+    sr.tmax = ls.dist;
+    sr.region = startRegion;
+    sr.endRegion = ls.boundary == kNone ? 0u : ls.region;
+    sr.depB = depB;
+    sr.depP = depP;
+    sr.path = pathIdx;
+    sr.errN = errN;
+    for (int k = 0; k < NW; ++k) sr.contrib[k] = contrib[k];
+    pb.shadow[slot] = sr;
+    q.shadow[slot] = slot;
+}
+
+// ------------------------------------------------------------------ medium
+template <int M>
+__global__ void __launch_bounds__(128) kMedium(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
+                                               int cur, StatCounters* st) {
+    using R = RT<M>;
+    const int nxt = cur ^ 1;
+    const uint32_t n = q.counts[cur];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t i = q.active[cur][k];
+        PathRay<R> ray = pb.ray[i];
+        PathSpec<R> sp = pb.spec[i];
+        PathAux aux = pb.aux[i];
+        const HitRec h = pb.hit[i];
+        Pcg32 rng{aux.rngState, (uint64_t(aux.stream) << 1u) | 1u};
+        const bool fault = h.boundary == kNone - 1u;
+        const bool found = h.boundary < kNone - 1u;
+        const owec_medium med = sc.media[sc.regionMedium[ray.region]];
+        const V3<R> d = rayDir(ray);
+        bool toSurface = false, cont = false, leak = false;
+        bool neeValid = false;
+        LightSampleD ls;
+        R fN[NW] = {R(0), R(0), R(0), R(0)};
+        R pdfS = R(0);
+        V3<double> sp3;
+        if (!fault) {
+            // sampleMedium (transport.cpp:95-113)
+            const double seg = found ? h.t : INFINITY;
+            int event = 0;  // 0 pass, 1 scatter, 2 end
+            double tS = 0;
+            if (mediumScatters(med, sc)) {
+                R sT[NW];
+                for (int j = 0; j < NW; ++j)
+                    sT[j] = evalSpectrum(sc, med.absorption, R(sp.lambda[j])) + evalSpectrum(sc, med.scattering, R(sp.lambda[j]));
+                tS = -log(1 - rng.uniform()) / double(sT[0]);
+                if (tS < seg) {
+                    const R pdf0 = sT[0] * exp(-sT[0] * R(tS));
+                    for (int j = 0; j < NW; ++j)
+                        sp.beta[j] *= evalSpectrum(sc, med.scattering, R(sp.lambda[j])) * exp(-sT[j] * R(tS)) / pdf0;
+                    event = 1;
+                } else if (isinf(seg)) {
+                    event = 2;
+                } else {
+                    const R pass0 = exp(-sT[0] * R(seg));
+                    for (int j = 0; j < NW; ++j) sp.beta[j] *= exp(-sT[j] * R(seg)) / pass0;
+                }
+            } else if (mediumAbsorbs(med, sc)) {
+                if (isinf(seg)) event = 2;
+                else
+                    for (int j = 0; j < NW; ++j)
+                        sp.beta[j] *= exp(-evalSpectrum(sc, med.absorption, R(sp.lambda[j])) * R(seg));
+            }
+            if (event == 1) {
+                // scatterInMedium (transport.cpp:379-397)
+                sp3 = rayOrigin(ray.o) + V3<double>(d) * tS;
+                if (int(aux.depth) < pp.maxDepth) {
+                    int li;
+                    if (sampleLight<R>(sc, sp3, rng, ls, li)) {
+                        bool leZero = true;
+                        for (int j = 0; j < NW; ++j)
+                            if (lightSampleLe<R>(sc, ls, R(sp.lambda[j])) != R(0)) leZero = false;
+                        if (!leZero && ls.pdf > 0) {
+                            const R ph = hgPhase(dot(-d, V3<R>(ls.wi)), R(med.g));
+                            pdfS = ph;
+                            for (int j = 0; j < NW; ++j) fN[j] = ph;
+                            neeValid = true;
+                        }
+                    }
+                    const Draw2<R> u(rng);
+                    V3<R> wi;
+                    aux.prevPdf = float(sampleHg(-d, R(med.g), u.u1, u.u2, wi));
+                    aux.flags &= ~kFlagSpecular;
+                    aux.prevP[0] = float(sp3.x);
+                    aux.prevP[1] = float(sp3.y);
+                    aux.prevP[2] = float(sp3.z);
+                    setOrigin<M>(ray.o, sp3);
+                    ray.d[0] = wi.x;
+                    ray.d[1] = wi.y;
+                    ray.d[2] = wi.z;
+                    ray.depB = kNone;
+                    ray.depP = kNone;
+                    ray.errN = 0.f;
+                    cont = int(aux.depth) < pp.rrDepth || survives(sp, rng);
+                }
+            } else if (event == 0 && !found) {
+                if (ray.region == 0) {
+                    // skyMet (transport.cpp:401-417)
+                    const bool spec = aux.flags & kFlagSpecular;
+                    const V3<double> dd(d);
+                    const bool inSun = sc.hasSun && dot(dd, V3<double>(sc.sunDir[0], sc.sunDir[1], sc.sunDir[2])) >= sc.sunCosMax;
+                    R w = R(1);
+                    if (!spec && inSun) w = powerHeuristic(R(aux.prevPdf), R(sc.sunSelectPdf / sc.sunSolidAngle));
+                    for (int j = 0; j < NW; ++j) {
+                        const R lam = R(sp.lambda[j]);
+                        const R sky = sc.skyModel == OWEC_SKY_UNIFORM ? evalSpectrum(sc, sc.skySpectrum, lam) : R(0);
+                        const R sun = inSun ? evalSpectrum(sc, sc.sunSpectrum, lam) : R(0);
+                        sp.L[j] += float(sp.beta[j] * (sky + sun * w));
+                    }
+                } else {
+                    leak = true;
+                }
+            } else if (event == 0) {
+                toSurface = true;
+            }
+        }
+        if (cont) aux.depth += 1;
+        if (!toSurface && !cont) aux.flags &= ~kFlagAlive;
+        aux.rngState = rng.state;
+        pb.ray[i] = ray;
+        pb.spec[i] = sp;
+        pb.aux[i] = aux;
+        queueNee<M>(sc, pb, q, i, sp, ls, fN, pdfS, R(1), sp3, ray.region, kNone, kNone, 0.f, neeValid);
+        warpCount(&st->leaks, leak);
+        warpPush(q.surface, &q.counts[2], toSurface, i);
+        warpPush(q.active[nxt], &q.counts[nxt], cont, i);
+    }
+}
+
+// ------------------------------------------------------------------ surface
+template <class R>
+__device__ __forceinline__ Interface<R> makeInterface(const DeviceScene& sc, const DBoundary& bd, const V3<R>& n, R lambda,
+                                                      R fresnelFloor) {
+    Interface<R> it;
+    it.o = sc.optics[bd.optics];
+    it.n = n;
+    it.nFront = regionIndex(sc, bd.front, lambda);
+    it.nBack = regionIndex(sc, bd.back, lambda);
+    it.lambda = lambda;
+    it.fresnelFloor = fresnelFloor;
+    it.albedo = it.o.reflectance >= 0 ? evalSpectrum(sc, it.o.reflectance, lambda) : R(1);
+    return it;
+}
+
+template <int M>
+__global__ void __launch_bounds__(128) kSurface(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
+                                                int cur, StatCounters* st) {
+    using R = RT<M>;
+    using Ro = typename Mode<M>::Ro;
+    using Rr = typename Mode<M>::Rr;
+    const int nxt = cur ^ 1;
+    const uint32_t n = q.counts[2];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t i = q.surface[k];
+        PathRay<R> ray = pb.ray[i];
+        PathSpec<R> sp = pb.spec[i];
+        PathAux aux = pb.aux[i];
+        const HitRec h = pb.hit[i];
+        Pcg32 rng{aux.rngState, (uint64_t(aux.stream) << 1u) | 1u};
+        const DBoundary bd = sc.boundaries[h.boundary];
+        const SurfacePoint<R> g = hitGeometry<R, Ro, Rr>(sc, ray, h);
+        const V3<R> d = rayDir(ray);
+        // meetBoundary (transport.cpp:121-133)
+        const bool fromFront = dot(d, g.n) < R(0);
+        const uint32_t inc = fromFront ? bd.front : bd.back;
+        const uint32_t other = fromFront ? bd.back : bd.front;
+        const bool inconsistent = inc != ray.region;
+        ray.region = inc;
+        aux.lastBoundary = h.boundary;
+        const bool specular = aux.flags & kFlagSpecular;
+        // emissionMet (transport.cpp:420-433)
+        if (bd.emission >= 0) {
+            const owec_emission e = sc.emissions[bd.emission];
+            if (fromFront ? e.front : e.back) {
+                R w = R(1);
+                if (!specular && bd.light >= 0) {
+                    const V3<double> prev(aux.prevP[0], aux.prevP[1], aux.prevP[2]);
+                    const double pl = sc.lights[bd.light].pdf * shapePdfFrom(bd, prev, g.p, V3<double>(g.n));
+                    if (pl > 0) w = powerHeuristic(R(aux.prevPdf), R(pl));
+                }
+                for (int j = 0; j < NW; ++j)
+                    sp.L[j] += float(sp.beta[j] * evalSpectrum(sc, e.radiance, R(sp.lambda[j])) * w);
+            }
+        }
+        const owec_optics o = sc.optics[bd.optics];
+        const float errN = anchorError<R>(g.p);
+        bool cont = false, neeValid = false;
+        LightSampleD ls;
+        R fN[NW] = {R(0), R(0), R(0), R(0)};
+        R pdfS = R(0), cosF = R(0);
+        uint32_t neeRegion = ray.region;
+        if (o.type == OWEC_SURF_NULL) {
+            ray.region = other;
+            setOrigin<M>(ray.o, g.p);
+            ray.depB = h.boundary;
+            ray.depP = h.prim;
+            ray.errN = errN;
+            cont = int(aux.depth) < 4 * pp.maxDepth;
+        } else if (o.type != OWEC_SURF_ABSORBER && o.type != OWEC_SURF_DETECTOR && int(aux.depth) < pp.maxDepth) {
+            // scatterAtSurface (transport.cpp:437-471)
+            const R hero = R(sp.lambda[0]);
+            const Interface<R> it = makeInterface(sc, bd, g.n, hero, R(pp.fresnelFloor));
+            if (o.type == OWEC_SURF_DIELECTRIC) {  // terminateIfDispersive
+                bool alive2 = false;
+                for (int j = 1; j < NW; ++j) alive2 = alive2 || sp.pdf[j] != 0.f;
+                if (alive2) {
+                    for (int j = 1; j < NW; ++j) {
+                        if (sp.pdf[j] == 0.f) continue;
+                        const Interface<R> it2 = makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(pp.fresnelFloor));
+                        if (isDispersive(it, it2)) {
+                            for (int m = 1; m < NW; ++m) sp.pdf[m] = 0.f;
+                            sp.pdf[0] /= float(NW);
+                            for (int m = 1; m < NW; ++m) sp.beta[m] = R(0);
+                            break;
+                        }
+                    }
+                }
+            }
+            if (!isDeltaOptics<R>(o)) {
+                int li;
+                if (sampleLight<R>(sc, g.p, rng, ls, li)) {
+                    bool leZero = true;
+                    for (int j = 0; j < NW; ++j)
+                        if (lightSampleLe<R>(sc, ls, R(sp.lambda[j])) != R(0)) leZero = false;
+                    if (!leZero && ls.pdf > 0) {
+                        const V3<R> wi(ls.wi);
+                        bool fZero = true;
+                        for (int j = 0; j < NW; ++j) {
+                            if (sp.pdf[j] == 0.f) continue;
+                            R pdf;
+                            const Interface<R> itj =
+                                j == 0 ? it : makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(pp.fresnelFloor));
+                            fN[j] = evalScatter(sc, itj, d, wi, true, pdf);
+                            if (j == 0) pdfS = pdf;
+                            if (fN[j] != R(0)) fZero = false;
+                        }
+                        if (!fZero) {
+                            cosF = fabs(dot(wi, g.n));
+                            neeRegion = dot(wi, g.n) > R(0) ? bd.front : bd.back;
+                            neeValid = true;
+                        }
+                    }
+                }
+            }
+            const Draw3<R> u(rng);
+            ScatterSample<R> s;
+            const bool ok = sampleScatter(sc, it, d, u.u1, u.u2, u.u3, true, s);
+            if (ok && s.weight > R(0)) {
+                // weighScatter (transport.cpp:227-233)
+                sp.beta[0] *= s.weight;
+                for (int j = 1; j < NW; ++j) {
+                    if (sp.pdf[j] == 0.f) continue;
+                    const Interface<R> itj = makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(pp.fresnelFloor));
+                    sp.beta[j] *= secondaryScatterWeight(sc, itj, d, s, true);
+                }
+                if (s.transmitted) ray.region = other;
+                aux.flags = s.delta ? (aux.flags | kFlagSpecular) : (aux.flags & ~kFlagSpecular);
+                aux.prevPdf = float(s.pdf);
+                aux.prevP[0] = float(g.p.x);
+                aux.prevP[1] = float(g.p.y);
+                aux.prevP[2] = float(g.p.z);
+                setOrigin<M>(ray.o, g.p);
+                ray.d[0] = s.wi.x;
+                ray.d[1] = s.wi.y;
+                ray.d[2] = s.wi.z;
+                ray.depB = h.boundary;
+                ray.depP = h.prim;
+                ray.errN = errN;
+                cont = !(int(aux.depth) >= pp.rrDepth && !survives(sp, rng));
+            }
+        }
+        if (cont) aux.depth += 1;
+        else aux.flags &= ~kFlagAlive;
+        aux.rngState = rng.state;
+        pb.ray[i] = ray;
+        pb.spec[i] = sp;
+        pb.aux[i] = aux;
+        queueNee<M>(sc, pb, q, i, sp, ls, fN, pdfS, cosF, g.p, neeRegion, h.boundary, h.prim, errN, neeValid);
+        warpCount(&st->inconsistencies, inconsistent);
+        warpPush(q.active[nxt], &q.counts[nxt], cont, i);
+    }
+}
+
+// ------------------------------------------------------------------ shadow rays
+// The visibility of a next-event sample (Tracer::transmittance / connectionTransmittance,
+// transport.cpp:237-308): blocked by any matter other than null boundaries, attenuated by the
+// media it crosses, and it must arrive in the region on the light's emitting side (the ambient
+// region for the sun).
+template <int M>
+__global__ void __launch_bounds__(128) kShadow(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
+                                               StatCounters* st) {
+    using R = RT<M>;
+    using Ro = typename Mode<M>::Ro;
+    using Rr = typename Mode<M>::Rr;
+    extern __shared__ StackEntry stackMem[];
+    StackEntry* stack = stackMem + threadIdx.x;
+    const uint32_t n = q.counts[3];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const ShadowRay<R> sr = pb.shadow[k];
+        const PathSpec<R> spc = pb.spec[sr.path];
+        R Tr[NW] = {R(1), R(1), R(1), R(1)};
+        bool clear = true;
+        bool fault = false;
+        RayQuery<R> rq;
+        rq.od = rayOrigin(sr.o);
+        rq.o = V3<R>(rq.od);
+        rq.d = V3<R>(sr.d[0], sr.d[1], sr.d[2]);
+        rq.depB = sr.depB;
+        rq.depP = sr.depP;
+        rq.region = sr.region;
+        rq.errN = R(sr.errN);
+        uint32_t region = sr.region;
+        double remaining = sr.tmax;
+        const bool finite = !isinf(sr.tmax);
+        for (int guard = 0; guard < 256 && clear; ++guard) {
+            // stop short of the light's own surface
+            const double tq = finite ? remaining - (4e-6 * remaining + double(sr.errN) + 1e-9) : INFINITY;
+            if (finite && tq <= 0) break;
+            rq.tmax = R(tq);
+            rq.region = region;
+            HitRec h;
+            h.boundary = kNone;
+            uint32_t nv = 0, nt = 0;
+            const int s = pp.anyHitShadows
+                              ? traceRay<R, Ro, Rr, true>(sc, rq, stack, blockDim.x, h, &nv, &nt)
+                              : traceRay<R, Ro, Rr, false>(sc, rq, stack, blockDim.x, h, &nv, &nt);
+            if (sc.travCounters) countTraversal(sc.travCounters + 3, nv, nt);
+            if (s == kTraceOverflow) { fault = true; clear = false; break; }
+            const bool found = s == kTraceHit;
+            const double seg = found ? fmin(h.t, remaining) : remaining;
+            const owec_medium med = sc.media[sc.regionMedium[region]];
+            if (mediumAbsorbs(med, sc) || mediumScatters(med, sc)) {
+                if (isinf(seg)) { clear = false; break; }
+                for (int j = 0; j < NW; ++j) {
+                    const R lam = R(spc.lambda[j]);
+                    Tr[j] *= exp(-(evalSpectrum(sc, med.absorption, lam) + evalSpectrum(sc, med.scattering, lam)) * R(seg));
+                }
+            }
+            if (!found) {
+                if (!finite && region != 0) clear = false;
+                break;
+            }
+            if (pp.anyHitShadows) { clear = false; break; }
+            const DBoundary bd = sc.boundaries[h.boundary];
+            if (sc.optics[bd.optics].type != OWEC_SURF_NULL) { clear = false; break; }
+            // pass the null boundary, if met from this region
+            PathRay<R> tmp;
+            tmp.o[0] = rq.od.x; tmp.o[1] = rq.od.y; tmp.o[2] = rq.od.z;
+            tmp.d[0] = rq.d.x; tmp.d[1] = rq.d.y; tmp.d[2] = rq.d.z;
+            const SurfacePoint<R> gp = hitGeometry<R, Ro, Rr>(sc, tmp, h);
+            const bool ff = dot(rq.d, gp.n) < R(0);
+            if ((ff ? bd.front : bd.back) != region) { clear = false; break; }
+            region = ff ? bd.back : bd.front;
+            rq.od = gp.p;
+            if (Mode<M>::plainOrigin) rq.od = V3<double>(V3<float>(gp.p));
+            rq.o = V3<R>(rq.od);
+            rq.depB = h.boundary;
+            rq.depP = h.prim;
+            rq.errN = R(anchorError<R>(gp.p));
+            if (finite) remaining -= h.t;
+        }
+        if (clear && finite && region != sr.endRegion) clear = false;
+        if (clear) {
+            float* L = pb.spec[sr.path].L;
+            for (int j = 0; j < NW; ++j) L[j] += float(R(sr.contrib[j]) * Tr[j]);
+        }
+        warpCount(&st->shadowRays, true);
+        warpCount(&st->faults, fault);
+    }
+}
+
+// ------------------------------------------------------------------ film
+// Folds the batch's samples of every pixel into the film in sample order: XYZ of each path
+// (Wavelengths::toXYZ of L * weight, wavelengths.hpp:71-84), skipping non-finite estimates as
+// CpuRenderer::pass does, with compensated (Kahan) FP64 sums.
+template <int M>
+__global__ void __launch_bounds__(256) kFilm(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, double* film,
+                                             double* comp, double* samples, uint32_t samplesPerPixel) {
+    using R = RT<M>;
+    const uint32_t pixel = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pixel >= pp.nPixels) return;
+    double s[3], c[3];
+    for (int ch = 0; ch < 3; ++ch) { s[ch] = film[3 * pixel + ch]; c[ch] = comp[3 * pixel + ch]; }
+    const double inv = 1.0 / (NW * sc.cieYIntegral);
+    for (uint32_t sub = 0; sub < samplesPerPixel; ++sub) {
+        const uint32_t i = sub * pp.nPixels + pixel;
+        const PathAux aux = pb.aux[i];
+        if (!(aux.weight > 0.f)) continue;
+        const PathSpec<R> sp = pb.spec[i];
+        double x = 0, y = 0, z = 0;
+        for (int k = 0; k < NW; ++k) {
+            const double Lk = double(sp.L[k]) * double(aux.weight);
+            if (sp.pdf[k] == 0.f || Lk == 0) continue;
+            const double w = Lk / double(sp.pdf[k]) * inv;
+            const double l = double(sp.lambda[k]);
+            x += w * cieX(l);
+            y += w * cieY(l);
+            z += w * cieZ(l);
+        }
+        if (!isfinite(x + y + z)) continue;
+        const double v[3] = {x, y, z};
+        for (int ch = 0; ch < 3; ++ch) {
+            const double yv = v[ch] - c[ch];
+            const double t = s[ch] + yv;
+            c[ch] = (t - s[ch]) - yv;
+            s[ch] = t;
+        }
+    }
+    for (int ch = 0; ch < 3; ++ch) { film[3 * pixel + ch] = s[ch]; comp[3 * pixel + ch] = c[ch]; }
+    samples[pixel] += samplesPerPixel;
+}
+
+// ------------------------------------------------------------------ ray casts
+template <int M>
+__global__ void __launch_bounds__(128) kCastRays(DeviceScene sc, uint64_t n, const double* o, const double* d,
+                                                 uint32_t* boundary, uint32_t* prim, double* t) {
+    using R = RT<M>;
+    extern __shared__ StackEntry stackMem[];
+    StackEntry* stack = stackMem + threadIdx.x;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        RayQuery<R> rq;
+        rq.od = V3<double>(o[3 * i] - sc.origin[0], o[3 * i + 1] - sc.origin[1], o[3 * i + 2] - sc.origin[2]);
+        if (Mode<M>::plainOrigin) rq.od = V3<double>(V3<float>(rq.od));
+        rq.o = V3<R>(rq.od);
+        rq.d = V3<R>(R(d[3 * i]), R(d[3 * i + 1]), R(d[3 * i + 2]));
+        rq.tmax = R(INFINITY);
+        rq.depB = rq.depP = kNone;
+        rq.region = kNone;
+        rq.errN = R(0);
+        HitRec h;
+        const int s = traceRay<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false>(sc, rq, stack, blockDim.x, h);
+        if (s == kTraceHit) {
+            boundary[i] = h.boundary;
+            prim[i] = h.prim;
+            t[i] = h.t;
+        } else {
+            boundary[i] = s == kTraceOverflow ? kNone - 1u : kNone;
+            prim[i] = 0;
+            t[i] = INFINITY;
+        }
+    }
+}
+
+// Device-resident FP32 camera-relative rays (the benchmark's ray-cast workload).
+__global__ void __launch_bounds__(128) kCastRaysF(DeviceScene sc, uint64_t n, const float* o, const float* d,
+                                                  uint32_t* boundary, uint32_t* prim, float* t) {
+    extern __shared__ StackEntry stackMem[];
+    StackEntry* stack = stackMem + threadIdx.x;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        RayQuery<float> rq;
+        rq.o = V3<float>(o[3 * i], o[3 * i + 1], o[3 * i + 2]);
+        rq.od = V3<double>(rq.o);
+        rq.d = V3<float>(d[3 * i], d[3 * i + 1], d[3 * i + 2]);
+        rq.tmax = INFINITY;
+        rq.depB = rq.depP = kNone;
+        rq.region = kNone;
+        rq.errN = 0.f;
+        HitRec h;
+        const int s = traceRay<float, float, double, false>(sc, rq, stack, blockDim.x, h);
+        boundary[i] = s == kTraceHit ? h.boundary : (s == kTraceOverflow ? kNone - 1u : kNone);
+        prim[i] = s == kTraceHit ? h.prim : 0u;
+        t[i] = s == kTraceHit ? float(h.t) : INFINITY;
+    }
+}
+
+// Primitive records in leaf order (the triangles' camera-relative vertices and identities).
+__global__ void kMaterialize(const uint32_t* leafOrder, uint32_t n, const float4* tri, const double* tri64,
+                             PrimRec* prims, PrimRec64* prims64) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const uint32_t p = leafOrder[s];
+    const float4 a = tri[3 * p], b = tri[3 * p + 1], c = tri[3 * p + 2];
+    PrimRec r;
+    r.ax = a.x; r.ay = a.y; r.az = a.z; r.aw = a.w;
+    r.bx = b.x; r.by = b.y; r.bz = b.z; r.bw = b.w;
+    r.cx = c.x; r.cy = c.y; r.cz = c.z; r.cw = c.w;
+    prims[s] = r;
+    if (prims64) {
+        PrimRec64 q;
+        for (int k = 0; k < 3; ++k) {
+            q.v0[k] = tri64[9 * size_t(p) + k];
+            q.v1[k] = tri64[9 * size_t(p) + 3 + k];
+            q.v2[k] = tri64[9 * size_t(p) + 6 + k];
+        }
+        q.boundary = __float_as_uint(a.w);
+        q.prim = __float_as_uint(b.w);
+        q.kind = __float_as_uint(c.w);
+        q.pad = 0;
+        prims64[s] = q;
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ launchers
+size_t traversalSharedBytes(int block) { return size_t(block) * kStackDepth * sizeof(StackEntry); }
+
+template <int M>
+void launchGenerate(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q,
+                    StatCounters* st, cudaStream_t s) {
+    kGenerate<M><<<(pp.nPaths + 255) / 256, 256, 0, s>>>(sc, pp, pb, q, st);
+}
+template <int M>
+void launchIntersect(const DeviceScene& sc, const PathBuffers<RT<M>>& pb, const Queues& q, int cur, StatCounters* st,
+                     int grid, cudaStream_t s) {
+    kIntersect<M><<<grid, 128, traversalSharedBytes(128), s>>>(sc, pb, q, cur, st);
+}
+template <int M>
+void launchMedium(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q, int cur,
+                  StatCounters* st, int grid, cudaStream_t s) {
+    kMedium<M><<<grid, 128, 0, s>>>(sc, pp, pb, q, cur, st);
+}
+template <int M>
+void launchSurface(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q, int cur,
+                   StatCounters* st, int grid, cudaStream_t s) {
+    kSurface<M><<<grid, 128, 0, s>>>(sc, pp, pb, q, cur, st);
+}
+template <int M>
+void launchShadow(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q,
+                  StatCounters* st, int grid, cudaStream_t s) {
+    kShadow<M><<<grid, 128, traversalSharedBytes(128), s>>>(sc, pp, pb, q, st);
+}
+template <int M>
+void launchFilm(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, double* film, double* comp,
+                double* samples, uint32_t spp, cudaStream_t s) {
+    kFilm<M><<<(pp.nPixels + 255) / 256, 256, 0, s>>>(sc, pp, pb, film, comp, samples, spp);
+}
+template <int M>
+void launchCastRays(const DeviceScene& sc, uint64_t n, const double* o, const double* d, uint32_t* b, uint32_t* p,
+                    double* t, int grid, cudaStream_t s) {
+    kCastRays<M><<<grid, 128, traversalSharedBytes(128), s>>>(sc, n, o, d, b, p, t);
+}
+void launchCastRaysF(const DeviceScene& sc, uint64_t n, const float* o, const float* d, uint32_t* b, uint32_t* p,
+                     float* t, int grid, cudaStream_t s) {
+    kCastRaysF<<<grid, 128, traversalSharedBytes(128), s>>>(sc, n, o, d, b, p, t);
+}
+void launchMaterialize(const uint32_t* leafOrder, uint32_t n, const float4* tri, const double* tri64, PrimRec* prims,
+                       PrimRec64* prims64, cudaStream_t s) {
+    kMaterialize<<<(n + 255) / 256, 256, 0, s>>>(leafOrder, n, tri, tri64, prims, prims64);
+}
+void configureKernels() {
+    const int smem = int(traversalSharedBytes(128));
+    cudaFuncSetAttribute(kIntersect<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kIntersect<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kIntersect<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
+#define OWEC_INSTANTIATE(M)                                                                                         \
+    template void launchGenerate<M>(const DeviceScene&, const PassParams&, const PathBuffers<RT<M>>&, const Queues&, \
+                                    StatCounters*, cudaStream_t);                                                   \
+    template void launchIntersect<M>(const DeviceScene&, const PathBuffers<RT<M>>&, const Queues&, int,             \
+                                     StatCounters*, int, cudaStream_t);                                             \
+    template void launchMedium<M>(const DeviceScene&, const PassParams&, const PathBuffers<RT<M>>&, const Queues&,   \
+                                  int, StatCounters*, int, cudaStream_t);                                           \
+    template void launchSurface<M>(const DeviceScene&, const PassParams&, const PathBuffers<RT<M>>&, const Queues&,  \
+                                   int, StatCounters*, int, cudaStream_t);                                          \
+    template void launchShadow<M>(const DeviceScene&, const PassParams&, const PathBuffers<RT<M>>&, const Queues&,   \
+                                  StatCounters*, int, cudaStream_t);                                                \
+    template void launchFilm<M>(const DeviceScene&, const PassParams&, const PathBuffers<RT<M>>&, double*, double*,  \
+                                double*, uint32_t, cudaStream_t);                                                   \
+    template void launchCastRays<M>(const DeviceScene&, uint64_t, const double*, const double*, uint32_t*,          \
+                                    uint32_t*, double*, int, cudaStream_t);
+
+OWEC_INSTANTIATE(0)
+OWEC_INSTANTIATE(1)
+OWEC_INSTANTIATE(2)
+
+}  // namespace owec

@@ -1,0 +1,217 @@
+"""The engine's `cuda` backend seen from Python: Backend / Renderer over the C ABI (include/owec.h).
+
+Mirrors the reference's rendering interface (src/owe/render/backend.hpp:31-52,
+src/owe/render/renderer.hpp:19-79) name for name: a Backend reports its name, summary, availability,
+devices and integrators and creates Renderers; a Renderer runs passes (run_pass), resolves the image,
+keeps pass / sample / time counts and transport statistics. Errors raise RuntimeError, as the
+reference throws std::runtime_error. There is no CPU fallback: without the CUDA library or a device,
+creating a renderer raises.
+"""
+import ctypes
+import time
+
+import numpy as np
+
+import owec_abi as A
+
+
+def _check(lib, status, what):
+    if status != A.OK:
+        raise RuntimeError(f"{what}: {lib.owec_last_error().decode()} (status {status})")
+
+
+class Context:
+    """One device context: a scene on the device, its BVH, settings and film."""
+
+    def __init__(self, device=-1):
+        self.lib = A.load_library()
+        self.handle = ctypes.c_void_p()
+        _check(self.lib, self.lib.owec_open(device, ctypes.byref(self.handle)), "owec_open")
+
+    def close(self):
+        if self.handle:
+            self.lib.owec_close(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def device_name(self):
+        buf = ctypes.create_string_buffer(256)
+        _check(self.lib, self.lib.owec_device_name(self.handle, buf, 256), "owec_device_name")
+        return buf.value.decode()
+
+    def upload(self, desc):
+        self._desc = desc  # the pointed-to arrays must outlive the call only; kept for inspection
+        _check(self.lib, self.lib.owec_upload_scene(self.handle, ctypes.byref(desc)), "owec_upload_scene")
+        self.width, self.height = desc.detector.width, desc.detector.height
+
+    def build_bvh(self):
+        _check(self.lib, self.lib.owec_build_bvh(self.handle), "owec_build_bvh")
+
+    def bvh_info(self):
+        info = (ctypes.c_uint64 * 6)()
+        _check(self.lib, self.lib.owec_bvh_info(self.handle, info), "owec_bvh_info")
+        keys = ("nodes", "prims", "triangles", "node_bytes", "prim_bytes", "analytic")
+        return dict(zip(keys, [int(v) for v in info]))
+
+    def set_settings(self, settings):
+        _check(self.lib, self.lib.owec_set_settings(self.handle, ctypes.byref(settings)), "owec_set_settings")
+
+    def run_pass(self, spp):
+        _check(self.lib, self.lib.owec_pass(self.handle, int(spp)), "owec_pass")
+
+    def resolve(self):
+        n = self.width * self.height
+        xyz = np.zeros(3 * n)
+        samples = np.zeros(n)
+        _check(self.lib, self.lib.owec_resolve(self.handle, xyz.ctypes.data_as(A.c_double_p),
+                                               samples.ctypes.data_as(A.c_double_p)), "owec_resolve")
+        return xyz.reshape(self.height, self.width, 3), samples.reshape(self.height, self.width)
+
+    def reset_film(self):
+        _check(self.lib, self.lib.owec_reset_film(self.handle), "owec_reset_film")
+
+    def stats(self):
+        s = A.Stats()
+        _check(self.lib, self.lib.owec_read_stats(self.handle, ctypes.byref(s)), "owec_read_stats")
+        return s.as_dict()
+
+    def last_pass_timing(self):
+        """(pass seconds, intersect-kernel seconds, shadow-kernel seconds, intersect launches)."""
+        out = (ctypes.c_double * 4)()
+        _check(self.lib, self.lib.owec_last_pass_timing(self.handle, out), "owec_last_pass_timing")
+        return out[0], out[1], out[2], int(out[3])
+
+    def cast_rays(self, origins, directions):
+        o = np.ascontiguousarray(origins, np.float64)
+        d = np.ascontiguousarray(directions, np.float64)
+        n = len(o)
+        b = np.zeros(n, np.uint32)
+        p = np.zeros(n, np.uint32)
+        t = np.zeros(n, np.float64)
+        _check(self.lib, self.lib.owec_cast_rays(self.handle, n, o.ctypes.data_as(A.c_double_p),
+                                                 d.ctypes.data_as(A.c_double_p), b.ctypes.data_as(A.c_u32_p),
+                                                 p.ctypes.data_as(A.c_u32_p), t.ctypes.data_as(A.c_double_p)),
+               "owec_cast_rays")
+        return b, p, t
+
+    def trace_counters(self, enable):
+        """[queries, nodes, prims, shadow queries, shadow nodes, shadow prims] counted since enabled."""
+        out = (ctypes.c_uint64 * 6)()
+        _check(self.lib, self.lib.owec_trace_counters(self.handle, int(enable), out), "owec_trace_counters")
+        return [int(v) for v in out]
+
+    def scene_origin(self):
+        o = (ctypes.c_double * 3)()
+        _check(self.lib, self.lib.owec_scene_origin(self.handle, o), "owec_scene_origin")
+        return np.array(list(o))
+
+
+class Renderer:
+    """A progressive estimator of one detector's image (owe::Renderer)."""
+
+    def __init__(self, backend, desc, settings, integrator="path", device=-1):
+        if integrator not in backend.integrators():
+            known = ", ".join(backend.integrators())
+            raise RuntimeError(f"unknown integrator '{integrator}' (expected {known})")
+        self._backend = backend
+        self.ctx = Context(device)
+        self.ctx.upload(desc)
+        self.ctx.build_bvh()
+        self.ctx.set_settings(settings)
+        self.settings = settings
+        self._passes = 0
+        self._spp = 0
+        self._seconds = 0.0
+
+    def run_pass(self, spp):
+        """Adds a pass of `spp` samples per pixel (Renderer::runPass)."""
+        if spp <= 0:
+            return
+        t0 = time.perf_counter()
+        self.ctx.run_pass(spp)
+        self._seconds += time.perf_counter() - t0
+        self._passes += 1
+        self._spp += spp
+
+    def resolve(self):
+        """Per-pixel mean XYZ, shape (height, width, 3)."""
+        return self.ctx.resolve()[0]
+
+    def passes(self):
+        return self._passes
+
+    def samples_per_pixel(self):
+        return self._spp
+
+    def seconds(self):
+        return self._seconds
+
+    def stats(self):
+        return self.ctx.stats()
+
+    def backend(self):
+        name = self.ctx.device_name()
+        mode = {A.PRECISION_MIXED: "float32 camera-relative + selective float64",
+                A.PRECISION_FP32: "float32", A.PRECISION_FP64: "float64"}[self.settings.precision]
+        return f"cuda: {name} (sm_100a wavefront; {mode})"
+
+    def reset_observer(self):
+        self.ctx.reset_film()
+        self._passes = self._spp = 0
+        self._seconds = 0.0
+        return True
+
+    def close(self):
+        self.ctx.close()
+
+
+class CudaBackend:
+    """The `cuda` backend (owe::Backend)."""
+
+    def name(self):
+        return "cuda"
+
+    def summary(self):
+        return "NVIDIA B200 (sm_100a) wavefront path tracer; float32 camera-relative with selective float64"
+
+    def available(self):
+        try:
+            c = Context()
+            c.close()
+            return True, ""
+        except Exception as e:  # the reason, as Backend::available(why) reports it
+            return False, str(e)
+
+    def devices(self):
+        ok, _ = self.available()
+        if not ok:
+            return []
+        c = Context()
+        try:
+            return [{"index": 0, "name": c.device_name(), "type": "discrete", "driver": "CUDA"}]
+        finally:
+            c.close()
+
+    def integrators(self):
+        return ["path"]
+
+    def supports(self, integrator):
+        return integrator in self.integrators()
+
+    def create_renderer(self, desc, settings, integrator="path", device=-1):
+        return Renderer(self, desc, settings, integrator, device)
+
+
+def cuda_backend():
+    return CudaBackend()

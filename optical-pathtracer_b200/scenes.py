@@ -1,0 +1,367 @@
+"""Scene descriptions for the CUDA backend: a small builder over include/owec.h's owec_scene_desc,
+and the procedural workloads the backend is measured on.
+
+The builder mirrors the reference's world model (Medium -> Region -> Boundary, src/owe/scene/world.hpp)
+and its builders (buildSphere, buildSheet, buildMesh, buildLens; src/owe/scene/builders.hpp:26-114):
+region 0 is the ambient region, filled with air (Ciddor), as World's constructor makes it
+(src/owe/scene/world.cpp:165-170).
+"""
+import ctypes
+import math
+
+import numpy as np
+
+import owec_abi as A
+
+
+def _arr(ctype, values):
+    values = list(values)
+    return (ctype * max(1, len(values)))(*values)
+
+
+def translate(x, y, z):
+    m = np.eye(3, 4)
+    m[:, 3] = (x, y, z)
+    return m
+
+
+def rotate_to(frm, to):
+    """Rigid rotation taking unit `frm` to unit `to` (Transform::rotateTo, src/owe/core/math.hpp:130-138)."""
+    frm = np.asarray(frm, float) / np.linalg.norm(frm)
+    to = np.asarray(to, float) / np.linalg.norm(to)
+    axis = np.cross(frm, to)
+    s = np.linalg.norm(axis)
+    c = float(np.dot(frm, to))
+    if s < 1e-12:
+        if c > 0:
+            return np.eye(3)
+        a = np.array([1.0, 0, 0]) if abs(to[0]) < 0.9 else np.array([0, 1.0, 0])
+        a = a - to * np.dot(a, to)
+        axis, angle = a / np.linalg.norm(a), math.pi
+    else:
+        axis, angle = axis / s, math.atan2(s, c)
+    x, y, z = axis
+    K = np.array([[0, -z, y], [z, 0, -x], [-y, x, 0]])
+    return np.eye(3) + math.sin(angle) * K + (1 - math.cos(angle)) * K @ K
+
+
+def pose(R=None, t=(0, 0, 0)):
+    m = np.zeros((3, 4))
+    m[:, :3] = np.eye(3) if R is None else R
+    m[:, 3] = t
+    return m
+
+
+class SceneBuilder:
+    """Accumulates a world and produces the owec_scene_desc that describes it."""
+
+    def __init__(self):
+        self.spectra, self.table = [], []
+        self.media, self.region_medium = [], []
+        self.optics, self.emissions, self.boundaries, self.meshes = [], [], [], []
+        self.vertices, self.triangles = [], []
+        self.n_vertices = self.n_triangles = 0
+        self.env = A.Environment(A.SKY_NONE, -1, 0, -1, (0, 0, 1), math.radians(0.2665), 0.0)
+        self.detector = None
+        air = self.medium_ciddor_air()
+        self.region_medium.append(air)  # region 0: the ambient region
+
+    # ---------------------------------------------------------- spectra and media
+    def spectrum_constant(self, v):
+        self.spectra.append(A.Spectrum(A.SPEC_CONSTANT, 0, 0, 0, float(v), 1.0))
+        return len(self.spectra) - 1
+
+    def spectrum_tabulated(self, lambdas, values, scale=1.0):
+        off = len(self.table) // 2
+        for l, v in zip(lambdas, values):
+            self.table += [float(l), float(v)]
+        self.spectra.append(A.Spectrum(A.SPEC_TABULATED, off, len(lambdas), 0, 0.0, float(scale)))
+        return len(self.spectra) - 1
+
+    def spectrum_blackbody(self, kelvin, scale):
+        self.spectra.append(A.Spectrum(A.SPEC_BLACKBODY, 0, 0, 0, float(kelvin), float(scale)))
+        return len(self.spectra) - 1
+
+    def _medium(self, kind, a=(), b=(), rel_air=False, absorption=-1, scattering=-1, g=0.0, opaque=False,
+                index_table=-1):
+        ca = list(a) + [0.0] * (4 - len(a))
+        cb = list(b) + [0.0] * (4 - len(b))
+        self.media.append(A.Medium(kind, len(a), int(rel_air), int(opaque), (ctypes.c_double * 4)(*ca),
+                                   (ctypes.c_double * 4)(*cb), absorption, scattering, index_table, 0, float(g)))
+        return len(self.media) - 1
+
+    def medium_ciddor_air(self, **kw):
+        return self._medium(A.INDEX_CIDDOR, **kw)
+
+    def medium_constant(self, n, **kw):
+        return self._medium(A.INDEX_CONSTANT, (n,), **kw)
+
+    def medium_sellmeier(self, B, C, rel_air=False, **kw):
+        return self._medium(A.INDEX_SELLMEIER, tuple(B), tuple(C), rel_air=rel_air, **kw)
+
+    def medium_opaque(self):
+        return self._medium(A.INDEX_CONSTANT, (1.0,), opaque=True)
+
+    def region(self, medium):
+        self.region_medium.append(medium)
+        return len(self.region_medium) - 1
+
+    # ---------------------------------------------------------- optics and emission
+    def optics_(self, type_, reflectance=-1, roughness=0.0, back_absorbs=False, cond_n=-1, cond_k=-1):
+        self.optics.append(A.Optics(type_, int(back_absorbs), reflectance, cond_n, cond_k, 0, float(roughness)))
+        return len(self.optics) - 1
+
+    def diffuse(self, albedo, **kw):
+        return self.optics_(A.SURF_DIFFUSE, self.spectrum_constant(albedo), **kw)
+
+    def dielectric(self, roughness=0.0):
+        return self.optics_(A.SURF_DIELECTRIC, roughness=roughness)
+
+    def absorber(self):
+        return self.optics_(A.SURF_ABSORBER)
+
+    def emission(self, radiance, front=True, back=False, nee=True, distant=False):
+        self.emissions.append(A.Emission(radiance, int(front), int(back), int(nee), int(distant), 0))
+        return len(self.emissions) - 1
+
+    # ---------------------------------------------------------- boundaries
+    def boundary(self, shape, params, xf, front, back, optics, emission=-1, mesh=-1):
+        xf = np.asarray(xf, float).reshape(3, 4)
+        p = list(params) + [0.0] * (4 - len(params))
+        self.boundaries.append(A.Boundary(shape, mesh, front, back, optics, emission,
+                                          (ctypes.c_double * 12)(*xf.ravel()), (ctypes.c_double * 4)(*p)))
+        return len(self.boundaries) - 1
+
+    def mesh(self, vertices, triangles):
+        v = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 3)
+        t = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1, 3)
+        self.meshes.append(A.Mesh(self.n_vertices, len(v), self.n_triangles, len(t)))
+        self.vertices.append(v)
+        self.triangles.append(t)
+        self.n_vertices += len(v)
+        self.n_triangles += len(t)
+        return len(self.meshes) - 1
+
+    def sphere_body(self, radius, center, interior_medium, optics, emission=-1):
+        """buildSphere (src/owe/scene/builders.cpp:155-161): outside in front, interior behind."""
+        inside = self.region(interior_medium)
+        return self.boundary(A.SHAPE_SPHERE, [radius], translate(*center), 0, inside, optics, emission), inside
+
+    def sheet(self, half_x, half_y, xf, optics, emission=-1, disk=False):
+        """buildSheet: a two-sided plane with the ambient region on both sides."""
+        if disk:
+            return self.boundary(A.SHAPE_PLANE, [A.APERTURE_DISK, half_x, 0.0], xf, 0, 0, optics, emission)
+        return self.boundary(A.SHAPE_PLANE, [A.APERTURE_RECT, half_x, half_y], xf, 0, 0, optics, emission)
+
+    def mesh_body(self, vertices, triangles, interior_medium, optics, xf=None, emission=-1):
+        """buildMesh (src/owe/scene/builders.cpp:174-181): a closed mesh, interior behind its faces."""
+        inside = self.region(interior_medium)
+        m = self.mesh(vertices, triangles)
+        return self.boundary(A.SHAPE_MESH, [], pose() if xf is None else xf, 0, inside, optics, emission, m), inside
+
+    # ---------------------------------------------------------- environment and detector
+    def sun(self, direction, radiance, angular_radius=math.radians(0.2665), nee_share=0.0):
+        d = np.asarray(direction, float)
+        d = d / np.linalg.norm(d)
+        self.env.has_sun = 1
+        self.env.sun_dir = (ctypes.c_double * 3)(*d)
+        self.env.sun_radiance = self.spectrum_constant(radiance)
+        self.env.sun_angular_radius = angular_radius
+        self.env.sun_nee_share = nee_share
+
+    def uniform_sky(self, radiance):
+        self.env.sky_model = A.SKY_UNIFORM
+        self.env.sky_radiance = self.spectrum_constant(radiance)
+
+    def observer(self, width, height, position, look_at, up=(0, 0, 1), fov_y_deg=40.0, pixel_sigma=0.0, region=0):
+        self.detector = A.Detector(A.DETECTOR_OBSERVER, width, height, region, (ctypes.c_double * 3)(*position),
+                                   (ctypes.c_double * 3)(*look_at), (ctypes.c_double * 3)(*up),
+                                   math.radians(fov_y_deg), float(pixel_sigma), 0, 0, 0.0, 0.0)
+
+    def sensor(self, width, height, boundary, half_x, half_y, pixel_sigma=0.0):
+        self.detector = A.Detector(A.DETECTOR_SENSOR, width, height, A.REGION_OUTSIDE, (ctypes.c_double * 3)(),
+                                   (ctypes.c_double * 3)(), (ctypes.c_double * 3)(), 0.0, float(pixel_sigma),
+                                   boundary, 0, float(half_x), float(half_y))
+
+    # ---------------------------------------------------------- the description
+    def desc(self):
+        """An owec_scene_desc; the arrays it points into live as long as the returned object."""
+        if self.detector is None:
+            raise ValueError("the scene needs a detector")
+        verts = np.concatenate(self.vertices) if self.vertices else np.zeros((1, 3))
+        tris = np.concatenate(self.triangles) if self.triangles else np.zeros((1, 3), np.uint32)
+        verts = np.ascontiguousarray(verts, np.float64)
+        tris = np.ascontiguousarray(tris, np.uint32)
+        keep = {
+            "spectra": _arr(A.Spectrum, self.spectra),
+            "table": _arr(ctypes.c_double, self.table),
+            "media": _arr(A.Medium, self.media),
+            "regions": _arr(ctypes.c_uint32, self.region_medium),
+            "optics": _arr(A.Optics, self.optics),
+            "emissions": _arr(A.Emission, self.emissions),
+            "boundaries": _arr(A.Boundary, self.boundaries),
+            "meshes": _arr(A.Mesh, self.meshes),
+            "verts": verts,
+            "tris": tris,
+        }
+        d = A.SceneDesc()
+        d.abi_version = A.ABI_VERSION
+        d.n_spectra, d.n_media, d.n_regions = len(self.spectra), len(self.media), len(self.region_medium)
+        d.n_optics, d.n_emissions, d.n_boundaries = len(self.optics), len(self.emissions), len(self.boundaries)
+        d.n_meshes, d.n_spectrum_table = len(self.meshes), len(self.table) // 2
+        d.n_vertices, d.n_triangles = self.n_vertices, self.n_triangles
+        d.spectra, d.spectrum_table = keep["spectra"], keep["table"]
+        d.media, d.region_medium, d.optics = keep["media"], keep["regions"], keep["optics"]
+        d.emissions, d.boundaries, d.meshes = keep["emissions"], keep["boundaries"], keep["meshes"]
+        d.vertices = verts.ctypes.data_as(A.c_double_p)
+        d.triangles = tris.ctypes.data_as(A.c_u32_p)
+        d.env = self.env
+        d.detector = self.detector
+        d._keep = keep  # the pointed-to arrays live as long as the description
+        return d
+
+
+# ------------------------------------------------------------------ glasses
+# Schott N-BK7, relative to air (src/owe/core/medium.cpp:119).
+NBK7 = ((1.03961212, 0.231792344, 1.01046945), (0.00600069867, 0.0200179144, 103.560653))
+# Schott N-SF5, relative to air.
+SF5 = ((1.52481889, 0.187085527, 1.42729015), (0.011254756, 0.0588995392, 129.141675))
+# PMMA, three-term Sellmeier (lambda in um).
+PMMA = ((0.99654, 0.18964, 0.00411), (0.00787, 0.02191, 3.85727))
+
+
+# ------------------------------------------------------------------ seeded noise
+def _pcg_hash(x):
+    """A 32-bit integer hash (PCG output permutation) used to seed lattice gradients."""
+    x = (x.astype(np.uint64) * np.uint64(747796405) + np.uint64(2891336453)) & np.uint64(0xFFFFFFFF)
+    shift = ((x >> np.uint64(28)) + np.uint64(4)) & np.uint64(31)
+    word = (((x >> shift) ^ x) * np.uint64(277803737)) & np.uint64(0xFFFFFFFF)
+    return ((word >> np.uint64(22)) ^ word) & np.uint64(0xFFFFFFFF)
+
+
+def gradient_noise3(p, seed):
+    """Seeded 3-D gradient noise (Perlin's construction: random unit gradients on the integer lattice,
+    quintic fade, trilinear blend of the corner ramps). Values in about [-1, 1]."""
+    p = np.asarray(p, np.float64)
+    i0 = np.floor(p).astype(np.int64)
+    f = p - i0
+    w = f * f * f * (f * (f * 6 - 15) + 10)
+    out = np.zeros(len(p))
+    for dz in (0, 1):
+        for dy in (0, 1):
+            for dx in (0, 1):
+                c = i0 + np.array([dx, dy, dz])
+                h = _pcg_hash((c[:, 0] * 73856093 ^ c[:, 1] * 19349663 ^ c[:, 2] * 83492791 ^ seed * 2654435761)
+                              & 0xFFFFFFFF)
+                # gradient: a direction from the hash (uniform on the sphere)
+                u = (h & np.uint64(0xFFFF)).astype(np.float64) / 65535.0
+                v = (h >> np.uint64(16)).astype(np.float64) / 65535.0
+                z = 1 - 2 * u
+                r = np.sqrt(np.maximum(0, 1 - z * z))
+                phi = 2 * math.pi * v
+                g = np.stack([r * np.cos(phi), r * np.sin(phi), z], 1)
+                d = f - np.array([dx, dy, dz])
+                ramp = (g * d).sum(1)
+                wx = w[:, 0] if dx else 1 - w[:, 0]
+                wy = w[:, 1] if dy else 1 - w[:, 1]
+                wz = w[:, 2] if dz else 1 - w[:, 2]
+                out += wx * wy * wz * ramp
+    return out * 1.6
+
+
+def uv_sphere(n_lon=1024, n_lat=512, radius=1.0, amplitude=0.05, frequency=4.0, seed=7):
+    """A UV sphere of n_lon meridians and n_lat rings between its poles: n_lon * n_lat * 2 triangles
+    (2^20 at 1024 x 512). Vertices are displaced radially by seeded gradient noise of amplitude
+    `amplitude * radius`; faces are counter-clockwise seen from outside."""
+    rings = n_lat
+    j = np.arange(1, n_lat + 1)
+    theta = math.pi * j / (n_lat + 1)
+    phi = 2 * math.pi * np.arange(n_lon) / n_lon
+    st, ct = np.sin(theta)[:, None], np.cos(theta)[:, None]
+    ring = np.stack([st * np.cos(phi)[None, :], st * np.sin(phi)[None, :], np.broadcast_to(ct, (rings, n_lon))], -1)
+    dirs = np.concatenate([np.array([[0, 0, 1.0]]), ring.reshape(-1, 3), np.array([[0, 0, -1.0]])])
+    n = gradient_noise3(dirs * frequency, seed)
+    n = np.clip(n, -1, 1)
+    verts = dirs * (radius * (1 + amplitude * n))[:, None]
+    north, south = 0, 1 + rings * n_lon
+    idx = lambda r, c: 1 + r * n_lon + (c % n_lon)  # noqa: E731
+    c = np.arange(n_lon)
+    tris = [np.stack([np.full(n_lon, north), idx(0, c), idx(0, c + 1)], 1)]
+    for r in range(rings - 1):
+        a, b = idx(r, c), idx(r, c + 1)
+        a2, b2 = idx(r + 1, c), idx(r + 1, c + 1)
+        tris.append(np.stack([a, a2, b2], 1))
+        tris.append(np.stack([a, b2, b], 1))
+    tris.append(np.stack([np.full(n_lon, south), idx(rings - 1, c + 1), idx(rings - 1, c)], 1))
+    tris = np.concatenate(tris).astype(np.uint32)
+    return verts, tris
+
+
+# ------------------------------------------------------------------ the workloads
+def glass_sphere_on_floor(width=256, height=256, pixel_sigma=0.0, sun_radiance=1.0e4):
+    """An N-BK7 sphere of radius 1 on a Lambertian floor (albedo 0.8) under the sun at 45 degrees
+    elevation; pinhole camera. The small plain-method workload."""
+    sb = SceneBuilder()
+    bk7 = sb.medium_sellmeier(*NBK7, rel_air=True)
+    sb.sphere_body(1.0, (0, 0, 1.0), bk7, sb.dielectric())
+    sb.sheet(20.0, 20.0, pose(), sb.diffuse(0.8))
+    el = math.radians(45.0)
+    az = math.atan2(0.35, 0.94)  # the sun stands behind the camera's right shoulder
+    sb.sun((math.sin(az) * math.cos(el), -math.cos(az) * math.cos(el), math.sin(el)), sun_radiance)
+    sb.observer(width, height, (0.0, -5.5, 2.6), (0.0, 0.0, 0.8), fov_y_deg=40.0, pixel_sigma=pixel_sigma)
+    return sb
+
+
+def bvh_stress_room(width=1920, height=1080, n_lon=1024, n_lat=512, pixel_sigma=0.0):
+    """A 2^20-triangle displaced UV sphere (radius 1, noise amplitude 5 %) inside a closed Lambertian
+    box with one area light on the ceiling. The BVH-stress workload."""
+    sb = SceneBuilder()
+    opaque = sb.medium_opaque()
+    verts, tris = uv_sphere(n_lon, n_lat)
+    sb.mesh_body(verts, tris, opaque, sb.diffuse(0.6), xf=translate(0, 0, 1.2))
+    wall = sb.diffuse(0.7)
+    h = 3.0  # box [-3, 3] x [-3, 3] x [0, 4]: five walls facing in, floor at z = 0
+    sb.sheet(h, h, pose(), wall)  # floor (front +z)
+    sb.sheet(h, h, pose(rotate_to((0, 0, 1), (0, 0, -1)), (0, 0, 4.0)), wall)  # ceiling
+    sb.sheet(2.0, h, pose(rotate_to((0, 0, 1), (1, 0, 0)), (-h, 0, 2.0)), wall)
+    sb.sheet(2.0, h, pose(rotate_to((0, 0, 1), (-1, 0, 0)), (h, 0, 2.0)), wall)
+    sb.sheet(h, 2.0, pose(rotate_to((0, 0, 1), (0, -1, 0)), (0, h, 2.0)), wall)
+    sb.sheet(h, 2.0, pose(rotate_to((0, 0, 1), (0, 1, 0)), (0, -h, 2.0)), wall)
+    lamp = sb.emission(sb.spectrum_constant(8.0))
+    sb.sheet(0.8, 0.8, pose(rotate_to((0, 0, 1), (0, 0, -1)), (0.0, 0.0, 3.98)), sb.absorber(), emission=lamp)
+    sb.observer(width, height, (0.3, -2.7, 1.6), (0.0, 0.0, 1.0), fov_y_deg=55.0, pixel_sigma=pixel_sigma)
+    return sb
+
+
+def furnace_sphere(rho, width=16, height=16):
+    """Inside a closed diffuse sphere of albedo rho emitting Le = 1 inward: L = Le / (1 - rho)
+    (tests/test_backends.cpp:349-378)."""
+    sb = SceneBuilder()
+    air = sb.medium_ciddor_air()
+    e = sb.emission(sb.spectrum_constant(1.0), front=False, back=True)
+    inside = sb.region(air)
+    sb.boundary(A.SHAPE_SPHERE, [1.0], pose(), 0, inside, sb.diffuse(rho), e)
+    sb.observer(width, height, (0.2, 0.1, -0.3), (1, 0.3, 0), fov_y_deg=70.0, region=inside)
+    return sb
+
+
+def invisible_sphere(width=24, height=24):
+    """A lossless N-SF11 sphere in a uniform radiance field is invisible (tests/test_backends.cpp:380-407)."""
+    sb = SceneBuilder()
+    sb.uniform_sky(1.0)
+    sf11 = sb.medium_sellmeier((1.73759695, 0.313747346, 1.89878101), (0.013188707, 0.0623068142, 155.23629),
+                               rel_air=True)
+    sb.sphere_body(1.0, (0, 0, 0), sf11, sb.dielectric())
+    sb.observer(width, height, (0, -4, 0), (0, 0, 0), fov_y_deg=30.0)
+    return sb
+
+
+def random_rays(n, seed, lo, hi, target_lo, target_hi):
+    """n rays from uniform points of box [lo, hi] toward uniform points of [target_lo, target_hi]
+    (seeded numpy PCG64). Unit directions."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    o = rng.uniform(lo, hi, size=(n, 3))
+    t = rng.uniform(target_lo, target_hi, size=(n, 3))
+    d = t - o
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return np.ascontiguousarray(o), np.ascontiguousarray(d)

@@ -1,0 +1,164 @@
+"""Parity of the CUDA backend with the reference engine (GPU).
+
+Ray casts: closest-hit boundary and primitive identities equal World::intersect's apart from rare
+grazing ties, distances within the stated tolerance. Images: analytic known answers of the
+reference's conformance suite (tests/test_backends.cpp) and statistical agreement with the
+reference's own FP64 transport on the same scene (compareRenderers' block z-test), plus per-path
+agreement where device and CPU paths draw the same random numbers.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import owec_abi as A
+import owe_cuda
+import scenes
+from oracle_ref import ReferenceEngine, block_z_test
+
+pytestmark = pytest.mark.gpu
+
+# Mixed precision: FP32 triangles and origins rounded to FP32 -> relative distance error of a few
+# float ulps of the coordinates' magnitude over the distance.
+T_REL_TOL = 2e-5
+
+
+def _ctx(desc, settings=None):
+    c = owe_cuda.Context()
+    c.upload(desc)
+    c.build_bvh()
+    if settings is not None:
+        c.set_settings(settings)
+    return c
+
+
+def test_cast_rays_match_world_intersect_on_displaced_sphere():
+    sb = scenes.bvh_stress_room(64, 48, n_lon=256, n_lat=128)
+    desc = sb.desc()
+    ref = ReferenceEngine(desc)
+    o, d = scenes.random_rays(200_000, 1234, (-2.8, -2.8, 0.1), (2.8, 2.8, 3.9), (-1.1, -1.1, 0.1), (1.1, 1.1, 2.3))
+    rb, rp, rt = ref.cast_rays(o, d)
+    with _ctx(desc) as c:
+        info = c.bvh_info()
+        assert info["triangles"] == 256 * 128 * 2
+        gb, gp, gt = c.cast_rays(o, d)
+    same = (gb == rb) & (gp == rp)
+    frac = 1 - same.mean()
+    # disagreements must be near-ties: the two distances agree although the primitives differ
+    diff = ~same
+    if diff.any():
+        both = diff & (rb != A.KNONE) & (gb != A.KNONE)
+        assert np.all(np.abs(gt[both] - rt[both]) <= 1e-4 * np.maximum(1, rt[both])), "a non-tie mismatch"
+    assert frac < 1e-3, f"{frac:.2e} of rays hit another primitive"
+    hit = same & (rb != A.KNONE)
+    rel = np.abs(gt[hit] - rt[hit]) / np.maximum(rt[hit], 1e-9)
+    assert np.max(rel) < T_REL_TOL, f"max relative t error {np.max(rel):.2e}"
+
+
+def test_cast_rays_hit_analytic_shapes_like_the_reference():
+    sb = scenes.glass_sphere_on_floor(32, 32)
+    desc = sb.desc()
+    ref = ReferenceEngine(desc)
+    o, d = scenes.random_rays(50_000, 99, (-4, -6, 0.2), (4, -3, 4), (-1.2, -1.2, -0.5), (1.2, 1.2, 2.2))
+    rb, rp, rt = ref.cast_rays(o, d)
+    with _ctx(desc) as c:
+        gb, gp, gt = c.cast_rays(o, d)
+    assert np.mean(gb == rb) > 0.9999
+    hit = (gb == rb) & (rb != A.KNONE)
+    rel = np.abs(gt[hit] - rt[hit]) / rt[hit]
+    assert np.max(rel) < 1e-9, "the sphere's roots are refined in FP64"
+
+
+@pytest.mark.parametrize("rho", [0.0, 0.5, 0.8])
+def test_white_furnace_closed_diffuse_sphere(rho):
+    """L = Le / (1 - rho) inside a closed emitting diffuse sphere (tests/test_backends.cpp:349-378)."""
+    desc = scenes.furnace_sphere(rho).desc()
+    r = owe_cuda.CudaBackend().create_renderer(desc, A.make_settings(seed=1))
+    r.run_pass(1024)
+    img = r.resolve()
+    assert abs(img[:, :, 1].mean() - 1 / (1 - rho)) < 0.01 / (1 - rho)
+    st = r.stats()
+    assert st["leaks"] == 0 and st["device_faults"] == 0
+    r.close()
+
+
+def test_lossless_dielectric_sphere_is_invisible():
+    """tests/test_backends.cpp:380-407: n^2 law, Fresnel, TIR and dispersion keep L = 1."""
+    desc = scenes.invisible_sphere().desc()
+    r = owe_cuda.CudaBackend().create_renderer(desc, A.make_settings(seed=1))
+    r.run_pass(1024)
+    img = r.resolve()
+    assert abs(img[:, :, 1].mean() - 1.0) < 0.004
+    assert abs(img[6:18, 6:18, 1].mean() - 1.0) < 0.01
+    r.close()
+
+
+def _glass_settings(seed):
+    return A.make_settings(seed=seed, max_depth=16, rr_depth=4, wavelength_mode=A.WAVELENGTHS_UNIFORM1)
+
+
+def test_glass_sphere_agrees_with_reference_statistically():
+    """The plain-method workload at 48 x 48: block z-test over independent seeds against the
+    reference's FP64 transport (compareRenderers)."""
+    desc = scenes.glass_sphere_on_floor(48, 48).desc()
+    ref = ReferenceEngine(desc)
+    runs_ref, runs_gpu = [], []
+    with _ctx(desc) as c:
+        for k in range(8):
+            img, st = ref.render(_glass_settings(1000 + k), 64)
+            runs_ref.append(img)
+            c.set_settings(_glass_settings(2000 + k))
+            c.reset_film()
+            c.run_pass(64)
+            runs_gpu.append(c.resolve()[0])
+            assert st["leaks"] == 0
+        assert c.stats()["device_faults"] == 0
+    ok, rep = block_z_test(runs_ref, runs_gpu)
+    assert ok, rep
+
+
+def test_one_sample_paths_follow_the_reference_paths():
+    """With one-sample passes both draw from the stream (hashCombine(seed, pixel), pass): most
+    device paths make every decision the CPU path makes and return the same value."""
+    desc = scenes.glass_sphere_on_floor(64, 64).desc()
+    ref = ReferenceEngine(desc)
+    s = _glass_settings(5)
+    img_ref, _ = ref.render(s, 1, passes=1)
+    with _ctx(desc, s) as c:
+        c.run_pass(1)
+        img_gpu = c.resolve()[0]
+    a, b = img_ref[:, :, 1].ravel(), img_gpu[:, :, 1].ravel()
+    close = np.abs(a - b) <= 1e-4 * np.maximum(np.abs(a), 1e-3)
+    assert close.mean() > 0.97, f"only {close.mean():.3f} of paths agree"
+
+
+def test_hero_wavelength_render_agrees_with_reference_backend():
+    """Four hero wavelengths (the reference's default) through its unchanged cpu Backend."""
+    desc = scenes.glass_sphere_on_floor(32, 32).desc()
+    ref = ReferenceEngine(desc)
+    runs_ref, runs_gpu = [], []
+    with _ctx(desc) as c:
+        for k in range(6):
+            s = A.make_settings(seed=300 + k, max_depth=16, rr_depth=4)
+            img, st, _ = ref.render_backend(s, 64)
+            runs_ref.append(img)
+            c.set_settings(A.make_settings(seed=400 + k, max_depth=16, rr_depth=4))
+            c.reset_film()
+            c.run_pass(64)
+            runs_gpu.append(c.resolve()[0])
+    ok, rep = block_z_test(runs_ref, runs_gpu)
+    assert ok, rep
+
+
+def test_film_is_deterministic_and_passes_accumulate():
+    desc = scenes.glass_sphere_on_floor(32, 32).desc()
+    s = _glass_settings(11)
+    with _ctx(desc, s) as c:
+        c.run_pass(3)
+        a, n = c.resolve()
+        c.reset_film()
+        c.run_pass(1)
+        c.run_pass(2)
+        b, n2 = c.resolve()
+    assert np.array_equal(n, n2) and n.max() == 3
+    assert np.array_equal(a, b), "a pass split into sub-passes must give the same film, bit for bit"
