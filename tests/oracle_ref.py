@@ -158,3 +158,79 @@ def block_z_test(runs_a, runs_b, block=6):
     report = {"meanA": float(ma), "meanB": float(mb), "seA": float(sa), "seB": float(sb), "zImage": float(z_image),
               "tests": tests, "over4": over4, "chi2PerTest": chi2, "maxAbsZ": float(np.max(np.abs(z))) if tests else 0}
     return consistent, report
+
+
+PORT_LIB = os.path.join(ROOT, "oracle", "_build", "libowe_oracle.so")
+_port = None
+
+
+def port_lib():
+    """The CPU restatement (oracle/owe_oracle.cpp), built by __graft_entry__.build()."""
+    global _port
+    if _port is None:
+        if not os.path.exists(PORT_LIB):
+            raise RuntimeError("oracle/_build/libowe_oracle.so is not built (run __graft_entry__.build())")
+        lib = ctypes.CDLL(PORT_LIB)
+        P = ctypes.c_void_p
+        lib.oweport_last_error.restype = ctypes.c_char_p
+        lib.oweport_scene_create.restype = P
+        lib.oweport_scene_create.argtypes = [ctypes.POINTER(A.SceneDesc)]
+        lib.oweport_scene_destroy.argtypes = [P]
+        lib.oweport_render.argtypes = lib_render_args = [P, ctypes.POINTER(A.Settings), ctypes.c_int, ctypes.c_int,
+                                                          ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64,
+                                                          A.c_double_p, A.c_double_p, ctypes.POINTER(A.Stats)]
+        lib.oweport_cast_rays.argtypes = [P, ctypes.c_uint64, A.c_double_p, A.c_double_p, ctypes.c_int, A.c_u32_p,
+                                          A.c_u32_p, A.c_double_p]
+        lib.oweport_light_pdfs.argtypes = [P, A.c_double_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        _port = lib
+    return _port
+
+
+class PortEngine:
+    """The oracle's own restatement of the reference transport, on the same scene description."""
+
+    def __init__(self, desc):
+        self.lib = port_lib()
+        self.desc = desc
+        self.h = self.lib.oweport_scene_create(ctypes.byref(desc))
+        if not self.h:
+            raise RuntimeError(self.lib.oweport_last_error().decode())
+        self.w, self.hgt = desc.detector.width, desc.detector.height
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.oweport_scene_destroy(self.h)
+            self.h = None
+
+    def render(self, settings, spp, passes=1, first_pass=0, threads=0, pixel_begin=0, pixel_end=0):
+        n = self.w * self.hgt
+        xyz = np.zeros(3 * n)
+        samples = np.zeros(n)
+        st = A.Stats()
+        r = self.lib.oweport_render(self.h, ctypes.byref(settings), spp, passes, first_pass, threads, pixel_begin,
+                                    pixel_end, xyz.ctypes.data_as(A.c_double_p), samples.ctypes.data_as(A.c_double_p),
+                                    ctypes.byref(st))
+        if r != 0:
+            raise RuntimeError(self.lib.oweport_last_error().decode())
+        xyz = xyz.reshape(n, 3) / np.maximum(samples, 1)[:, None]
+        return xyz.reshape(self.hgt, self.w, 3), st.as_dict()
+
+    def cast_rays(self, o, d, threads=0):
+        o = np.ascontiguousarray(o, np.float64)
+        d = np.ascontiguousarray(d, np.float64)
+        n = len(o)
+        b = np.zeros(n, np.uint32)
+        p = np.zeros(n, np.uint32)
+        t = np.zeros(n)
+        r = self.lib.oweport_cast_rays(self.h, n, o.ctypes.data_as(A.c_double_p), d.ctypes.data_as(A.c_double_p),
+                                       threads, b.ctypes.data_as(A.c_u32_p), p.ctypes.data_as(A.c_u32_p),
+                                       t.ctypes.data_as(A.c_double_p))
+        if r != 0:
+            raise RuntimeError(self.lib.oweport_last_error().decode())
+        return b, p, t
+
+    def light_pdfs(self):
+        out = np.zeros(64)
+        n = ctypes.c_int()
+        self.lib.oweport_light_pdfs(self.h, out.ctypes.data_as(A.c_double_p), 64, ctypes.byref(n))
+        return out[: n.value].tolist()
