@@ -552,7 +552,8 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
 
     // Upload.
     c.dSpectra.upload(c.spectra.data(), c.spectra.size(), s);
-    c.dTable.upload(c.table.data(), std::max<size_t>(2, c.table.size()), s);  // never empty
+    if (c.table.empty()) c.table.assign(2, 0.0);  // never empty, so its device pointer is valid
+    c.dTable.upload(c.table.data(), c.table.size(), s);
     c.dMedia.upload(c.media.data(), c.media.size(), s);
     c.dRegionMedium.upload(c.regionMedium.data(), c.regionMedium.size(), s);
     c.dOptics.upload(c.optics.data(), c.optics.size(), s);
