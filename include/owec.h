@@ -281,6 +281,75 @@ int owec_trace_counters(owec_ctx* ctx, int enable, uint64_t out[6]);
 /* The camera-relative origin the device geometry is stored against (world = stored + origin). */
 int owec_scene_origin(owec_ctx* ctx, double origin[3]);
 
+/* ------------------------------------------------------------------ forward light walks
+ * Walks from an emitter through the world to a detector surface, binned where they end on it:
+ * the reference's Tracer::walk (src/owe/transport/transport.cpp:531-595) for every walk of a
+ * batch, with the emitter sampling of the lens analyser and the inspector's emission probes
+ * (src/owe/analysis/analysis.cpp:50-52, src/owe/analysis/inspect.cpp:250-262). Walk i of a batch
+ * draws from the PCG32 stream (hashCombine(seed, first_walk + i), stream): first a uniform for its
+ * wavelength (uniform in [lambda_min, lambda_max]), then a Draw2 for its emission, then the walk's
+ * own draws in the reference's order. */
+
+#define OWEC_SOURCE_POINT 0       /* a point emitting uniformly into a cone about `axis` */
+#define OWEC_SOURCE_COLLIMATED 1  /* a parallel beam along `axis` over a disk of radius `extent` */
+#define OWEC_SOURCE_COLLIMATED_SQUARE 2 /* the same over a square of half-size `extent` */
+
+#define OWEC_WALK_STOCHASTIC 0            /* WalkMode::Stochastic: Monte-Carlo branching */
+#define OWEC_WALK_PRIMARY_TRANSMISSION 1  /* WalkMode::PrimaryTransmission: refract with weight T */
+
+#define OWEC_SPLAT_NEAREST 0   /* each walk adds to the bin it lands in */
+#define OWEC_SPLAT_BILINEAR 1  /* a tent one bin wide: smooth in the landing point (differentiable) */
+
+typedef struct owec_walk_desc {
+    int32_t source_kind;
+    int32_t mode;
+    int32_t max_events;      /* the reference's maxEvents (256) */
+    int32_t splat;
+    double position[3];      /* point source position, or the beam's centre */
+    double axis[3];          /* cone axis / beam direction (unit) */
+    double extent;           /* point: cone half-angle (radians); collimated: beam radius or half-size */
+    double lambda_min, lambda_max;
+    uint32_t region;         /* region the walks start in */
+    uint32_t target;         /* boundary whose walk endings are binned */
+    int32_t width, height;   /* bins over the target's rectangle [-half_x, half_x] x [-half_y, half_y] */
+    double half_x, half_y;   /* in the target shape's frame (x, y) */
+    uint64_t seed;
+    uint64_t stream;
+} owec_walk_desc;
+
+typedef struct owec_walk_stats {
+    uint64_t walks, binned, escaped, events, faults;
+} owec_walk_stats;
+
+/* Adds n walks (first_walk .. first_walk + n - 1) to the walk film of `walk` (one film per
+ * context; a different walk description starts it over). Synchronous. */
+int owec_walk(owec_ctx* ctx, const owec_walk_desc* walk, uint64_t first_walk, uint64_t n);
+/* The walk film: per bin, the sum of the binned walks' throughput times (source measure) /
+ * (walks * bin area), where the source measure is the cone's solid angle (point source) or the
+ * beam's area (collimated): irradiance per unit source intensity or irradiance. */
+int owec_walk_resolve(owec_ctx* ctx, double* bins, owec_walk_stats* stats);
+int owec_walk_reset(owec_ctx* ctx);
+
+/* ------------------------------------------------------------------ heightfields and the adjoint
+ * A refractive heightfield is a mesh boundary whose vertices move along the z axis of its frame:
+ * vertex k of its mesh sits at (x_k, y_k, base_z + h[k]) (x_k, y_k as uploaded). The reference has
+ * no heightfield shape; it is a MeshShape (src/owe/scene/mesh.cpp) whose vertices the optimiser
+ * moves. */
+
+/* Sets the heights (one per vertex of the boundary's mesh) of mesh boundary `boundary`, makes it the
+ * heightfield the adjoint differentiates, and rebuilds the BVH on the device. The caller keeps the
+ * vertices shared with other boundaries (a slab's sides) where those boundaries have them. */
+int owec_set_heightfield(owec_ctx* ctx, uint32_t boundary, uint64_t n_vertices, double base_z, const double* heights);
+/* Path-replay adjoint of the walk film: the gradient of sum_b g[b] * bins[b] (bins as
+ * owec_walk_resolve gives them for walks first .. first + n - 1 of `walk`, which must use
+ * OWEC_WALK_PRIMARY_TRANSMISSION and OWEC_SPLAT_BILINEAR) with respect to the heights set by
+ * owec_set_heightfield, accumulated into dheights (one per vertex). Each walk is recomputed from its seed
+ * and differentiated through its crossings; nothing of the forward pass is stored. */
+int owec_walk_adjoint(owec_ctx* ctx, const owec_walk_desc* walk, uint64_t first, uint64_t n, const double* g,
+                      double* dheights);
+/* Device seconds of the last owec_walk and owec_walk_adjoint calls. */
+int owec_walk_timing(owec_ctx* ctx, double out[2]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -15,6 +15,7 @@
 #include "bvh_build.hpp"
 #include "owec.h"
 #include "spectral.cuh"
+#include "walk.hpp"
 #include "wavefront.hpp"
 
 using namespace owec;
@@ -168,6 +169,21 @@ double shapeArea(const owec_scene_desc& d, const owec_boundary& b, bool& canSamp
     }
 }
 
+// A primitive's box in FP32, padded outward by a relative 1e-6 (so the FP32 traversal of rays
+// rounded to FP32 stays conservative) and rounded outward.
+void padPrimBox(const double lo[3], const double hi[3], float4& flo, float4& fhi) {
+    double ext = 0, mag = 0;
+    for (int k = 0; k < 3; ++k) {
+        ext = std::max(ext, hi[k] - lo[k]);
+        mag = std::max({mag, std::fabs(lo[k]), std::fabs(hi[k])});
+    }
+    const double pad = 1e-6 * (mag + ext) + 1e-9;
+    flo = make_float4(std::nextafter(float(lo[0] - pad), -INFINITY), std::nextafter(float(lo[1] - pad), -INFINITY),
+                      std::nextafter(float(lo[2] - pad), -INFINITY), 0.f);
+    fhi = make_float4(std::nextafter(float(hi[0] + pad), INFINITY), std::nextafter(float(hi[1] + pad), INFINITY),
+                      std::nextafter(float(hi[2] + pad), INFINITY), 0.f);
+}
+
 void invertRigid(const double m[12], double out[12]) {
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) out[4 * i + j] = m[4 * j + i];
@@ -198,6 +214,8 @@ struct owec_ctx {
     std::vector<DBoundary> boundaries;
     std::vector<DLight> lights;
     std::vector<float4> primLo, primHi, triRecs;
+    std::vector<uint32_t> triBase;       // first primitive of each mesh boundary
+    std::vector<uint64_t> triCount;      // its triangle count
     std::vector<double> tri64;
     uint32_t nTriangles = 0, nPrims = 0;
     bool hasNull = false;
@@ -233,6 +251,23 @@ struct owec_ctx {
     uint32_t capacity = 0;
     double lastPassSeconds = 0, lastIntersectSeconds = 0, lastShadowSeconds = 0, lastIntersectLaunches = 0;
     uint32_t* hostCounts = nullptr;  // pinned
+
+    // the heightfield the adjoint differentiates
+    HeightfieldParams hf{kNone, nullptr, {0, 0, 1}};
+    uint64_t hfVertices = 0;
+    DBuf<uint32_t> dHfTris;
+    struct MeshCopy {
+        std::vector<double> verts;    // shape-frame vertices as uploaded
+        std::vector<uint32_t> tris;
+    };
+    std::vector<MeshCopy> meshes;    // per boundary (empty for analytic ones)
+    double lastWalkSeconds = 0, lastAdjointSeconds = 0;
+
+    // forward light walks
+    owec_walk_desc walk{};
+    bool hasWalk = false;
+    uint64_t walks = 0;
+    DBuf<unsigned long long> dWalkBins, dWalkStats;
 };
 
 namespace {
@@ -447,23 +482,19 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
     c.tri64.clear();
     c.primLo.clear();
     c.primHi.clear();
-    auto padBox = [](const double lo[3], const double hi[3], float4& flo, float4& fhi) {
-        double ext = 0, mag = 0;
-        for (int k = 0; k < 3; ++k) {
-            ext = std::max(ext, hi[k] - lo[k]);
-            mag = std::max({mag, std::fabs(lo[k]), std::fabs(hi[k])});
-        }
-        const double pad = 1e-6 * (mag + ext) + 1e-9;
-        flo = make_float4(std::nextafter(float(lo[0] - pad), -INFINITY), std::nextafter(float(lo[1] - pad), -INFINITY),
-                          std::nextafter(float(lo[2] - pad), -INFINITY), 0.f);
-        fhi = make_float4(std::nextafter(float(hi[0] + pad), INFINITY), std::nextafter(float(hi[1] + pad), INFINITY),
-                          std::nextafter(float(hi[2] + pad), INFINITY), 0.f);
-    };
     auto asF = [](uint32_t v) { float f; std::memcpy(&f, &v, 4); return f; };
+    c.triBase.assign(d.n_boundaries, 0);
+    c.triCount.assign(d.n_boundaries, 0);
+    c.hf = HeightfieldParams{kNone, nullptr, {0, 0, 1}};
+    c.meshes.assign(d.n_boundaries, owec_ctx::MeshCopy{});
     for (uint32_t i = 0; i < d.n_boundaries; ++i) {
         const owec_boundary& b = d.boundaries[i];
         if (b.shape != OWEC_SHAPE_MESH) continue;
         const owec_mesh& m = d.meshes[b.mesh];
+        c.triBase[i] = uint32_t(c.primLo.size());
+        c.triCount[i] = m.tri_count;
+        c.meshes[i].verts.assign(d.vertices + 3 * m.vertex_offset, d.vertices + 3 * (m.vertex_offset + m.vertex_count));
+        c.meshes[i].tris.assign(d.triangles + 3 * m.tri_offset, d.triangles + 3 * (m.tri_offset + m.tri_count));
         double rel[12];
         std::memcpy(rel, c.boundaries[i].toWorld.m, sizeof(rel));
         for (uint64_t t = 0; t < m.tri_count; ++t) {
@@ -483,7 +514,7 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
                 hi[a] = std::max({double(f0), double(f1), double(f2), w[0][a], w[1][a], w[2][a]});
             }
             float4 flo, fhi;
-            padBox(lo, hi, flo, fhi);
+            padPrimBox(lo, hi, flo, fhi);
             c.primLo.push_back(flo);
             c.primHi.push_back(fhi);
         }
@@ -499,7 +530,7 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
         double lo[3], hi[3];
         for (int k = 0; k < 3; ++k) { lo[k] = wboxes[i].lo[k] - origin[k]; hi[k] = wboxes[i].hi[k] - origin[k]; }
         float4 flo, fhi;
-        padBox(lo, hi, flo, fhi);
+        padPrimBox(lo, hi, flo, fhi);
         c.primLo.push_back(flo);
         c.primHi.push_back(fhi);
     }
@@ -1011,6 +1042,176 @@ int owec_trace_counters(owec_ctx* ctx, int enable, uint64_t out[6]) {
         } else {
             ctx->ds.travCounters = nullptr;
         }
+    });
+}
+
+int owec_walk(owec_ctx* ctx, const owec_walk_desc* w, uint64_t first, uint64_t n) {
+    return guarded([&] {
+        require(ctx && w, "owec_walk: null argument");
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        ensureReady(*ctx);
+        require(w->source_kind >= OWEC_SOURCE_POINT && w->source_kind <= OWEC_SOURCE_COLLIMATED_SQUARE, "unknown source kind");
+        require(w->mode == OWEC_WALK_STOCHASTIC || w->mode == OWEC_WALK_PRIMARY_TRANSMISSION, "unknown walk mode");
+        require(w->splat == OWEC_SPLAT_NEAREST || w->splat == OWEC_SPLAT_BILINEAR, "unknown splat");
+        require(w->max_events > 0 && w->max_events <= 4096, "max_events out of range");
+        require(w->target < ctx->ds.nBoundaries && w->region < ctx->ds.nRegions, "walk target or region out of range");
+        require(w->width > 0 && w->height > 0 && uint64_t(w->width) * w->height <= (1ull << 26), "walk film size out of range");
+        require(w->half_x > 0 && w->half_y > 0 && w->extent > 0, "walk film or source size out of range");
+        require(w->lambda_min > 0 && w->lambda_max >= w->lambda_min, "bad wavelength range");
+        const double al = std::sqrt(w->axis[0] * w->axis[0] + w->axis[1] * w->axis[1] + w->axis[2] * w->axis[2]);
+        require(al > 0, "walk axis is zero");
+        if (!ctx->hasWalk || std::memcmp(w, &ctx->walk, sizeof(owec_walk_desc)) != 0) {
+            ctx->walk = *w;
+            ctx->hasWalk = true;
+            ctx->walks = 0;
+            ctx->dWalkBins.resize(size_t(w->width) * w->height);
+            ctx->dWalkStats.resize(5);
+            OWEC_CUDA(cudaMemsetAsync(ctx->dWalkBins.get(), 0, ctx->dWalkBins.bytes(), ctx->stream));
+            OWEC_CUDA(cudaMemsetAsync(ctx->dWalkStats.get(), 0, ctx->dWalkStats.bytes(), ctx->stream));
+        }
+        if (n == 0) return;
+        OWEC_CUDA(cudaEventRecord(ctx->passStart, ctx->stream));
+        launchWalk(ctx->settings.precision, ctx->ds, *w, ctx->boundaries[w->target].toLocal, first, n,
+                   ctx->dWalkBins.get(), ctx->dWalkStats.get(), ctx->numSMs * 8, ctx->stream);
+        checkLaunch();
+        OWEC_CUDA(cudaEventRecord(ctx->passStop, ctx->stream));
+        OWEC_CUDA(cudaEventSynchronize(ctx->passStop));
+        float ms = 0;
+        OWEC_CUDA(cudaEventElapsedTime(&ms, ctx->passStart, ctx->passStop));
+        ctx->lastWalkSeconds = ms * 1e-3;
+        ctx->walks += n;
+    });
+}
+
+int owec_walk_resolve(owec_ctx* ctx, double* bins, owec_walk_stats* stats) {
+    return guarded([&] {
+        require(ctx != nullptr, "owec_walk_resolve: null context");
+        require(ctx->hasWalk, "no walks run", OWEC_E_STATE);
+        const owec_walk_desc& w = ctx->walk;
+        const size_t nb = size_t(w.width) * w.height;
+        std::vector<unsigned long long> fixed(nb), st(5);
+        OWEC_CUDA(cudaMemcpyAsync(fixed.data(), ctx->dWalkBins.get(), nb * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        OWEC_CUDA(cudaMemcpyAsync(st.data(), ctx->dWalkStats.get(), 5 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (bins) {
+            double measure;
+            if (w.source_kind == OWEC_SOURCE_POINT) measure = 2 * kPi * (1 - std::cos(w.extent));
+            else if (w.source_kind == OWEC_SOURCE_COLLIMATED) measure = kPi * w.extent * w.extent;
+            else measure = 4 * w.extent * w.extent;
+            const double binArea = (2 * w.half_x / w.width) * (2 * w.half_y / w.height);
+            const double scale = ctx->walks ? measure / (double(ctx->walks) * binArea) / 4294967296.0 : 0.0;
+            for (size_t i = 0; i < nb; ++i) bins[i] = double(fixed[i]) * scale;
+        }
+        if (stats) {
+            stats->walks = st[0];
+            stats->binned = st[1];
+            stats->escaped = st[2];
+            stats->events = st[3];
+            stats->faults = st[4];
+        }
+    });
+}
+
+int owec_set_heightfield(owec_ctx* ctx, uint32_t boundary, uint64_t n_vertices, double base_z, const double* heights) {
+    return guarded([&] {
+        require(ctx && heights, "owec_set_heightfield: null argument");
+        require(ctx->hasScene, "no scene uploaded", OWEC_E_STATE);
+        require(boundary < ctx->boundaries.size() && ctx->boundaries[boundary].shape == OWEC_SHAPE_MESH,
+                "the heightfield must be a mesh boundary");
+        const owec_ctx::MeshCopy& m = ctx->meshes[boundary];
+        require(n_vertices == m.verts.size() / 3, "one height per vertex of the mesh");
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        const DBoundary& bd = ctx->boundaries[boundary];
+        auto asF = [](uint32_t v) { float f; std::memcpy(&f, &v, 4); return f; };
+        const uint32_t base = ctx->triBase[boundary];
+        const size_t nt = m.tris.size() / 3;
+        for (size_t t = 0; t < nt; ++t) {
+            double w[3][3];
+            for (int k = 0; k < 3; ++k) {
+                const uint32_t v = m.tris[3 * t + k];
+                const double local[3] = {m.verts[3 * v], m.verts[3 * v + 1], base_z + heights[v]};
+                xfPoint(bd.toWorld.m, local, w[k]);
+            }
+            const size_t p = base + t;
+            const uint32_t ids[3] = {boundary, uint32_t(t), kPrimTriangle};
+            double lo[3], hi[3];
+            for (int k = 0; k < 3; ++k) {
+                ctx->triRecs[3 * p + k] = make_float4(float(w[k][0]), float(w[k][1]), float(w[k][2]), asF(ids[k]));
+                for (int a = 0; a < 3; ++a) ctx->tri64[9 * p + 3 * k + a] = w[k][a];
+            }
+            for (int a = 0; a < 3; ++a) {
+                const float f0 = float(w[0][a]), f1 = float(w[1][a]), f2 = float(w[2][a]);
+                lo[a] = std::min({double(f0), double(f1), double(f2), w[0][a], w[1][a], w[2][a]});
+                hi[a] = std::max({double(f0), double(f1), double(f2), w[0][a], w[1][a], w[2][a]});
+            }
+            padPrimBox(lo, hi, ctx->primLo[p], ctx->primHi[p]);
+        }
+        OWEC_CUDA(cudaMemcpyAsync(ctx->dTri.get() + 3 * size_t(base), ctx->triRecs.data() + 3 * size_t(base),
+                                  3 * nt * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
+        OWEC_CUDA(cudaMemcpyAsync(ctx->dPrimLo.get() + base, ctx->primLo.data() + base, nt * sizeof(float4),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+        OWEC_CUDA(cudaMemcpyAsync(ctx->dPrimHi.get() + base, ctx->primHi.data() + base, nt * sizeof(float4),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+        ctx->dHfTris.upload(m.tris.data(), m.tris.size(), ctx->stream);
+        buildBvh(*ctx);
+        ctx->hf.boundary = boundary;
+        ctx->hf.tris = ctx->dHfTris.get();
+        ctx->hfVertices = n_vertices;
+        for (int k = 0; k < 3; ++k) ctx->hf.zdir[k] = bd.toWorld.m[4 * k + 2];
+        ctx->hasWalk = false;  // the walk film of the old heights is stale
+    });
+}
+
+int owec_walk_adjoint(owec_ctx* ctx, const owec_walk_desc* w, uint64_t first, uint64_t n, const double* g,
+                      double* dheights) {
+    return guarded([&] {
+        require(ctx && w && g && dheights, "owec_walk_adjoint: null argument");
+        require(ctx->hf.boundary != kNone, "no heightfield set (owec_set_heightfield)", OWEC_E_STATE);
+        require(w->mode == OWEC_WALK_PRIMARY_TRANSMISSION && w->splat == OWEC_SPLAT_BILINEAR,
+                "the adjoint needs primary-transmission walks and the bilinear splat");
+        require(w->target < ctx->ds.nBoundaries && w->width > 0 && w->height > 0 && w->half_x > 0 && w->half_y > 0,
+                "bad walk description");
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        ensureReady(*ctx);
+        const size_t nb = size_t(w->width) * w->height, nh = ctx->hfVertices;
+        DBuf<double> dG(nb), dDH(nh);
+        DBuf<unsigned long long> st(5);
+        OWEC_CUDA(cudaMemcpyAsync(dG.get(), g, nb * 8, cudaMemcpyHostToDevice, ctx->stream));
+        OWEC_CUDA(cudaMemsetAsync(dDH.get(), 0, nh * 8, ctx->stream));
+        OWEC_CUDA(cudaMemsetAsync(st.get(), 0, 5 * 8, ctx->stream));
+        double measure;
+        if (w->source_kind == OWEC_SOURCE_POINT) measure = 2 * kPi * (1 - std::cos(w->extent));
+        else if (w->source_kind == OWEC_SOURCE_COLLIMATED) measure = kPi * w->extent * w->extent;
+        else measure = 4 * w->extent * w->extent;
+        const double binArea = (2 * w->half_x / w->width) * (2 * w->half_y / w->height);
+        OWEC_CUDA(cudaEventRecord(ctx->passStart, ctx->stream));
+        launchWalkAdjoint(ctx->settings.precision, ctx->ds, *w, ctx->boundaries[w->target].toLocal, ctx->hf, first, n,
+                          measure / (double(n) * binArea), dG.get(), dDH.get(), st.get(), ctx->numSMs * 8, ctx->stream);
+        checkLaunch();
+        OWEC_CUDA(cudaEventRecord(ctx->passStop, ctx->stream));
+        std::vector<double> h(nh);
+        OWEC_CUDA(cudaMemcpyAsync(h.data(), dDH.get(), nh * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+        float ms = 0;
+        OWEC_CUDA(cudaEventElapsedTime(&ms, ctx->passStart, ctx->passStop));
+        ctx->lastAdjointSeconds = ms * 1e-3;
+        for (size_t i = 0; i < nh; ++i) dheights[i] += h[i];
+    });
+}
+
+int owec_walk_timing(owec_ctx* ctx, double out[2]) {
+    return guarded([&] {
+        require(ctx && out, "owec_walk_timing: null argument");
+        out[0] = ctx->lastWalkSeconds;
+        out[1] = ctx->lastAdjointSeconds;
+    });
+}
+
+int owec_walk_reset(owec_ctx* ctx) {
+    return guarded([&] {
+        require(ctx != nullptr, "owec_walk_reset: null context");
+        ctx->hasWalk = false;
+        ctx->walks = 0;
     });
 }
 

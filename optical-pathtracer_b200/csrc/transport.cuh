@@ -119,7 +119,7 @@ __device__ __forceinline__ double sphereConeSize(const V3<double>& ref, double R
 
 // Shape::pdfFrom / SphereShape::pdfFrom (src/owe/scene/geometry.cpp:24-27, 477-480) for an emitter
 // point seen from ref (both camera-relative world).
-__device__ double shapePdfFrom(const DBoundary& bd, const V3<double>& ref, const V3<double>& p, const V3<double>& n) {
+__device__ inline double shapePdfFrom(const DBoundary& bd, const V3<double>& ref, const V3<double>& p, const V3<double>& n) {
     if (bd.shape == OWEC_SHAPE_SPHERE) {
         const double omc = sphereConeSize(bd.toLocal.point(ref), bd.params[0]);
         if (omc > 0) return 1.0 / (2 * kPi * omc);
@@ -130,7 +130,7 @@ __device__ double shapePdfFrom(const DBoundary& bd, const V3<double>& ref, const
 
 // A point drawn on an emitting shape (Shape::sampleArea of the reference's shapes:
 // geometry.cpp sphere / plane / flat sag / cylinder), in the shape's frame.
-__device__ void sampleShapeArea(const DBoundary& bd, double u1, double u2, V3<double>& p, V3<double>& n) {
+__device__ inline void sampleShapeArea(const DBoundary& bd, double u1, double u2, V3<double>& p, V3<double>& n) {
     const double* P = bd.params;
     n = V3<double>(0, 0, 1);
     switch (bd.shape) {

@@ -1,0 +1,349 @@
+// The engine-side binding of the CUDA backend: `CudaBackend : owe::Backend` and
+// `CudaRenderer : owe::Renderer` over the C ABI of include/owec.h.
+//
+// This file belongs in the engine's tree as src/owe/backends/cuda/cuda_backend.cpp, beside the cpu
+// and gpu backends; the registry lists it (src/owe/backends/registry.cpp:10-13) and the layering
+// rule allows it core/, scene/, render/ and backends/cuda/ (not transport/). It flattens the world
+// model into owec_scene_desc: media, regions, optics, emitters, boundaries with their rigid frames,
+// the sun and sky, and the detector. Scenes using features the CUDA backend does not implement
+// (textures, environment maps, aspheres, lathe and wave shapes, thin-lens observers, aim guides)
+// are refused with std::runtime_error, as Backend::createRenderer does for unsupported settings
+// (src/owe/render/backend.hpp:44).
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "owe/render/backend.hpp"
+#include "owe/scene/geometry.hpp"
+#include "owec.h"
+
+namespace owe {
+
+namespace {
+
+void check(int status, const char* what) {
+    if (status != OWEC_OK) throw std::runtime_error(std::string(what) + ": " + owec_last_error());
+}
+
+// The flattened arrays an owec_scene_desc points into.
+struct Flat {
+    std::vector<owec_spectrum> spectra;
+    std::vector<double> table;
+    std::vector<owec_medium> media;
+    std::vector<uint32_t> regionMedium;
+    std::vector<owec_optics> optics;
+    std::vector<owec_emission> emissions;
+    std::vector<owec_boundary> boundaries;
+    std::vector<owec_mesh> meshes;
+    std::vector<double> vertices;
+    std::vector<uint32_t> triangles;
+    owec_scene_desc desc{};
+
+    int32_t spectrum(const Spectrum& s) {
+        owec_spectrum o{};
+        o.scale = 1;
+        switch (s.kind()) {
+            case Spectrum::Kind::Constant:
+                o.kind = OWEC_SPEC_CONSTANT;
+                o.a = s.paramA() * s.paramScale();
+                break;
+            case Spectrum::Kind::Blackbody:
+                o.kind = OWEC_SPEC_BLACKBODY;
+                o.a = s.paramA();
+                o.scale = s.paramScale();
+                break;
+            default: {  // tabulated, and the RGB spectra sampled every nanometre over the visible range
+                o.kind = OWEC_SPEC_TABULATED;
+                o.table_offset = int32_t(table.size() / 2);
+                if (s.kind() == Spectrum::Kind::Tabulated) {
+                    const auto& L = *s.tableLambdas();
+                    const auto& V = *s.tableValues();
+                    for (size_t i = 0; i < L.size(); ++i) { table.push_back(L[i]); table.push_back(V[i]); }
+                    o.table_count = int32_t(L.size());
+                    o.scale = s.paramScale();
+                } else {
+                    int n = 0;
+                    for (double l = LambdaMin; l <= LambdaMax; l += 1.0, ++n) {
+                        table.push_back(l);
+                        table.push_back(s.eval(l));
+                    }
+                    o.table_count = n;
+                }
+            }
+        }
+        spectra.push_back(o);
+        return int32_t(spectra.size() - 1);
+    }
+};
+
+std::unique_ptr<Flat> flatten(const Scene& sc, int detectorIndex) {
+    auto f = std::make_unique<Flat>();
+    const World& w = sc.world;
+    for (const Medium& m : w.media()) {
+        owec_medium o{};
+        o.absorption = o.scattering = o.index_table = -1;
+        o.rel_air = m.index.isRelativeToAir();
+        o.opaque = m.opaque;
+        o.g = m.g;
+        switch (m.index.kind()) {
+            case IndexModel::Kind::Constant: o.index_kind = OWEC_INDEX_CONSTANT; o.coef_a[0] = m.index.coeffA()[0]; break;
+            case IndexModel::Kind::Cauchy:
+                o.index_kind = OWEC_INDEX_CAUCHY;
+                for (int i = 0; i < 3; ++i) o.coef_a[i] = m.index.coeffA()[size_t(i)];
+                break;
+            case IndexModel::Kind::Sellmeier:
+                if (m.index.coeffA().size() > OWEC_MAX_SELLMEIER_TERMS)
+                    throw std::runtime_error("medium '" + m.name + "': more Sellmeier terms than the cuda backend takes");
+                o.index_kind = OWEC_INDEX_SELLMEIER;
+                o.n_terms = int32_t(m.index.coeffA().size());
+                for (int i = 0; i < o.n_terms; ++i) {
+                    o.coef_a[i] = m.index.coeffA()[size_t(i)];
+                    o.coef_b[i] = m.index.coeffB()[size_t(i)];
+                }
+                break;
+            case IndexModel::Kind::Ciddor: o.index_kind = OWEC_INDEX_CIDDOR; break;
+            case IndexModel::Kind::Tabulated:
+                o.index_kind = OWEC_INDEX_TABULATED;
+                o.index_table = f->spectrum(m.index.table());
+                break;
+        }
+        if (m.absorbs()) o.absorption = f->spectrum(m.absorption);
+        if (m.scatters()) o.scattering = f->spectrum(m.scattering);
+        f->media.push_back(o);
+    }
+    for (const Region& r : w.regions()) f->regionMedium.push_back(r.medium);
+    for (const SurfaceOptics& so : w.optics()) {
+        if (so.texture.kind != Texture::Kind::None || so.sampleAimShare > 0 || !so.roughnessMap.empty() ||
+            so.reliefDepth != 0 || so.normalImage.image || so.roughnessImage.image)
+            throw std::runtime_error("material '" + so.name + "' uses textures, maps or aim guides, which the cuda backend does not render");
+        if (so.type == SurfaceType::StainedGlass) throw std::runtime_error("stained glass is not rendered by the cuda backend");
+        owec_optics o{};
+        o.type = int32_t(so.type);
+        o.back_absorbs = so.backAbsorbs;
+        o.roughness = so.roughness;
+        o.reflectance = f->spectrum(so.reflectance);
+        o.conductor_n = so.type == SurfaceType::Conductor ? f->spectrum(so.conductor.n) : -1;
+        o.conductor_k = so.type == SurfaceType::Conductor ? f->spectrum(so.conductor.k) : -1;
+        f->optics.push_back(o);
+    }
+    for (const Emission& e : w.emissions()) {
+        owec_emission o{};
+        o.radiance = f->spectrum(e.radiance);
+        o.front = e.front;
+        o.back = e.back;
+        o.nee = e.nee;
+        o.distant = e.distant;
+        f->emissions.push_back(o);
+    }
+    for (const Boundary& b : w.boundaries()) {
+        owec_boundary o{};
+        o.mesh = -1;
+        o.front = b.front;
+        o.back = b.back;
+        o.optics = b.optics;
+        o.emission = b.emission;
+        for (int i = 0; i < 3; ++i) {
+            for (int j = 0; j < 3; ++j) o.to_world[4 * i + j] = b.toWorld.R.m[i][j];
+            o.to_world[4 * i + 3] = b.toWorld.t[i];
+        }
+        const Shape* s = b.shape.get();
+        if (auto* sp = dynamic_cast<const SphereShape*>(s)) {
+            o.shape = OWEC_SHAPE_SPHERE;
+            o.params[0] = sp->radius();
+        } else if (auto* sg = dynamic_cast<const SagSurface*>(s)) {
+            if (!sg->asphere().empty()) throw std::runtime_error("boundary '" + b.name + "': aspheres are not rendered by the cuda backend");
+            o.shape = OWEC_SHAPE_SAG;
+            o.params[0] = sg->curvature();
+            o.params[1] = sg->conic();
+            o.params[2] = sg->rMax();
+            o.params[3] = sg->rMin();
+        } else if (auto* pl = dynamic_cast<const PlaneShape*>(s)) {
+            if (pl->aperture() == PlaneShape::Aperture::DiskHole)
+                throw std::runtime_error("boundary '" + b.name + "': holed disks are not rendered by the cuda backend");
+            o.shape = OWEC_SHAPE_PLANE;
+            o.params[0] = pl->aperture() == PlaneShape::Aperture::Disk ? OWEC_APERTURE_DISK
+                          : pl->aperture() == PlaneShape::Aperture::Rect ? OWEC_APERTURE_RECT : OWEC_APERTURE_ELLIPSE;
+            o.params[1] = pl->a();
+            o.params[2] = pl->b();
+        } else if (auto* cy = dynamic_cast<const CylinderShape*>(s)) {
+            o.shape = OWEC_SHAPE_CYLINDER;
+            o.params[0] = cy->radius();
+            o.params[1] = cy->z0();
+            o.params[2] = cy->z1();
+        } else if (auto* me = dynamic_cast<const MeshShape*>(s)) {
+            o.shape = OWEC_SHAPE_MESH;
+            o.mesh = int32_t(f->meshes.size());
+            owec_mesh m{};
+            m.vertex_offset = f->vertices.size() / 3;
+            m.vertex_count = me->positions().size();
+            m.tri_offset = f->triangles.size() / 3;
+            m.tri_count = me->triangles().size();
+            for (const Vec3& p : me->positions()) { f->vertices.push_back(p.x); f->vertices.push_back(p.y); f->vertices.push_back(p.z); }
+            for (const auto& t : me->triangles()) for (uint32_t v : t) f->triangles.push_back(v);
+            f->meshes.push_back(m);
+        } else {
+            throw std::runtime_error("boundary '" + b.name + "' has a shape the cuda backend does not render (" + s->describe() + ")");
+        }
+        f->boundaries.push_back(o);
+    }
+    owec_scene_desc& d = f->desc;
+    d.abi_version = OWEC_ABI_VERSION;
+    const Environment& env = w.env;
+    if (env.skyModel != Environment::Sky::None && env.skyModel != Environment::Sky::Uniform)
+        throw std::runtime_error("the cuda backend renders no sky but a uniform one");
+    d.env.sky_model = env.skyModel == Environment::Sky::Uniform ? OWEC_SKY_UNIFORM : OWEC_SKY_NONE;
+    d.env.sky_radiance = d.env.sky_model == OWEC_SKY_UNIFORM ? f->spectrum(env.zenith) : -1;
+    d.env.has_sun = env.hasSun;
+    d.env.sun_radiance = env.hasSun ? f->spectrum(env.sunRadiance) : -1;
+    for (int k = 0; k < 3; ++k) d.env.sun_dir[k] = env.sunDir[k];
+    d.env.sun_angular_radius = env.sunAngularRadius;
+    d.env.sun_nee_share = env.sunNeeShare;
+    const Detector& det = *sc.detectors.at(size_t(detectorIndex));
+    d.detector.width = det.width;
+    d.detector.height = det.height;
+    d.detector.pixel_sigma = det.pixelSigma;
+    d.detector.region = det.region;
+    if (auto* eye = dynamic_cast<const IdealObserver*>(&det)) {
+        if (eye->pupilRadius > 0) throw std::runtime_error("the cuda backend renders pinhole observers only");
+        d.detector.kind = OWEC_DETECTOR_OBSERVER;
+        for (int k = 0; k < 3; ++k) {
+            d.detector.position[k] = eye->position[k];
+            d.detector.look_at[k] = eye->lookAt[k];
+            d.detector.up[k] = eye->up[k];
+        }
+        d.detector.fov_y = eye->fovY;
+    } else if (auto* sen = dynamic_cast<const SurfaceSensor*>(&det)) {
+        if (sen->hasAim || sen->flipX || sen->flipY) throw std::runtime_error("the cuda backend renders unaimed, unflipped sensors only");
+        d.detector.kind = OWEC_DETECTOR_SENSOR;
+        d.detector.boundary = sen->boundaryIndex;
+        d.detector.half_x = sen->halfX;
+        d.detector.half_y = sen->halfY;
+    } else {
+        throw std::runtime_error("unknown detector type");
+    }
+    d.n_spectra = uint32_t(f->spectra.size());
+    d.n_media = uint32_t(f->media.size());
+    d.n_regions = uint32_t(f->regionMedium.size());
+    d.n_optics = uint32_t(f->optics.size());
+    d.n_emissions = uint32_t(f->emissions.size());
+    d.n_boundaries = uint32_t(f->boundaries.size());
+    d.n_meshes = uint32_t(f->meshes.size());
+    d.n_spectrum_table = f->table.size() / 2;
+    d.n_vertices = f->vertices.size() / 3;
+    d.n_triangles = f->triangles.size() / 3;
+    d.spectra = f->spectra.data();
+    d.spectrum_table = f->table.data();
+    d.media = f->media.data();
+    d.region_medium = f->regionMedium.data();
+    d.optics = f->optics.data();
+    d.emissions = f->emissions.data();
+    d.boundaries = f->boundaries.data();
+    d.meshes = f->meshes.data();
+    d.vertices = f->vertices.data();
+    d.triangles = f->triangles.data();
+    return f;
+}
+
+class CudaRenderer final : public Renderer {
+public:
+    CudaRenderer(const Scene& scene, int detectorIndex, const RenderSettings& settings)
+        : Renderer(scene, detectorIndex, settings, {"path"}), detectorIndex_(detectorIndex) {
+        check(owec_open(settings.device, &ctx_), "cuda backend");
+        upload();
+        owec_settings s{};
+        s.seed = settings.seed;
+        s.max_depth = settings.maxDepth;
+        s.rr_depth = settings.rrDepth;
+        s.wavelength_mode = OWEC_WAVELENGTHS_HERO4;
+        s.precision = OWEC_PRECISION_MIXED;
+        s.lambda_min = 380;
+        s.lambda_max = 780;
+        s.fresnel_floor = settings.fresnelFloor;
+        check(owec_set_settings(ctx_, &s), "cuda backend");
+    }
+    ~CudaRenderer() override { owec_close(ctx_); }
+
+    Image resolve() const override {
+        Image img;
+        img.width = det_->width;
+        img.height = det_->height;
+        img.xyz.assign(size_t(img.width) * img.height * 3, 0.0);
+        check(owec_resolve(ctx_, img.xyz.data(), nullptr), "cuda backend");
+        return img;
+    }
+    std::string backend() const override {
+        char name[256];
+        owec_device_name(ctx_, name, sizeof name);
+        return std::string("cuda: ") + name + " (sm_100a wavefront; float32 camera-relative + selective float64)";
+    }
+    bool resetObserver() override {
+        upload();  // the pose lives in the scene description; the film starts over
+        resetProgress();
+        return true;
+    }
+
+private:
+    void pass(int spp) override {
+        check(owec_pass(ctx_, spp), "cuda backend");
+        owec_stats st{};
+        check(owec_read_stats(ctx_, &st), "cuda backend");
+        stats_ = {};
+        stats_.paths = st.paths;
+        stats_.segments = st.segments;
+        stats_.inconsistencies = st.inconsistencies;
+        stats_.leaks = st.leaks;
+    }
+    void upload() {
+        auto flat = flatten(scene_, detectorIndex_);
+        check(owec_upload_scene(ctx_, &flat->desc), "cuda backend");
+        check(owec_build_bvh(ctx_), "cuda backend");
+    }
+
+    owec_ctx* ctx_ = nullptr;
+    int detectorIndex_;
+};
+
+class CudaBackend final : public Backend {
+public:
+    std::string name() const override { return "cuda"; }
+    std::string summary() const override {
+        return "NVIDIA B200 (sm_100a) wavefront path tracer; float32 camera-relative with selective float64";
+    }
+    bool available(std::string* why) const override {
+        owec_ctx* c = nullptr;
+        if (owec_open(-1, &c) != OWEC_OK) {
+            if (why) *why = owec_last_error();
+            return false;
+        }
+        owec_close(c);
+        return true;
+    }
+    std::vector<DeviceInfo> devices() const override {
+        owec_ctx* c = nullptr;
+        if (owec_open(-1, &c) != OWEC_OK) return {};
+        DeviceInfo d;
+        char name[256];
+        owec_device_name(c, name, sizeof name);
+        d.name = name;
+        d.type = "discrete";
+        d.driver = "CUDA";
+        owec_close(c);
+        return {d};
+    }
+    std::vector<std::string> integrators() const override { return {"path"}; }
+    std::unique_ptr<Renderer> createRenderer(const Scene& scene, int detectorIndex,
+                                             const RenderSettings& settings) const override {
+        return std::make_unique<CudaRenderer>(scene, detectorIndex, settings);
+    }
+};
+
+}  // namespace
+
+const Backend& cudaBackend() {
+    static const CudaBackend backend;
+    return backend;
+}
+
+}  // namespace owe

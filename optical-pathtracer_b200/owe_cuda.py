@@ -111,6 +111,43 @@ class Context:
         _check(self.lib, self.lib.owec_trace_counters(self.handle, int(enable), out), "owec_trace_counters")
         return [int(v) for v in out]
 
+    def walk(self, desc, first, n):
+        """n forward light walks (walk indices first .. first + n - 1) binned on desc.target."""
+        self._walk_shape = (desc.height, desc.width)
+        _check(self.lib, self.lib.owec_walk(self.handle, ctypes.byref(desc), int(first), int(n)), "owec_walk")
+
+    def walk_resolve(self):
+        h, w = self._walk_shape
+        bins = np.zeros(h * w)
+        st = A.WalkStats()
+        _check(self.lib, self.lib.owec_walk_resolve(self.handle, bins.ctypes.data_as(A.c_double_p), ctypes.byref(st)),
+               "owec_walk_resolve")
+        return bins.reshape(h, w), st.as_dict()
+
+    def set_heightfield(self, boundary, base_z, heights):
+        """Moves the vertices of mesh boundary `boundary` to z = base_z + heights (one per vertex)."""
+        h = np.ascontiguousarray(heights, np.float64).ravel()
+        _check(self.lib, self.lib.owec_set_heightfield(self.handle, boundary, len(h), base_z,
+                                                       h.ctypes.data_as(A.c_double_p)), "owec_set_heightfield")
+        self._hf_n = len(h)
+
+    def walk_adjoint(self, desc, first, n, g):
+        """d(sum_b g_b bins_b) / d heights by path replay of walks first .. first + n - 1."""
+        gg = np.ascontiguousarray(g, np.float64).ravel()
+        out = np.zeros(self._hf_n)
+        _check(self.lib, self.lib.owec_walk_adjoint(self.handle, ctypes.byref(desc), int(first), int(n),
+                                                    gg.ctypes.data_as(A.c_double_p), out.ctypes.data_as(A.c_double_p)),
+               "owec_walk_adjoint")
+        return out
+
+    def walk_timing(self):
+        out = (ctypes.c_double * 2)()
+        _check(self.lib, self.lib.owec_walk_timing(self.handle, out), "owec_walk_timing")
+        return out[0], out[1]
+
+    def walk_reset(self):
+        _check(self.lib, self.lib.owec_walk_reset(self.handle), "owec_walk_reset")
+
     def scene_origin(self):
         o = (ctypes.c_double * 3)()
         _check(self.lib, self.lib.owec_scene_origin(self.handle, o), "owec_scene_origin")

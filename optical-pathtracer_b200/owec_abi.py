@@ -101,6 +101,28 @@ class Settings(ctypes.Structure):
                 ("fresnel_floor", ctypes.c_double)]
 
 
+SOURCE_POINT, SOURCE_COLLIMATED, SOURCE_COLLIMATED_SQUARE = 0, 1, 2
+WALK_STOCHASTIC, WALK_PRIMARY_TRANSMISSION = 0, 1
+SPLAT_NEAREST, SPLAT_BILINEAR = 0, 1
+
+
+class WalkDesc(ctypes.Structure):
+    _fields_ = [("source_kind", ctypes.c_int32), ("mode", ctypes.c_int32), ("max_events", ctypes.c_int32),
+                ("splat", ctypes.c_int32), ("position", ctypes.c_double * 3), ("axis", ctypes.c_double * 3),
+                ("extent", ctypes.c_double), ("lambda_min", ctypes.c_double), ("lambda_max", ctypes.c_double),
+                ("region", ctypes.c_uint32), ("target", ctypes.c_uint32), ("width", ctypes.c_int32),
+                ("height", ctypes.c_int32), ("half_x", ctypes.c_double), ("half_y", ctypes.c_double),
+                ("seed", ctypes.c_uint64), ("stream", ctypes.c_uint64)]
+
+
+class WalkStats(ctypes.Structure):
+    _fields_ = [("walks", ctypes.c_uint64), ("binned", ctypes.c_uint64), ("escaped", ctypes.c_uint64),
+                ("events", ctypes.c_uint64), ("faults", ctypes.c_uint64)]
+
+    def as_dict(self):
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("paths", ctypes.c_uint64), ("segments", ctypes.c_uint64), ("inconsistencies", ctypes.c_uint64),
                 ("leaks", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64), ("device_faults", ctypes.c_uint64)]
@@ -147,6 +169,13 @@ def load_library(path=LIB_PATH):
         "owec_cast_rays_device": ([P, ctypes.c_uint64, P, P, P, P, P, c_double_p], ctypes.c_int),
         "owec_scene_origin": ([P, c_double_p], ctypes.c_int),
         "owec_trace_counters": ([P, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+        "owec_walk": ([P, ctypes.POINTER(WalkDesc), ctypes.c_uint64, ctypes.c_uint64], ctypes.c_int),
+        "owec_walk_resolve": ([P, c_double_p, ctypes.POINTER(WalkStats)], ctypes.c_int),
+        "owec_walk_reset": ([P], ctypes.c_int),
+        "owec_set_heightfield": ([P, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_double, c_double_p], ctypes.c_int),
+        "owec_walk_adjoint": ([P, ctypes.POINTER(WalkDesc), ctypes.c_uint64, ctypes.c_uint64, c_double_p, c_double_p],
+                              ctypes.c_int),
+        "owec_walk_timing": ([P, c_double_p], ctypes.c_int),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(lib, name)

@@ -365,3 +365,212 @@ def random_rays(n, seed, lo, hi, target_lo, target_hi):
     d = t - o
     d /= np.linalg.norm(d, axis=1, keepdims=True)
     return np.ascontiguousarray(o), np.ascontiguousarray(d)
+
+
+# ------------------------------------------------------------------ lenses and forward walks
+def sag_z(c, k, r):
+    """The conic sag at radius r (conicSag, src/owe/core/shared/surfaces.hpp:162)."""
+    return c * r * r / (1 + math.sqrt(max(0.0, 1 - (1 + k) * c * c * r * r)))
+
+
+def ciddor_air(lam_nm):
+    l2 = (lam_nm * 1e-3) ** 2
+    s2 = 1 / l2
+    return 1 + 0.05792105 / (238.0185 - s2) + 0.00167917 / (57.362 - s2)
+
+
+def sellmeier_index(coefs, lam_nm, rel_air=True):
+    l2 = (lam_nm * 1e-3) ** 2
+    n = math.sqrt(1 + sum(b * l2 / (l2 - c) for b, c in zip(*coefs)))
+    return n * ciddor_air(lam_nm) if rel_air else n
+
+
+def paraxial_image_distance(radii, thicknesses, indices, object_distance):
+    """Distance behind the last vertex where a paraxial ray from an on-axis point `object_distance`
+    in front of the first vertex crosses the axis (y-nu trace). indices: the media before, between
+    and after the surfaces, relative to the surrounding air."""
+    y, nu = 1e-6, 1e-6 / object_distance  # nu = n u
+    for i, R in enumerate(radii):
+        c = 0.0 if math.isinf(R) else 1.0 / R
+        nu = nu - y * c * (indices[i + 1] - indices[i])
+        if i < len(thicknesses):
+            y = y + thicknesses[i] * nu / indices[i + 1]
+    u = nu / indices[-1]
+    return -y / u
+
+
+def lens_body(sb, surfaces, media, thickness, z0=0.0, rim="ground"):
+    """buildLens (src/owe/scene/builders.cpp:24-70): conic surfaces S1..Sn+1 along +z from z0, the
+    media between them, cylindrical rims between the surfaces' edges. Cemented surfaces are one
+    boundary between two glasses. surfaces: (R, semi_diameter)."""
+    n = len(media)
+    edge = max(sd for _, sd in surfaces)
+    regions = [sb.region(m) for m in media]
+    dielectric = sb.dielectric()
+    rim_optics = sb.absorber() if rim == "black" else sb.dielectric(0.35 if rim == "ground" else 0.0)
+    zv = [z0]
+    for t in thickness:
+        zv.append(zv[-1] + t)
+    z_edge = []
+    for i, (R, sd) in enumerate(surfaces):
+        c = 0.0 if math.isinf(R) else 1.0 / R
+        front = regions[i] if i < n else 0
+        back = regions[i - 1] if i > 0 else 0
+        sb.boundary(A.SHAPE_SAG, [c, 0.0, sd, 0.0], translate(0, 0, zv[i]), front, back, dielectric)
+        z_edge.append(zv[i] + sag_z(c, 0.0, sd))
+        if sd < edge:
+            sb.boundary(A.SHAPE_PLANE, [A.APERTURE_DISK, edge, sd], translate(0, 0, z_edge[i]), front, back, rim_optics)
+    for i in range(n):
+        assert z_edge[i + 1] > z_edge[i], "non-positive edge thickness"
+        sb.boundary(A.SHAPE_CYLINDER, [edge, z_edge[i], z_edge[i + 1]], pose(), 0, regions[i], rim_optics)
+    return regions, zv
+
+
+def achromat_scene(film=1024, half_size=2.5e-4, wavelength=587.5618):
+    """A cemented achromat: N-BK7 crown (R1 = 61.5 mm, R2 = -44.6 mm, 6 mm) and N-SF5 flint
+    (R3 = -129 mm, 2.5 mm), 25 mm diameter, with a point source 10 m in front on its axis and a
+    detector sheet at the paraxial focus (at `wavelength`). Returns (builder, walk description
+    fields: detector boundary, source position, focus z)."""
+    sb = SceneBuilder()
+    bk7 = sb.medium_sellmeier(*NBK7, rel_air=True)
+    sf5 = sb.medium_sellmeier(*SF5, rel_air=True)
+    radii = [0.0615, -0.0446, -0.129]
+    lens_body(sb, [(r, 0.0125) for r in radii], [bk7, sf5], [0.006, 0.0025])
+    na = ciddor_air(wavelength)
+    idx = [1.0, sellmeier_index(NBK7, wavelength) / na, sellmeier_index(SF5, wavelength) / na, 1.0]
+    back_focus = paraxial_image_distance(radii, [0.006, 0.0025], idx, 10.0)
+    z_focus = 0.0085 + back_focus
+    det = sb.optics_(A.SURF_DETECTOR)
+    target = sb.boundary(A.SHAPE_PLANE, [A.APERTURE_RECT, half_size, half_size], translate(0, 0, z_focus), 0, 0, det)
+    sb.observer(8, 8, (0, 0, -1.0), (0, 0, 0), fov_y_deg=5.0)  # a camera for the renderer's origin; walks bin on the sheet
+    return sb, {"target": target, "source": (0.0, 0.0, -10.0), "z_focus": z_focus, "half": half_size, "film": film}
+
+
+def achromat_walk(info, seed=0, mode=A.WALK_STOCHASTIC, splat=A.SPLAT_NEAREST, lambda_range=(380.0, 780.0),
+                  max_events=32):
+    """Walks from the point source into the cone that just covers the lens (13 mm at 10 m)."""
+    w = A.WalkDesc()
+    w.source_kind = A.SOURCE_POINT
+    w.mode = mode
+    w.max_events = max_events
+    w.splat = splat
+    w.position = (ctypes.c_double * 3)(*info["source"])
+    w.axis = (ctypes.c_double * 3)(0.0, 0.0, 1.0)
+    w.extent = math.atan(0.013 / 10.0)
+    w.lambda_min, w.lambda_max = lambda_range
+    w.region = 0
+    w.target = info["target"]
+    w.width = w.height = info["film"]
+    w.half_x = w.half_y = info["half"]
+    w.seed = seed
+    w.stream = 0
+    return w
+
+
+# ------------------------------------------------------------------ the differentiable caustic slab
+def heightfield_grid(nx, ny, half_x, half_y, base_z, heights):
+    """Vertices and triangles of an nx x ny heightfield over [-half_x, half_x] x [-half_y, half_y]:
+    vertex j * nx + i at (x_i, y_j, base_z + heights[j, i]); cell (i, j) is split into
+    (v00, v10, v11) and (v00, v11, v01), counter-clockwise seen from +z (front: +z)."""
+    h = np.asarray(heights, np.float64).reshape(ny, nx)
+    x = np.linspace(-half_x, half_x, nx)
+    y = np.linspace(-half_y, half_y, ny)
+    X, Y = np.meshgrid(x, y)
+    v = np.stack([X.ravel(), Y.ravel(), base_z + h.ravel()], 1)
+    i, j = np.meshgrid(np.arange(nx - 1), np.arange(ny - 1))
+    v00 = (j * nx + i).ravel()
+    v10, v01, v11 = v00 + 1, v00 + nx, v00 + nx + 1
+    tris = np.empty((2 * len(v00), 3), np.uint32)
+    tris[0::2] = np.stack([v00, v10, v11], 1)
+    tris[1::2] = np.stack([v00, v11, v01], 1)
+    return v, tris
+
+
+def slab_rest(nx, ny, half_x, half_y, top_z_edges):
+    """The bottom (z = 0) and the four sides of a slab whose top is a heightfield: the sides follow
+    the heightfield's edge vertices exactly (the same coordinates), so the body is closed and
+    watertight. top_z_edges(i, j) gives the top z at edge vertex (i, j). Faces point outward."""
+    x = np.linspace(-half_x, half_x, nx)
+    y = np.linspace(-half_y, half_y, ny)
+    verts, tris = [], []
+
+    def quad(a, b, c, d):  # counter-clockwise seen from outside
+        base = len(verts)
+        verts.extend([a, b, c, d])
+        tris.append((base, base + 1, base + 2))
+        tris.append((base, base + 2, base + 3))
+
+    # bottom as a grid with the same edge vertices (no T-junctions with the sides), facing -z
+    for j in range(ny - 1):
+        for i in range(nx - 1):
+            quad((x[i], y[j], 0.0), (x[i], y[j + 1], 0.0), (x[i + 1], y[j + 1], 0.0), (x[i + 1], y[j], 0.0))
+    for i in range(nx - 1):  # side y = -half (normal -y) and y = +half (normal +y)
+        quad((x[i], y[0], 0.0), (x[i + 1], y[0], 0.0), (x[i + 1], y[0], top_z_edges(i + 1, 0)), (x[i], y[0], top_z_edges(i, 0)))
+        quad((x[i + 1], y[-1], 0.0), (x[i], y[-1], 0.0), (x[i], y[-1], top_z_edges(i, ny - 1)),
+             (x[i + 1], y[-1], top_z_edges(i + 1, ny - 1)))
+    for j in range(ny - 1):  # side x = -half (normal -x) and x = +half (normal +x)
+        quad((x[0], y[j + 1], 0.0), (x[0], y[j], 0.0), (x[0], y[j], top_z_edges(0, j)), (x[0], y[j + 1], top_z_edges(0, j + 1)))
+        quad((x[-1], y[j], 0.0), (x[-1], y[j + 1], 0.0), (x[-1], y[j + 1], top_z_edges(nx - 1, j + 1)),
+             (x[-1], y[j], top_z_edges(nx - 1, j)))
+    return np.array(verts), np.array(tris, np.uint32)
+
+
+def caustic_slab_scene(n=256, heights=None, wall_bins=512, wall_half=0.075, size=0.1, thickness=0.01,
+                       wall_distance=1.0):
+    """A PMMA slab (size x size x thickness) whose exit face (+z) is an n x n heightfield, lit by a
+    collimated beam along +z; a Lambertian wall `wall_distance` behind the exit face records the
+    irradiance in wall_bins^2 bins. The heightfield is boundary `info['heightfield']`, a mesh whose
+    vertex j * n + i has height heights[j, i] over z = thickness."""
+    sb = SceneBuilder()
+    pmma = sb.medium_sellmeier(*PMMA, rel_air=False)
+    h = np.zeros((n, n)) if heights is None else np.asarray(heights, np.float64).reshape(n, n)
+    half = size / 2
+    inside = sb.region(pmma)
+    top_v, top_t = heightfield_grid(n, n, half, half, thickness, h)
+    glass = sb.dielectric()
+    m_top = sb.mesh(top_v, top_t)
+    hf = sb.boundary(A.SHAPE_MESH, [], pose(), 0, inside, glass, -1, m_top)
+    rest_v, rest_t = slab_rest(n, n, half, half, lambda i, j: thickness + h[j, i])
+    m_rest = sb.mesh(rest_v, rest_t)
+    sb.boundary(A.SHAPE_MESH, [], pose(), 0, inside, glass, -1, m_rest)
+    wall_z = thickness + wall_distance
+    wall = sb.boundary(A.SHAPE_PLANE, [A.APERTURE_RECT, 0.5, 0.5], pose(rotate_to((0, 0, 1), (0, 0, -1)), (0, 0, wall_z)),
+                       0, 0, sb.diffuse(0.8))
+    sb.observer(8, 8, (0.0, 0.0, -1.0), (0, 0, 0), fov_y_deg=10.0)
+    info = {"heightfield": hf, "wall": wall, "n": n, "half": half, "thickness": thickness, "wall_half": wall_half,
+            "bins": wall_bins, "wall_z": wall_z}
+    return sb, info
+
+
+def caustic_walk(info, seed=0, splat=A.SPLAT_BILINEAR, wavelength=550.0):
+    """The collimated sun beam over the slab's entry face, primary transmission (deterministic
+    Fresnel weights), binned on the wall."""
+    w = A.WalkDesc()
+    w.source_kind = A.SOURCE_COLLIMATED_SQUARE
+    w.mode = A.WALK_PRIMARY_TRANSMISSION
+    w.max_events = 32
+    w.splat = splat
+    w.position = (ctypes.c_double * 3)(0.0, 0.0, -0.05)
+    w.axis = (ctypes.c_double * 3)(0.0, 0.0, 1.0)
+    w.extent = info["half"] * 0.999
+    w.lambda_min = w.lambda_max = wavelength
+    w.region = 0
+    w.target = info["wall"]
+    w.width = w.height = info["bins"]
+    w.half_x = w.half_y = info["wall_half"]
+    w.seed = seed
+    w.stream = 0
+    return w
+
+
+def gaussian_blobs(bins, count=64, seed=0, sigma_range=(5.0, 20.0)):
+    """A seeded target image: `count` Gaussian blobs of sigma in sigma_range bins, normalised to
+    unit mean."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    yy, xx = np.mgrid[0:bins, 0:bins] + 0.5
+    img = np.zeros((bins, bins))
+    for _ in range(count):
+        cx, cy = rng.uniform(0.15 * bins, 0.85 * bins, 2)
+        s = rng.uniform(*sigma_range)
+        img += rng.uniform(0.5, 1.0) * np.exp(-((xx - cx) ** 2 + (yy - cy) ** 2) / (2 * s * s))
+    return img / img.mean()

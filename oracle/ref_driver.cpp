@@ -9,6 +9,7 @@
 //     mode the reference lacks (the pattern of tests/test_transport.cpp:185-186);
 //   - oweref_render_backend: the same through the reference's own `cpu` Backend, unchanged;
 //   - oweref_cast_rays: World::intersect (src/owe/scene/world.cpp:553-582) for hit-ID parity.
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -367,6 +368,87 @@ int oweref_cast_rays(void* scene, uint64_t n, const double* o, const double* d, 
                 }
             }
         });
+    });
+}
+
+// Forward light walks through Tracer::walk (src/owe/transport/transport.cpp:531-595), emitted and
+// binned as owec_walk describes (include/owec.h): walk i draws from the stream
+// (hashCombine(seed, first + i), stream): its wavelength, its emission (Draw2), then the walk's own
+// draws. bins (width * height) receive the sum of the binned walks' throughput times their splat
+// weights; stats: [walks, binned, escaped, events].
+int oweref_walk(void* scene, const owec_walk_desc* w, uint64_t first, uint64_t n, int threads, double* bins,
+                uint64_t* stats) {
+    return guarded([&] {
+        const RefScene& rs = *static_cast<const RefScene*>(scene);
+        const World& world = rs.scene.world;
+        Tracer tracer(rs.scene, 64, 6);
+        const Vec3 axis = normalize(Vec3(w->axis[0], w->axis[1], w->axis[2]));
+        Vec3 S, T;
+        orthonormalBasis(axis, S, T);
+        const double cosMax = std::cos(w->extent);
+        const Boundary& target = world.boundaries().at(w->target);
+        const WalkMode mode = w->mode == OWEC_WALK_PRIMARY_TRANSMISSION ? WalkMode::PrimaryTransmission : WalkMode::Stochastic;
+        const int nt = threads > 0 ? threads : int(hardwareThreads());
+        const size_t nb = size_t(w->width) * w->height;
+        std::vector<std::vector<double>> part(size_t(nt), std::vector<double>(nb, 0.0));
+        std::vector<std::array<uint64_t, 4>> st(size_t(nt), {0, 0, 0, 0});
+        parallelParts(size_t(n), size_t(nt), [&](size_t t, size_t b, size_t e) {
+            for (size_t k = b; k < e; ++k) {
+                Rng rng(hashCombine(w->seed, first + k), w->stream);
+                const double lambda = w->lambda_min + (w->lambda_max - w->lambda_min) * rng.uniform();
+                const Draw2 u(rng);
+                Vec3 o(w->position[0], w->position[1], w->position[2]), d;
+                if (w->source_kind == OWEC_SOURCE_POINT) {
+                    const double cosT = (1 - u.u1) + u.u1 * cosMax, sinT = safeSqrt(1 - cosT * cosT), phi = 2 * Pi * u.u2;
+                    d = S * (std::cos(phi) * sinT) + T * (std::sin(phi) * sinT) + axis * cosT;
+                } else if (w->source_kind == OWEC_SOURCE_COLLIMATED) {
+                    const Vec2 q = sampleUniformDiskConcentric(u.u1, u.u2);
+                    o = o + (S * q.x + T * q.y) * w->extent;
+                    d = axis;
+                } else {
+                    o = o + (S * (2 * u.u1 - 1) + T * (2 * u.u2 - 1)) * w->extent;
+                    d = axis;
+                }
+                const PathRecord rec = tracer.walk(Ray{o, d}, rs.regionMap.at(w->region), lambda, mode, rng, w->max_events);
+                st[t][0]++;
+                st[t][3] += rec.v.size() - 1;
+                const PathVertex& last = rec.v.back();
+                if (last.event == EventKind::Escape) { st[t][2]++; continue; }
+                if (last.boundary != w->target) continue;
+                if (last.event != EventKind::Detect && last.event != EventKind::Diffuse && last.event != EventKind::Absorb)
+                    continue;
+                const Vec3 pl = target.toLocal.point(last.p);
+                const double fx = (pl.x / w->half_x + 1) * 0.5 * w->width, fy = (1 - pl.y / w->half_y) * 0.5 * w->height;
+                bool any = false;
+                if (w->splat == OWEC_SPLAT_NEAREST) {
+                    if (fx >= 0 && fy >= 0 && fx < w->width && fy < w->height) {
+                        part[t][size_t(int(fy)) * w->width + size_t(int(fx))] += last.beta;
+                        any = true;
+                    }
+                } else {
+                    const double gx = fx - 0.5, gy = fy - 0.5;
+                    const int x0 = int(std::floor(gx)), y0 = int(std::floor(gy));
+                    const double ax = gx - x0, ay = gy - y0;
+                    for (int j = 0; j < 2; ++j)
+                        for (int i = 0; i < 2; ++i) {
+                            const int xi = x0 + i, yj = y0 + j;
+                            if (xi < 0 || yj < 0 || xi >= w->width || yj >= w->height) continue;
+                            part[t][size_t(yj) * w->width + size_t(xi)] += last.beta * (i ? ax : 1 - ax) * (j ? ay : 1 - ay);
+                            any = true;
+                        }
+                }
+                if (any) st[t][1]++;
+            }
+        });
+        for (size_t i = 0; i < nb; ++i) {
+            double acc = 0;
+            for (int t = 0; t < nt; ++t) acc += part[size_t(t)][i];
+            bins[i] += acc;
+        }
+        for (int k = 0; k < 4; ++k) {
+            stats[k] = 0;
+            for (int t = 0; t < nt; ++t) stats[k] += st[size_t(t)][size_t(k)];
+        }
     });
 }
 

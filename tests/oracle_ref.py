@@ -39,6 +39,8 @@ def ref_lib():
         lib.oweref_scene_info.argtypes = [P, A.c_double_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int), A.c_double_p,
                                           A.c_u32_p]
         lib.oweref_medium_index.argtypes = [P, ctypes.c_uint32, ctypes.c_double, A.c_double_p]
+        lib.oweref_walk.argtypes = [P, ctypes.POINTER(A.WalkDesc), ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int,
+                                    A.c_double_p, ctypes.POINTER(ctypes.c_uint64)]
         _ref = lib
     return _ref
 
@@ -98,6 +100,26 @@ class ReferenceEngine:
         if r != 0:
             raise RuntimeError(self.lib.oweref_last_error().decode())
         return b, p, t
+
+    def walk(self, desc, first, n, threads=0):
+        """Tracer::walk for n walks, binned as owec_walk bins them; returns (bins normalised like
+        owec_walk_resolve, stats)."""
+        nb = desc.width * desc.height
+        bins = np.zeros(nb)
+        st = (ctypes.c_uint64 * 4)()
+        r = self.lib.oweref_walk(self.h, ctypes.byref(desc), first, n, threads, bins.ctypes.data_as(A.c_double_p), st)
+        if r != 0:
+            raise RuntimeError(self.lib.oweref_last_error().decode())
+        if desc.source_kind == A.SOURCE_POINT:
+            measure = 2 * np.pi * (1 - np.cos(desc.extent))
+        elif desc.source_kind == A.SOURCE_COLLIMATED:
+            measure = np.pi * desc.extent ** 2
+        else:
+            measure = 4 * desc.extent ** 2
+        bin_area = (2 * desc.half_x / desc.width) * (2 * desc.half_y / desc.height)
+        bins *= measure / (n * bin_area)
+        return bins.reshape(desc.height, desc.width), {"walks": st[0], "binned": st[1], "escaped": st[2],
+                                                       "events": st[3]}
 
     def info(self):
         pdfs = np.zeros(64)
