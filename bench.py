@@ -312,11 +312,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--width", type=int, default=WIDTH, help="film width (a smaller case for profiling)")
-    ap.add_argument("--height", type=int, default=HEIGHT)
+    ap.add_argument("--width", type=int, default=1920, help="film width (a smaller case for profiling)")
+    ap.add_argument("--height", type=int, default=1080)
     args = ap.parse_args()
-    global WIDTH, HEIGHT
-    WIDTH, HEIGHT = args.width, args.height
+    globals()["WIDTH"], globals()["HEIGHT"] = args.width, args.height
     if args.impl == "reference":
         return run_reference(args)
     return run_cuda(args)

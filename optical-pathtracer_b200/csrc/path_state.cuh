@@ -47,10 +47,11 @@ struct alignas(16) PathAux {
     uint32_t stream;    // PCG32 stream (the pass index of this sample)
     uint32_t pixel;
     uint32_t depth;     // bounce count (the reference's loop variable)
-    uint32_t flags;     // kFlagSpecular | kFlagAlive | kFlagHasPrev
+    uint32_t flags;     // kFlagSpecular | kFlagAlive
     float prevPdf;
     float weight;       // detector importance / pdf
-    float prevP[3];     // last scattering vertex (camera-relative), for emission MIS
+    double prevP[3];    // last scattering vertex (camera-relative FP64: emission MIS decides inside or
+                        // outside an emitting sphere from it, which FP32 rounding can flip)
     uint32_t lastBoundary;
 };
 constexpr uint32_t kFlagSpecular = 1u, kFlagAlive = 2u;

@@ -146,9 +146,9 @@ __global__ void __launch_bounds__(256) kGenerate(DeviceScene sc, PassParams pp, 
         ray.d[1] = R(dir.y);
         ray.d[2] = R(dir.z);
         aux.flags = kFlagSpecular | kFlagAlive;
-        aux.prevP[0] = float(o.x);
-        aux.prevP[1] = float(o.y);
-        aux.prevP[2] = float(o.z);
+        aux.prevP[0] = o.x;
+        aux.prevP[1] = o.y;
+        aux.prevP[2] = o.z;
     }
     aux.rngState = rng.state;
     pb.ray[i] = ray;
@@ -198,7 +198,8 @@ __global__ void __launch_bounds__(128) kIntersect(DeviceScene sc, PathBuffers<RT
 // interface given) or a medium point (phase g), and queues it with its contribution.
 template <int M>
 __device__ void queueNee(const DeviceScene& sc, PathBuffers<RT<M>>& pb, Queues& q, uint32_t pathIdx,
-                         const PathSpec<RT<M>>& sp, const LightSampleD& ls, const RT<M> f[NW], RT<M> pdfScatter,
+                         const PathSpec<RT<M>>& sp, const RT<M> beta[NW], const LightSampleD& ls, const RT<M> f[NW],
+                         RT<M> pdfScatter,
                          RT<M> cosFactor, const V3<double>& p, uint32_t startRegion, uint32_t depB, uint32_t depP,
                          float errN, bool valid) {
     using R = RT<M>;
@@ -210,7 +211,7 @@ __device__ void queueNee(const DeviceScene& sc, PathBuffers<RT<M>>& pb, Queues& 
         for (int k = 0; k < NW; ++k) {
             if (sp.pdf[k] == 0.f && k > 0) continue;
             const R Le = lightSampleLe<R>(sc, ls, R(sp.lambda[k]));
-            const R c = sp.beta[k] * f[k] * Le * (cosFactor * w / R(ls.pdf));
+            const R c = beta[k] * f[k] * Le * (cosFactor * w / R(ls.pdf));
             contrib[k] = float(c);
             any = any || (c != R(0));
         }
@@ -263,6 +264,7 @@ __global__ void __launch_bounds__(128) kMedium(DeviceScene sc, PassParams pp, Pa
         bool neeValid = false;
         LightSampleD ls;
         R fN[NW] = {R(0), R(0), R(0), R(0)};
+        R betaNee[NW] = {R(0), R(0), R(0), R(0)};
         R pdfS = R(0);
         V3<double> sp3;
         if (!fault) {
@@ -296,6 +298,7 @@ __global__ void __launch_bounds__(128) kMedium(DeviceScene sc, PassParams pp, Pa
                 // scatterInMedium (transport.cpp:379-397)
                 sp3 = rayOrigin(ray.o) + V3<double>(d) * tS;
                 if (int(aux.depth) < pp.maxDepth) {
+                    for (int j = 0; j < NW; ++j) betaNee[j] = sp.beta[j];  // directLighting sees beta before RR
                     int li;
                     if (sampleLight<R>(sc, sp3, rng, ls, li)) {
                         bool leZero = true;
@@ -312,9 +315,9 @@ __global__ void __launch_bounds__(128) kMedium(DeviceScene sc, PassParams pp, Pa
                     V3<R> wi;
                     aux.prevPdf = float(sampleHg(-d, R(med.g), u.u1, u.u2, wi));
                     aux.flags &= ~kFlagSpecular;
-                    aux.prevP[0] = float(sp3.x);
-                    aux.prevP[1] = float(sp3.y);
-                    aux.prevP[2] = float(sp3.z);
+                    aux.prevP[0] = sp3.x;
+                    aux.prevP[1] = sp3.y;
+                    aux.prevP[2] = sp3.z;
                     setOrigin<M>(ray.o, sp3);
                     ray.d[0] = wi.x;
                     ray.d[1] = wi.y;
@@ -351,7 +354,7 @@ __global__ void __launch_bounds__(128) kMedium(DeviceScene sc, PassParams pp, Pa
         pb.ray[i] = ray;
         pb.spec[i] = sp;
         pb.aux[i] = aux;
-        queueNee<M>(sc, pb, q, i, sp, ls, fN, pdfS, R(1), sp3, ray.region, kNone, kNone, 0.f, neeValid);
+        queueNee<M>(sc, pb, q, i, sp, betaNee, ls, fN, pdfS, R(1), sp3, ray.region, kNone, kNone, 0.f, neeValid);
         warpCount(&st->leaks, leak);
         warpPush(q.surface, &q.counts[2], toSurface, i);
         warpPush(q.active[nxt], &q.counts[nxt], cont, i);
@@ -418,6 +421,7 @@ __global__ void __launch_bounds__(128) kSurface(DeviceScene sc, PassParams pp, P
         bool cont = false, neeValid = false;
         LightSampleD ls;
         R fN[NW] = {R(0), R(0), R(0), R(0)};
+        R betaNee[NW] = {R(0), R(0), R(0), R(0)};
         R pdfS = R(0), cosF = R(0);
         uint32_t neeRegion = ray.region;
         if (o.type == OWEC_SURF_NULL) {
@@ -447,6 +451,7 @@ __global__ void __launch_bounds__(128) kSurface(DeviceScene sc, PassParams pp, P
                     }
                 }
             }
+            for (int j = 0; j < NW; ++j) betaNee[j] = sp.beta[j];  // directLighting sees beta before the scatter
             if (!isDeltaOptics<R>(o)) {
                 int li;
                 if (sampleLight<R>(sc, g.p, rng, ls, li)) {
@@ -487,9 +492,9 @@ __global__ void __launch_bounds__(128) kSurface(DeviceScene sc, PassParams pp, P
                 if (s.transmitted) ray.region = other;
                 aux.flags = s.delta ? (aux.flags | kFlagSpecular) : (aux.flags & ~kFlagSpecular);
                 aux.prevPdf = float(s.pdf);
-                aux.prevP[0] = float(g.p.x);
-                aux.prevP[1] = float(g.p.y);
-                aux.prevP[2] = float(g.p.z);
+                aux.prevP[0] = g.p.x;
+                aux.prevP[1] = g.p.y;
+                aux.prevP[2] = g.p.z;
                 setOrigin<M>(ray.o, g.p);
                 ray.d[0] = s.wi.x;
                 ray.d[1] = s.wi.y;
@@ -506,7 +511,7 @@ __global__ void __launch_bounds__(128) kSurface(DeviceScene sc, PassParams pp, P
         pb.ray[i] = ray;
         pb.spec[i] = sp;
         pb.aux[i] = aux;
-        queueNee<M>(sc, pb, q, i, sp, ls, fN, pdfS, cosF, g.p, neeRegion, h.boundary, h.prim, errN, neeValid);
+        queueNee<M>(sc, pb, q, i, sp, betaNee, ls, fN, pdfS, cosF, g.p, neeRegion, h.boundary, h.prim, errN, neeValid);
         warpCount(&st->inconsistencies, inconsistent);
         warpPush(q.active[nxt], &q.counts[nxt], cont, i);
     }

@@ -52,7 +52,7 @@ def test_adjoint_gradient_matches_fp64_central_differences():
         grad = c.walk_adjoint(w, 0, WALKS, g).reshape(N, N)
     # the forward agrees with the reference's walks
     _, ref_bins = _ref_loss(h, 7, target)
-    assert np.abs(bins - ref_bins).sum() <= 1e-3 * ref_bins.sum()
+    assert np.abs(bins - ref_bins).sum() <= 1e-2 * ref_bins.sum()
     # central differences on 32 interior vertices with a clear gradient
     rng = np.random.default_rng(11)
     interior = [(j, i) for j in range(2, N - 2) for i in range(2, N - 2)]
