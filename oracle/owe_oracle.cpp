@@ -17,6 +17,8 @@
 //   Tracer::radiance and helpers      src/owe/transport/transport.cpp:72-529
 //   detectors, the pass loop          src/owe/scene/detector.cpp:61-148, backends/cpu/cpu_backend.cpp:52-94
 //
+//   Tracer::walk                      src/owe/transport/transport.cpp:531-595
+//
 // Shapes the scene description does not carry (waves, lathe patches, domes, walls, aspheres) and
 // environment maps, textures and aim guides are not restated; the double-double near-sphere solve
 // of world.cpp:384-438 (planet-sized spheres) is not either.
@@ -968,30 +970,187 @@ struct Iface {
     const owec_optics* o;
     V n, p;
     double nFront = 1, nBack = 1, lambda = 550, floorP = 0, albedo = 1;
+    double condN = 0, condK = 0;  // conductor n, k at lambda
 };
 struct Sample {
     V wi;
     double weight = 0, pdf = 0;
     bool delta = false, transmitted = false;
+    double R = 0, T = 0;
 };
 bool isDelta(const owec_optics& o) {
     if (o.type == OWEC_SURF_DIELECTRIC || o.type == OWEC_SURF_CONDUCTOR) return o.roughness < 1e-3;
     return o.type == OWEC_SURF_MIRROR;
 }
-// The smooth dielectric, Lambertian and mirror branches of sampleScatter (scattering.cpp:65-145).
-// Rough lobes and conductors are parity-checked against the reference engine directly.
+
+// complex arithmetic as (re, im) pairs
+struct Cx { double re, im; };
+Cx cmul(Cx a, Cx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+Cx cdiv(Cx a, Cx b) { const double d = b.re * b.re + b.im * b.im; return {(a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d}; }
+Cx csqrt(Cx z) {
+    const double r = std::sqrt(z.re * z.re + z.im * z.im);
+    return {std::sqrt(std::max(0.0, (r + z.re) / 2)), std::copysign(std::sqrt(std::max(0.0, (r - z.re) / 2)), z.im)};
+}
+// Reflectance of a conductor of complex relative index eta (optics.hpp:69-79).
+double fresnelConductor(double c, Cx eta) {
+    c = clampd(c, 0, 1);
+    const Cx s2 = cdiv({1 - c * c, 0}, cmul(eta, eta));
+    const Cx ct = csqrt({1 - s2.re, -s2.im});
+    const Cx ec{eta.re * c, eta.im * c}, ect = cmul(eta, ct);
+    const Cx rp = cdiv({ec.re - ct.re, ec.im - ct.im}, {ec.re + ct.re, ec.im + ct.im});
+    const Cx rs = cdiv({c - ect.re, -ect.im}, {c + ect.re, ect.im});
+    return (rp.re * rp.re + rp.im * rp.im + rs.re * rs.re + rs.im * rs.im) / 2;
+}
+
+// GGX (Trowbridge-Reitz) with visible-normal sampling (optics.hpp:104-246).
+double ggxAlpha(double r) { return std::max(r, 1e-4); }
+double ggxD(double a, V m) {
+    const double c2 = m.z * m.z;
+    if (c2 <= 0) return 0;
+    const double c4 = c2 * c2;
+    if (c4 < 1e-16) return 0;
+    const double e = (1 - c2) / c2 / (a * a);
+    return 1 / (Pi * a * a * c4 * sq(1 + e));
+}
+double ggxLambda(double a, V w) {
+    const double c2 = w.z * w.z;
+    if (c2 <= 0) return 0;
+    return (std::sqrt(1 + a * a * ((1 - c2) / c2)) - 1) / 2;
+}
+double ggxG1(double a, V w) { return 1 / (1 + ggxLambda(a, w)); }
+double ggxG(double a, V wo, V wi) { return 1 / (1 + ggxLambda(a, wo) + ggxLambda(a, wi)); }
+double ggxPdf(double a, V w, V m) { return w.z == 0 ? 0 : ggxG1(a, w) / std::fabs(w.z) * ggxD(a, m) * std::fabs(dot(w, m)); }
+V ggxSampleWm(double a, V w, double u1, double u2) {
+    V wh = unit(V(a * w.x, a * w.y, w.z));
+    if (wh.z < 0) wh = -wh;
+    const V T1 = wh.z < 0.99999 ? unit(cross(V(0, 0, 1), wh)) : V(1, 0, 0);
+    const V T2 = cross(wh, T1);
+    const double r = std::sqrt(u1), phi = 2 * Pi * u2;
+    const double px = r * std::cos(phi);
+    double py = r * std::sin(phi);
+    const double h = std::sqrt(std::max(0.0, 1 - px * px)), s = (1 + wh.z) / 2;
+    py = (1 - s) * h + s * py;
+    const double pz = safeSqrt(1 - px * px - py * py);
+    const V nh = T1 * px + T2 * py + wh * pz;
+    return unit(V(a * nh.x, a * nh.y, std::max(1e-6, nh.z)));
+}
+bool sameHemi(V a, V b) { return a.z * b.z > 0; }
+bool refractLocal(V wi, V n, double eta, double& etap, V& wt) {
+    double cosI = dot(n, wi);
+    etap = 1;
+    wt = wi;
+    if (cosI < 0) { eta = 1 / eta; cosI = -cosI; n = -n; }
+    const double s2 = std::max(0.0, 1 - cosI * cosI) / (eta * eta);
+    if (s2 >= 1) return false;
+    const double cosT = safeSqrt(1 - s2);
+    wt = -wi / eta + n * (cosI / eta - cosT);
+    etap = eta;
+    return true;
+}
+struct Lobe { V wi; double weight = 0, pdf = 0; bool transmitted = false; double R = 0, T = 0; };
+bool sampleRoughDielectric(double a, V wo, double eta, double uc, double u1, double u2, bool radiance, Lobe& s) {
+    const V wm = ggxSampleWm(a, wo, u1, u2);
+    const double R = fresnelDielectric(dot(wo, wm), eta), T = 1 - R;
+    s = Lobe{};
+    s.wi = wo;
+    s.R = R;
+    s.T = T;
+    if (uc < R / (R + T)) {
+        s.wi = reflectV(-wo, wm);
+        if (!sameHemi(wo, s.wi)) return false;
+        s.pdf = ggxPdf(a, wo, wm) / (4 * std::fabs(dot(wo, wm))) * R / (R + T);
+        const double f = ggxD(a, wm) * ggxG(a, wo, s.wi) * R / (4 * std::fabs(s.wi.z) * std::fabs(wo.z));
+        s.weight = f * std::fabs(s.wi.z) / s.pdf;
+    } else {
+        double etap;
+        V wi;
+        if (!refractLocal(wo, wm, eta, etap, wi)) return false;
+        if (sameHemi(wo, wi) || wi.z == 0) return false;
+        s.wi = wi;
+        s.transmitted = true;
+        const double den = sq(dot(wi, wm) + dot(wo, wm) / etap);
+        s.pdf = ggxPdf(a, wo, wm) * (std::fabs(dot(wi, wm)) / den) * T / (R + T);
+        double ft = T * ggxD(a, wm) * ggxG(a, wo, wi) * std::fabs(dot(wi, wm) * dot(wo, wm) / (wi.z * wo.z * den));
+        if (radiance) ft /= sq(etap);
+        s.weight = ft * std::fabs(wi.z) / s.pdf;
+    }
+    return std::isfinite(s.weight) && s.pdf > 0;
+}
+double evalRoughDielectric(double a, V wo, V wi, double eta, bool radiance, double& pdf) {
+    pdf = 0;
+    const double co = wo.z, ci = wi.z;
+    if (co == 0 || ci == 0) return 0;
+    const bool refl = co * ci > 0;
+    double etap = 1;
+    if (!refl) etap = co > 0 ? eta : 1 / eta;
+    V wm = wi * etap + wo;
+    if (dot(wm, wm) == 0) return 0;
+    wm = unit(wm);
+    if (wm.z < 0) wm = -wm;
+    if (dot(wm, wi) * ci < 0 || dot(wm, wo) * co < 0) return 0;
+    const double R = fresnelDielectric(dot(wo, wm), eta), T = 1 - R;
+    if (refl) {
+        pdf = ggxPdf(a, wo, wm) / (4 * std::fabs(dot(wo, wm))) * R / (R + T);
+        return ggxD(a, wm) * ggxG(a, wo, wi) * R / std::fabs(4 * ci * co);
+    }
+    const double den = sq(dot(wi, wm) + dot(wo, wm) / etap);
+    pdf = ggxPdf(a, wo, wm) * std::fabs(dot(wi, wm)) / den * T / (R + T);
+    double ft = ggxD(a, wm) * T * ggxG(a, wo, wi) * std::fabs(dot(wi, wm) * dot(wo, wm) / (den * ci * co));
+    if (radiance) ft /= sq(etap);
+    return ft;
+}
+bool sampleRoughConductor(double a, V w, Cx eta, double tint, double u1, double u2, Lobe& s) {
+    const V wm = ggxSampleWm(a, w, u1, u2);
+    s = Lobe{};
+    s.wi = reflectV(-w, wm);
+    s.R = fresnelConductor(std::fabs(dot(w, wm)), eta) * tint;
+    if (s.wi.z <= 0) return false;
+    s.pdf = ggxPdf(a, w, wm) / (4 * std::fabs(dot(w, wm)));
+    if (!(s.pdf > 0)) return false;
+    const double f = ggxD(a, wm) * s.R * ggxG(a, w, s.wi) / (4 * s.wi.z * w.z);
+    s.weight = f * s.wi.z / s.pdf;
+    return std::isfinite(s.weight);
+}
+double evalRoughConductor(double a, V wo, V wi, Cx eta, double tint, double& pdf) {
+    pdf = 0;
+    V wm = wo + wi;
+    if (dot(wm, wm) == 0) return 0;
+    wm = unit(wm);
+    const double F = fresnelConductor(std::fabs(dot(wo, wm)), eta) * tint;
+    pdf = ggxPdf(a, wo, wm) / (4 * std::fabs(dot(wo, wm)));
+    return ggxD(a, wm) * F * ggxG(a, wo, wi) / (4 * wi.z * wo.z);
+}
+Cx conductorEta(const Iface& it, double nMed) { return {it.condN / nMed, it.condK / nMed}; }
+
+// sampleScatter (scattering.cpp:65-145)
 bool sampleScatter(const Iface& it, V d, double uc, double u1, double u2, bool radiance, Sample& s) {
     const Frame fr(it.n);
     const V wo = fr.toLocal(-d);
     const bool fromFront = wo.z > 0;
     s = Sample{};
-    switch (it.o->type) {
+    const owec_optics& o = *it.o;
+    auto fromLobe = [&](const Lobe& l) {
+        s.wi = fr.toWorld(l.wi);
+        s.weight = l.weight;
+        s.pdf = l.pdf;
+        s.transmitted = l.transmitted;
+        s.R = l.R;
+        s.T = l.T;
+    };
+    switch (o.type) {
         case OWEC_SURF_DIELECTRIC: {
-            if (it.o->roughness >= 1e-3) throw std::runtime_error("rough dielectrics are not restated");
             const double eta = it.nBack / it.nFront;
+            if (o.roughness >= 1e-3 && eta != 1) {
+                Lobe l;
+                if (!sampleRoughDielectric(ggxAlpha(o.roughness), wo, eta, uc, u1, u2, radiance, l)) return false;
+                fromLobe(l);
+                return true;
+            }
             const double ni = fromFront ? it.nFront : it.nBack, nt = fromFront ? it.nBack : it.nFront;
             const double R = fresnelDielectric(wo.z, eta);
             const double pR = it.floorP > 0 && R < 1 ? clampd(R, it.floorP, 1 - it.floorP) : R;
+            s.R = R;
+            s.T = 1 - R;
             s.delta = true;
             if (uc < pR) {
                 s.wi = fr.toWorld(V(-wo.x, -wo.y, wo.z));
@@ -1004,7 +1163,7 @@ bool sampleScatter(const Iface& it, V d, double uc, double u1, double u2, bool r
             return true;
         }
         case OWEC_SURF_DIFFUSE: {
-            if (!fromFront && it.o->back_absorbs) return false;
+            if (!fromFront && o.back_absorbs) return false;
             if (it.albedo <= 0) return false;
             const double a = 2 * u1 - 1, b = 2 * u2 - 1;
             double dx = 0, dy = 0;
@@ -1020,28 +1179,61 @@ bool sampleScatter(const Iface& it, V d, double uc, double u1, double u2, bool r
             s.wi = fr.toWorld(w);
             s.pdf = std::fabs(w.z) * InvPi;
             s.weight = it.albedo;
+            s.R = it.albedo;
             return s.pdf > 0;
         }
         case OWEC_SURF_MIRROR:
-            if (!fromFront && it.o->back_absorbs) return false;
+            if (!fromFront && o.back_absorbs) return false;
             s.wi = fr.toWorld(V(-wo.x, -wo.y, wo.z));
             s.weight = it.albedo;
             s.delta = true;
+            s.R = s.weight;
             return s.weight > 0;
-        case OWEC_SURF_CONDUCTOR: throw std::runtime_error("conductors are not restated");
+        case OWEC_SURF_CONDUCTOR: {
+            if (!fromFront && o.back_absorbs) return false;
+            const Cx eta = conductorEta(it, fromFront ? it.nFront : it.nBack);
+            const V w = fromFront ? wo : V(wo.x, wo.y, -wo.z);
+            if (o.roughness < 1e-3) {
+                s.wi = fr.toWorld(V(-wo.x, -wo.y, wo.z));
+                s.weight = fresnelConductor(w.z, eta) * it.albedo;
+                s.delta = true;
+                s.R = s.weight;
+                return s.weight > 0;
+            }
+            Lobe l;
+            if (!sampleRoughConductor(ggxAlpha(o.roughness), w, eta, it.albedo, u1, u2, l)) return false;
+            if (!fromFront) l.wi.z = -l.wi.z;
+            fromLobe(l);
+            return true;
+        }
         default: return false;
     }
 }
-double evalScatter(const Iface& it, V d, V wiW, double& pdf) {
+// evalScatter (scattering.cpp:147-172)
+double evalScatter(const Iface& it, V d, V wiW, double& pdf, bool radiance = true) {
     pdf = 0;
-    if (isDelta(*it.o)) return 0;
+    const owec_optics& o = *it.o;
+    if (isDelta(o)) return 0;
     const Frame fr(it.n);
-    const V wo = fr.toLocal(-d), wi = fr.toLocal(wiW);
-    if (it.o->type != OWEC_SURF_DIFFUSE) throw std::runtime_error("only Lambertian lobes are restated for evaluation");
-    if (!(wo.z > 0) && it.o->back_absorbs) return 0;
-    if (!(wo.z * wi.z > 0)) return 0;
-    pdf = std::fabs(wi.z) * InvPi;
-    return it.albedo * InvPi;
+    V wo = fr.toLocal(-d), wi = fr.toLocal(wiW);
+    const bool fromFront = wo.z > 0;
+    switch (o.type) {
+        case OWEC_SURF_DIFFUSE:
+            if (!fromFront && o.back_absorbs) return 0;
+            if (!sameHemi(wo, wi)) return 0;
+            pdf = std::fabs(wi.z) * InvPi;
+            return it.albedo * InvPi;
+        case OWEC_SURF_CONDUCTOR: {
+            if (!fromFront && o.back_absorbs) return 0;
+            if (!sameHemi(wo, wi)) return 0;
+            if (!fromFront) { wo.z = -wo.z; wi.z = -wi.z; }
+            return evalRoughConductor(ggxAlpha(o.roughness), wo, wi, conductorEta(it, fromFront ? it.nFront : it.nBack),
+                                      it.albedo, pdf);
+        }
+        case OWEC_SURF_DIELECTRIC:
+            return evalRoughDielectric(ggxAlpha(o.roughness), wo, wi, it.nBack / it.nFront, radiance, pdf);
+        default: return 0;
+    }
 }
 
 // ------------------------------------------------------------------ the tracer (transport.cpp)
@@ -1080,6 +1272,8 @@ struct Tracer {
         it.lambda = lambda;
         it.floorP = floorP;
         it.albedo = it.o->reflectance >= 0 ? w.specEval(it.o->reflectance, lambda) : 1.0;
+        it.condN = w.specEval(it.o->conductor_n, lambda);
+        it.condK = w.specEval(it.o->conductor_k, lambda);
         return it;
     }
     Iface atWavelength(const Iface& base, const Hit& h, double lambda) const {
@@ -1089,6 +1283,8 @@ struct Tracer {
         it.nBack = w.indexOf(b.back, lambda);
         it.lambda = lambda;
         it.albedo = it.o->reflectance >= 0 ? w.specEval(it.o->reflectance, lambda) : 1.0;
+        it.condN = w.specEval(it.o->conductor_n, lambda);
+        it.condK = w.specEval(it.o->conductor_k, lambda);
         return it;
     }
     double secondaryWeight(const Iface& it, V d, const Sample& s) const {
@@ -1099,6 +1295,10 @@ struct Tracer {
         }
         if (it.o->type == OWEC_SURF_DIELECTRIC) return s.weight;
         if (it.o->type == OWEC_SURF_MIRROR) return it.albedo;
+        if (it.o->type == OWEC_SURF_CONDUCTOR) {
+            const bool fromFront = dot(d, it.n) < 0;
+            return fresnelConductor(std::fabs(dot(d, it.n)), conductorEta(it, fromFront ? it.nFront : it.nBack)) * it.albedo;
+        }
         return 0;
     }
 
@@ -1306,6 +1506,62 @@ struct Tracer {
         S4 out{};
         for (int i = 0; i < NW; ++i) out[size_t(i)] = f[size_t(i)] * Tr[size_t(i)] * ls.Le[size_t(i)] * (cosF * wmis / ls.pdf);
         return out;
+    }
+
+    // Tracer::walk (transport.cpp:531-595), without the record: the last event's kind, boundary,
+    // point and throughput. kind: 0 escape, 1 detect/diffuse/absorb (the walk ends on matter),
+    // 2 the event budget ran out, 3 the scattering sample failed.
+    struct WalkEnd { int kind = 0; uint32_t boundary = kNone; V p; double beta = 0; int events = 0; };
+    WalkEnd walk(Ray ray, uint32_t region, double lambda, bool primary, Rng& rng, int maxEvents) const {
+        WalkEnd end;
+        double beta = 1;
+        for (int ev = 0; ev < maxEvents; ++ev) {
+            ++end.events;
+            Hit hit;
+            ray.hint = region;
+            if (!w.intersect(ray, Inf, hit)) { end.kind = 0; end.beta = beta; return end; }
+            const Medium& med = w.mediumOf(region);
+            if (med.absorbs()) beta *= std::exp(-med.absorption.eval(lambda) * hit.t);
+            const Boundary& b = w.boundaries[hit.boundary];
+            const bool fromFront = dot(ray.d, hit.n) < 0;
+            const uint32_t inc = fromFront ? b.front : b.back, other = fromFront ? b.back : b.front;
+            region = inc;
+            const owec_optics& o = w.optics[b.optics];
+            if (o.type == OWEC_SURF_NULL) {
+                region = other;
+                ray = w.spawn(hit, ray.d, region);
+                continue;
+            }
+            if (o.type == OWEC_SURF_ABSORBER || o.type == OWEC_SURF_DETECTOR || (primary && o.type == OWEC_SURF_DIFFUSE)) {
+                end.kind = 1;
+                end.boundary = hit.boundary;
+                end.p = hit.p;
+                end.beta = beta;
+                return end;
+            }
+            const Iface it = makeInterface(hit, lambda);
+            Sample s;
+            bool ok;
+            if (primary && o.type == OWEC_SURF_DIELECTRIC) {
+                const D2 u(rng);
+                ok = sampleScatter(it, ray.d, 1.0, u.u1, u.u2, false, s);
+                if (!ok) {
+                    const D2 v(rng);
+                    ok = sampleScatter(it, ray.d, 0.0, v.u1, v.u2, false, s);
+                }
+                if (ok && s.delta) s.weight = s.transmitted ? s.T : s.R;
+            } else {
+                const D3 u(rng);
+                ok = sampleScatter(it, ray.d, u.u1, u.u2, u.u3, false, s);
+            }
+            if (!ok) { end.kind = 3; end.beta = 0; return end; }
+            beta *= s.weight;
+            if (s.transmitted) region = other;
+            ray = w.spawn(hit, s.wi, region);
+        }
+        end.kind = 2;
+        end.beta = beta;
+        return end;
     }
 
     // Tracer::radiance (transport.cpp:473-529)
@@ -1744,6 +2000,97 @@ int oweport_cast_rays(void* scene, uint64_t n, const double* o, const double* d,
         for (int k = 1; k < threads; ++k) pool.emplace_back(work, k);
         work(0);
         for (auto& th : pool) th.join();
+        return 0;
+    } catch (const std::exception& e) {
+        oracle::g_error = e.what();
+        return -1;
+    }
+}
+
+// Forward walks, emitted and binned as owec_walk describes them (include/owec.h). bins receive the
+// sum of the binned walks' throughput times their splat weights; stats: [walks, binned, escaped,
+// events].
+int oweport_walk(void* scene, const owec_walk_desc* w, uint64_t first, uint64_t n, int threads, double* bins,
+                 uint64_t* stats) {
+    using namespace oracle;
+    try {
+        const auto& sc = *static_cast<const Scene*>(scene);
+        Tracer tr{sc, 64, 6, 0};
+        const V axis = unit(V(w->axis[0], w->axis[1], w->axis[2]));
+        V S, T;
+        basis(axis, S, T);
+        const double cosMax = std::cos(w->extent);
+        const Boundary& target = sc.boundaries.at(w->target);
+        threads = threads > 0 ? threads : int(std::max(1u, std::thread::hardware_concurrency()));
+        const size_t nb = size_t(w->width) * w->height;
+        std::vector<std::vector<double>> part(size_t(threads), std::vector<double>(nb, 0.0));
+        std::vector<std::array<uint64_t, 4>> st(size_t(threads), {0, 0, 0, 0});
+        auto work = [&](int t) {
+            const uint64_t b = n * uint64_t(t) / uint64_t(threads), e = n * uint64_t(t + 1) / uint64_t(threads);
+            for (uint64_t k = b; k < e; ++k) {
+                Rng rng(hashCombine(w->seed, first + k), w->stream);
+                const double lambda = w->lambda_min + (w->lambda_max - w->lambda_min) * rng.uniform();
+                const D2 u(rng);
+                Ray ray;
+                ray.o = V(w->position[0], w->position[1], w->position[2]);
+                if (w->source_kind == OWEC_SOURCE_POINT) {
+                    const double cosT = (1 - u.u1) + u.u1 * cosMax, sinT = safeSqrt(1 - cosT * cosT), phi = 2 * Pi * u.u2;
+                    ray.d = S * (std::cos(phi) * sinT) + T * (std::sin(phi) * sinT) + axis * cosT;
+                } else if (w->source_kind == OWEC_SOURCE_COLLIMATED) {
+                    const double a = 2 * u.u1 - 1, bb = 2 * u.u2 - 1;
+                    double dx = 0, dy = 0;
+                    if (!(a == 0 && bb == 0)) {
+                        double r, phi;
+                        if (std::fabs(a) > std::fabs(bb)) { r = a; phi = (Pi / 4) * (bb / a); }
+                        else { r = bb; phi = Pi / 2 - (Pi / 4) * (a / bb); }
+                        dx = r * std::cos(phi);
+                        dy = r * std::sin(phi);
+                    }
+                    ray.o = ray.o + (S * dx + T * dy) * w->extent;
+                    ray.d = axis;
+                } else {
+                    ray.o = ray.o + (S * (2 * u.u1 - 1) + T * (2 * u.u2 - 1)) * w->extent;
+                    ray.d = axis;
+                }
+                const Tracer::WalkEnd end = tr.walk(ray, w->region, lambda, w->mode == OWEC_WALK_PRIMARY_TRANSMISSION, rng,
+                                                    w->max_events);
+                st[size_t(t)][0]++;
+                st[size_t(t)][3] += uint64_t(end.events);
+                if (end.kind == 0) { st[size_t(t)][2]++; continue; }
+                if (end.kind != 1 || end.boundary != w->target) continue;
+                const V pl = target.toLocal.point(end.p);
+                const double fx = (pl.x / w->half_x + 1) * 0.5 * w->width, fy = (1 - pl.y / w->half_y) * 0.5 * w->height;
+                bool any = false;
+                if (w->splat == OWEC_SPLAT_NEAREST) {
+                    if (fx >= 0 && fy >= 0 && fx < w->width && fy < w->height) {
+                        part[size_t(t)][size_t(int(fy)) * w->width + size_t(int(fx))] += end.beta;
+                        any = true;
+                    }
+                } else {
+                    const double gx = fx - 0.5, gy = fy - 0.5;
+                    const int x0 = int(std::floor(gx)), y0 = int(std::floor(gy));
+                    const double ax = gx - x0, ay = gy - y0;
+                    for (int j = 0; j < 2; ++j)
+                        for (int i = 0; i < 2; ++i) {
+                            const int xi = x0 + i, yj = y0 + j;
+                            if (xi < 0 || yj < 0 || xi >= w->width || yj >= w->height) continue;
+                            part[size_t(t)][size_t(yj) * w->width + size_t(xi)] += end.beta * (i ? ax : 1 - ax) * (j ? ay : 1 - ay);
+                            any = true;
+                        }
+                }
+                if (any) st[size_t(t)][1]++;
+            }
+        };
+        std::vector<std::thread> pool;
+        for (int t = 1; t < threads; ++t) pool.emplace_back(work, t);
+        work(0);
+        for (auto& th : pool) th.join();
+        for (size_t i = 0; i < nb; ++i)
+            for (int t = 0; t < threads; ++t) bins[i] += part[size_t(t)][i];
+        for (int k = 0; k < 4; ++k) {
+            stats[k] = 0;
+            for (int t = 0; t < threads; ++t) stats[k] += st[size_t(t)][size_t(k)];
+        }
         return 0;
     } catch (const std::exception& e) {
         oracle::g_error = e.what();

@@ -110,16 +110,8 @@ class ReferenceEngine:
         r = self.lib.oweref_walk(self.h, ctypes.byref(desc), first, n, threads, bins.ctypes.data_as(A.c_double_p), st)
         if r != 0:
             raise RuntimeError(self.lib.oweref_last_error().decode())
-        if desc.source_kind == A.SOURCE_POINT:
-            measure = 2 * np.pi * (1 - np.cos(desc.extent))
-        elif desc.source_kind == A.SOURCE_COLLIMATED:
-            measure = np.pi * desc.extent ** 2
-        else:
-            measure = 4 * desc.extent ** 2
-        bin_area = (2 * desc.half_x / desc.width) * (2 * desc.half_y / desc.height)
-        bins *= measure / (n * bin_area)
-        return bins.reshape(desc.height, desc.width), {"walks": st[0], "binned": st[1], "escaped": st[2],
-                                                       "events": st[3]}
+        return normalise_walk_bins(desc, bins, n), {"walks": st[0], "binned": st[1], "escaped": st[2],
+                                                    "events": st[3]}
 
     def info(self):
         pdfs = np.zeros(64)
@@ -136,6 +128,19 @@ class ReferenceEngine:
         v = ctypes.c_double()
         self.lib.oweref_medium_index(self.h, region, lam, ctypes.byref(v))
         return v.value
+
+
+def normalise_walk_bins(desc, bins, n):
+    """Binned throughput sums as irradiance per unit source intensity / irradiance, as
+    owec_walk_resolve reports them: times (source measure) / (walks * bin area)."""
+    if desc.source_kind == A.SOURCE_POINT:
+        measure = 2 * np.pi * (1 - np.cos(desc.extent))
+    elif desc.source_kind == A.SOURCE_COLLIMATED:
+        measure = np.pi * desc.extent ** 2
+    else:
+        measure = 4 * desc.extent ** 2
+    bin_area = (2 * desc.half_x / desc.width) * (2 * desc.half_y / desc.height)
+    return (bins * measure / (n * bin_area)).reshape(desc.height, desc.width)
 
 
 def block_z_test(runs_a, runs_b, block=6):
@@ -204,6 +209,8 @@ def port_lib():
         lib.oweport_cast_rays.argtypes = [P, ctypes.c_uint64, A.c_double_p, A.c_double_p, ctypes.c_int, A.c_u32_p,
                                           A.c_u32_p, A.c_double_p]
         lib.oweport_light_pdfs.argtypes = [P, A.c_double_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        lib.oweport_walk.argtypes = [P, ctypes.POINTER(A.WalkDesc), ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int,
+                                     A.c_double_p, ctypes.POINTER(ctypes.c_uint64)]
         _port = lib
     return _port
 
@@ -250,6 +257,16 @@ class PortEngine:
         if r != 0:
             raise RuntimeError(self.lib.oweport_last_error().decode())
         return b, p, t
+
+    def walk(self, desc, first, n, threads=0):
+        """The restated Tracer::walk, binned like owec_walk; (bins, stats)."""
+        nb = desc.width * desc.height
+        bins = np.zeros(nb)
+        st = (ctypes.c_uint64 * 4)()
+        r = self.lib.oweport_walk(self.h, ctypes.byref(desc), first, n, threads, bins.ctypes.data_as(A.c_double_p), st)
+        if r != 0:
+            raise RuntimeError(self.lib.oweport_last_error().decode())
+        return normalise_walk_bins(desc, bins, n), {"walks": st[0], "binned": st[1], "escaped": st[2], "events": st[3]}
 
     def light_pdfs(self):
         out = np.zeros(64)
