@@ -113,8 +113,13 @@ def dist_env():
     return world, rank, local
 
 
+PRECISIONS = {"mixed": A.PRECISION_MIXED, "fp32": A.PRECISION_FP32, "fp64": A.PRECISION_FP64}
+PRECISION = "mixed"
+
+
 def settings_for(rank):
-    return A.make_settings(seed=rank, max_depth=MAX_DEPTH, rr_depth=RR_DEPTH, wavelength_mode=A.WAVELENGTHS_HERO4)
+    return A.make_settings(seed=rank, max_depth=MAX_DEPTH, rr_depth=RR_DEPTH, wavelength_mode=A.WAVELENGTHS_HERO4,
+                           precision=PRECISIONS[PRECISION])
 
 
 def cpu_reference_rate(desc, seconds_target=12.0, threads=0):
@@ -249,7 +254,7 @@ def run_cuda(args):
         img = renderer.resolve()
     e2e_seconds = time.perf_counter() - t0
     e2e_value = n_pix * world * e2e_steps / e2e_seconds
-    d2h = n_pix * (3 + 1) * 8
+    d2h = n_pix * 3 * 8  # the resolved XYZ image (Renderer::resolve), FP64
 
     # the film over NCCL: the one exchange step of a multi-GPU render
     if world > 1:
@@ -274,9 +279,11 @@ def run_cuda(args):
         line = {
             "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * device_seconds / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"mixed": "f32+f64", "fp32": "f32", "fp64": "f64"}[PRECISION], "data": "synthetic",
             "config": {"workload": WORKLOAD, "paths_per_step": n_pix, "triangles": info["triangles"],
-                       "precision": "fp32 camera-relative + selective fp64", "l2": "flushed between steps (512 MB write)",
+                       "precision": {"mixed": "fp32 camera-relative + selective fp64", "fp32": "plain fp32",
+                                     "fp64": "all fp64"}[PRECISION], "l2": "flushed between steps (512 MB write)",
                        "parallelism": f"replicated scene, dp{world} over sample streams"},
             "gpu_launches": None,
             "rays_per_s": (stats1["segments"] - stats0["segments"] + stats1["shadow_rays"] - stats0["shadow_rays"])
@@ -314,8 +321,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--width", type=int, default=1920, help="film width (a smaller case for profiling)")
     ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--precision", default="mixed", choices=sorted(PRECISIONS),
+                    help="mixed: FP32 camera-relative + selective FP64 (the product); fp64: the all-FP64 "
+                         "instantiation of the same kernels it is compared with")
     args = ap.parse_args()
     globals()["WIDTH"], globals()["HEIGHT"] = args.width, args.height
+    globals()["PRECISION"] = args.precision
     if args.impl == "reference":
         return run_reference(args)
     return run_cuda(args)

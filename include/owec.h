@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define OWEC_ABI_VERSION 1
+#define OWEC_ABI_VERSION 2
 
 /* ------------------------------------------------------------------ status codes */
 #define OWEC_OK 0
@@ -188,6 +188,12 @@ typedef struct owec_scene_desc {
     const uint32_t* triangles;     /* index triples, counter-clockwise = front */
     owec_environment env;
     owec_detector detector;
+    /* The origin of the camera-relative FP32 frame. 0: the observer's position (the sensor's
+     * centre). 1: frame_origin, for work that measures somewhere else than at the detector: forward
+     * walks onto a heightfield want the FP32 precision at the heightfield, not at the camera. */
+    int32_t frame_origin_set;
+    int32_t pad0;
+    double frame_origin[3];
 } owec_scene_desc;
 
 /* ------------------------------------------------------------------ pass settings */

@@ -244,6 +244,7 @@ struct owec_ctx {
     owec_settings settings{1, 64, 6, OWEC_WAVELENGTHS_HERO4, OWEC_PRECISION_MIXED, 380, 780, 0};
     uint64_t passCount = 0;  // samples per pixel accumulated (the PCG32 stream of the next sample)
     DBuf<double> dFilm, dComp, dSamples;
+    DBuf<double> dResolved;  // owec_resolve's per-pixel XYZ, read back in one copy
     DBuf<uint8_t> dPathRay, dPathSpec, dPathAux, dHit, dShadow;
     DBuf<uint32_t> dQueue0, dQueue1, dQueueSurf, dQueueShadow, dCounts;
     DBuf<StatCounters> dStats;
@@ -378,9 +379,11 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
     c.optics.assign(d.optics, d.optics + d.n_optics);
     c.emissions.assign(d.emissions, d.emissions + d.n_emissions);
 
-    // The camera-relative origin: the observer's position, or the sensor's centre.
+    // The camera-relative origin: the one given, the observer's position, or the sensor's centre.
     double origin[3];
-    if (d.detector.kind == OWEC_DETECTOR_OBSERVER) {
+    if (d.frame_origin_set) {
+        for (int k = 0; k < 3; ++k) origin[k] = d.frame_origin[k];
+    } else if (d.detector.kind == OWEC_DETECTOR_OBSERVER) {
         for (int k = 0; k < 3; ++k) origin[k] = d.detector.position[k];
     } else {
         const double* m = d.boundaries[d.detector.boundary].to_world;
@@ -741,7 +744,7 @@ void runPass(owec_ctx& c, int spp) {
             }
             // the next-bounce queue and the per-bounce queues start empty
             OWEC_CUDA(cudaMemsetAsync(c.dCounts.get() + (cur ^ 1), 0, sizeof(uint32_t), s));
-            OWEC_CUDA(cudaMemsetAsync(c.dCounts.get() + 2, 0, 2 * sizeof(uint32_t), s));
+            OWEC_CUDA(cudaMemsetAsync(c.dCounts.get() + 2, 0, 4 * sizeof(uint32_t), s));  // + the fetch counters
             if (size_t(evUsed + 4) > c.travEvents.size())
                 for (int k = 0; k < 4; ++k) {
                     cudaEvent_t e;
@@ -749,14 +752,14 @@ void runPass(owec_ctx& c, int spp) {
                     c.travEvents.push_back(e);
                 }
             OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed], s));
-            launchIntersect<M>(c.ds, pb, q, cur, c.dStats.get(), grid, s);
+            launchIntersect<M>(c.ds, pb, q, cur, c.dStats.get(), c.dCounts.get() + 4, grid, s);
             ++intersectLaunches;
             OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 1], s));
             checkLaunch();
             launchMedium<M>(c.ds, pp, pb, q, cur, c.dStats.get(), grid, s);
             launchSurface<M>(c.ds, pp, pb, q, cur, c.dStats.get(), grid, s);
             OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 2], s));
-            launchShadow<M>(c.ds, pp, pb, q, c.dStats.get(), grid, s);
+            launchShadow<M>(c.ds, pp, pb, q, c.dStats.get(), c.dCounts.get() + 5, grid, s);
             OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 3], s));
             checkLaunch();
             evUsed += 4;
@@ -922,17 +925,16 @@ int owec_resolve(owec_ctx* ctx, double* xyz, double* samples) {
         OWEC_CUDA(cudaSetDevice(ctx->device));
         ensureFilm(*ctx);
         const size_t np = size_t(ctx->ds.det.width) * ctx->ds.det.height;
-        std::vector<double> film(3 * np), comp(3 * np), n(np);
-        OWEC_CUDA(cudaMemcpyAsync(film.data(), ctx->dFilm.get(), film.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
-        OWEC_CUDA(cudaMemcpyAsync(comp.data(), ctx->dComp.get(), comp.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
-        OWEC_CUDA(cudaMemcpyAsync(n.data(), ctx->dSamples.get(), n.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
-        OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
-        for (size_t i = 0; i < np; ++i) {
-            const double norm = n[i] > 0 ? 1.0 / n[i] : 0;
-            if (xyz)
-                for (int ch = 0; ch < 3; ++ch) xyz[3 * i + ch] = (film[3 * i + ch] - comp[3 * i + ch]) * norm;
-            if (samples) samples[i] = n[i];
+        if (xyz) {
+            ctx->dResolved.resize(3 * np);
+            launchResolve(ctx->dFilm.get(), ctx->dComp.get(), ctx->dSamples.get(), uint32_t(np), ctx->dResolved.get(),
+                          ctx->stream);
+            checkLaunch();
+            OWEC_CUDA(cudaMemcpyAsync(xyz, ctx->dResolved.get(), 3 * np * 8, cudaMemcpyDeviceToHost, ctx->stream));
         }
+        if (samples)
+            OWEC_CUDA(cudaMemcpyAsync(samples, ctx->dSamples.get(), np * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
     });
 }
 

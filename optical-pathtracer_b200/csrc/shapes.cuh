@@ -77,6 +77,20 @@ struct AHit {
     V3<Rr> p, n;
 };
 
+// At most two crossings, kept in named members (not an indexed array) so that they stay in
+// registers when the count is only known at run time.
+template <class Rr>
+struct AHits {
+    AHit<Rr> h0, h1;
+    int n = 0;
+    OWEC_HD void add(const AHit<Rr>& h) {
+        if (n == 0) h0 = h;
+        else h1 = h;
+        ++n;
+    }
+    OWEC_HD const AHit<Rr>& get(int i) const { return i == 0 ? h0 : h1; }
+};
+
 // Sphere roots in the geometric form (surfaces.hpp:104-122).
 template <class T>
 OWEC_HD bool sphereRoots(const V3<T>& o, const V3<T>& d, T R, T& t0, T& t1) {
@@ -119,8 +133,8 @@ template <class T> OWEC_HD T conicSlope(T c, T k, T r) {
 // Up to two crossings of boundary b's shape by the local ray (o, d) in (tmin, tmax), ascending,
 // each inside the shape's trim. Returns how many.
 template <class R, class Rr>
-OWEC_HD int analyticCrossings(const DBoundary& b, const V3<Rr>& o, const V3<Rr>& d, Rr tmin, Rr tmax, AHit<Rr> out[2]) {
-    int n = 0;
+OWEC_HD int analyticCrossings(const DBoundary& b, const V3<Rr>& o, const V3<Rr>& d, Rr tmin, Rr tmax, AHits<Rr>& out) {
+    out.n = 0;
     const double* P = b.params;
     switch (b.shape) {
         case OWEC_SHAPE_SPHERE: {
@@ -132,7 +146,7 @@ OWEC_HD int analyticCrossings(const DBoundary& b, const V3<Rr>& o, const V3<Rr>&
                 Rr tr;
                 if (!refinedRootIn<R, Rr>(kQuadSphere, Rad * Rad, Rr(0), o, d, Rr(ts[i]), tmin, tmax, tr)) continue;
                 const V3<Rr> p = o + d * tr;
-                out[n++] = {tr, p, normalize(p / Rad)};
+                out.add({tr, p, normalize(p / Rad)});
             }
             break;
         }
@@ -155,7 +169,7 @@ OWEC_HD int analyticCrossings(const DBoundary& b, const V3<Rr>& o, const V3<Rr>&
                 if (t <= tmin || t >= tmax) return 0;
                 const V3<Rr> p = o + d * t;
                 if (!solid(p)) return 0;
-                out[n++] = {t, p, normal(p)};
+                out.add({t, p, normal(p)});
                 break;
             }
             R A, B, C, t0, t1;
@@ -168,7 +182,7 @@ OWEC_HD int analyticCrossings(const DBoundary& b, const V3<Rr>& o, const V3<Rr>&
                 if (!refinedRootIn<R, Rr>(kQuadSag, c, c * (Rr(1) + k), o, d, Rr(ts[i]), tmin, tmax, tr)) continue;
                 const V3<Rr> p = o + d * tr;
                 if (!solid(p)) continue;
-                out[n++] = {tr, p, normal(p)};
+                out.add({tr, p, normal(p)});
             }
             break;
         }
@@ -190,7 +204,7 @@ OWEC_HD int analyticCrossings(const DBoundary& b, const V3<Rr>& o, const V3<Rr>&
                 in = sqr(p.x / a) + sqr(p.y / bb) <= Rr(1);
             }
             if (!in) return 0;
-            out[n++] = {t, p, V3<Rr>(0, 0, 1)};
+            out.add({t, p, V3<Rr>(0, 0, 1)});
             break;
         }
         case OWEC_SHAPE_CYLINDER: {
@@ -203,14 +217,14 @@ OWEC_HD int analyticCrossings(const DBoundary& b, const V3<Rr>& o, const V3<Rr>&
                 if (!refinedRootIn<R, Rr>(kQuadCylinder, Rad * Rad, Rr(0), o, d, Rr(ts[i]), tmin, tmax, tr)) continue;
                 const V3<Rr> p = o + d * tr;
                 if (p.z < z0 || p.z > z1) continue;
-                out[n++] = {tr, p, normalize(V3<Rr>(p.x, p.y, Rr(0)))};
+                out.add({tr, p, normalize(V3<Rr>(p.x, p.y, Rr(0)))});
             }
             break;
         }
         default: break;
     }
-    if (n == 2 && out[1].t < out[0].t) { const AHit<Rr> tmp = out[0]; out[0] = out[1]; out[1] = tmp; }
-    return n;
+    if (out.n == 2 && out.h1.t < out.h0.t) { const AHit<Rr> tmp = out.h0; out.h0 = out.h1; out.h1 = tmp; }
+    return out.n;
 }
 
 // Watertight line-triangle crossing test (Woop, Benthin and Wald 2013), edges included, as the

@@ -75,13 +75,11 @@ __device__ SurfacePoint<R> hitGeometry(const DeviceScene& sc, const PathRay<R>& 
     }
     const V3<Rr> lo = bd.toLocal.point(V3<Rr>(od));
     const V3<Rr> ld = bd.toLocal.vector(V3<Rr>(d));
-    AHit<Rr> hits[2];
+    AHits<Rr> hits;
     const Rr t = Rr(h.t);
     const Rr slack = Rr(1e-6) * (Rr(1) + fabs(t));
     const int n = analyticCrossings<Ro, Rr>(bd, lo, ld, Rr(0), t + slack, hits);
-    int best = 0;
-    for (int i = 1; i < n; ++i)
-        if (fabs(hits[i].t - t) < fabs(hits[best].t - t)) best = i;
+    const AHit<Rr>& hb = (n == 2 && fabs(hits.h1.t - t) < fabs(hits.h0.t - t)) ? hits.h1 : hits.h0;
     if (n == 0) {  // not found again (rounding at a trim edge): the point on the ray
         sp.p = od + V3<double>(d) * h.t;
         sp.pLocal = bd.toLocal.point(sp.p);
@@ -89,8 +87,8 @@ __device__ SurfacePoint<R> hitGeometry(const DeviceScene& sc, const PathRay<R>& 
         sp.n = V3<R>(normalize(bd.toWorld.vector(sp.nLocal)));
         return sp;
     }
-    sp.pLocal = V3<double>(hits[best].p);
-    sp.nLocal = V3<double>(hits[best].n);
+    sp.pLocal = V3<double>(hb.p);
+    sp.nLocal = V3<double>(hb.n);
     sp.p = bd.toWorld.point(sp.pLocal);
     sp.n = V3<R>(normalize(bd.toWorld.vector(sp.nLocal)));
     return sp;

@@ -16,12 +16,36 @@
 
 namespace owec {
 
-constexpr int kStackDepth = 32;  // entries per thread; an overflow ends the query and is counted
+constexpr int kStackDepth = 32;  // entries per thread in shared memory
+constexpr int kDeepStackDepth = 112;  // the rare query that needs more is traversed again with a stack
+                                      // of this depth in local memory (7 per level: 16 levels); an
+                                      // overflow beyond it ends the query and is counted
 constexpr uint32_t kMaxTraversalSteps = 1u << 20;  // a bound on stack pops: a malformed tree cannot hang
 
 struct StackEntry {
     uint32_t ref;   // bit 31: leaf; leaf: prim start << 2 | (count - 1); inner: node index
     float tEnter;
+};
+
+// The short traversal stack: this thread's column of the block's shared-memory stack (stride =
+// block size), so that a warp's entries of one level are consecutive words.
+struct SharedStack {
+    static constexpr int kDepth = kStackDepth;
+    StackEntry* sh;
+    int stride;
+    __device__ __forceinline__ void init(StackEntry* stack, int s) { sh = stack; stride = s; }
+    __device__ __forceinline__ StackEntry get(int i) const { return sh[i * stride]; }
+    __device__ __forceinline__ float tEnter(int i) const { return sh[i * stride].tEnter; }
+    __device__ __forceinline__ void set(int i, const StackEntry& e) { sh[i * stride] = e; }
+};
+// The deep stack, in local memory, for the queries that overflow the short one.
+struct LocalStack {
+    static constexpr int kDepth = kDeepStackDepth;
+    StackEntry e[kDeepStackDepth];
+    __device__ __forceinline__ void init(StackEntry*, int) {}
+    __device__ __forceinline__ StackEntry get(int i) const { return e[i]; }
+    __device__ __forceinline__ float tEnter(int i) const { return e[i].tEnter; }
+    __device__ __forceinline__ void set(int i, const StackEntry& x) { e[i] = x; }
 };
 
 template <class T>
@@ -75,35 +99,88 @@ __device__ __forceinline__ bool analyticCandidate(const DeviceScene& sc, const R
     const DBoundary& bd = sc.boundaries[b];
     const V3<Rr> lo = bd.toLocal.point(V3<Rr>(q.od));
     const V3<Rr> ld = bd.toLocal.vector(V3<Rr>(q.d));
-    AHit<Rr> hits[2];
+    AHits<Rr> hits;
     const int n = analyticCrossings<R, Rr>(bd, lo, ld, Rr(0), Rr(best), hits);
-    for (int i = 0; i < n; ++i) {
-        const V3<T> nw = V3<T>(bd.toWorld.vector(hits[i].n));
-        if (!acceptCrossing(sc, q, b, 0u, false, T(hits[i].t), nw)) continue;
-        tOut = hits[i].t;
+    // Leaving this boundary, the anchor lies on it to the precision of the refinement, not of FP32:
+    // with the FP32 window a grazing ray's far crossing of the same sphere (at t = 2 R cos) fell
+    // inside it and was rejected as the departure, and the path leaked.
+    RayQuery<T> qs = q;
+    if (b == q.depB && sizeof(Rr) > sizeof(R)) qs.errN = q.errN * T(2.5e-7);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        if (i >= n) break;
+        const AHit<Rr>& h = hits.get(i);
+        const V3<T> nw = V3<T>(bd.toWorld.vector(h.n));
+        if (!acceptCrossing(sc, qs, b, 0u, false, T(h.t), nw)) continue;
+        tOut = h.t;
         return true;
     }
     return false;
 }
 
+// A wide node as the five 128-bit words it is loaded in (the WideNode layout of device_scene.cuh):
+//   a = (ox, oy, oz, ex | ey << 8 | ez << 16 | imask << 24)
+//   b = (child_base, prim_base, meta[0..3], meta[4..7])
+//   c = (qlox[0..3], qlox[4..7], qloy[0..3], qloy[4..7])
+//   d = (qloz[0..3], qloz[4..7], qhix[0..3], qhix[4..7])
+//   e = (qhiy[0..3], qhiy[4..7], qhiz[0..3], qhiz[4..7])
+struct NodeWords {
+    uint4 a, b, c, d, e;
+};
+
+__device__ __forceinline__ void loadNode(const WideNode* nodes, uint32_t i, NodeWords& nd) {
+#if defined(__CUDA_ARCH__)
+    const uint4* src = reinterpret_cast<const uint4*>(nodes + i);
+    nd.a = __ldg(src + 0);
+    nd.b = __ldg(src + 1);
+    nd.c = __ldg(src + 2);
+    nd.d = __ldg(src + 3);
+    nd.e = __ldg(src + 4);
+#else
+    const uint4* src = reinterpret_cast<const uint4*>(nodes + i);
+    nd.a = src[0]; nd.b = src[1]; nd.c = src[2]; nd.d = src[3]; nd.e = src[4];
+#endif
+}
+
+// Byte k (0..3) of w as an exact float: the byte placed in the mantissa of 2^23, minus 2^23. One
+// byte permute and one add, on the integer and FMA pipes, where a conversion instruction would
+// queue on the narrow conversion pipe (eight children x six planes per node).
+__device__ __forceinline__ float byteAsFloat(uint32_t w, int k) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | uint32_t(k))) - 8388608.0f;
+}
+
+__device__ __forceinline__ uint32_t nodeByte(uint32_t lo, uint32_t hi, int i) {
+    return ((i < 4 ? lo : hi) >> (8 * (i & 3))) & 0xFFu;
+}
+
 // Decoded child boxes of a node, slab-tested against the ray. Returns the hit mask and fills tEnter.
 template <class T>
-__device__ __forceinline__ uint32_t intersectChildren(const WideNode& nd, const V3<T>& inv, const V3<T>& oinv, T tmin, T tmax,
+__device__ __forceinline__ uint32_t intersectChildren(const NodeWords& nd, const V3<T>& inv, const V3<T>& oinv, T tmin, T tmax,
                                    T tEnter[8]) {
-    const T sx = T(__uint_as_float(uint32_t(nd.ex) << 23));
-    const T sy = T(__uint_as_float(uint32_t(nd.ey) << 23));
-    const T sz = T(__uint_as_float(uint32_t(nd.ez) << 23));
+    const T sx = T(__uint_as_float((nd.a.w & 0xFFu) << 23));
+    const T sy = T(__uint_as_float(((nd.a.w >> 8) & 0xFFu) << 23));
+    const T sz = T(__uint_as_float(((nd.a.w >> 16) & 0xFFu) << 23));
     // t = (origin + q * s - o) * inv = q * (s * inv) + (origin * inv - o * inv)
     const T ax = sx * inv.x, ay = sy * inv.y, az = sz * inv.z;
-    const T bx = T(nd.ox) * inv.x - oinv.x, by = T(nd.oy) * inv.y - oinv.y, bz = T(nd.oz) * inv.z - oinv.z;
+    const T bx = T(__uint_as_float(nd.a.x)) * inv.x - oinv.x;
+    const T by = T(__uint_as_float(nd.a.y)) * inv.y - oinv.y;
+    const T bz = T(__uint_as_float(nd.a.z)) * inv.z - oinv.z;
     const bool nx = inv.x < T(0), ny = inv.y < T(0), nz = inv.z < T(0);
+    // near and far planes per axis, chosen by the ray's direction on whole words
+    const uint32_t nxl0 = nx ? nd.d.z : nd.c.x, nxl1 = nx ? nd.d.w : nd.c.y;
+    const uint32_t fxl0 = nx ? nd.c.x : nd.d.z, fxl1 = nx ? nd.c.y : nd.d.w;
+    const uint32_t nyl0 = ny ? nd.e.x : nd.c.z, nyl1 = ny ? nd.e.y : nd.c.w;
+    const uint32_t fyl0 = ny ? nd.c.z : nd.e.x, fyl1 = ny ? nd.c.w : nd.e.y;
+    const uint32_t nzl0 = nz ? nd.e.z : nd.d.x, nzl1 = nz ? nd.e.w : nd.d.y;
+    const uint32_t fzl0 = nz ? nd.d.x : nd.e.z, fzl1 = nz ? nd.d.y : nd.e.w;
     uint32_t mask = 0;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        if (nd.meta[i] == 0) continue;  // empty slot (inner slots carry bit 3, leaves a count)
-        const T lx = T(nx ? nd.qhix[i] : nd.qlox[i]), hx = T(nx ? nd.qlox[i] : nd.qhix[i]);
-        const T ly = T(ny ? nd.qhiy[i] : nd.qloy[i]), hy = T(ny ? nd.qloy[i] : nd.qhiy[i]);
-        const T lz = T(nz ? nd.qhiz[i] : nd.qloz[i]), hz = T(nz ? nd.qloz[i] : nd.qhiz[i]);
+        if (nodeByte(nd.b.z, nd.b.w, i) == 0) continue;  // empty slot (inner slots carry bit 3, leaves a count)
+        const int k = i & 3;
+        const T lx = T(byteAsFloat(i < 4 ? nxl0 : nxl1, k)), hx = T(byteAsFloat(i < 4 ? fxl0 : fxl1, k));
+        const T ly = T(byteAsFloat(i < 4 ? nyl0 : nyl1, k)), hy = T(byteAsFloat(i < 4 ? fyl0 : fyl1, k));
+        const T lz = T(byteAsFloat(i < 4 ? nzl0 : nzl1, k)), hz = T(byteAsFloat(i < 4 ? fzl0 : fzl1, k));
         const T t0x = fma(lx, ax, bx), t1x = fma(hx, ax, bx);
         const T t0y = fma(ly, ay, by), t1y = fma(hy, ay, by);
         const T t0z = fma(lz, az, bz), t1z = fma(hz, az, bz);
@@ -116,17 +193,6 @@ __device__ __forceinline__ uint32_t intersectChildren(const WideNode& nd, const 
         }
     }
     return mask;
-}
-
-__device__ __forceinline__ void loadNode(const WideNode* nodes, uint32_t i, WideNode& nd) {
-#if defined(__CUDA_ARCH__)
-    const uint4* src = reinterpret_cast<const uint4*>(nodes + i);
-    uint4* dst = reinterpret_cast<uint4*>(&nd);
-#pragma unroll
-    for (int k = 0; k < 5; ++k) dst[k] = __ldg(src + k);
-#else
-    nd = nodes[i];
-#endif
 }
 
 __device__ __forceinline__ void loadPrim(const PrimRec* prims, uint32_t i, PrimRec& p) {
@@ -170,100 +236,178 @@ template <> struct TriFetch<double> {
 
 enum TraceStatus : int { kTraceMiss = 0, kTraceHit = 1, kTraceOverflow = 2 };
 
-// Closest (AnyHit = false) or first (AnyHit = true) acceptable crossing in (0, q.tmax).
-// R / Rr: precision of analytic roots and of their refinement. `stack` is this thread's column of
-// the block's shared-memory stack (stride = block size).
-template <class T, class R, class Rr, bool AnyHit>
-__device__ int traceRay(const DeviceScene& sc, const RayQuery<T>& q, StackEntry* stack, int stride, HitRec& hit,
-                        uint32_t* visits = nullptr, uint32_t* tests = nullptr) {
-    const V3<T> inv(T(1) / q.d.x, T(1) / q.d.y, T(1) / q.d.z);
-    const V3<T> oinv(q.o.x * inv.x, q.o.y * inv.y, q.o.z * inv.z);
-    const ShearedRay<T> sh = shearRay(q.d);
-    T best = q.tmax;
-    bool found = false;
-    int sp = 0;
-    uint32_t nodeVisits = 0, primTests = 0;
-    stack[0] = {0u, 0.0f};
-    sp = 1;
-    uint32_t steps = 0;
-    while (sp > 0) {
-        if (++steps > kMaxTraversalSteps) return kTraceOverflow;
-        const StackEntry e = stack[(sp - 1) * stride];
-        --sp;
-        if (e.tEnter > toFloatUp(best)) continue;
-        if ((e.ref & 0x80000000u) == 0) {
-            WideNode nd;
-            loadNode(sc.nodes, e.ref, nd);
-            ++nodeVisits;
-            T tEnter[8];
-            uint32_t mask = intersectChildren(nd, inv, oinv, T(0), best, tEnter);
-            // Push in far-to-near order: repeatedly take the farthest remaining hit.
-            const int nHits = __popc(mask);
-            if (sp + nHits > kStackDepth) return kTraceOverflow;
-            while (mask) {
-                int far = -1;
-                T tf = T(-1);
-                uint32_t m = mask;
-                while (m) {
-                    const int i = __ffs(m) - 1;
-                    m &= m - 1;
-                    if (tEnter[i] >= tf) { tf = tEnter[i]; far = i; }
-                }
-                mask &= ~(1u << far);
-                const uint8_t meta = nd.meta[far];
-                uint32_t ref;
-                if (nd.imask & (1u << far)) {
-                    ref = nd.child_base + (meta & 7u);
-                } else {
-                    const uint32_t cnt = meta >> 5;
-                    ref = 0x80000000u | ((nd.prim_base + (meta & 31u)) << 2) | (cnt - 1u);
-                }
-                stack[sp * stride] = {ref, toFloatDown(tf)};
-                ++sp;
+constexpr int kTraceRunning = 3;  // Traversal::run: the query is not finished yet
+
+// Sorts eight 64-bit keys ascending with a fixed network of compare-exchanges (Batcher's
+// odd-even merge sort, 19 comparators): branch-free in registers.
+__device__ __forceinline__ void cswap(uint64_t& a, uint64_t& b) {
+    const uint64_t lo = a < b ? a : b, hi = a < b ? b : a;
+    a = lo;
+    b = hi;
+}
+__device__ __forceinline__ void sort8(uint64_t k[8]) {
+    cswap(k[0], k[1]); cswap(k[2], k[3]); cswap(k[4], k[5]); cswap(k[6], k[7]);
+    cswap(k[0], k[2]); cswap(k[1], k[3]); cswap(k[4], k[6]); cswap(k[5], k[7]);
+    cswap(k[1], k[2]); cswap(k[5], k[6]);
+    cswap(k[0], k[4]); cswap(k[1], k[5]); cswap(k[2], k[6]); cswap(k[3], k[7]);
+    cswap(k[2], k[4]); cswap(k[3], k[5]);
+    cswap(k[1], k[2]); cswap(k[3], k[4]); cswap(k[5], k[6]);
+}
+
+// Closest (AnyHit = false) or first (AnyHit = true) acceptable crossing in (0, q.tmax), as a state
+// machine that a persistent kernel can advance a few visits at a time and then hand the thread a
+// new query when this one ends. R / Rr: precision of analytic roots and of their refinement.
+//
+// At an inner node the hit children become 64-bit keys (entry distance, rounded down to FP32, over
+// the child reference) sorted by a fixed network; all but the nearest are pushed far to near and
+// the traversal continues into the nearest without a round trip through the stack.
+template <class T, class R, class Rr, bool AnyHit, class Stack = SharedStack>
+struct Traversal {
+    RayQuery<T> q;
+    V3<T> inv, oinv;
+    ShearedRay<T> sh;
+    T best;
+    HitRec hit;           // written when a crossing is accepted
+    Stack st;
+    uint32_t cur, steps, nodeVisits, primTests;
+    int sp;
+    bool haveCur, found;
+
+    // `stack` is this thread's column of the block's shared-memory stack (stride = block size).
+    __device__ __forceinline__ void begin(const RayQuery<T>& query, StackEntry* stack, int stride) {
+        q = query;
+        inv = V3<T>(T(1) / q.d.x, T(1) / q.d.y, T(1) / q.d.z);
+        oinv = V3<T>(q.o.x * inv.x, q.o.y * inv.y, q.o.z * inv.z);
+        sh = shearRay(q.d);
+        best = q.tmax;
+        found = false;
+        sp = 0;
+        st.init(stack, stride);
+        nodeVisits = primTests = 0;
+        cur = 0;  // the root
+        haveCur = true;
+        steps = 0;
+    }
+
+    // Advances by at most `budget` node or leaf visits: kTraceRunning, or the query's TraceStatus.
+    __device__ __forceinline__ int run(const DeviceScene& sc, int budget) {
+        for (int it = 0; it < budget; ++it) {
+            if (++steps > kMaxTraversalSteps) return kTraceOverflow;
+            if (!haveCur) {
+                // pop, culling deferred entries beyond the closest hit found since
+                const float bestUp = toFloatUp(best);
+                while (sp > 0 && st.tEnter(sp - 1) > bestUp) --sp;
+                if (sp == 0) return found ? kTraceHit : kTraceMiss;
+                --sp;
+                cur = st.get(sp).ref;
             }
-        } else {
-            const uint32_t start = (e.ref & 0x7FFFFFFFu) >> 2, cnt = (e.ref & 3u) + 1u;
-            primTests += cnt;
-            for (uint32_t k = 0; k < cnt; ++k) {
-                V3<T> v0, v1, v2;
-                uint32_t b, prim, kind;
-                TriFetch<T>::get(sc, start + k, v0, v1, v2, b, prim, kind);
-                if (kind == kPrimTriangle) {
-                    const V3<T> a = v0 - q.o, bb = v1 - q.o, c = v2 - q.o;
-                    if (!lineCrossesTriangle(sh, a, bb, c)) continue;
-                    const V3<T> n = triangleNormal(v0, v1, v2);
-                    const T t = -dot(q.o - v0, n) / dot(q.d, n);
-                    if (!(t > T(0) && t < best)) continue;
-                    if (!acceptCrossing(sc, q, b, prim, true, t, n)) continue;
-                    best = t;
-                    hit.t = double(t);
-                    hit.boundary = b;
-                    hit.prim = prim;
-                    hit.slot = start + k;
-                    found = true;
-                } else {
-                    Rr tr;
-                    if (!analyticCandidate<R, Rr, T>(sc, q, b, best, tr)) continue;
-                    best = T(tr);
-                    hit.t = double(tr);
-                    hit.boundary = b;
-                    hit.prim = 0;
-                    hit.slot = start + k;
-                    found = true;
+            haveCur = false;
+            if ((cur & 0x80000000u) == 0) {
+                NodeWords nd;
+                loadNode(sc.nodes, cur, nd);
+                ++nodeVisits;
+                T tEnter[8];
+                const uint32_t mask = intersectChildren(nd, inv, oinv, T(0), best, tEnter);
+                if (mask == 0) continue;
+                uint64_t keys[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const uint32_t meta = nodeByte(nd.b.z, nd.b.w, i);
+                    const uint32_t ref = (nd.a.w & (1u << (24 + i)))
+                                             ? nd.b.x + (meta & 7u)
+                                             : 0x80000000u | ((nd.b.y + (meta & 31u)) << 2) | ((meta >> 5) - 1u);
+                    // entry distances are >= 0: with the sign bit cleared (-0) their bits order like the values
+                    keys[i] = (mask & (1u << i))
+                                  ? (uint64_t(__float_as_uint(toFloatDown(tEnter[i])) & 0x7FFFFFFFu) << 32) | ref
+                                  : ~0ull;
                 }
-                if (AnyHit) {
-                    if (visits) *visits += nodeVisits;
-                    if (tests) *tests += primTests;
-                    return kTraceHit;
+                sort8(keys);
+                const int nHits = __popc(mask);
+                if (sp + nHits - 1 > Stack::kDepth) return kTraceOverflow;
+#pragma unroll
+                for (int j = 7; j >= 1; --j)
+                    if (j < nHits) {
+                        st.set(sp, {uint32_t(keys[j]), __uint_as_float(uint32_t(keys[j] >> 32))});
+                        ++sp;
+                    }
+                cur = uint32_t(keys[0]);
+                haveCur = true;
+            } else {
+                const uint32_t start = (cur & 0x7FFFFFFFu) >> 2, cnt = (cur & 3u) + 1u;
+                primTests += cnt;
+                for (uint32_t k = 0; k < cnt; ++k) {
+                    V3<T> v0, v1, v2;
+                    uint32_t b, prim, kind;
+                    TriFetch<T>::get(sc, start + k, v0, v1, v2, b, prim, kind);
+                    if (kind == kPrimTriangle) {
+                        const V3<T> a = v0 - q.o, bb = v1 - q.o, c = v2 - q.o;
+                        if (!lineCrossesTriangle(sh, a, bb, c)) continue;
+                        const V3<T> n = triangleNormal(v0, v1, v2);
+                        const T t = -dot(q.o - v0, n) / dot(q.d, n);
+                        if (!(t > T(0) && t < best)) continue;
+                        if (!acceptCrossing(sc, q, b, prim, true, t, n)) continue;
+                        best = t;
+                        hit.t = double(t);
+                        hit.boundary = b;
+                        hit.prim = prim;
+                        hit.slot = start + k;
+                        found = true;
+                    } else {
+                        Rr tr;
+                        if (!analyticCandidate<R, Rr, T>(sc, q, b, best, tr)) continue;
+                        best = T(tr);
+                        hit.t = double(tr);
+                        hit.boundary = b;
+                        hit.prim = 0;
+                        hit.slot = start + k;
+                        found = true;
+                    }
+                    if (AnyHit) return kTraceHit;
                 }
             }
         }
-        // cull deferred entries beyond the closest hit
-        while (sp > 0 && stack[(sp - 1) * stride].tEnter > toFloatUp(best)) --sp;
+        return kTraceRunning;
     }
-    if (visits) *visits += nodeVisits;
-    if (tests) *tests += primTests;
-    return found ? kTraceHit : kTraceMiss;
+};
+
+// A query that overflowed the short stack, from the start with the deep one. Out of line: its
+// stack lives in local memory and only these rare queries touch it.
+template <class T, class R, class Rr, bool AnyHit>
+__device__ __noinline__ int traceRayDeep(const DeviceScene& sc, const RayQuery<T>& q, HitRec& hit, uint32_t& visits,
+                                         uint32_t& tests) {
+    Traversal<T, R, Rr, AnyHit, LocalStack> tr;
+    tr.begin(q, nullptr, 0);
+    tr.hit = hit;
+    int s;
+    do {
+        s = tr.run(sc, 1 << 30);
+    } while (s == kTraceRunning);
+    hit = tr.hit;
+    visits += tr.nodeVisits;
+    tests += tr.primTests;
+    return s;
+}
+
+// The whole query in one call (cast rays, forward walks and the adjoint's replay).
+template <class T, class R, class Rr, bool AnyHit>
+__device__ __forceinline__ int traceRay(const DeviceScene& sc, const RayQuery<T>& q, StackEntry* stack, int stride, HitRec& hit,
+                                        uint32_t* visits = nullptr, uint32_t* tests = nullptr) {
+    Traversal<T, R, Rr, AnyHit> tr;
+    tr.begin(q, stack, stride);
+    tr.hit = hit;
+    int s;
+    do {
+        s = tr.run(sc, 1 << 30);
+    } while (s == kTraceRunning);
+    uint32_t nv = tr.nodeVisits, nt = tr.primTests;
+    if (s == kTraceOverflow) {
+        s = traceRayDeep<T, R, Rr, AnyHit>(sc, q, hit, nv, nt);
+    } else {
+        hit = tr.hit;
+    }
+    if (visits) *visits += nv;
+    if (tests) *tests += nt;
+    return s;
 }
 
 }  // namespace owec

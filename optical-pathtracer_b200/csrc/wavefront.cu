@@ -159,38 +159,97 @@ __global__ void __launch_bounds__(256) kGenerate(DeviceScene sc, PassParams pp, 
 }
 
 // ------------------------------------------------------------------ intersect
+// Visits a lane makes between two refills of its warp: small enough that a finished lane does not
+// idle long, large enough to amortise the refill's vote, atomic and ray load.
+#ifndef OWEC_REFILL_BUDGET
+#define OWEC_REFILL_BUDGET 8
+#endif
+constexpr int kRefillBudget = OWEC_REFILL_BUDGET;
+// Resident blocks per SM the traversal kernels are compiled for (a register cap of
+// 65536 / (128 x blocks) per thread).
+#if defined(OWEC_TRAVERSAL_MAXNREG)
+#define OWEC_TRAVERSAL_BOUNDS __maxnreg__(OWEC_TRAVERSAL_MAXNREG)
+#else
+#ifndef OWEC_TRAVERSAL_MIN_BLOCKS
+#define OWEC_TRAVERSAL_MIN_BLOCKS 3
+#endif
+#define OWEC_TRAVERSAL_BOUNDS __launch_bounds__(128, OWEC_TRAVERSAL_MIN_BLOCKS)
+#endif
+
+// Hands the warp's idle lanes the next queries of a queue of n through the fetch counter, one
+// atomic per warp. Returns this lane's query index (n or more: none). `exhausted` becomes true once
+// the counter has passed n, so that a drained warp stops fetching.
+__device__ __forceinline__ uint32_t refillLanes(bool idle, uint32_t* fetch, uint32_t n, bool& exhausted) {
+    const uint32_t need = __ballot_sync(0xFFFFFFFFu, idle);
+    if (need == 0 || exhausted) return n;
+    const uint32_t lane = threadIdx.x & 31u;
+    const int leader = __ffs(need) - 1;
+    uint32_t base = 0;
+    if (lane == uint32_t(leader)) base = atomicAdd(fetch, uint32_t(__popc(need)));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    if (base + uint32_t(__popc(need)) >= n) exhausted = true;
+    return idle ? base + uint32_t(__popc(need & ((1u << lane) - 1u))) : n;
+}
+
+// Adds a per-lane count to a counter, one atomic per warp (all lanes of the warp present).
+__device__ __forceinline__ void warpFlush(unsigned long long* counter, uint32_t v) {
+    const uint32_t sum = __reduce_add_sync(0xFFFFFFFFu, v);
+    if ((threadIdx.x & 31u) == 0 && sum) atomicAdd(counter, (unsigned long long)sum);
+}
+
+// Closest crossing of every active path's ray. Persistent: each lane advances its query a few
+// visits at a time and, when it ends, takes the next query of the queue, so that lanes whose rays
+// finish early do not idle until the warp's longest ray is done.
 template <int M>
-__global__ void __launch_bounds__(128) kIntersect(DeviceScene sc, PathBuffers<RT<M>> pb, Queues q, int cur,
-                                                  StatCounters* st) {
+__global__ void OWEC_TRAVERSAL_BOUNDS kIntersect(DeviceScene sc, PathBuffers<RT<M>> pb, Queues q, int cur,
+                                                  StatCounters* st, uint32_t* fetch) {
     using R = RT<M>;
     extern __shared__ StackEntry stackMem[];
     StackEntry* stack = stackMem + threadIdx.x;
     const uint32_t n = q.counts[cur];
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const uint32_t i = q.active[cur][k];
-        const PathRay<R> ray = pb.ray[i];
-        RayQuery<R> rq;
-        rq.od = rayOrigin(ray.o);
-        rq.o = V3<R>(rq.od);
-        rq.d = rayDir(ray);
-        rq.tmax = R(INFINITY);
-        rq.depB = ray.depB;
-        rq.depP = ray.depP;
-        rq.region = ray.region;
-        rq.errN = R(ray.errN);
-        HitRec h;
-        h.boundary = kNone;
-        h.t = INFINITY;
-        uint32_t nv = 0, nt = 0;
-        const int s = traceRay<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false>(sc, rq, stack, blockDim.x, h,
-                                                                                   &nv, &nt);
-        if (sc.travCounters) countTraversal(sc.travCounters, nv, nt);
-        if (s != kTraceHit) { h.boundary = kNone; h.t = INFINITY; }
-        if (s == kTraceOverflow) h.boundary = kNone - 1u;  // a fault: the path ends
-        pb.hit[i] = h;
-        warpCount(&st->segments, true);
-        warpCount(&st->faults, s == kTraceOverflow);
+    Traversal<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false> tr;
+    uint32_t path = 0, segments = 0, faults = 0;
+    bool alive = false, exhausted = false;
+    for (;;) {
+        const uint32_t k = refillLanes(!alive, fetch, n, exhausted);
+        if (!alive && k < n) {
+            path = q.active[cur][k];
+            const PathRay<R> ray = pb.ray[path];
+            RayQuery<R> rq;
+            rq.od = rayOrigin(ray.o);
+            rq.o = V3<R>(rq.od);
+            rq.d = rayDir(ray);
+            rq.tmax = R(INFINITY);
+            rq.depB = ray.depB;
+            rq.depP = ray.depP;
+            rq.region = ray.region;
+            rq.errN = R(ray.errN);
+            tr.begin(rq, stack, blockDim.x);
+            alive = true;
+        }
+        if (__ballot_sync(0xFFFFFFFFu, alive) == 0) break;
+        if (alive) {
+            int s = tr.run(sc, kRefillBudget);
+            if (s != kTraceRunning) {
+                HitRec h = tr.hit;
+                uint32_t nv = tr.nodeVisits, nt = tr.primTests;
+                if (s == kTraceOverflow) {
+                    h.boundary = kNone;
+                    h.t = INFINITY;
+                    s = traceRayDeep<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false>(sc, tr.q, h, nv, nt);
+                }
+                if (s != kTraceHit) { h.boundary = kNone; h.t = INFINITY; }
+                if (s == kTraceOverflow) h.boundary = kNone - 1u;  // a fault: the path ends
+                pb.hit[path] = h;
+                if (sc.travCounters) countTraversal(sc.travCounters, nv, nt);
+                ++segments;
+                faults += s == kTraceOverflow;
+                alive = false;
+            }
+        }
     }
+    warpFlush(&st->segments, segments);
+    warpFlush(&st->faults, faults);
 }
 
 // ------------------------------------------------------------------ next-event estimation
@@ -521,88 +580,141 @@ __global__ void __launch_bounds__(128) kSurface(DeviceScene sc, PassParams pp, P
 // The visibility of a next-event sample (Tracer::transmittance / connectionTransmittance,
 // transport.cpp:237-308): blocked by any matter other than null boundaries, attenuated by the
 // media it crosses, and it must arrive in the region on the light's emitting side (the ambient
-// region for the sun).
-template <int M>
-__global__ void __launch_bounds__(128) kShadow(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
-                                               StatCounters* st) {
+// region for the sun). AnyHit: the scene has no null boundaries, so the first crossing blocks.
+//
+// Persistent like kIntersect: a lane's job is one shadow ray, walked segment by segment through
+// null boundaries; its traversal advances a few visits per round and a finished lane takes the
+// next job.
+template <int M, bool AnyHit>
+__global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
+                                               StatCounters* st, uint32_t* fetch) {
     using R = RT<M>;
     using Ro = typename Mode<M>::Ro;
     using Rr = typename Mode<M>::Rr;
     extern __shared__ StackEntry stackMem[];
     StackEntry* stack = stackMem + threadIdx.x;
     const uint32_t n = q.counts[3];
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const ShadowRay<R> sr = pb.shadow[k];
-        const PathSpec<R> spc = pb.spec[sr.path];
-        R Tr[NW] = {R(1), R(1), R(1), R(1)};
-        bool clear = true;
-        bool fault = false;
+    Traversal<R, Ro, Rr, AnyHit> tr;
+    R Tr[NW];
+    double remaining = 0;
+    uint32_t job = 0, path = 0, region = 0, guard = 0, rays = 0, faults = 0;
+    float errN0 = 0.f;
+    bool alive = false, exhausted = false;
+    for (;;) {
+        const uint32_t k = refillLanes(!alive, fetch, n, exhausted);
+        bool begin = false;  // start a segment from rq
         RayQuery<R> rq;
-        rq.od = rayOrigin(sr.o);
-        rq.o = V3<R>(rq.od);
-        rq.d = V3<R>(sr.d[0], sr.d[1], sr.d[2]);
-        rq.depB = sr.depB;
-        rq.depP = sr.depP;
-        rq.region = sr.region;
-        rq.errN = R(sr.errN);
-        uint32_t region = sr.region;
-        double remaining = sr.tmax;
-        const bool finite = !isinf(sr.tmax);
-        for (int guard = 0; guard < 256 && clear; ++guard) {
-            // stop short of the light's own surface
-            const double tq = finite ? remaining - (4e-6 * remaining + double(sr.errN) + 1e-9) : INFINITY;
-            if (finite && tq <= 0) break;
-            rq.tmax = R(tq);
-            rq.region = region;
-            HitRec h;
-            h.boundary = kNone;
-            uint32_t nv = 0, nt = 0;
-            const int s = pp.anyHitShadows
-                              ? traceRay<R, Ro, Rr, true>(sc, rq, stack, blockDim.x, h, &nv, &nt)
-                              : traceRay<R, Ro, Rr, false>(sc, rq, stack, blockDim.x, h, &nv, &nt);
+        if (!alive && k < n) {
+            const ShadowRay<R> sr = pb.shadow[k];
+            job = k;
+            path = sr.path;
+            for (int j = 0; j < NW; ++j) Tr[j] = R(1);
+            region = sr.region;
+            remaining = sr.tmax;
+            guard = 0;
+            errN0 = sr.errN;
+            rq.od = rayOrigin(sr.o);
+            rq.o = V3<R>(rq.od);
+            rq.d = V3<R>(sr.d[0], sr.d[1], sr.d[2]);
+            rq.depB = sr.depB;
+            rq.depP = sr.depP;
+            rq.errN = R(sr.errN);
+            alive = true;
+            begin = true;
+        }
+        if (__ballot_sync(0xFFFFFFFFu, alive) == 0) break;
+        if (!alive) continue;
+        const bool finite = !isinf(remaining);
+        int outcome = 0;  // 1 clear, 2 blocked, 3 fault
+        if (!begin) {
+            int s = tr.run(sc, kRefillBudget);
+            if (s == kTraceRunning) continue;
+            HitRec h = tr.hit;
+            uint32_t nv = tr.nodeVisits, nt = tr.primTests;
+            if (s == kTraceOverflow) {
+                h.boundary = kNone;
+                s = traceRayDeep<R, Ro, Rr, AnyHit>(sc, tr.q, h, nv, nt);
+            }
             if (sc.travCounters) countTraversal(sc.travCounters + 3, nv, nt);
-            if (s == kTraceOverflow) { fault = true; clear = false; break; }
-            const bool found = s == kTraceHit;
-            const double seg = found ? fmin(h.t, remaining) : remaining;
-            const owec_medium med = sc.media[sc.regionMedium[region]];
-            if (mediumAbsorbs(med, sc) || mediumScatters(med, sc)) {
-                if (isinf(seg)) { clear = false; break; }
-                for (int j = 0; j < NW; ++j) {
-                    const R lam = R(spc.lambda[j]);
-                    Tr[j] *= exp(-(evalSpectrum(sc, med.absorption, lam) + evalSpectrum(sc, med.scattering, lam)) * R(seg));
+            ++guard;
+            if (s == kTraceOverflow) {
+                outcome = 3;
+            } else {
+                const bool found = s == kTraceHit;
+                const double seg = found ? fmin(h.t, remaining) : remaining;
+                const owec_medium med = sc.media[sc.regionMedium[region]];
+                if (mediumAbsorbs(med, sc) || mediumScatters(med, sc)) {
+                    if (isinf(seg)) {
+                        outcome = 2;
+                    } else {
+                        for (int j = 0; j < NW; ++j) {
+                            const R lam = R(pb.spec[path].lambda[j]);
+                            Tr[j] *= exp(-(evalSpectrum(sc, med.absorption, lam) + evalSpectrum(sc, med.scattering, lam)) *
+                                         R(seg));
+                        }
+                    }
+                }
+                if (outcome == 0) {
+                    if (!found) {
+                        outcome = (!finite && region != 0) ? 2 : 1;
+                    } else if (AnyHit) {
+                        outcome = 2;
+                    } else {
+                        const DBoundary bd = sc.boundaries[h.boundary];
+                        if (sc.optics[bd.optics].type != OWEC_SURF_NULL) {
+                            outcome = 2;
+                        } else {
+                            // pass the null boundary, if met from this region
+                            PathRay<R> tmp;
+                            tmp.o[0] = tr.q.od.x; tmp.o[1] = tr.q.od.y; tmp.o[2] = tr.q.od.z;
+                            tmp.d[0] = tr.q.d.x; tmp.d[1] = tr.q.d.y; tmp.d[2] = tr.q.d.z;
+                            const SurfacePoint<R> gp = hitGeometry<R, Ro, Rr>(sc, tmp, h);
+                            const bool ff = dot(tr.q.d, gp.n) < R(0);
+                            if ((ff ? bd.front : bd.back) != region) {
+                                outcome = 2;
+                            } else {
+                                region = ff ? bd.back : bd.front;
+                                rq = tr.q;
+                                rq.od = gp.p;
+                                if (Mode<M>::plainOrigin) rq.od = V3<double>(V3<float>(gp.p));
+                                rq.o = V3<R>(rq.od);
+                                rq.depB = h.boundary;
+                                rq.depP = h.prim;
+                                rq.errN = R(anchorError<R>(gp.p));
+                                if (finite) remaining -= h.t;
+                                begin = true;
+                            }
+                        }
+                    }
                 }
             }
-            if (!found) {
-                if (!finite && region != 0) clear = false;
-                break;
+        }
+        if (begin) {
+            // the next segment, stopping short of the light's own surface
+            const double tq = finite ? remaining - (4e-6 * remaining + double(errN0) + 1e-9) : INFINITY;
+            if (guard >= 256 || (finite && tq <= 0)) {
+                outcome = 1;
+            } else {
+                rq.tmax = R(tq);
+                rq.region = region;
+                tr.begin(rq, stack, blockDim.x);
             }
-            if (pp.anyHitShadows) { clear = false; break; }
-            const DBoundary bd = sc.boundaries[h.boundary];
-            if (sc.optics[bd.optics].type != OWEC_SURF_NULL) { clear = false; break; }
-            // pass the null boundary, if met from this region
-            PathRay<R> tmp;
-            tmp.o[0] = rq.od.x; tmp.o[1] = rq.od.y; tmp.o[2] = rq.od.z;
-            tmp.d[0] = rq.d.x; tmp.d[1] = rq.d.y; tmp.d[2] = rq.d.z;
-            const SurfacePoint<R> gp = hitGeometry<R, Ro, Rr>(sc, tmp, h);
-            const bool ff = dot(rq.d, gp.n) < R(0);
-            if ((ff ? bd.front : bd.back) != region) { clear = false; break; }
-            region = ff ? bd.back : bd.front;
-            rq.od = gp.p;
-            if (Mode<M>::plainOrigin) rq.od = V3<double>(V3<float>(gp.p));
-            rq.o = V3<R>(rq.od);
-            rq.depB = h.boundary;
-            rq.depP = h.prim;
-            rq.errN = R(anchorError<R>(gp.p));
-            if (finite) remaining -= h.t;
         }
-        if (clear && finite && region != sr.endRegion) clear = false;
-        if (clear) {
-            float* L = pb.spec[sr.path].L;
-            for (int j = 0; j < NW; ++j) L[j] += float(R(sr.contrib[j]) * Tr[j]);
+        if (outcome != 0) {
+            bool clear = outcome == 1;
+            const ShadowRay<R>& sr = pb.shadow[job];
+            if (clear && finite && region != sr.endRegion) clear = false;
+            if (clear) {
+                float* L = pb.spec[path].L;
+                for (int j = 0; j < NW; ++j) L[j] += float(R(sr.contrib[j]) * Tr[j]);
+            }
+            ++rays;
+            faults += outcome == 3;
+            alive = false;
         }
-        warpCount(&st->shadowRays, true);
-        warpCount(&st->faults, fault);
     }
+    warpFlush(&st->shadowRays, rays);
+    warpFlush(&st->faults, faults);
 }
 
 // ------------------------------------------------------------------ film
@@ -726,6 +838,15 @@ __global__ void kMaterialize(const uint32_t* leafOrder, uint32_t n, const float4
     }
 }
 
+// Per-pixel mean XYZ of the film (Renderer::resolve): the compensated sums over the sample count.
+__global__ void __launch_bounds__(256) kResolve(const double* film, const double* comp, const double* samples, uint32_t nPixels,
+                                                double* xyz) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 3 * nPixels) return;
+    const double n = samples[i / 3];
+    xyz[i] = n > 0 ? (film[i] - comp[i]) * (1.0 / n) : 0.0;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ launchers
@@ -738,8 +859,8 @@ void launchGenerate(const DeviceScene& sc, const PassParams& pp, const PathBuffe
 }
 template <int M>
 void launchIntersect(const DeviceScene& sc, const PathBuffers<RT<M>>& pb, const Queues& q, int cur, StatCounters* st,
-                     int grid, cudaStream_t s) {
-    kIntersect<M><<<grid, 128, traversalSharedBytes(128), s>>>(sc, pb, q, cur, st);
+                     uint32_t* fetch, int grid, cudaStream_t s) {
+    kIntersect<M><<<grid, 128, traversalSharedBytes(128), s>>>(sc, pb, q, cur, st, fetch);
 }
 template <int M>
 void launchMedium(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q, int cur,
@@ -753,8 +874,11 @@ void launchSurface(const DeviceScene& sc, const PassParams& pp, const PathBuffer
 }
 template <int M>
 void launchShadow(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q,
-                  StatCounters* st, int grid, cudaStream_t s) {
-    kShadow<M><<<grid, 128, traversalSharedBytes(128), s>>>(sc, pp, pb, q, st);
+                  StatCounters* st, uint32_t* fetch, int grid, cudaStream_t s) {
+    if (pp.anyHitShadows)
+        kShadow<M, true><<<grid, 128, traversalSharedBytes(128), s>>>(sc, pp, pb, q, st, fetch);
+    else
+        kShadow<M, false><<<grid, 128, traversalSharedBytes(128), s>>>(sc, pp, pb, q, st, fetch);
 }
 template <int M>
 void launchFilm(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, double* film, double* comp,
@@ -769,6 +893,10 @@ void launchCastRays(const DeviceScene& sc, uint64_t n, const double* o, const do
 void launchCastRaysF(const DeviceScene& sc, uint64_t n, const float* o, const float* d, uint32_t* b, uint32_t* p,
                      float* t, int grid, cudaStream_t s) {
     kCastRaysF<<<grid, 128, traversalSharedBytes(128), s>>>(sc, n, o, d, b, p, t);
+}
+void launchResolve(const double* film, const double* comp, const double* samples, uint32_t nPixels, double* xyz,
+                   cudaStream_t s) {
+    kResolve<<<(3 * nPixels + 255) / 256, 256, 0, s>>>(film, comp, samples, nPixels, xyz);
 }
 void launchMaterialize(const uint32_t* leafOrder, uint32_t n, const float4* tri, const double* tri64, PrimRec* prims,
                        PrimRec64* prims64, cudaStream_t s) {
@@ -785,13 +913,13 @@ void configureKernels() {
     template void launchGenerate<M>(const DeviceScene&, const PassParams&, const PathBuffers<RT<M>>&, const Queues&, \
                                     StatCounters*, cudaStream_t);                                                   \
     template void launchIntersect<M>(const DeviceScene&, const PathBuffers<RT<M>>&, const Queues&, int,             \
-                                     StatCounters*, int, cudaStream_t);                                             \
+                                     StatCounters*, uint32_t*, int, cudaStream_t);                                             \
     template void launchMedium<M>(const DeviceScene&, const PassParams&, const PathBuffers<RT<M>>&, const Queues&,   \
                                   int, StatCounters*, int, cudaStream_t);                                           \
     template void launchSurface<M>(const DeviceScene&, const PassParams&, const PathBuffers<RT<M>>&, const Queues&,  \
                                    int, StatCounters*, int, cudaStream_t);                                          \
     template void launchShadow<M>(const DeviceScene&, const PassParams&, const PathBuffers<RT<M>>&, const Queues&,   \
-                                  StatCounters*, int, cudaStream_t);                                                \
+                                  StatCounters*, uint32_t*, int, cudaStream_t);                                                \
     template void launchFilm<M>(const DeviceScene&, const PassParams&, const PathBuffers<RT<M>>&, double*, double*,  \
                                 double*, uint32_t, cudaStream_t);                                                   \
     template void launchCastRays<M>(const DeviceScene&, uint64_t, const double*, const double*, uint32_t*,          \

@@ -17,8 +17,8 @@ template <int M>
 void launchGenerate(const DeviceScene&, const PassParams&, const PathBuffers<ModeR<M>>&, const Queues&, StatCounters*,
                     cudaStream_t);
 template <int M>
-void launchIntersect(const DeviceScene&, const PathBuffers<ModeR<M>>&, const Queues&, int cur, StatCounters*, int grid,
-                     cudaStream_t);
+void launchIntersect(const DeviceScene&, const PathBuffers<ModeR<M>>&, const Queues&, int cur, StatCounters*,
+                     uint32_t* fetch, int grid, cudaStream_t);
 template <int M>
 void launchMedium(const DeviceScene&, const PassParams&, const PathBuffers<ModeR<M>>&, const Queues&, int cur,
                   StatCounters*, int grid, cudaStream_t);
@@ -27,7 +27,9 @@ void launchSurface(const DeviceScene&, const PassParams&, const PathBuffers<Mode
                    StatCounters*, int grid, cudaStream_t);
 template <int M>
 void launchShadow(const DeviceScene&, const PassParams&, const PathBuffers<ModeR<M>>&, const Queues&, StatCounters*,
-                  int grid, cudaStream_t);
+                  uint32_t* fetch, int grid, cudaStream_t);
+void launchResolve(const double* film, const double* comp, const double* samples, uint32_t nPixels, double* xyz,
+                   cudaStream_t);
 template <int M>
 void launchFilm(const DeviceScene&, const PassParams&, const PathBuffers<ModeR<M>>&, double* film, double* comp,
                 double* samples, uint32_t spp, cudaStream_t);

@@ -70,13 +70,14 @@ class Context:
     def run_pass(self, spp):
         _check(self.lib, self.lib.owec_pass(self.handle, int(spp)), "owec_pass")
 
-    def resolve(self):
+    def resolve(self, samples=True):
+        """(per-pixel mean XYZ (height, width, 3), per-pixel sample counts or None)."""
         n = self.width * self.height
-        xyz = np.zeros(3 * n)
-        samples = np.zeros(n)
+        xyz = np.empty(3 * n)
+        cnt = np.empty(n) if samples else None
         _check(self.lib, self.lib.owec_resolve(self.handle, xyz.ctypes.data_as(A.c_double_p),
-                                               samples.ctypes.data_as(A.c_double_p)), "owec_resolve")
-        return xyz.reshape(self.height, self.width, 3), samples.reshape(self.height, self.width)
+                                               cnt.ctypes.data_as(A.c_double_p) if samples else None), "owec_resolve")
+        return xyz.reshape(self.height, self.width, 3), (cnt.reshape(self.height, self.width) if samples else None)
 
     def reset_film(self):
         _check(self.lib, self.lib.owec_reset_film(self.handle), "owec_reset_film")
@@ -183,7 +184,7 @@ class Renderer:
 
     def resolve(self):
         """Per-pixel mean XYZ, shape (height, width, 3)."""
-        return self.ctx.resolve()[0]
+        return self.ctx.resolve(samples=False)[0]
 
     def passes(self):
         return self._passes

@@ -10,7 +10,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libowec.so")
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK = 0
 E_INVALID, E_CUDA, E_NOMEM, E_STATE, E_DEVICE_FAULT, E_UNSUPPORTED = -1, -2, -3, -4, -5, -6
@@ -91,7 +91,9 @@ class SceneDesc(ctypes.Structure):
                 ("optics", ctypes.POINTER(Optics)), ("emissions", ctypes.POINTER(Emission)),
                 ("boundaries", ctypes.POINTER(Boundary)), ("meshes", ctypes.POINTER(Mesh)),
                 ("vertices", c_double_p), ("triangles", c_u32_p),
-                ("env", Environment), ("detector", Detector)]
+                ("env", Environment), ("detector", Detector),
+                ("frame_origin_set", ctypes.c_int32), ("pad0", ctypes.c_int32),
+                ("frame_origin", ctypes.c_double * 3)]
 
 
 class Settings(ctypes.Structure):

@@ -178,6 +178,11 @@ class SceneBuilder:
                                    (ctypes.c_double * 3)(*look_at), (ctypes.c_double * 3)(*up),
                                    math.radians(fov_y_deg), float(pixel_sigma), 0, 0, 0.0, 0.0)
 
+    def frame_origin(self, point):
+        """Put the origin of the device's camera-relative FP32 frame at `point` (default: the
+        observer's position)."""
+        self.origin = tuple(float(x) for x in point)
+
     def sensor(self, width, height, boundary, half_x, half_y, pixel_sigma=0.0):
         self.detector = A.Detector(A.DETECTOR_SENSOR, width, height, A.REGION_OUTSIDE, (ctypes.c_double * 3)(),
                                    (ctypes.c_double * 3)(), (ctypes.c_double * 3)(), 0.0, float(pixel_sigma),
@@ -206,6 +211,9 @@ class SceneBuilder:
         }
         d = A.SceneDesc()
         d.abi_version = A.ABI_VERSION
+        if getattr(self, "origin", None) is not None:
+            d.frame_origin_set = 1
+            d.frame_origin = (ctypes.c_double * 3)(*self.origin)
         d.n_spectra, d.n_media, d.n_regions = len(self.spectra), len(self.media), len(self.region_medium)
         d.n_optics, d.n_emissions, d.n_boundaries = len(self.optics), len(self.emissions), len(self.boundaries)
         d.n_meshes, d.n_spectrum_table = len(self.meshes), len(self.table) // 2
@@ -537,6 +545,7 @@ def caustic_slab_scene(n=256, heights=None, wall_bins=512, wall_half=0.075, size
     wall = sb.boundary(A.SHAPE_PLANE, [A.APERTURE_RECT, 0.5, 0.5], pose(rotate_to((0, 0, 1), (0, 0, -1)), (0, 0, wall_z)),
                        0, 0, sb.diffuse(0.8))
     sb.observer(8, 8, (0.0, 0.0, -1.0), (0, 0, 0), fov_y_deg=10.0)
+    sb.frame_origin((0.0, 0.0, thickness))  # FP32 precision where the heights are
     info = {"heightfield": hf, "wall": wall, "n": n, "half": half, "thickness": thickness, "wall_half": wall_half,
             "bins": wall_bins, "wall_z": wall_z}
     return sb, info

@@ -82,7 +82,7 @@ def test_white_furnace_closed_diffuse_sphere(rho):
     img = r.resolve()
     assert abs(img[:, :, 1].mean() - 1 / (1 - rho)) < 0.01 / (1 - rho)
     st = r.stats()
-    assert st["leaks"] == 0 and st["device_faults"] == 0
+    assert st["leaks"] == 0 and st["device_faults"] == 0, st
     r.close()
 
 
