@@ -1,11 +1,15 @@
 // Closest-hit and any-hit traversal of the 8-wide quantised BVH.
 //
-// One thread follows one ray. Node records (80 B) are read with five 128-bit read-only loads;
-// the eight child boxes are decoded from 8-bit offsets against the node's origin and power-of-two
-// scales and slab-tested together; the hits are ordered near-first and pushed on a short per-thread
-// stack staged in shared memory (transposed so that a warp's entries of one level are consecutive
-// words). Deferred entries whose entry distance lies beyond the closest hit found since are culled
-// on pop, as the reference's Bvh::traverseSlots does (src/owe/scene/bvh.hpp:39-78).
+// One thread follows one ray. Node records (80 B) are read with five 128-bit read-only loads; the
+// eight child boxes are decoded from 8-bit offsets against the node's origin and power-of-two
+// scales and slab-tested together. The hits are not sorted: the builder placed each child in the
+// slot of the octant it lies towards, so visiting the hit slots in the order slot ^ (ray octant
+// ^ 7) meets them roughly near to far (Ylitie, Karras and Laine, HPG 2017). A visited node leaves
+// two groups behind: its hit leaf primitives (a 24-bit mask over the node's primitive range),
+// tested first, and its hit inner children (an 8-bit mask in visiting order), of which one is
+// entered and the rest go on the stack as one 8-byte entry. The stack therefore grows by at most
+// one entry per level. Crossings beyond the closest found so far are cut by the box tests, as
+// the reference's Bvh::traverseSlots cuts them (src/owe/scene/bvh.hpp:39-78).
 //
 // Which crossings count near a ray's departure follows the reference's contact rule
 // (src/owe/scene/world.cpp:451-513): the face the ray left never does, and within the anchor's
@@ -16,15 +20,16 @@
 
 namespace owec {
 
-constexpr int kStackDepth = 32;  // entries per thread in shared memory
-constexpr int kDeepStackDepth = 112;  // the rare query that needs more is traversed again with a stack
-                                      // of this depth in local memory (7 per level: 16 levels); an
-                                      // overflow beyond it ends the query and is counted
-constexpr uint32_t kMaxTraversalSteps = 1u << 20;  // a bound on stack pops: a malformed tree cannot hang
+constexpr int kStackDepth = 32;      // group entries per thread in shared memory: one per level
+constexpr int kDeepStackDepth = 96;  // the rare query of a deeper tree is traversed again with a stack
+                                     // of this depth in local memory; beyond it the query ends and is
+                                     // counted as a fault
+constexpr uint32_t kMaxTraversalSteps = 1u << 20;  // a bound on visits: a malformed tree cannot hang
 
+// A deferred node group: the inner children of one node still to be visited.
 struct StackEntry {
-    uint32_t ref;   // bit 31: leaf; leaf: prim start << 2 | (count - 1); inner: node index
-    float tEnter;
+    uint32_t base;  // node index of the node's first inner child (child_base)
+    uint32_t bits;  // bits 0-7: hit children left, by visiting position; bits 8-15: the node's inner-slot mask
 };
 
 // The short traversal stack: this thread's column of the block's shared-memory stack (stride =
@@ -35,7 +40,6 @@ struct SharedStack {
     int stride;
     __device__ __forceinline__ void init(StackEntry* stack, int s) { sh = stack; stride = s; }
     __device__ __forceinline__ StackEntry get(int i) const { return sh[i * stride]; }
-    __device__ __forceinline__ float tEnter(int i) const { return sh[i * stride].tEnter; }
     __device__ __forceinline__ void set(int i, const StackEntry& e) { sh[i * stride] = e; }
 };
 // The deep stack, in local memory, for the queries that overflow the short one.
@@ -44,7 +48,6 @@ struct LocalStack {
     StackEntry e[kDeepStackDepth];
     __device__ __forceinline__ void init(StackEntry*, int) {}
     __device__ __forceinline__ StackEntry get(int i) const { return e[i]; }
-    __device__ __forceinline__ float tEnter(int i) const { return e[i].tEnter; }
     __device__ __forceinline__ void set(int i, const StackEntry& x) { e[i] = x; }
 };
 
@@ -86,13 +89,6 @@ template <class T> __device__ __forceinline__ T farWiden();
 template <> __device__ __forceinline__ float farWiden<float>() { return 1.0000004f; }
 template <> __device__ __forceinline__ double farWiden<double>() { return 1.0 + 4e-16; }
 
-// Entry distances on the stack are FP32: rounded down when stored, compared with the closest hit
-// rounded up, so an FP64 query never culls an entry it must visit.
-__device__ __forceinline__ float toFloatDown(float x) { return x; }
-__device__ __forceinline__ float toFloatDown(double x) { return __double2float_rd(x); }
-__device__ __forceinline__ float toFloatUp(float x) { return x; }
-__device__ __forceinline__ float toFloatUp(double x) { return __double2float_ru(x); }
-
 // The analytic boundary b's first acceptable crossing in (0, best); FP64 refinement when Rr = double.
 template <class R, class Rr, class T>
 __device__ __forceinline__ bool analyticCandidate(const DeviceScene& sc, const RayQuery<T>& q, uint32_t b, T best, Rr& tOut) {
@@ -116,6 +112,32 @@ __device__ __forceinline__ bool analyticCandidate(const DeviceScene& sc, const R
         return true;
     }
     return false;
+}
+
+// analyticCandidate out of line: the FP64 refinement of every analytic shape needs many registers,
+// and inlined it would set the register count of the whole traversal loop. Arguments and result go
+// by value, so that nothing of the caller's has to live in memory for the call.
+template <class Rr>
+struct AnalyticResult {
+    Rr t;
+    bool ok;
+};
+template <class T, class R, class Rr>
+__device__ __noinline__ AnalyticResult<Rr> analyticHit(const DeviceScene& sc, uint32_t b, V3<double> od, V3<T> d, T best,
+                                                        uint32_t depB, uint32_t region, T errN) {
+    RayQuery<T> q;
+    q.od = od;
+    q.o = V3<T>(od);
+    q.d = d;
+    q.tmax = best;
+    q.depB = depB;
+    q.depP = kNone;
+    q.region = region;
+    q.errN = errN;
+    AnalyticResult<Rr> r;
+    r.t = Rr(0);
+    r.ok = analyticCandidate<R, Rr, T>(sc, q, b, best, r.t);
+    return r;
 }
 
 // A wide node as the five 128-bit words it is loaded in (the WideNode layout of device_scene.cuh):
@@ -153,10 +175,9 @@ __device__ __forceinline__ uint32_t nodeByte(uint32_t lo, uint32_t hi, int i) {
     return ((i < 4 ? lo : hi) >> (8 * (i & 3))) & 0xFFu;
 }
 
-// Decoded child boxes of a node, slab-tested against the ray. Returns the hit mask and fills tEnter.
+// Decoded child boxes of a node, slab-tested against the ray. Returns the hit mask (slot order).
 template <class T>
-__device__ __forceinline__ uint32_t intersectChildren(const NodeWords& nd, const V3<T>& inv, const V3<T>& oinv, T tmin, T tmax,
-                                   T tEnter[8]) {
+__device__ __forceinline__ uint32_t intersectChildren(const NodeWords& nd, const V3<T>& inv, const V3<T>& oinv, T tmin, T tmax) {
     const T sx = T(__uint_as_float((nd.a.w & 0xFFu) << 23));
     const T sy = T(__uint_as_float(((nd.a.w >> 8) & 0xFFu) << 23));
     const T sz = T(__uint_as_float(((nd.a.w >> 16) & 0xFFu) << 23));
@@ -187,10 +208,7 @@ __device__ __forceinline__ uint32_t intersectChildren(const NodeWords& nd, const
         const T te = fmax(fmax(t0x, t0y), fmax(t0z, tmin));
         const T tx = fmin(fmin(t1x, t1y), t1z) * farWiden<T>();
         const T tl = fmin(tx, tmax);
-        if (te <= tl) {
-            mask |= 1u << i;
-            tEnter[i] = te;
-        }
+        if (te <= tl) mask |= 1u << i;
     }
     return mask;
 }
@@ -238,29 +256,17 @@ enum TraceStatus : int { kTraceMiss = 0, kTraceHit = 1, kTraceOverflow = 2 };
 
 constexpr int kTraceRunning = 3;  // Traversal::run: the query is not finished yet
 
-// Sorts eight 64-bit keys ascending with a fixed network of compare-exchanges (Batcher's
-// odd-even merge sort, 19 comparators): branch-free in registers.
-__device__ __forceinline__ void cswap(uint64_t& a, uint64_t& b) {
-    const uint64_t lo = a < b ? a : b, hi = a < b ? b : a;
-    a = lo;
-    b = hi;
-}
-__device__ __forceinline__ void sort8(uint64_t k[8]) {
-    cswap(k[0], k[1]); cswap(k[2], k[3]); cswap(k[4], k[5]); cswap(k[6], k[7]);
-    cswap(k[0], k[2]); cswap(k[1], k[3]); cswap(k[4], k[6]); cswap(k[5], k[7]);
-    cswap(k[1], k[2]); cswap(k[5], k[6]);
-    cswap(k[0], k[4]); cswap(k[1], k[5]); cswap(k[2], k[6]); cswap(k[3], k[7]);
-    cswap(k[2], k[4]); cswap(k[3], k[5]);
-    cswap(k[1], k[2]); cswap(k[3], k[4]); cswap(k[5], k[6]);
+// Moves bit s of an 8-bit mask to bit s ^ x: slot order to visiting order and back.
+__device__ __forceinline__ uint32_t permuteSlots(uint32_t m, uint32_t x) {
+    m = (x & 1u) ? (((m & 0x55u) << 1) | ((m >> 1) & 0x55u)) : m;
+    m = (x & 2u) ? (((m & 0x33u) << 2) | ((m >> 2) & 0x33u)) : m;
+    m = (x & 4u) ? (((m & 0x0Fu) << 4) | ((m >> 4) & 0x0Fu)) : m;
+    return m;
 }
 
 // Closest (AnyHit = false) or first (AnyHit = true) acceptable crossing in (0, q.tmax), as a state
 // machine that a persistent kernel can advance a few visits at a time and then hand the thread a
 // new query when this one ends. R / Rr: precision of analytic roots and of their refinement.
-//
-// At an inner node the hit children become 64-bit keys (entry distance, rounded down to FP32, over
-// the child reference) sorted by a fixed network; all but the nearest are pushed far to near and
-// the traversal continues into the nearest without a round trip through the stack.
 template <class T, class R, class Rr, bool AnyHit, class Stack = SharedStack>
 struct Traversal {
     RayQuery<T> q;
@@ -269,9 +275,12 @@ struct Traversal {
     T best;
     HitRec hit;           // written when a crossing is accepted
     Stack st;
-    uint32_t cur, steps, nodeVisits, primTests;
+    uint32_t nodeBase, nodeBits;  // the current node group (as a stack entry)
+    uint32_t primBase, primBits;  // the current primitive group: primBase + bit, 24 bits
+    uint32_t first;               // the slot visited first: the octant opposite the ray's
+    uint32_t steps, nodeVisits, primTests;
     int sp;
-    bool haveCur, found;
+    bool found;
 
     // `stack` is this thread's column of the block's shared-memory stack (stride = block size).
     __device__ __forceinline__ void begin(const RayQuery<T>& query, StackEntry* stack, int stride) {
@@ -284,108 +293,116 @@ struct Traversal {
         sp = 0;
         st.init(stack, stride);
         nodeVisits = primTests = 0;
-        cur = 0;  // the root
-        haveCur = true;
         steps = 0;
+        // bit k set: the ray runs towards +k, so it meets the children on the negative side first
+        first = ((q.d.x < T(0)) ? 0u : 1u) | ((q.d.y < T(0)) ? 0u : 2u) | ((q.d.z < T(0)) ? 0u : 4u);
+        // the root as a group of one: position 0, an inner slot of rank 0
+        nodeBase = 0;
+        nodeBits = 1u | (1u << (8 + first));
+        primBase = 0;
+        primBits = 0;
     }
 
-    // Advances by at most `budget` node or leaf visits: kTraceRunning, or the query's TraceStatus.
+    // Advances by at most `budget` node or primitive visits: kTraceRunning, or the query's TraceStatus.
     __device__ __forceinline__ int run(const DeviceScene& sc, int budget) {
+        if (sc.nNodes == 0) return kTraceMiss;
         for (int it = 0; it < budget; ++it) {
             if (++steps > kMaxTraversalSteps) return kTraceOverflow;
-            if (!haveCur) {
-                // pop, culling deferred entries beyond the closest hit found since
-                const float bestUp = toFloatUp(best);
-                while (sp > 0 && st.tEnter(sp - 1) > bestUp) --sp;
+            if (primBits) {
+                const uint32_t b = uint32_t(__ffs(primBits) - 1);
+                primBits &= primBits - 1u;
+                ++primTests;
+                if (testPrim(sc, primBase + b) && AnyHit) return kTraceHit;
+                continue;
+            }
+            if ((nodeBits & 0xFFu) == 0) {
                 if (sp == 0) return found ? kTraceHit : kTraceMiss;
                 --sp;
-                cur = st.get(sp).ref;
+                const StackEntry e = st.get(sp);
+                nodeBase = e.base;
+                nodeBits = e.bits;
             }
-            haveCur = false;
-            if ((cur & 0x80000000u) == 0) {
-                NodeWords nd;
-                loadNode(sc.nodes, cur, nd);
-                ++nodeVisits;
-                T tEnter[8];
-                const uint32_t mask = intersectChildren(nd, inv, oinv, T(0), best, tEnter);
-                if (mask == 0) continue;
-                uint64_t keys[8];
-#pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    const uint32_t meta = nodeByte(nd.b.z, nd.b.w, i);
-                    const uint32_t ref = (nd.a.w & (1u << (24 + i)))
-                                             ? nd.b.x + (meta & 7u)
-                                             : 0x80000000u | ((nd.b.y + (meta & 31u)) << 2) | ((meta >> 5) - 1u);
-                    // entry distances are >= 0: with the sign bit cleared (-0) their bits order like the values
-                    keys[i] = (mask & (1u << i))
-                                  ? (uint64_t(__float_as_uint(toFloatDown(tEnter[i])) & 0x7FFFFFFFu) << 32) | ref
-                                  : ~0ull;
-                }
-                sort8(keys);
-                const int nHits = __popc(mask);
-                if (sp + nHits - 1 > Stack::kDepth) return kTraceOverflow;
-#pragma unroll
-                for (int j = 7; j >= 1; --j)
-                    if (j < nHits) {
-                        st.set(sp, {uint32_t(keys[j]), __uint_as_float(uint32_t(keys[j] >> 32))});
-                        ++sp;
-                    }
-                cur = uint32_t(keys[0]);
-                haveCur = true;
-            } else {
-                const uint32_t start = (cur & 0x7FFFFFFFu) >> 2, cnt = (cur & 3u) + 1u;
-                primTests += cnt;
-                for (uint32_t k = 0; k < cnt; ++k) {
-                    V3<T> v0, v1, v2;
-                    uint32_t b, prim, kind;
-                    TriFetch<T>::get(sc, start + k, v0, v1, v2, b, prim, kind);
-                    if (kind == kPrimTriangle) {
-                        const V3<T> a = v0 - q.o, bb = v1 - q.o, c = v2 - q.o;
-                        if (!lineCrossesTriangle(sh, a, bb, c)) continue;
-                        const V3<T> n = triangleNormal(v0, v1, v2);
-                        const T t = -dot(q.o - v0, n) / dot(q.d, n);
-                        if (!(t > T(0) && t < best)) continue;
-                        if (!acceptCrossing(sc, q, b, prim, true, t, n)) continue;
-                        best = t;
-                        hit.t = double(t);
-                        hit.boundary = b;
-                        hit.prim = prim;
-                        hit.slot = start + k;
-                        found = true;
-                    } else {
-                        Rr tr;
-                        if (!analyticCandidate<R, Rr, T>(sc, q, b, best, tr)) continue;
-                        best = T(tr);
-                        hit.t = double(tr);
-                        hit.boundary = b;
-                        hit.prim = 0;
-                        hit.slot = start + k;
-                        found = true;
-                    }
-                    if (AnyHit) return kTraceHit;
-                }
+            // the group's next child in visiting order; the rest of the group waits on the stack
+            const uint32_t pos = uint32_t(__ffs(nodeBits & 0xFFu) - 1);
+            nodeBits &= ~(1u << pos);
+            const uint32_t slot = pos ^ first;
+            const uint32_t node = nodeBase + uint32_t(__popc((nodeBits >> 8) & ((1u << slot) - 1u)));
+            if (nodeBits & 0xFFu) {
+                if (sp >= Stack::kDepth) return kTraceOverflow;
+                st.set(sp, {nodeBase, nodeBits});
+                ++sp;
             }
+            NodeWords nd;
+            loadNode(sc.nodes, node, nd);
+            ++nodeVisits;
+            const uint32_t mask = intersectChildren(nd, inv, oinv, T(0), best);
+            const uint32_t inner = nd.a.w >> 24;
+            nodeBase = nd.b.x;
+            nodeBits = permuteSlots(mask & inner, first) | (inner << 8);
+            primBase = nd.b.y;
+            uint32_t pb = 0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const uint32_t meta = nodeByte(nd.b.z, nd.b.w, i);
+                pb |= (mask & ~inner & (1u << i)) ? ((1u << (meta >> 5)) - 1u) << (meta & 31u) : 0u;
+            }
+            primBits = pb;
         }
         return kTraceRunning;
+    }
+
+    // Tests primitive slot i; true when its crossing was accepted as the new closest.
+    __device__ __forceinline__ bool testPrim(const DeviceScene& sc, uint32_t i) {
+        V3<T> v0, v1, v2;
+        uint32_t b, prim, kind;
+        TriFetch<T>::get(sc, i, v0, v1, v2, b, prim, kind);
+        if (kind == kPrimTriangle) {
+            const V3<T> a = v0 - q.o, bb = v1 - q.o, c = v2 - q.o;
+            if (!lineCrossesTriangle(sh, a, bb, c)) return false;
+            const V3<T> n = triangleNormal(v0, v1, v2);
+            const T t = -dot(q.o - v0, n) / dot(q.d, n);
+            if (!(t > T(0) && t < best)) return false;
+            if (!acceptCrossing(sc, q, b, prim, true, t, n)) return false;
+            best = t;
+            hit.t = double(t);
+            hit.prim = prim;
+        } else {
+            const AnalyticResult<Rr> ar = analyticHit<T, R, Rr>(sc, b, q.od, q.d, best, q.depB, q.region, q.errN);
+            if (!ar.ok) return false;
+            best = T(ar.t);
+            hit.t = double(ar.t);
+            hit.prim = 0;
+        }
+        hit.boundary = b;
+        hit.slot = i;
+        found = true;
+        return true;
     }
 };
 
 // A query that overflowed the short stack, from the start with the deep one. Out of line: its
-// stack lives in local memory and only these rare queries touch it.
+// stack lives in local memory and only these rare queries touch it. By value in and out, so that
+// the caller's query need not live in memory.
+struct DeepResult {
+    HitRec hit;
+    int status;
+    uint32_t visits, tests;
+};
 template <class T, class R, class Rr, bool AnyHit>
-__device__ __noinline__ int traceRayDeep(const DeviceScene& sc, const RayQuery<T>& q, HitRec& hit, uint32_t& visits,
-                                         uint32_t& tests) {
+__device__ __noinline__ DeepResult traceRayDeep(const DeviceScene& sc, RayQuery<T> q, HitRec hitIn) {
     Traversal<T, R, Rr, AnyHit, LocalStack> tr;
     tr.begin(q, nullptr, 0);
-    tr.hit = hit;
+    tr.hit = hitIn;
     int s;
     do {
         s = tr.run(sc, 1 << 30);
     } while (s == kTraceRunning);
-    hit = tr.hit;
-    visits += tr.nodeVisits;
-    tests += tr.primTests;
-    return s;
+    DeepResult r;
+    r.hit = tr.hit;
+    r.status = s;
+    r.visits = tr.nodeVisits;
+    r.tests = tr.primTests;
+    return r;
 }
 
 // The whole query in one call (cast rays, forward walks and the adjoint's replay).
@@ -401,7 +418,11 @@ __device__ __forceinline__ int traceRay(const DeviceScene& sc, const RayQuery<T>
     } while (s == kTraceRunning);
     uint32_t nv = tr.nodeVisits, nt = tr.primTests;
     if (s == kTraceOverflow) {
-        s = traceRayDeep<T, R, Rr, AnyHit>(sc, q, hit, nv, nt);
+        const DeepResult d = traceRayDeep<T, R, Rr, AnyHit>(sc, q, hit);
+        s = d.status;
+        hit = d.hit;
+        nv += d.visits;
+        nt += d.tests;
     } else {
         hit = tr.hit;
     }

@@ -236,7 +236,11 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kIntersect(DeviceScene sc, PathBuffers<RT<
                 if (s == kTraceOverflow) {
                     h.boundary = kNone;
                     h.t = INFINITY;
-                    s = traceRayDeep<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false>(sc, tr.q, h, nv, nt);
+                    const DeepResult d = traceRayDeep<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false>(sc, tr.q, h);
+                    s = d.status;
+                    h = d.hit;
+                    nv += d.visits;
+                    nt += d.tests;
                 }
                 if (s != kTraceHit) { h.boundary = kNone; h.t = INFINITY; }
                 if (s == kTraceOverflow) h.boundary = kNone - 1u;  // a fault: the path ends
@@ -633,7 +637,11 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
             uint32_t nv = tr.nodeVisits, nt = tr.primTests;
             if (s == kTraceOverflow) {
                 h.boundary = kNone;
-                s = traceRayDeep<R, Ro, Rr, AnyHit>(sc, tr.q, h, nv, nt);
+                const DeepResult d = traceRayDeep<R, Ro, Rr, AnyHit>(sc, tr.q, h);
+                s = d.status;
+                h = d.hit;
+                nv += d.visits;
+                nt += d.tests;
             }
             if (sc.travCounters) countTraversal(sc.travCounters + 3, nv, nt);
             ++guard;

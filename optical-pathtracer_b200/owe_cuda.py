@@ -70,10 +70,17 @@ class Context:
     def run_pass(self, spp):
         _check(self.lib, self.lib.owec_pass(self.handle, int(spp)), "owec_pass")
 
-    def resolve(self, samples=True):
-        """(per-pixel mean XYZ (height, width, 3), per-pixel sample counts or None)."""
+    def resolve(self, samples=True, out=None):
+        """(per-pixel mean XYZ (height, width, 3), per-pixel sample counts or None). `out`: a
+        C-contiguous float64 array of height x width x 3 values to write the image into (pinned
+        host memory reads back fastest)."""
         n = self.width * self.height
-        xyz = np.empty(3 * n)
+        if out is not None:
+            if not (out.dtype == np.float64 and out.flags.c_contiguous and out.size == 3 * n):
+                raise ValueError("resolve: out must be a C-contiguous float64 array of height x width x 3")
+            xyz = out.reshape(-1)
+        else:
+            xyz = np.empty(3 * n)
         cnt = np.empty(n) if samples else None
         _check(self.lib, self.lib.owec_resolve(self.handle, xyz.ctypes.data_as(A.c_double_p),
                                                cnt.ctypes.data_as(A.c_double_p) if samples else None), "owec_resolve")
@@ -182,9 +189,10 @@ class Renderer:
         self._passes += 1
         self._spp += spp
 
-    def resolve(self):
-        """Per-pixel mean XYZ, shape (height, width, 3)."""
-        return self.ctx.resolve(samples=False)[0]
+    def resolve(self, out=None):
+        """Per-pixel mean XYZ, shape (height, width, 3) (Renderer::resolve), written into `out` when
+        given."""
+        return self.ctx.resolve(samples=False, out=out)[0]
 
     def passes(self):
         return self._passes
