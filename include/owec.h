@@ -353,6 +353,21 @@ int owec_set_heightfield(owec_ctx* ctx, uint32_t boundary, uint64_t n_vertices, 
  * and differentiated through its crossings; nothing of the forward pass is stored. */
 int owec_walk_adjoint(owec_ctx* ctx, const owec_walk_desc* walk, uint64_t first, uint64_t n, const double* g,
                       double* dheights);
+/* owec_walk_adjoint for callers that must not allocate device memory once they are running, such
+ * as an optimiser loop inside a host application that fixed its GPU memory at start-up, or that
+ * shares the device with a framework whose allocator already holds the free memory: there a
+ * cudaMalloc can fail, and every cudaMalloc / cudaFree pair stalls the whole device. It has no
+ * counterpart in the reference. Its scratch (loss gradient, height-gradient accumulator,
+ * counters) is a fixed array in the library image, 10.5 MB on every GPU that loads the library,
+ * so the walk film may have at most 512 x 512 bins and the heightfield at most 1048576 vertices;
+ * larger calls return OWEC_E_INVALID. The scene must be uploaded and its BVH built (and, in the
+ * FP64 mode, one owec_walk run) beforehand, since those steps allocate. The first call on a
+ * device looks up the array's device address, which also loads it onto the device: make that
+ * first call before any stream capture. Calls share the array, so two calls that overlap on the
+ * GPU (from two threads, or two contexts on one device) race and corrupt each other's results.
+ * Same arguments and result as owec_walk_adjoint. */
+int owec_walk_adjoint_noalloc(owec_ctx* ctx, const owec_walk_desc* walk, uint64_t first, uint64_t n,
+                              const double* g, double* dheights);
 /* Device seconds of the last owec_walk and owec_walk_adjoint calls. */
 int owec_walk_timing(owec_ctx* ctx, double out[2]);
 

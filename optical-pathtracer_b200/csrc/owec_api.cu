@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -797,6 +798,37 @@ void runPass(owec_ctx& c, int spp) {
 
 }  // namespace
 
+// ------------------------------------------------------------------ adjoint scratch that is never allocated
+// owec_walk_adjoint_noalloc's scratch: the loss gradient per bin, the height-gradient accumulator and
+// the walk counters, in one array that is part of the library image. Every GPU that loads the
+// library holds these 10.5 MB until the process exits; every call of that entry point shares them.
+constexpr size_t kNoAllocMaxBins = 512 * 512;      // walk film bins (width x height)
+constexpr size_t kNoAllocMaxHeights = 1u << 20;    // heightfield vertices
+constexpr size_t kNoAllocStatsWords = 8;           // walk counters (5 used)
+static __device__ __align__(256) double gAdjointScratch[kNoAllocMaxBins + kNoAllocMaxHeights + kNoAllocStatsWords];
+
+namespace {
+
+// The device address of gAdjointScratch on `device`, which must be current. In host code the array's
+// name is only a host-side stand-in, so the address is asked of the runtime, once per device; that
+// first request also loads the array onto the device.
+constexpr int kMaxNoAllocDevices = 64;
+std::mutex gScratchMutex;
+double* gScratchAddress[kMaxNoAllocDevices] = {};
+
+double* adjointScratch(int device) {
+    require(device >= 0 && device < kMaxNoAllocDevices, "owec_walk_adjoint_noalloc: device index out of range");
+    std::lock_guard<std::mutex> lock(gScratchMutex);
+    if (!gScratchAddress[device]) {
+        void* p = nullptr;
+        OWEC_CUDA(cudaGetSymbolAddress(&p, gAdjointScratch));
+        gScratchAddress[device] = static_cast<double*>(p);
+    }
+    return gScratchAddress[device];
+}
+
+}  // namespace
+
 // ------------------------------------------------------------------ the C ABI
 extern "C" {
 
@@ -1198,6 +1230,52 @@ int owec_walk_adjoint(owec_ctx* ctx, const owec_walk_desc* w, uint64_t first, ui
         OWEC_CUDA(cudaEventElapsedTime(&ms, ctx->passStart, ctx->passStop));
         ctx->lastAdjointSeconds = ms * 1e-3;
         for (size_t i = 0; i < nh; ++i) dheights[i] += h[i];
+    });
+}
+
+int owec_walk_adjoint_noalloc(owec_ctx* ctx, const owec_walk_desc* w, uint64_t first, uint64_t n, const double* g,
+                              double* dheights) {
+    return guarded([&] {
+        require(ctx && w && g && dheights, "owec_walk_adjoint_noalloc: null argument");
+        require(ctx->hf.boundary != kNone, "no heightfield set (owec_set_heightfield)", OWEC_E_STATE);
+        require(w->mode == OWEC_WALK_PRIMARY_TRANSMISSION && w->splat == OWEC_SPLAT_BILINEAR,
+                "the adjoint needs primary-transmission walks and the bilinear splat");
+        require(w->target < ctx->ds.nBoundaries && w->width > 0 && w->height > 0 && w->half_x > 0 && w->half_y > 0,
+                "bad walk description");
+        const size_t nb = size_t(w->width) * w->height, nh = ctx->hfVertices;
+        require(nb <= kNoAllocMaxBins, "owec_walk_adjoint_noalloc: the walk film has more than 512 x 512 = 262144 bins");
+        require(nh <= kNoAllocMaxHeights,
+                "owec_walk_adjoint_noalloc: the heightfield has more than 1048576 vertices");
+        // building the BVH (or its FP64 primitives) would allocate: that belongs to set-up
+        require(!ctx->bvhDirty, "owec_walk_adjoint_noalloc: build the BVH first (owec_build_bvh)", OWEC_E_STATE);
+        require(ctx->settings.precision != OWEC_PRECISION_FP64 || ctx->prims64Ready,
+                "owec_walk_adjoint_noalloc: in FP64 mode run one owec_walk first, which prepares the FP64 primitives",
+                OWEC_E_STATE);
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        double* base = adjointScratch(ctx->device);
+        double* dG = base;
+        double* dDH = base + kNoAllocMaxBins;
+        auto* st = reinterpret_cast<unsigned long long*>(base + kNoAllocMaxBins + kNoAllocMaxHeights);
+        // the scratch keeps the previous call's contents: the accumulator starts from the caller's
+        // dheights (so the kernel adds into it directly) and the counters from zero
+        OWEC_CUDA(cudaMemcpyAsync(dG, g, nb * 8, cudaMemcpyHostToDevice, ctx->stream));
+        OWEC_CUDA(cudaMemcpyAsync(dDH, dheights, nh * 8, cudaMemcpyHostToDevice, ctx->stream));
+        OWEC_CUDA(cudaMemsetAsync(st, 0, kNoAllocStatsWords * 8, ctx->stream));
+        double measure;
+        if (w->source_kind == OWEC_SOURCE_POINT) measure = 2 * kPi * (1 - std::cos(w->extent));
+        else if (w->source_kind == OWEC_SOURCE_COLLIMATED) measure = kPi * w->extent * w->extent;
+        else measure = 4 * w->extent * w->extent;
+        const double binArea = (2 * w->half_x / w->width) * (2 * w->half_y / w->height);
+        OWEC_CUDA(cudaEventRecord(ctx->passStart, ctx->stream));
+        launchWalkAdjoint(ctx->settings.precision, ctx->ds, *w, ctx->boundaries[w->target].toLocal, ctx->hf, first, n,
+                          measure / (double(n) * binArea), dG, dDH, st, ctx->numSMs * 8, ctx->stream);
+        checkLaunch();
+        OWEC_CUDA(cudaEventRecord(ctx->passStop, ctx->stream));
+        OWEC_CUDA(cudaMemcpyAsync(dheights, dDH, nh * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+        float ms = 0;
+        OWEC_CUDA(cudaEventElapsedTime(&ms, ctx->passStart, ctx->passStop));
+        ctx->lastAdjointSeconds = ms * 1e-3;
     });
 }
 

@@ -148,6 +148,18 @@ class Context:
                "owec_walk_adjoint")
         return out
 
+    def walk_adjoint_noalloc(self, desc, first, n, g, dheights=None):
+        """walk_adjoint through owec_walk_adjoint_noalloc, which allocates no device memory: its
+        scratch is a fixed array in the library (at most 512 x 512 bins, 2^20 vertices). The
+        gradient is added to `dheights` (zeros when not given) and returned."""
+        gg = np.ascontiguousarray(g, np.float64).ravel()
+        out = np.zeros(self._hf_n) if dheights is None else np.ascontiguousarray(dheights, np.float64).ravel().copy()
+        _check(self.lib, self.lib.owec_walk_adjoint_noalloc(self.handle, ctypes.byref(desc), int(first), int(n),
+                                                            gg.ctypes.data_as(A.c_double_p),
+                                                            out.ctypes.data_as(A.c_double_p)),
+               "owec_walk_adjoint_noalloc")
+        return out
+
     def walk_timing(self):
         out = (ctypes.c_double * 2)()
         _check(self.lib, self.lib.owec_walk_timing(self.handle, out), "owec_walk_timing")

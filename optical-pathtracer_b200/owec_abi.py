@@ -177,6 +177,8 @@ def load_library(path=LIB_PATH):
         "owec_set_heightfield": ([P, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_double, c_double_p], ctypes.c_int),
         "owec_walk_adjoint": ([P, ctypes.POINTER(WalkDesc), ctypes.c_uint64, ctypes.c_uint64, c_double_p, c_double_p],
                               ctypes.c_int),
+        "owec_walk_adjoint_noalloc": ([P, ctypes.POINTER(WalkDesc), ctypes.c_uint64, ctypes.c_uint64, c_double_p,
+                                       c_double_p], ctypes.c_int),
         "owec_walk_timing": ([P, c_double_p], ctypes.c_int),
     }
     for name, (args, res) in sigs.items():
