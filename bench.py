@@ -270,6 +270,13 @@ def run_cuda(args):
         per_launch_bytes = bytes_isec / max(1, launches_prof)
         per_launch_s = isec_prof / max(1, launches_prof)
         achieved = per_launch_bytes / per_launch_s / 1e9
+        # DRAM traffic per launch: the ncu-measured bytes per query (profiles/) times this launch's queries
+        traffic = None
+        try:
+            with open(os.path.join(ROOT, "profiles", "kIntersect_dram_per_query.json")) as f:
+                traffic = json.load(f)["dram_bytes_per_query"] * q / max(1, launches_prof)
+        except (OSError, KeyError, ValueError):
+            pass
         clk = clocks.summary()
         cpu_rate, cores, sample = (None, None, "skipped")
         if not args.no_cpu_baseline:
@@ -294,9 +301,10 @@ def run_cuda(args):
             "intersect_share": sum(isec) / sum(times),
             "shadow_share": sum(shadow) / sum(times),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "peak_kind": peak_kind, "traffic": None, "kernel": "kIntersect",
+                         "peak_kind": peak_kind, "traffic": traffic, "kernel": "kIntersect",
                          "bytes_per_launch": per_launch_bytes,
-                         "per_query": {"nodes": nodes / max(1, q), "prims": prims / max(1, q)}},
+                         "per_query": {"nodes": nodes / max(1, q), "prims": prims / max(1, q)},
+                         "queries_per_pass": q, "launches_per_pass": launches_prof},
             "clocks": clk,
             "cpu_baseline": {"value": cpu_rate, "unit": "paths/s", "cores": cores, "kind": "reference",
                              "sample": sample},
