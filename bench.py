@@ -188,6 +188,64 @@ def run_reference(args):
     return 0
 
 
+def precision_study(device, width=480, height=270, spp=16, ref_spp=256):
+    """The metric's RMSE half: the same workload at a reduced film, FP64 kernels at ref_spp as the
+    oracle image, then the mixed and the all-FP64 instantiations at spp on the same sample streams.
+    Returns their RMSEs against the oracle (over pixels and XYZ), their paths/s, and the speed-up
+    of mixed over FP64 at that (equal) RMSE."""
+    import owe_cuda
+    desc = scenes.bvh_stress_room(width, height).desc()
+
+    def render(precision, seed, n):
+        with owe_cuda.Context(device) as c:
+            c.upload(desc)
+            c.build_bvh()
+            c.set_settings(A.make_settings(seed=seed, max_depth=MAX_DEPTH, rr_depth=RR_DEPTH,
+                                           wavelength_mode=A.WAVELENGTHS_HERO4, precision=precision))
+            c.run_pass(1)  # warm-up: the FP64 primitives, the path buffers
+            c.reset_film()
+            seconds = 0.0
+            for _ in range(n):
+                c.run_pass(1)
+                seconds += c.last_pass_timing()[0]
+            return c.resolve()[0], width * height * n / seconds
+
+    oracle, _ = render(A.PRECISION_FP64, 1000, ref_spp)
+    out = {"film": f"{width}x{height}", "spp": spp, "oracle": f"fp64 kernels, {ref_spp} spp, other seed"}
+    for name, prec in (("mixed", A.PRECISION_MIXED), ("fp64", A.PRECISION_FP64)):
+        img, rate = render(prec, 7, spp)
+        out[name] = {"rmse": float(np.sqrt(np.mean((img - oracle) ** 2))), "paths_per_s": rate}
+    out["rmse_ratio_mixed_over_fp64"] = out["mixed"]["rmse"] / out["fp64"]["rmse"]
+    out["speedup_at_equal_rmse"] = out["mixed"]["paths_per_s"] / out["fp64"]["paths_per_s"]
+    return out
+
+
+def adjoint_study(device, n=256, bins=512, walks=1 << 24):
+    """The metric's adjoint half at the differentiable caustic's size: a 256 x 256 heightfield
+    (heights 0), a 512 x 512 wall, 2^24 walks per step; device seconds of the forward walks and of
+    the adjoint replay."""
+    import owe_cuda
+    sb, info = scenes.caustic_slab_scene(n=n, wall_bins=bins)
+    w = scenes.caustic_walk(info, seed=1)
+    target = scenes.gaussian_blobs(bins, count=64, seed=3)
+    with owe_cuda.Context(device) as c:
+        c.upload(sb.desc())
+        c.build_bvh()
+        c.set_heightfield(info["heightfield"], info["thickness"], np.zeros((n, n)))
+        fw, ad = [], []
+        for _ in range(3):
+            c.walk_reset()
+            c.walk(w, 0, walks)
+            fw.append(c.walk_timing()[0])
+            img, _ = c.walk_resolve()
+            g = 2 * (img - target * img.mean())
+            c.walk_adjoint(w, 0, walks, g)
+            ad.append(c.walk_timing()[1])
+    f, a = min(fw), min(ad)
+    return {"heightfield": f"{n}x{n}", "bins": f"{bins}x{bins}", "walks": walks, "forward_s": f, "adjoint_s": a,
+            "adjoint_over_forward": a / f, "forward_walks_per_s": walks / f}
+
+
 def run_cuda(args):
     import torch
     world, rank, local = dist_env()
@@ -250,9 +308,13 @@ def run_cuda(args):
     image = torch.empty((HEIGHT, WIDTH, 3), dtype=torch.float64, pin_memory=True).numpy()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    split = []
     for _ in range(e2e_steps):
+        ta = time.perf_counter()
         renderer.run_pass(1)
+        tb = time.perf_counter()
         img = renderer.resolve(out=image)
+        split.append((tb - ta, time.perf_counter() - tb))
     e2e_seconds = time.perf_counter() - t0
     e2e_value = n_pix * world * e2e_steps / e2e_seconds
     d2h = n_pix * 3 * 8  # the resolved XYZ image (Renderer::resolve), FP64
@@ -309,9 +371,13 @@ def run_cuda(args):
             "cpu_baseline": {"value": cpu_rate, "unit": "paths/s", "cores": cores, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
-                    "steps": e2e_steps, "note": "pass + resolved image read back into pinned host memory per step through owe_cuda.Renderer"},
+                    "steps": e2e_steps, "pass_ms": [round(1e3 * a, 2) for a, _ in split],
+                    "resolve_ms": [round(1e3 * b, 2) for _, b in split], "note": "pass + resolved image read back into pinned host memory per step through owe_cuda.Renderer"},
             "faults": stats1["device_faults"],
         }
+        if not args.no_extras and world == 1:
+            line["precision_study"] = precision_study(local)
+            line["adjoint_study"] = adjoint_study(local)
         # our own kernel launches in the timed region: 4 per bounce + generate + film, per step
         line["gpu_launches"] = int(launches * 4 // max(1, args.steps) * args.steps + 2 * args.steps)
         print(json.dumps(line))
@@ -328,6 +394,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the RMSE-at-equal-paths precision study and the adjoint/forward study")
     ap.add_argument("--width", type=int, default=1920, help="film width (a smaller case for profiling)")
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--precision", default="mixed", choices=sorted(PRECISIONS),

@@ -260,6 +260,14 @@ int owec_pass(owec_ctx* ctx, int spp);
 /* Resolved image: XYZ per pixel (3 doubles, row-major) and samples per pixel
  * (CpuRenderer::resolve, src/owe/backends/cpu/cpu_backend.cpp:96-107). Either pointer may be NULL. */
 int owec_resolve(owec_ctx* ctx, double* xyz, double* samples);
+/* The film as sums: the compensated per-pixel XYZ sums (3 doubles, row-major) and the samples per
+ * pixel, which the ranks of a multi-GPU render add up before dividing. No counterpart in the
+ * reference, which renders on one device. Either pointer may be NULL. */
+int owec_read_film(owec_ctx* ctx, double* xyz_sums, double* samples);
+/* Sets the index of the next pass's first sample stream (the pass index of owec_pass): each rank
+ * of a multi-GPU render starts its share of the streams there, so that the ranks together draw
+ * exactly the streams one device would. */
+int owec_set_pass_index(owec_ctx* ctx, uint64_t pass_index);
 /* Discards the film and the pass count (Renderer::resetObserver, src/owe/render/renderer.hpp:60). */
 int owec_reset_film(owec_ctx* ctx);
 int owec_read_stats(owec_ctx* ctx, owec_stats* stats);
@@ -360,8 +368,8 @@ int owec_walk_adjoint(owec_ctx* ctx, const owec_walk_desc* walk, uint64_t first,
  * counterpart in the reference. Its scratch (loss gradient, height-gradient accumulator,
  * counters) is a fixed array in the library image, 10.5 MB on every GPU that loads the library,
  * so the walk film may have at most 512 x 512 bins and the heightfield at most 1048576 vertices;
- * larger calls return OWEC_E_INVALID. The scene must be uploaded and its BVH built (and, in the
- * FP64 mode, one owec_walk run) beforehand, since those steps allocate. The first call on a
+ * larger calls return OWEC_E_INVALID. The scene must be uploaded and its BVH built, after the
+ * settings, beforehand, since those steps allocate. The first call on a
  * device looks up the array's device address, which also loads it onto the device: make that
  * first call before any stream capture. Calls share the array, so two calls that overlap on the
  * GPU (from two threads, or two contexts on one device) race and corrupt each other's results.

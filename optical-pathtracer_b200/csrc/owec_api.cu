@@ -642,6 +642,8 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
     c.dSamples.release();
 }
 
+void ensurePrims64(owec_ctx& c);
+
 void buildBvh(owec_ctx& c) {
     require(c.hasScene, "no scene uploaded", OWEC_E_STATE);
     require(c.nPrims > 0, "the scene has no boundaries");
@@ -656,6 +658,7 @@ void buildBvh(owec_ctx& c) {
     c.ds.nPrims = c.nPrims;
     c.bvhDirty = false;
     c.prims64Ready = false;
+    if (c.settings.precision != OWEC_PRECISION_FP32) ensurePrims64(c);
 }
 
 void ensurePrims64(owec_ctx& c) {
@@ -673,7 +676,8 @@ void ensurePrims64(owec_ctx& c) {
 void ensureReady(owec_ctx& c) {
     require(c.hasScene, "no scene uploaded", OWEC_E_STATE);
     if (c.bvhDirty) buildBvh(c);
-    if (c.settings.precision == OWEC_PRECISION_FP64) ensurePrims64(c);
+    // FP64 vertices: the traversal's in the FP64 mode, the refined triangle distances in the mixed one
+    if (c.settings.precision != OWEC_PRECISION_FP32) ensurePrims64(c);
 }
 
 void ensureFilm(owec_ctx& c) {
@@ -737,11 +741,17 @@ void runPass(owec_ctx& c, int spp) {
         launchGenerate<M>(c.ds, pp, pb, q, c.dStats.get(), s);
         checkLaunch();
         int cur = 0;
+        // The kernels read their queue lengths on the device, so the bounces are queued without a
+        // look at the host: maxDepth + 1 of them first (a path without null boundaries ends by
+        // then), then four at a time until the queue is empty. The host waits once per batch, not
+        // once per bounce.
+        int nextCheck = pp.maxDepth + 1;
         for (int bounce = 0; bounce < 4 * pp.maxDepth + 8; ++bounce) {
-            if ((bounce & 1) == 0 || bounce > 2) {
+            if (bounce == nextCheck) {
                 OWEC_CUDA(cudaMemcpyAsync(c.hostCounts, c.dCounts.get(), 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
                 OWEC_CUDA(cudaStreamSynchronize(s));
                 if (c.hostCounts[cur] == 0) break;
+                nextCheck = bounce + 4;
             }
             // the next-bounce queue and the per-bounce queues start empty
             OWEC_CUDA(cudaMemsetAsync(c.dCounts.get() + (cur ^ 1), 0, sizeof(uint32_t), s));
@@ -958,7 +968,7 @@ int owec_resolve(owec_ctx* ctx, double* xyz, double* samples) {
         ensureFilm(*ctx);
         const size_t np = size_t(ctx->ds.det.width) * ctx->ds.det.height;
         if (xyz) {
-            ctx->dResolved.resize(3 * np);
+            ctx->dResolved.reserve(3 * np);
             launchResolve(ctx->dFilm.get(), ctx->dComp.get(), ctx->dSamples.get(), uint32_t(np), ctx->dResolved.get(),
                           ctx->stream);
             checkLaunch();
@@ -967,6 +977,35 @@ int owec_resolve(owec_ctx* ctx, double* xyz, double* samples) {
         if (samples)
             OWEC_CUDA(cudaMemcpyAsync(samples, ctx->dSamples.get(), np * 8, cudaMemcpyDeviceToHost, ctx->stream));
         OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int owec_read_film(owec_ctx* ctx, double* xyz_sums, double* samples) {
+    return guarded([&] {
+        require(ctx != nullptr, "owec_read_film: null context");
+        require(ctx->hasScene, "no scene uploaded", OWEC_E_STATE);
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        ensureFilm(*ctx);
+        const size_t np = size_t(ctx->ds.det.width) * ctx->ds.det.height;
+        if (xyz_sums) {
+            std::vector<double> film(3 * np), comp(3 * np);
+            OWEC_CUDA(cudaMemcpyAsync(film.data(), ctx->dFilm.get(), 3 * np * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            OWEC_CUDA(cudaMemcpyAsync(comp.data(), ctx->dComp.get(), 3 * np * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+            for (size_t i = 0; i < 3 * np; ++i) xyz_sums[i] = film[i] - comp[i];
+        }
+        if (samples) {
+            OWEC_CUDA(cudaMemcpyAsync(samples, ctx->dSamples.get(), np * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+        }
+    });
+}
+
+int owec_set_pass_index(owec_ctx* ctx, uint64_t pass_index) {
+    return guarded([&] {
+        require(ctx != nullptr, "owec_set_pass_index: null context");
+        require(pass_index < (1ull << 32), "owec_set_pass_index: the PCG32 stream index is 32 bits");
+        ctx->passCount = pass_index;
     });
 }
 
@@ -1248,8 +1287,9 @@ int owec_walk_adjoint_noalloc(owec_ctx* ctx, const owec_walk_desc* w, uint64_t f
                 "owec_walk_adjoint_noalloc: the heightfield has more than 1048576 vertices");
         // building the BVH (or its FP64 primitives) would allocate: that belongs to set-up
         require(!ctx->bvhDirty, "owec_walk_adjoint_noalloc: build the BVH first (owec_build_bvh)", OWEC_E_STATE);
-        require(ctx->settings.precision != OWEC_PRECISION_FP64 || ctx->prims64Ready,
-                "owec_walk_adjoint_noalloc: in FP64 mode run one owec_walk first, which prepares the FP64 primitives",
+        require(ctx->settings.precision == OWEC_PRECISION_FP32 || ctx->prims64Ready,
+                "owec_walk_adjoint_noalloc: build the BVH after setting the precision (owec_set_settings, then "
+                "owec_build_bvh): that prepares the FP64 primitives",
                 OWEC_E_STATE);
         OWEC_CUDA(cudaSetDevice(ctx->device));
         double* base = adjointScratch(ctx->device);

@@ -57,6 +57,19 @@ struct SurfacePoint {
 // from the two shorter edges (src/owe/scene/mesh.cpp:73-97). Analytic shapes: the crossing found
 // again in the shape's frame, carried to the world by its transform (World::intersect,
 // src/owe/scene/world.cpp:570-580).
+// A triangle crossing's distance recomputed in FP64 from the triangle's FP64 vertices (leaf-order
+// PrimRec64): the traversal finds the triangle in FP32, and the point a path continues from, built
+// as origin + t d in FP64, then carries the FP64 vertices' precision instead of the FP32 ones'.
+// Kept only when it lies near the FP32 distance (a degenerate triangle keeps the FP32 one).
+__device__ __forceinline__ double refineTriangleT(const DeviceScene& sc, uint32_t slot, const V3<double>& od,
+                                                  const V3<double>& d, double t32) {
+    const PrimRec64& p = sc.prims64[slot];
+    const V3<double> v0(p.v0[0], p.v0[1], p.v0[2]), v1(p.v1[0], p.v1[1], p.v1[2]), v2(p.v2[0], p.v2[1], p.v2[2]);
+    const V3<double> n = triangleNormal(v0, v1, v2);
+    const double t = dot(v0 - od, n) / dot(d, n);
+    return (t > 0 && fabs(t - t32) <= 1e-3 * (1 + fabs(t32))) ? t : t32;
+}
+
 template <class R, class Ro, class Rr>
 __device__ SurfacePoint<R> hitGeometry(const DeviceScene& sc, const PathRay<R>& ray, const HitRec& h) {
     SurfacePoint<R> sp;
@@ -67,7 +80,8 @@ __device__ SurfacePoint<R> hitGeometry(const DeviceScene& sc, const PathRay<R>& 
         V3<R> v0, v1, v2;
         uint32_t b, prim, kind;
         TriFetch<R>::get(sc, h.slot, v0, v1, v2, b, prim, kind);
-        sp.p = od + V3<double>(d) * h.t;
+        const double t = sizeof(Rr) == sizeof(double) ? refineTriangleT(sc, h.slot, od, V3<double>(d), h.t) : h.t;
+        sp.p = od + V3<double>(d) * t;
         sp.n = normalize(triangleNormal(v0, v1, v2));
         sp.pLocal = bd.toLocal.point(sp.p);
         sp.nLocal = bd.toLocal.vector(V3<double>(sp.n));

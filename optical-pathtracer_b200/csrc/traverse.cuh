@@ -256,6 +256,15 @@ enum TraceStatus : int { kTraceMiss = 0, kTraceHit = 1, kTraceOverflow = 2 };
 
 constexpr int kTraceRunning = 3;  // Traversal::run: the query is not finished yet
 
+// 1 / d for the slab tests, with a zero component taken as a tiny one of its sign: an infinite
+// inverse makes the affine slab distances inf - inf = NaN, which the min / max ignore, and a ray
+// parallel to an axis (a collimated beam, normal incidence) would then pass every box's slab on
+// that axis and visit the whole tree. 1e-18 keeps every product finite in FP32.
+template <class T>
+__device__ __forceinline__ T safeInverse(T d) {
+    return T(1) / (fabs(d) > T(1e-18) ? d : copysign(T(1e-18), d));
+}
+
 // Moves bit s of an 8-bit mask to bit s ^ x: slot order to visiting order and back.
 __device__ __forceinline__ uint32_t permuteSlots(uint32_t m, uint32_t x) {
     m = (x & 1u) ? (((m & 0x55u) << 1) | ((m >> 1) & 0x55u)) : m;
@@ -285,7 +294,7 @@ struct Traversal {
     // `stack` is this thread's column of the block's shared-memory stack (stride = block size).
     __device__ __forceinline__ void begin(const RayQuery<T>& query, StackEntry* stack, int stride) {
         q = query;
-        inv = V3<T>(T(1) / q.d.x, T(1) / q.d.y, T(1) / q.d.z);
+        inv = V3<T>(safeInverse(q.d.x), safeInverse(q.d.y), safeInverse(q.d.z));
         oinv = V3<T>(q.o.x * inv.x, q.o.y * inv.y, q.o.z * inv.z);
         sh = shearRay(q.d);
         best = q.tmax;

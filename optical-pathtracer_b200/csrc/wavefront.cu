@@ -167,11 +167,16 @@ __global__ void __launch_bounds__(256) kGenerate(DeviceScene sc, PassParams pp, 
 constexpr int kRefillBudget = OWEC_REFILL_BUDGET;
 // Resident blocks per SM the traversal kernels are compiled for (a register cap of
 // 65536 / (128 x blocks) per thread).
+// Resident blocks per SM the medium and surface kernels are compiled for: they wait on their
+// path-state loads, which more resident warps hide.
+#ifndef OWEC_SHADING_MIN_BLOCKS
+#define OWEC_SHADING_MIN_BLOCKS 3
+#endif
 #if defined(OWEC_TRAVERSAL_MAXNREG)
 #define OWEC_TRAVERSAL_BOUNDS __maxnreg__(OWEC_TRAVERSAL_MAXNREG)
 #else
 #ifndef OWEC_TRAVERSAL_MIN_BLOCKS
-#define OWEC_TRAVERSAL_MIN_BLOCKS 3
+#define OWEC_TRAVERSAL_MIN_BLOCKS 4
 #endif
 #define OWEC_TRAVERSAL_BOUNDS __launch_bounds__(128, OWEC_TRAVERSAL_MIN_BLOCKS)
 #endif
@@ -307,7 +312,7 @@ __device__ void queueNee(const DeviceScene& sc, PathBuffers<RT<M>>& pb, Queues& 
 
 // ------------------------------------------------------------------ medium
 template <int M>
-__global__ void __launch_bounds__(128) kMedium(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
+__global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kMedium(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
                                                int cur, StatCounters* st) {
     using R = RT<M>;
     const int nxt = cur ^ 1;
@@ -440,7 +445,7 @@ __device__ __forceinline__ Interface<R> makeInterface(const DeviceScene& sc, con
 }
 
 template <int M>
-__global__ void __launch_bounds__(128) kSurface(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
+__global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kSurface(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
                                                 int cur, StatCounters* st) {
     using R = RT<M>;
     using Ro = typename Mode<M>::Ro;
@@ -454,7 +459,7 @@ __global__ void __launch_bounds__(128) kSurface(DeviceScene sc, PassParams pp, P
         PathAux aux = pb.aux[i];
         const HitRec h = pb.hit[i];
         Pcg32 rng{aux.rngState, (uint64_t(aux.stream) << 1u) | 1u};
-        const DBoundary bd = sc.boundaries[h.boundary];
+        const DBoundary& bd = sc.boundaries[h.boundary];
         const SurfacePoint<R> g = hitGeometry<R, Ro, Rr>(sc, ray, h);
         const V3<R> d = rayDir(ray);
         // meetBoundary (transport.cpp:121-133)
@@ -479,7 +484,7 @@ __global__ void __launch_bounds__(128) kSurface(DeviceScene sc, PassParams pp, P
                     sp.L[j] += float(sp.beta[j] * evalSpectrum(sc, e.radiance, R(sp.lambda[j])) * w);
             }
         }
-        const owec_optics o = sc.optics[bd.optics];
+        const owec_optics& o = sc.optics[bd.optics];
         const float errN = anchorError<R>(g.p);
         bool cont = false, neeValid = false;
         LightSampleD ls;
@@ -668,7 +673,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
                     } else if (AnyHit) {
                         outcome = 2;
                     } else {
-                        const DBoundary bd = sc.boundaries[h.boundary];
+                        const DBoundary& bd = sc.boundaries[h.boundary];
                         if (sc.optics[bd.optics].type != OWEC_SURF_NULL) {
                             outcome = 2;
                         } else {
@@ -788,7 +793,8 @@ __global__ void __launch_bounds__(128) kCastRays(DeviceScene sc, uint64_t n, con
         if (s == kTraceHit) {
             boundary[i] = h.boundary;
             prim[i] = h.prim;
-            t[i] = h.t;
+            const bool refine = sizeof(typename Mode<M>::Rr) == sizeof(double) && sc.boundaries[h.boundary].shape == OWEC_SHAPE_MESH;
+            t[i] = refine ? refineTriangleT(sc, h.slot, rq.od, V3<double>(d[3 * i], d[3 * i + 1], d[3 * i + 2]), h.t) : h.t;
         } else {
             boundary[i] = s == kTraceOverflow ? kNone - 1u : kNone;
             prim[i] = 0;

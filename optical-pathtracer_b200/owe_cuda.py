@@ -86,6 +86,19 @@ class Context:
                                                cnt.ctypes.data_as(A.c_double_p) if samples else None), "owec_resolve")
         return xyz.reshape(self.height, self.width, 3), (cnt.reshape(self.height, self.width) if samples else None)
 
+    def read_film(self):
+        """(compensated XYZ sums (height, width, 3), samples per pixel (height, width))."""
+        n = self.width * self.height
+        sums = np.empty(3 * n)
+        cnt = np.empty(n)
+        _check(self.lib, self.lib.owec_read_film(self.handle, sums.ctypes.data_as(A.c_double_p),
+                                                 cnt.ctypes.data_as(A.c_double_p)), "owec_read_film")
+        return sums.reshape(self.height, self.width, 3), cnt.reshape(self.height, self.width)
+
+    def set_pass_index(self, index):
+        """The sample stream the next pass starts at."""
+        _check(self.lib, self.lib.owec_set_pass_index(self.handle, int(index)), "owec_set_pass_index")
+
     def reset_film(self):
         _check(self.lib, self.lib.owec_reset_film(self.handle), "owec_reset_film")
 

@@ -163,6 +163,8 @@ def load_library(path=LIB_PATH):
         "owec_set_settings": ([P, ctypes.POINTER(Settings)], ctypes.c_int),
         "owec_pass": ([P, ctypes.c_int], ctypes.c_int),
         "owec_resolve": ([P, c_double_p, c_double_p], ctypes.c_int),
+        "owec_read_film": ([P, c_double_p, c_double_p], ctypes.c_int),
+        "owec_set_pass_index": ([P, ctypes.c_uint64], ctypes.c_int),
         "owec_reset_film": ([P], ctypes.c_int),
         "owec_read_stats": ([P, ctypes.POINTER(Stats)], ctypes.c_int),
         "owec_last_pass_timing": ([P, c_double_p], ctypes.c_int),
