@@ -341,6 +341,45 @@ def bvh_stress_room(width=1920, height=1080, n_lon=1024, n_lat=512, pixel_sigma=
     return sb
 
 
+def fog_room(width=64, height=48, n_lon=128, n_lat=64, panel_n=16, sigma_s=0.5, sigma_a=0.05, g=0.8, seed=3):
+    """The participating-medium configuration at a reduced size: the closed Lambertian box of
+    bvh_stress_room filled with a homogeneous medium (scattering sigma_s, absorption sigma_a per
+    metre, Henyey-Greenstein g), a displaced-sphere prop, and a PMMA panel whose top face is a
+    panel_n x panel_n heightfield of seeded heights, under one area light."""
+    sb = SceneBuilder()
+    fog = sb._medium(A.INDEX_CONSTANT, (1.0,), absorption=sb.spectrum_constant(sigma_a),
+                     scattering=sb.spectrum_constant(sigma_s), g=g)
+    sb.region_medium[0] = fog  # the ambient region, where the camera is, holds the medium
+    opaque = sb.medium_opaque()
+    verts, tris = uv_sphere(n_lon, n_lat, radius=0.6, seed=seed)
+    sb.mesh_body(verts, tris, opaque, sb.diffuse(0.6), xf=translate(-1.0, 0.5, 0.8))
+    pmma = sb.medium_sellmeier(*PMMA, rel_air=False)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    h = rng.uniform(-2e-3, 2e-3, (panel_n, panel_n))
+    h[0, :] = h[-1, :] = h[:, 0] = h[:, -1] = 0
+    inside = sb.region(pmma)
+    half, thick = 0.4, 0.05
+    top_v, top_t = heightfield_grid(panel_n, panel_n, half, half, thick, h)
+    top_v = np.asarray(top_v, float).reshape(-1, 3) + (0.8, -0.4, 0.6)
+    glass = sb.dielectric()
+    sb.boundary(A.SHAPE_MESH, [], pose(), 0, inside, glass, -1, sb.mesh(top_v, top_t))
+    rest_v, rest_t = slab_rest(panel_n, panel_n, half, half, lambda i, j: thick + h[j, i])
+    rest_v = np.asarray(rest_v, float).reshape(-1, 3) + (0.8, -0.4, 0.6)
+    sb.boundary(A.SHAPE_MESH, [], pose(), 0, inside, glass, -1, sb.mesh(rest_v, rest_t))
+    wall = sb.diffuse(0.7)
+    w = 3.0
+    sb.sheet(w, w, pose(), wall)
+    sb.sheet(w, w, pose(rotate_to((0, 0, 1), (0, 0, -1)), (0, 0, 4.0)), wall)
+    sb.sheet(2.0, w, pose(rotate_to((0, 0, 1), (1, 0, 0)), (-w, 0, 2.0)), wall)
+    sb.sheet(2.0, w, pose(rotate_to((0, 0, 1), (-1, 0, 0)), (w, 0, 2.0)), wall)
+    sb.sheet(w, 2.0, pose(rotate_to((0, 0, 1), (0, -1, 0)), (0, w, 2.0)), wall)
+    sb.sheet(w, 2.0, pose(rotate_to((0, 0, 1), (0, 1, 0)), (0, -w, 2.0)), wall)
+    lamp = sb.emission(sb.spectrum_constant(8.0))
+    sb.sheet(0.8, 0.8, pose(rotate_to((0, 0, 1), (0, 0, -1)), (0.0, 0.0, 3.98)), sb.absorber(), emission=lamp)
+    sb.observer(width, height, (0.3, -2.7, 1.6), (0.0, 0.0, 1.0), fov_y_deg=55.0)
+    return sb
+
+
 def furnace_sphere(rho, width=16, height=16):
     """Inside a closed diffuse sphere of albedo rho emitting Le = 1 inward: L = Le / (1 - rho)
     (tests/test_backends.cpp:349-378)."""

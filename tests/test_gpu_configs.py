@@ -69,3 +69,36 @@ def test_c1_film_at_4096_spp_matches_the_reference_streams():
     rel = np.abs(y_gpu[lit] - y_ref[lit]) / y_ref[lit]
     assert rel.mean() < 0.01, (rel.mean(), rel.max())
     assert abs(y_gpu.mean() / y_ref.mean() - 1) < 0.005
+
+
+def test_c5_fog_room_paths_follow_the_reference_and_agree_statistically():
+    """The participating-medium configuration at a reduced size (sigma_s 0.5 /m, sigma_a 0.05 /m,
+    HG g = 0.8, a PMMA heightfield panel, depth 24): one-sample paths make the reference's
+    decisions, and independent 32-spp runs pass the block z-test."""
+    from oracle_ref import block_z_test
+    desc = scenes.fog_room(48, 36).desc()
+    ref = ReferenceEngine(desc)
+    s = A.make_settings(seed=5, max_depth=24, rr_depth=6)
+    one_ref, _ = ref.render(s, 1, passes=1)
+    with owe_cuda.Context() as c:
+        c.upload(desc)
+        c.build_bvh()
+        c.set_settings(s)
+        c.run_pass(1)
+        one_gpu = c.resolve()[0]
+        a, b = one_ref[:, :, 1].ravel(), one_gpu[:, :, 1].ravel()
+        close = np.abs(a - b) <= 1e-4 * np.maximum(np.abs(a), 1e-3)
+        assert close.mean() > 0.95, close.mean()
+        runs_ref, runs_gpu = [], []
+        for k in range(6):
+            img, st = ref.render(A.make_settings(seed=100 + k, max_depth=24, rr_depth=6), 32)
+            runs_ref.append(img)
+            assert st["leaks"] == 0
+            c.set_settings(A.make_settings(seed=200 + k, max_depth=24, rr_depth=6))
+            c.reset_film()
+            c.run_pass(32)
+            runs_gpu.append(c.resolve()[0])
+        assert c.stats()["device_faults"] == 0
+    save_artifact("c5_fog_room_runs", ref=np.array(runs_ref), gpu=np.array(runs_gpu))
+    ok, rep = block_z_test(runs_ref, runs_gpu)
+    assert ok, rep

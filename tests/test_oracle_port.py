@@ -103,3 +103,15 @@ def test_port_rough_glass_and_metal_equal_reference():
     b, _ = PortEngine(desc).render(s, 2)
     close = np.abs(a - b) <= 1e-9 * np.maximum(np.abs(a), 1e-12)
     assert close.mean() > 0.99
+
+
+def test_port_fog_room_equals_reference():
+    """Participating medium (free flight, HG scattering, medium NEE) with a PMMA heightfield panel:
+    every one-sample path of the restatement is the reference's."""
+    desc = scenes.fog_room(32, 24).desc()
+    s = A.make_settings(seed=2, max_depth=24, rr_depth=6)
+    a, sa = ReferenceEngine(desc).render(s, 1, passes=4)
+    b, sb_ = PortEngine(desc).render(s, 1, passes=4)
+    assert sa == sb_
+    close = np.abs(a - b) <= 1e-9 * np.maximum(np.abs(a), 1e-12)
+    assert close.mean() > 0.999
