@@ -246,6 +246,35 @@ def adjoint_study(device, n=256, bins=512, walks=1 << 24):
             "adjoint_over_forward": a / f, "forward_walks_per_s": walks / f}
 
 
+def configs_study(device):
+    """The other configurations' own rates: C1 (N-BK7 sphere on a floor under the sun, 256 x 256,
+    one uniform wavelength per path, depth 16) in paths/s over 64 one-sample passes, and C3 (the
+    achromat imaging a point source onto a 1024 x 1024 detector, stochastic Fresnel branching with
+    ghosts, depth 32) in walks/s over 2^24 walks."""
+    import owe_cuda
+    out = {}
+    with owe_cuda.Context(device) as c:
+        c.upload(scenes.glass_sphere_on_floor(256, 256).desc())
+        c.build_bvh()
+        c.set_settings(A.make_settings(seed=0, max_depth=16, rr_depth=4, wavelength_mode=A.WAVELENGTHS_UNIFORM1))
+        c.run_pass(1)
+        seconds = 0.0
+        for _ in range(64):
+            c.run_pass(1)
+            seconds += c.last_pass_timing()[0]
+        out["c1_paths_per_s"] = 256 * 256 * 64 / seconds
+    sb, info = scenes.achromat_scene(film=1024)
+    w = scenes.achromat_walk(info, seed=1, mode=A.WALK_STOCHASTIC, max_events=32)
+    with owe_cuda.Context(device) as c:
+        c.upload(sb.desc())
+        c.build_bvh()
+        c.walk(w, 0, 1 << 20)
+        c.walk_reset()
+        c.walk(w, 0, 1 << 24)
+        out["c3_walks_per_s"] = (1 << 24) / c.walk_timing()[0]
+    return out
+
+
 def run_cuda(args):
     import torch
     world, rank, local = dist_env()
@@ -304,7 +333,7 @@ def run_cuda(args):
     value = total_paths / device_seconds
 
     # end to end through the public API: a pass and the film read back to the host, every step
-    e2e_steps = max(2, min(args.steps, 5))
+    e2e_steps = max(2, min(args.steps, 10))
     image = torch.empty((HEIGHT, WIDTH, 3), dtype=torch.float64, pin_memory=True).numpy()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -371,6 +400,7 @@ def run_cuda(args):
             "cpu_baseline": {"value": cpu_rate, "unit": "paths/s", "cores": cores, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
+                    "value_at_median_step": n_pix * world / statistics.median(a + b for a, b in split),
                     "steps": e2e_steps, "pass_ms": [round(1e3 * a, 2) for a, _ in split],
                     "resolve_ms": [round(1e3 * b, 2) for _, b in split], "note": "pass + resolved image read back into pinned host memory per step through owe_cuda.Renderer"},
             "faults": stats1["device_faults"],
@@ -378,6 +408,7 @@ def run_cuda(args):
         if not args.no_extras and world == 1:
             line["precision_study"] = precision_study(local)
             line["adjoint_study"] = adjoint_study(local)
+            line["configs_study"] = configs_study(local)
         # our own kernel launches in the timed region: 4 per bounce + generate + film, per step
         line["gpu_launches"] = int(launches * 4 // max(1, args.steps) * args.steps + 2 * args.steps)
         print(json.dumps(line))

@@ -232,25 +232,31 @@ OWEC_HD int analyticCrossings(const DBoundary& b, const V3<Rr>& o, const V3<Rr>&
 // along an axis, the side of each edge is a 2-D cross product of that edge's own vertices.
 template <class T>
 struct ShearedRay {
-    int kx, ky, kz;
-    T sx, sy;
+    V3<T> X, Y;  // a point's sheared coordinates are dot(X, p) and dot(Y, p)
 };
 template <class T>
 OWEC_HD ShearedRay<T> shearRay(const V3<T>& d) {
     const T dx = fabs(d.x), dy = fabs(d.y), dz = fabs(d.z);
+    const int kz = dx > dy ? (dx > dz ? 0 : 2) : (dy > dz ? 1 : 2);
+    const int kx = kz == 2 ? 0 : kz + 1;
+    const int ky = kx == 2 ? 0 : kx + 1;
+    const T sx = d[kx] / d[kz], sy = d[ky] / d[kz];
     ShearedRay<T> s;
-    s.kz = dx > dy ? (dx > dz ? 0 : 2) : (dy > dz ? 1 : 2);
-    s.kx = s.kz == 2 ? 0 : s.kz + 1;
-    s.ky = s.kx == 2 ? 0 : s.kx + 1;
-    s.sx = d[s.kx] / d[s.kz];
-    s.sy = d[s.ky] / d[s.kz];
+    s.X = V3<T>(kx == 0 ? T(1) : (kz == 0 ? -sx : T(0)), kx == 1 ? T(1) : (kz == 1 ? -sx : T(0)),
+                kx == 2 ? T(1) : (kz == 2 ? -sx : T(0)));
+    s.Y = V3<T>(ky == 0 ? T(1) : (kz == 0 ? -sy : T(0)), ky == 1 ? T(1) : (kz == 1 ? -sy : T(0)),
+                ky == 2 ? T(1) : (kz == 2 ? -sy : T(0)));
     return s;
 }
 template <class T>
+OWEC_HD T shearDot(const V3<T>& k, const V3<T>& p) {
+    return fma(k.z, p.z, fma(k.y, p.y, k.x * p.x));
+}
+template <class T>
 OWEC_HD bool lineCrossesTriangle(const ShearedRay<T>& s, const V3<T>& a, const V3<T>& b, const V3<T>& c) {
-    const T ax = a[s.kx] - s.sx * a[s.kz], ay = a[s.ky] - s.sy * a[s.kz];
-    const T bx = b[s.kx] - s.sx * b[s.kz], by = b[s.ky] - s.sy * b[s.kz];
-    const T cx = c[s.kx] - s.sx * c[s.kz], cy = c[s.ky] - s.sy * c[s.kz];
+    const T ax = shearDot(s.X, a), ay = shearDot(s.Y, a);
+    const T bx = shearDot(s.X, b), by = shearDot(s.Y, b);
+    const T cx = shearDot(s.X, c), cy = shearDot(s.Y, c);
     const T u = cx * by - cy * bx, v = ax * cy - ay * cx, w = bx * ay - by * ax;
     if ((u < T(0) || v < T(0) || w < T(0)) && (u > T(0) || v > T(0) || w > T(0))) return false;
     return u + v + w != T(0);

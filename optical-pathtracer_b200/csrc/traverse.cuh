@@ -85,9 +85,10 @@ __device__ __forceinline__ bool acceptCrossing(const DeviceScene& sc, const RayQ
     return incident == q.region;
 }
 
+// Relative widening of far planes against the rounding of the slab distances (a few ulps).
 template <class T> __device__ __forceinline__ T farWiden();
-template <> __device__ __forceinline__ float farWiden<float>() { return 1.0000004f; }
-template <> __device__ __forceinline__ double farWiden<double>() { return 1.0 + 4e-16; }
+template <> __device__ __forceinline__ float farWiden<float>() { return 4e-7f; }
+template <> __device__ __forceinline__ double farWiden<double>() { return 4e-16; }
 
 // The analytic boundary b's first acceptable crossing in (0, best); FP64 refinement when Rr = double.
 template <class R, class Rr, class T>
@@ -171,10 +172,6 @@ __device__ __forceinline__ float byteAsFloat(uint32_t w, int k) {
     return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | uint32_t(k))) - 8388608.0f;
 }
 
-__device__ __forceinline__ uint32_t nodeByte(uint32_t lo, uint32_t hi, int i) {
-    return ((i < 4 ? lo : hi) >> (8 * (i & 3))) & 0xFFu;
-}
-
 // Decoded child boxes of a node, slab-tested against the ray. Returns the hit mask (slot order).
 template <class T>
 __device__ __forceinline__ uint32_t intersectChildren(const NodeWords& nd, const V3<T>& inv, const V3<T>& oinv, T tmin, T tmax) {
@@ -186,6 +183,12 @@ __device__ __forceinline__ uint32_t intersectChildren(const NodeWords& nd, const
     const T bx = T(__uint_as_float(nd.a.x)) * inv.x - oinv.x;
     const T by = T(__uint_as_float(nd.a.y)) * inv.y - oinv.y;
     const T bz = T(__uint_as_float(nd.a.z)) * inv.z - oinv.z;
+    // Far planes are widened against rounding once per node: by a few ulps of the largest far
+    // distance the node's children can have on that axis, where a factor per child cost eight
+    // multiplies.
+    const T fbx = bx + (fabs(bx) + T(255) * fabs(ax)) * farWiden<T>();
+    const T fby = by + (fabs(by) + T(255) * fabs(ay)) * farWiden<T>();
+    const T fbz = bz + (fabs(bz) + T(255) * fabs(az)) * farWiden<T>();
     const bool nx = inv.x < T(0), ny = inv.y < T(0), nz = inv.z < T(0);
     // near and far planes per axis, chosen by the ray's direction on whole words
     const uint32_t nxl0 = nx ? nd.d.z : nd.c.x, nxl1 = nx ? nd.d.w : nd.c.y;
@@ -195,18 +198,18 @@ __device__ __forceinline__ uint32_t intersectChildren(const NodeWords& nd, const
     const uint32_t nzl0 = nz ? nd.e.z : nd.d.x, nzl1 = nz ? nd.e.w : nd.d.y;
     const uint32_t fzl0 = nz ? nd.d.x : nd.e.z, fzl1 = nz ? nd.d.y : nd.e.w;
     uint32_t mask = 0;
+    // an empty slot's box is stored inverted (low planes 255, high planes 0), so it never passes
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        if (nodeByte(nd.b.z, nd.b.w, i) == 0) continue;  // empty slot (inner slots carry bit 3, leaves a count)
         const int k = i & 3;
         const T lx = T(byteAsFloat(i < 4 ? nxl0 : nxl1, k)), hx = T(byteAsFloat(i < 4 ? fxl0 : fxl1, k));
         const T ly = T(byteAsFloat(i < 4 ? nyl0 : nyl1, k)), hy = T(byteAsFloat(i < 4 ? fyl0 : fyl1, k));
         const T lz = T(byteAsFloat(i < 4 ? nzl0 : nzl1, k)), hz = T(byteAsFloat(i < 4 ? fzl0 : fzl1, k));
-        const T t0x = fma(lx, ax, bx), t1x = fma(hx, ax, bx);
-        const T t0y = fma(ly, ay, by), t1y = fma(hy, ay, by);
-        const T t0z = fma(lz, az, bz), t1z = fma(hz, az, bz);
+        const T t0x = fma(lx, ax, bx), t1x = fma(hx, ax, fbx);
+        const T t0y = fma(ly, ay, by), t1y = fma(hy, ay, fby);
+        const T t0z = fma(lz, az, bz), t1z = fma(hz, az, fbz);
         const T te = fmax(fmax(t0x, t0y), fmax(t0z, tmin));
-        const T tx = fmin(fmin(t1x, t1y), t1z) * farWiden<T>();
+        const T tx = fmin(fmin(t1x, t1y), t1z);
         const T tl = fmin(tx, tmax);
         if (te <= tl) mask |= 1u << i;
     }
@@ -350,10 +353,11 @@ struct Traversal {
             nodeBits = permuteSlots(mask & inner, first) | (inner << 8);
             primBase = nd.b.y;
             uint32_t pb = 0;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const uint32_t meta = nodeByte(nd.b.z, nd.b.w, i);
-                pb |= (mask & ~inner & (1u << i)) ? ((1u << (meta >> 5)) - 1u) << (meta & 31u) : 0u;
+            // the hit leaf slots' primitive ranges (meta: count << 5 | offset), one leaf at a time
+            for (uint32_t leaves = mask & ~inner; leaves; leaves &= leaves - 1u) {
+                const uint32_t i = uint32_t(__ffs(leaves) - 1);
+                const uint32_t meta = ((i < 4 ? nd.b.z : nd.b.w) >> (8 * (i & 3))) & 0xFFu;
+                pb |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
             }
             primBits = pb;
         }

@@ -436,8 +436,14 @@ __device__ __forceinline__ Interface<R> makeInterface(const DeviceScene& sc, con
     Interface<R> it;
     it.o = sc.optics[bd.optics];
     it.n = n;
-    it.nFront = regionIndex(sc, bd.front, lambda);
-    it.nBack = regionIndex(sc, bd.back, lambda);
+    // only the dielectric and conductor lobes read the indices (a Lambertian surface, the most
+    // common, skips two index evaluations per wavelength)
+    if (it.o.type == OWEC_SURF_DIELECTRIC || it.o.type == OWEC_SURF_CONDUCTOR) {
+        it.nFront = regionIndex(sc, bd.front, lambda);
+        it.nBack = regionIndex(sc, bd.back, lambda);
+    } else {
+        it.nFront = it.nBack = R(1);
+    }
     it.lambda = lambda;
     it.fresnelFloor = fresnelFloor;
     it.albedo = it.o.reflectance >= 0 ? evalSpectrum(sc, it.o.reflectance, lambda) : R(1);
