@@ -247,7 +247,7 @@ struct owec_ctx {
     DBuf<double> dFilm, dComp, dSamples;
     DBuf<double> dResolved;  // owec_resolve's per-pixel XYZ, read back in one copy
     DBuf<uint8_t> dPathRay, dPathSpec, dPathAux, dHit, dShadow;
-    DBuf<uint32_t> dQueue0, dQueue1, dQueueSurf, dQueueShadow, dCounts;
+    DBuf<uint32_t> dQueue0, dQueue1, dQueueSurf, dQueueSurfSimple, dQueueShadow, dCounts;
     DBuf<StatCounters> dStats;
     DBuf<unsigned long long> dTravCounters;
     uint32_t capacity = 0;
@@ -710,13 +710,15 @@ void runPass(owec_ctx& c, int spp) {
         c.dQueue0.resize(cap);
         c.dQueue1.resize(cap);
         c.dQueueSurf.resize(cap);
+        c.dQueueSurfSimple.resize(cap);
         c.dQueueShadow.resize(cap);
         c.capacity = cap;
     }
     PathBuffers<R> pb{reinterpret_cast<PathRay<R>*>(c.dPathRay.get()), reinterpret_cast<PathSpec<R>*>(c.dPathSpec.get()),
                       reinterpret_cast<PathAux*>(c.dPathAux.get()), reinterpret_cast<HitRec*>(c.dHit.get()),
                       reinterpret_cast<ShadowRay<R>*>(c.dShadow.get())};
-    Queues q{{c.dQueue0.get(), c.dQueue1.get()}, c.dQueueSurf.get(), c.dQueueShadow.get(), c.dCounts.get()};
+    Queues q{{c.dQueue0.get(), c.dQueue1.get()}, c.dQueueSurf.get(), c.dQueueShadow.get(), c.dCounts.get(),
+             c.dQueueSurfSimple.get()};
     PassParams pp{};
     pp.seed = c.settings.seed;
     pp.maxDepth = c.settings.max_depth;
@@ -755,7 +757,7 @@ void runPass(owec_ctx& c, int spp) {
             }
             // the next-bounce queue and the per-bounce queues start empty
             OWEC_CUDA(cudaMemsetAsync(c.dCounts.get() + (cur ^ 1), 0, sizeof(uint32_t), s));
-            OWEC_CUDA(cudaMemsetAsync(c.dCounts.get() + 2, 0, 4 * sizeof(uint32_t), s));  // + the fetch counters
+            OWEC_CUDA(cudaMemsetAsync(c.dCounts.get() + 2, 0, 5 * sizeof(uint32_t), s));  // + fetch counters, simple queue
             if (size_t(evUsed + 4) > c.travEvents.size())
                 for (int k = 0; k < 4; ++k) {
                     cudaEvent_t e;

@@ -72,9 +72,11 @@ struct alignas(16) ShadowRay {
 
 struct Queues {
     uint32_t* active[2];
-    uint32_t* surface;
+    uint32_t* surface;        // surface events with any optics
     uint32_t* shadow;
-    uint32_t* counts;     // [0], [1] active ping-pong, [2] surface, [3] shadow
+    uint32_t* counts;         // [0], [1] active ping-pong, [2] surface, [3] shadow, [4], [5] fetch
+                              // counters of the persistent kernels, [6] simple surface
+    uint32_t* surfaceSimple;  // surface events on Lambertian, absorbing and detecting boundaries
 };
 
 struct StatCounters {

@@ -279,7 +279,8 @@ __device__ __forceinline__ uint32_t permuteSlots(uint32_t m, uint32_t x) {
 // Closest (AnyHit = false) or first (AnyHit = true) acceptable crossing in (0, q.tmax), as a state
 // machine that a persistent kernel can advance a few visits at a time and then hand the thread a
 // new query when this one ends. R / Rr: precision of analytic roots and of their refinement.
-template <class T, class R, class Rr, bool AnyHit, class Stack = SharedStack>
+// Count: keep the per-query visit and test counts (the counting pass; the timed kernels leave them out).
+template <class T, class R, class Rr, bool AnyHit, class Stack = SharedStack, bool Count = true>
 struct Traversal {
     RayQuery<T> q;
     V3<T> inv, oinv;
@@ -323,7 +324,7 @@ struct Traversal {
             if (primBits) {
                 const uint32_t b = uint32_t(__ffs(primBits) - 1);
                 primBits &= primBits - 1u;
-                ++primTests;
+                if (Count) ++primTests;
                 if (testPrim(sc, primBase + b) && AnyHit) return kTraceHit;
                 continue;
             }
@@ -346,7 +347,7 @@ struct Traversal {
             }
             NodeWords nd;
             loadNode(sc.nodes, node, nd);
-            ++nodeVisits;
+            if (Count) ++nodeVisits;
             const uint32_t mask = intersectChildren(nd, inv, oinv, T(0), best);
             const uint32_t inner = nd.a.w >> 24;
             nodeBase = nd.b.x;

@@ -205,14 +205,14 @@ __device__ __forceinline__ void warpFlush(unsigned long long* counter, uint32_t 
 // Closest crossing of every active path's ray. Persistent: each lane advances its query a few
 // visits at a time and, when it ends, takes the next query of the queue, so that lanes whose rays
 // finish early do not idle until the warp's longest ray is done.
-template <int M>
+template <int M, bool Count>
 __global__ void OWEC_TRAVERSAL_BOUNDS kIntersect(DeviceScene sc, PathBuffers<RT<M>> pb, Queues q, int cur,
                                                   StatCounters* st, uint32_t* fetch) {
     using R = RT<M>;
     extern __shared__ StackEntry stackMem[];
     StackEntry* stack = stackMem + threadIdx.x;
     const uint32_t n = q.counts[cur];
-    Traversal<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false> tr;
+    Traversal<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false, SharedStack, Count> tr;
     uint32_t path = 0, segments = 0, faults = 0;
     bool alive = false, exhausted = false;
     for (;;) {
@@ -250,7 +250,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kIntersect(DeviceScene sc, PathBuffers<RT<
                 if (s != kTraceHit) { h.boundary = kNone; h.t = INFINITY; }
                 if (s == kTraceOverflow) h.boundary = kNone - 1u;  // a fault: the path ends
                 pb.hit[path] = h;
-                if (sc.travCounters) countTraversal(sc.travCounters, nv, nt);
+                if (Count) countTraversal(sc.travCounters, nv, nt);
                 ++segments;
                 faults += s == kTraceOverflow;
                 alive = false;
@@ -424,18 +424,28 @@ __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kMedium(DeviceSc
         pb.aux[i] = aux;
         queueNee<M>(sc, pb, q, i, sp, betaNee, ls, fN, pdfS, R(1), sp3, ray.region, kNone, kNone, 0.f, neeValid);
         warpCount(&st->leaks, leak);
-        warpPush(q.surface, &q.counts[2], toSurface, i);
+        // surface events on Lambertian, absorbing and detecting boundaries go to the lean kernel
+        bool simple = false;
+        if (toSurface) {
+            const int32_t ot = sc.optics[sc.boundaries[h.boundary].optics].type;
+            simple = ot == OWEC_SURF_DIFFUSE || ot == OWEC_SURF_ABSORBER || ot == OWEC_SURF_DETECTOR;
+        }
+        warpPush(q.surface, &q.counts[2], toSurface && !simple, i);
+        warpPush(q.surfaceSimple, &q.counts[6], toSurface && simple, i);
         warpPush(q.active[nxt], &q.counts[nxt], cont, i);
     }
 }
 
 // ------------------------------------------------------------------ surface
-template <class R>
+template <class R, bool Lambertian = false>
 __device__ __forceinline__ Interface<R> makeInterface(const DeviceScene& sc, const DBoundary& bd, const V3<R>& n, R lambda,
                                                       R fresnelFloor) {
     Interface<R> it;
     it.o = sc.optics[bd.optics];
     it.n = n;
+    // a Lambertian interface as a compile-time fact (the lean surface kernel), so that the lobe
+    // switches fold away
+    if (Lambertian) it.o.type = OWEC_SURF_DIFFUSE;
     // only the dielectric and conductor lobes read the indices (a Lambertian surface, the most
     // common, skips two index evaluations per wavelength)
     if (it.o.type == OWEC_SURF_DIELECTRIC || it.o.type == OWEC_SURF_CONDUCTOR) {
@@ -450,16 +460,20 @@ __device__ __forceinline__ Interface<R> makeInterface(const DeviceScene& sc, con
     return it;
 }
 
-template <int M>
+// Simple: the lean instantiation for the simple surface queue (Lambertian, absorbing and detecting
+// boundaries): the other lobes, dispersion and the index models compile out, and with them most of
+// the registers.
+template <int M, bool Simple>
 __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kSurface(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
                                                 int cur, StatCounters* st) {
     using R = RT<M>;
     using Ro = typename Mode<M>::Ro;
     using Rr = typename Mode<M>::Rr;
     const int nxt = cur ^ 1;
-    const uint32_t n = q.counts[2];
+    const uint32_t n = Simple ? q.counts[6] : q.counts[2];
+    const uint32_t* queue = Simple ? q.surfaceSimple : q.surface;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const uint32_t i = q.surface[k];
+        const uint32_t i = queue[k];
         PathRay<R> ray = pb.ray[i];
         PathSpec<R> sp = pb.spec[i];
         PathAux aux = pb.aux[i];
@@ -498,18 +512,19 @@ __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kSurface(DeviceS
         R betaNee[NW] = {R(0), R(0), R(0), R(0)};
         R pdfS = R(0), cosF = R(0);
         uint32_t neeRegion = ray.region;
-        if (o.type == OWEC_SURF_NULL) {
+        if (!Simple && o.type == OWEC_SURF_NULL) {
             ray.region = other;
             setOrigin<M>(ray.o, g.p);
             ray.depB = h.boundary;
             ray.depP = h.prim;
             ray.errN = errN;
             cont = int(aux.depth) < 4 * pp.maxDepth;
-        } else if (o.type != OWEC_SURF_ABSORBER && o.type != OWEC_SURF_DETECTOR && int(aux.depth) < pp.maxDepth) {
+        } else if ((Simple ? o.type == OWEC_SURF_DIFFUSE : (o.type != OWEC_SURF_ABSORBER && o.type != OWEC_SURF_DETECTOR)) &&
+                   int(aux.depth) < pp.maxDepth) {
             // scatterAtSurface (transport.cpp:437-471)
             const R hero = R(sp.lambda[0]);
-            const Interface<R> it = makeInterface(sc, bd, g.n, hero, R(pp.fresnelFloor));
-            if (o.type == OWEC_SURF_DIELECTRIC) {  // terminateIfDispersive
+            const Interface<R> it = makeInterface<R, Simple>(sc, bd, g.n, hero, R(pp.fresnelFloor));
+            if (!Simple && o.type == OWEC_SURF_DIELECTRIC) {  // terminateIfDispersive
                 bool alive2 = false;
                 for (int j = 1; j < NW; ++j) alive2 = alive2 || sp.pdf[j] != 0.f;
                 if (alive2) {
@@ -526,7 +541,7 @@ __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kSurface(DeviceS
                 }
             }
             for (int j = 0; j < NW; ++j) betaNee[j] = sp.beta[j];  // directLighting sees beta before the scatter
-            if (!isDeltaOptics<R>(o)) {
+            if (Simple || !isDeltaOptics<R>(o)) {
                 int li;
                 if (sampleLight<R>(sc, g.p, rng, ls, li)) {
                     bool leZero = true;
@@ -539,7 +554,7 @@ __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kSurface(DeviceS
                             if (sp.pdf[j] == 0.f) continue;
                             R pdf;
                             const Interface<R> itj =
-                                j == 0 ? it : makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(pp.fresnelFloor));
+                                j == 0 ? it : makeInterface<R, Simple>(sc, bd, g.n, R(sp.lambda[j]), R(pp.fresnelFloor));
                             fN[j] = evalScatter(sc, itj, d, wi, true, pdf);
                             if (j == 0) pdfS = pdf;
                             if (fN[j] != R(0)) fZero = false;
@@ -560,7 +575,7 @@ __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kSurface(DeviceS
                 sp.beta[0] *= s.weight;
                 for (int j = 1; j < NW; ++j) {
                     if (sp.pdf[j] == 0.f) continue;
-                    const Interface<R> itj = makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(pp.fresnelFloor));
+                    const Interface<R> itj = makeInterface<R, Simple>(sc, bd, g.n, R(sp.lambda[j]), R(pp.fresnelFloor));
                     sp.beta[j] *= secondaryScatterWeight(sc, itj, d, s, true);
                 }
                 if (s.transmitted) ray.region = other;
@@ -600,7 +615,7 @@ __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kSurface(DeviceS
 // Persistent like kIntersect: a lane's job is one shadow ray, walked segment by segment through
 // null boundaries; its traversal advances a few visits per round and a finished lane takes the
 // next job.
-template <int M, bool AnyHit>
+template <int M, bool AnyHit, bool Count>
 __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
                                                StatCounters* st, uint32_t* fetch) {
     using R = RT<M>;
@@ -609,7 +624,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
     extern __shared__ StackEntry stackMem[];
     StackEntry* stack = stackMem + threadIdx.x;
     const uint32_t n = q.counts[3];
-    Traversal<R, Ro, Rr, AnyHit> tr;
+    Traversal<R, Ro, Rr, AnyHit, SharedStack, Count> tr;
     R Tr[NW];
     double remaining = 0;
     uint32_t job = 0, path = 0, region = 0, guard = 0, rays = 0, faults = 0;
@@ -654,7 +669,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
                 nv += d.visits;
                 nt += d.tests;
             }
-            if (sc.travCounters) countTraversal(sc.travCounters + 3, nv, nt);
+            if (Count) countTraversal(sc.travCounters + 3, nv, nt);
             ++guard;
             if (s == kTraceOverflow) {
                 outcome = 3;
@@ -880,7 +895,10 @@ void launchGenerate(const DeviceScene& sc, const PassParams& pp, const PathBuffe
 template <int M>
 void launchIntersect(const DeviceScene& sc, const PathBuffers<RT<M>>& pb, const Queues& q, int cur, StatCounters* st,
                      uint32_t* fetch, int grid, cudaStream_t s) {
-    kIntersect<M><<<grid, 128, traversalSharedBytes(128), s>>>(sc, pb, q, cur, st, fetch);
+    if (sc.travCounters)
+        kIntersect<M, true><<<grid, 128, traversalSharedBytes(128), s>>>(sc, pb, q, cur, st, fetch);
+    else
+        kIntersect<M, false><<<grid, 128, traversalSharedBytes(128), s>>>(sc, pb, q, cur, st, fetch);
 }
 template <int M>
 void launchMedium(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q, int cur,
@@ -890,15 +908,20 @@ void launchMedium(const DeviceScene& sc, const PassParams& pp, const PathBuffers
 template <int M>
 void launchSurface(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q, int cur,
                    StatCounters* st, int grid, cudaStream_t s) {
-    kSurface<M><<<grid, 128, 0, s>>>(sc, pp, pb, q, cur, st);
+    kSurface<M, true><<<grid, 128, 0, s>>>(sc, pp, pb, q, cur, st);
+    kSurface<M, false><<<grid, 128, 0, s>>>(sc, pp, pb, q, cur, st);
 }
 template <int M>
 void launchShadow(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q,
                   StatCounters* st, uint32_t* fetch, int grid, cudaStream_t s) {
-    if (pp.anyHitShadows)
-        kShadow<M, true><<<grid, 128, traversalSharedBytes(128), s>>>(sc, pp, pb, q, st, fetch);
-    else
-        kShadow<M, false><<<grid, 128, traversalSharedBytes(128), s>>>(sc, pp, pb, q, st, fetch);
+    const size_t smem = traversalSharedBytes(128);
+    if (pp.anyHitShadows) {
+        if (sc.travCounters) kShadow<M, true, true><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch);
+        else kShadow<M, true, false><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch);
+    } else {
+        if (sc.travCounters) kShadow<M, false, true><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch);
+        else kShadow<M, false, false><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch);
+    }
 }
 template <int M>
 void launchFilm(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, double* film, double* comp,
@@ -924,9 +947,12 @@ void launchMaterialize(const uint32_t* leafOrder, uint32_t n, const float4* tri,
 }
 void configureKernels() {
     const int smem = int(traversalSharedBytes(128));
-    cudaFuncSetAttribute(kIntersect<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(kIntersect<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(kIntersect<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kIntersect<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kIntersect<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kIntersect<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kIntersect<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kIntersect<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kIntersect<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
 #define OWEC_INSTANTIATE(M)                                                                                         \
