@@ -409,9 +409,9 @@ def run_cuda(args):
             line["precision_study"] = precision_study(local)
             line["adjoint_study"] = adjoint_study(local)
             line["configs_study"] = configs_study(local)
-        # our own kernel launches in the timed region: intersect, medium, two surface kernels and
-        # shadow per bounce, and generate + film per step
-        line["gpu_launches"] = int(5 * launches + 2 * args.steps)
+        # our own kernel launches in the timed region: intersect, medium, two surface kernels, the
+        # shadow visibility and its contributions per bounce, and generate + film per step
+        line["gpu_launches"] = int(6 * launches + 2 * args.steps)
         print(json.dumps(line))
     renderer.close()
     if world > 1:

@@ -248,6 +248,7 @@ struct owec_ctx {
     DBuf<double> dResolved;  // owec_resolve's per-pixel XYZ, read back in one copy
     DBuf<uint8_t> dPathRay, dPathSpec, dPathAux, dHit, dShadow;
     DBuf<uint32_t> dQueue0, dQueue1, dQueueSurf, dQueueSurfSimple, dQueueShadow, dCounts;
+    DBuf<uint8_t> dShadowVis;  // per shadow-queue entry: 0 blocked, 1 clear, 2 fault
     DBuf<StatCounters> dStats;
     DBuf<unsigned long long> dTravCounters;
     uint32_t capacity = 0;
@@ -711,6 +712,7 @@ void runPass(owec_ctx& c, int spp) {
         c.dQueue1.resize(cap);
         c.dQueueSurf.resize(cap);
         c.dQueueSurfSimple.resize(cap);
+        c.dShadowVis.resize(cap);
         c.dQueueShadow.resize(cap);
         c.capacity = cap;
     }
@@ -772,7 +774,7 @@ void runPass(owec_ctx& c, int spp) {
             launchMedium<M>(c.ds, pp, pb, q, cur, c.dStats.get(), grid, s);
             launchSurface<M>(c.ds, pp, pb, q, cur, c.dStats.get(), grid, s);
             OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 2], s));
-            launchShadow<M>(c.ds, pp, pb, q, c.dStats.get(), c.dCounts.get() + 5, grid, s);
+            launchShadow<M>(c.ds, pp, pb, q, c.dStats.get(), c.dCounts.get() + 5, c.dShadowVis.get(), grid, s);
             OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 3], s));
             checkLaunch();
             evUsed += 4;

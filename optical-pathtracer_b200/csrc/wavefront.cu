@@ -751,6 +751,105 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
     warpFlush(&st->faults, faults);
 }
 
+// Without null boundaries a shadow ray is one any-hit query, and its bookkeeping (the medium's
+// transmittance, the arrival region, the contribution) needs nothing of the traversal. kShadowVis
+// runs the queries alone, persistent like kIntersect, and records one visibility byte per shadow ray
+// (0 blocked, 1 clear, 2 fault); kShadowApply then adds the contributions in one coalesced pass,
+// so the bookkeeping does not run divergently inside the traversal loop.
+template <int M, bool Count>
+__global__ void OWEC_TRAVERSAL_BOUNDS kShadowVis(DeviceScene sc, PathBuffers<RT<M>> pb, Queues q, uint8_t* vis,
+                                                  uint32_t* fetch) {
+    using R = RT<M>;
+    using Ro = typename Mode<M>::Ro;
+    using Rr = typename Mode<M>::Rr;
+    extern __shared__ StackEntry stackMem[];
+    StackEntry* stack = stackMem + threadIdx.x;
+    const uint32_t n = q.counts[3];
+    Traversal<R, Ro, Rr, true, SharedStack, Count> tr;
+    uint32_t job = 0;
+    bool alive = false, exhausted = false;
+    for (;;) {
+        const uint32_t k = refillLanes(!alive, fetch, n, exhausted);
+        if (!alive && k < n) {
+            const ShadowRay<R>& sr = pb.shadow[k];
+            job = k;
+            const double tmax = sr.tmax;
+            const bool finite = !isinf(tmax);
+            // stop short of the light's own surface
+            const double tq = finite ? tmax - (4e-6 * tmax + double(sr.errN) + 1e-9) : INFINITY;
+            if (finite && tq <= 0) {
+                vis[k] = 1;
+            } else {
+                RayQuery<R> rq;
+                rq.od = rayOrigin(sr.o);
+                rq.o = V3<R>(rq.od);
+                rq.d = V3<R>(sr.d[0], sr.d[1], sr.d[2]);
+                rq.depB = sr.depB;
+                rq.depP = sr.depP;
+                rq.errN = R(sr.errN);
+                rq.tmax = R(tq);
+                rq.region = sr.region;
+                tr.begin(rq, stack, blockDim.x);
+                alive = true;
+            }
+        }
+        if (__ballot_sync(0xFFFFFFFFu, alive) == 0 && exhausted) break;
+        if (!alive) continue;
+        int s = tr.run(sc, kRefillBudget);
+        if (s == kTraceRunning) continue;
+        uint32_t nv = tr.nodeVisits, nt = tr.primTests;
+        if (s == kTraceOverflow) {
+            HitRec h = tr.hit;
+            h.boundary = kNone;
+            const DeepResult d = traceRayDeep<R, Ro, Rr, true>(sc, tr.q, h);
+            s = d.status;
+            nv += d.visits;
+            nt += d.tests;
+        }
+        if (Count) countTraversal(sc.travCounters + 3, nv, nt);
+        vis[job] = s == kTraceOverflow ? uint8_t(2) : (s == kTraceHit ? uint8_t(0) : uint8_t(1));
+        alive = false;
+    }
+}
+
+template <int M>
+__global__ void __launch_bounds__(256) kShadowApply(DeviceScene sc, PathBuffers<RT<M>> pb, Queues q, const uint8_t* vis,
+                                                    StatCounters* st) {
+    using R = RT<M>;
+    const uint32_t n = q.counts[3];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint8_t v = vis[k];
+        bool clear = v == 1;
+        if (clear) {
+            const ShadowRay<R> sr = pb.shadow[k];
+            const bool finite = !isinf(sr.tmax);
+            // Tracer::transmittance's one segment (transport.cpp:237-308): the medium it crosses
+            R Tr[NW] = {R(1), R(1), R(1), R(1)};
+            const owec_medium& med = sc.media[sc.regionMedium[sr.region]];
+            if (mediumAbsorbs(med, sc) || mediumScatters(med, sc)) {
+                if (!finite) {
+                    clear = false;
+                } else {
+                    const PathSpec<R>& spc = pb.spec[sr.path];
+                    for (int j = 0; j < NW; ++j) {
+                        const R lam = R(spc.lambda[j]);
+                        Tr[j] = exp(-(evalSpectrum(sc, med.absorption, lam) + evalSpectrum(sc, med.scattering, lam)) *
+                                    R(sr.tmax));
+                    }
+                }
+            }
+            if (!finite && sr.region != 0) clear = false;
+            if (finite && sr.region != sr.endRegion) clear = false;
+            if (clear) {
+                float* L = pb.spec[sr.path].L;
+                for (int j = 0; j < NW; ++j) L[j] += float(R(sr.contrib[j]) * Tr[j]);
+            }
+        }
+        warpCount(&st->shadowRays, true);
+        warpCount(&st->faults, v == 2);
+    }
+}
+
 // ------------------------------------------------------------------ film
 // Folds the batch's samples of every pixel into the film in sample order: XYZ of each path
 // (Wavelengths::toXYZ of L * weight, wavelengths.hpp:71-84), skipping non-finite estimates as
@@ -913,11 +1012,12 @@ void launchSurface(const DeviceScene& sc, const PassParams& pp, const PathBuffer
 }
 template <int M>
 void launchShadow(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q,
-                  StatCounters* st, uint32_t* fetch, int grid, cudaStream_t s) {
+                  StatCounters* st, uint32_t* fetch, uint8_t* vis, int grid, cudaStream_t s) {
     const size_t smem = traversalSharedBytes(128);
     if (pp.anyHitShadows) {
-        if (sc.travCounters) kShadow<M, true, true><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch);
-        else kShadow<M, true, false><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch);
+        if (sc.travCounters) kShadowVis<M, true><<<grid, 128, smem, s>>>(sc, pb, q, vis, fetch);
+        else kShadowVis<M, false><<<grid, 128, smem, s>>>(sc, pb, q, vis, fetch);
+        kShadowApply<M><<<grid, 256, 0, s>>>(sc, pb, q, vis, st);
     } else {
         if (sc.travCounters) kShadow<M, false, true><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch);
         else kShadow<M, false, false><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch);
@@ -965,7 +1065,7 @@ void configureKernels() {
     template void launchSurface<M>(const DeviceScene&, const PassParams&, const PathBuffers<RT<M>>&, const Queues&,  \
                                    int, StatCounters*, int, cudaStream_t);                                          \
     template void launchShadow<M>(const DeviceScene&, const PassParams&, const PathBuffers<RT<M>>&, const Queues&,   \
-                                  StatCounters*, uint32_t*, int, cudaStream_t);                                                \
+                                  StatCounters*, uint32_t*, uint8_t*, int, cudaStream_t);                                                \
     template void launchFilm<M>(const DeviceScene&, const PassParams&, const PathBuffers<RT<M>>&, double*, double*,  \
                                 double*, uint32_t, cudaStream_t);                                                   \
     template void launchCastRays<M>(const DeviceScene&, uint64_t, const double*, const double*, uint32_t*,          \

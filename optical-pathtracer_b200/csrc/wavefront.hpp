@@ -27,7 +27,7 @@ void launchSurface(const DeviceScene&, const PassParams&, const PathBuffers<Mode
                    StatCounters*, int grid, cudaStream_t);
 template <int M>
 void launchShadow(const DeviceScene&, const PassParams&, const PathBuffers<ModeR<M>>&, const Queues&, StatCounters*,
-                  uint32_t* fetch, int grid, cudaStream_t);
+                  uint32_t* fetch, uint8_t* vis, int grid, cudaStream_t);
 void launchResolve(const double* film, const double* comp, const double* samples, uint32_t nPixels, double* xyz,
                    cudaStream_t);
 template <int M>
