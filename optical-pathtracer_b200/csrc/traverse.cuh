@@ -165,12 +165,6 @@ __device__ __forceinline__ void loadNode(const WideNode* nodes, uint32_t i, Node
 #endif
 }
 
-// Byte k (0..3) of w as an exact float: the byte placed in the mantissa of 2^23, minus 2^23. One
-// byte permute and one add, on the integer and FMA pipes, where a conversion instruction would
-// queue on the narrow conversion pipe (eight children x six planes per node).
-__device__ __forceinline__ float byteAsFloat(uint32_t w, int k) {
-    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | uint32_t(k))) - 8388608.0f;
-}
 
 // Decoded child boxes of a node, slab-tested against the ray. Returns the hit mask (slot order).
 template <class T>
@@ -178,17 +172,25 @@ __device__ __forceinline__ uint32_t intersectChildren(const NodeWords& nd, const
     const T sx = T(__uint_as_float((nd.a.w & 0xFFu) << 23));
     const T sy = T(__uint_as_float(((nd.a.w >> 8) & 0xFFu) << 23));
     const T sz = T(__uint_as_float(((nd.a.w >> 16) & 0xFFu) << 23));
-    // t = (origin + q * s - o) * inv = q * (s * inv) + (origin * inv - o * inv)
+    // t = (origin + q * s - o) * inv = q * (s * inv) + (origin * inv - o * inv). A plane byte q enters
+    // as the float f = 2^23 + 256 q (one byte permute places it in the second mantissa byte), so
+    // t = f * (a / 256) + (b - 2^15 a) with a = s * inv: one FMA per plane and no conversion. a / 256
+    // and 2^15 a are exact; the one rounding of b - 2^15 a is below 2^-9 a + half an ulp of b, taken
+    // off the near planes and added to the far ones (with their widening against the FMA's own
+    // rounding), so the boxes stay conservative and grow by well under a percent of a quantum.
     const T ax = sx * inv.x, ay = sy * inv.y, az = sz * inv.z;
-    const T bx = T(__uint_as_float(nd.a.x)) * inv.x - oinv.x;
-    const T by = T(__uint_as_float(nd.a.y)) * inv.y - oinv.y;
-    const T bz = T(__uint_as_float(nd.a.z)) * inv.z - oinv.z;
-    // Far planes are widened against rounding once per node: by a few ulps of the largest far
-    // distance the node's children can have on that axis, where a factor per child cost eight
-    // multiplies.
-    const T fbx = bx + (fabs(bx) + T(255) * fabs(ax)) * farWiden<T>();
-    const T fby = by + (fabs(by) + T(255) * fabs(ay)) * farWiden<T>();
-    const T fbz = bz + (fabs(bz) + T(255) * fabs(az)) * farWiden<T>();
+    const T ax8 = ax * T(0.00390625), ay8 = ay * T(0.00390625), az8 = az * T(0.00390625);
+    const T b0x = T(__uint_as_float(nd.a.x)) * inv.x - oinv.x;
+    const T b0y = T(__uint_as_float(nd.a.y)) * inv.y - oinv.y;
+    const T b0z = T(__uint_as_float(nd.a.z)) * inv.z - oinv.z;
+    const T bx = b0x - T(32768) * ax, by = b0y - T(32768) * ay, bz = b0z - T(32768) * az;
+    const T mx = T(0.00390625) * fabs(ax) + T(2.4e-7) * fabs(bx);
+    const T my = T(0.00390625) * fabs(ay) + T(2.4e-7) * fabs(by);
+    const T mz = T(0.00390625) * fabs(az) + T(2.4e-7) * fabs(bz);
+    const T nbx = bx - mx, nby = by - my, nbz = bz - mz;
+    const T fbx = bx + mx + (fabs(b0x) + T(255) * fabs(ax)) * farWiden<T>();
+    const T fby = by + my + (fabs(b0y) + T(255) * fabs(ay)) * farWiden<T>();
+    const T fbz = bz + mz + (fabs(b0z) + T(255) * fabs(az)) * farWiden<T>();
     const bool nx = inv.x < T(0), ny = inv.y < T(0), nz = inv.z < T(0);
     // near and far planes per axis, chosen by the ray's direction on whole words
     const uint32_t nxl0 = nx ? nd.d.z : nd.c.x, nxl1 = nx ? nd.d.w : nd.c.y;
@@ -201,13 +203,16 @@ __device__ __forceinline__ uint32_t intersectChildren(const NodeWords& nd, const
     // an empty slot's box is stored inverted (low planes 255, high planes 0), so it never passes
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        const int k = i & 3;
-        const T lx = T(byteAsFloat(i < 4 ? nxl0 : nxl1, k)), hx = T(byteAsFloat(i < 4 ? fxl0 : fxl1, k));
-        const T ly = T(byteAsFloat(i < 4 ? nyl0 : nyl1, k)), hy = T(byteAsFloat(i < 4 ? fyl0 : fyl1, k));
-        const T lz = T(byteAsFloat(i < 4 ? nzl0 : nzl1, k)), hz = T(byteAsFloat(i < 4 ? fzl0 : fzl1, k));
-        const T t0x = fma(lx, ax, bx), t1x = fma(hx, ax, fbx);
-        const T t0y = fma(ly, ay, by), t1y = fma(hy, ay, fby);
-        const T t0z = fma(lz, az, bz), t1z = fma(hz, az, fbz);
+        const uint32_t sel = 0x7504u | (uint32_t(i & 3) << 4);
+        const T lx = T(__uint_as_float(__byte_perm(i < 4 ? nxl0 : nxl1, 0x4B000000u, sel)));
+        const T hx = T(__uint_as_float(__byte_perm(i < 4 ? fxl0 : fxl1, 0x4B000000u, sel)));
+        const T ly = T(__uint_as_float(__byte_perm(i < 4 ? nyl0 : nyl1, 0x4B000000u, sel)));
+        const T hy = T(__uint_as_float(__byte_perm(i < 4 ? fyl0 : fyl1, 0x4B000000u, sel)));
+        const T lz = T(__uint_as_float(__byte_perm(i < 4 ? nzl0 : nzl1, 0x4B000000u, sel)));
+        const T hz = T(__uint_as_float(__byte_perm(i < 4 ? fzl0 : fzl1, 0x4B000000u, sel)));
+        const T t0x = fma(lx, ax8, nbx), t1x = fma(hx, ax8, fbx);
+        const T t0y = fma(ly, ay8, nby), t1y = fma(hy, ay8, fby);
+        const T t0z = fma(lz, az8, nbz), t1z = fma(hz, az8, fbz);
         const T te = fmax(fmax(t0x, t0y), fmax(t0z, tmin));
         const T tx = fmin(fmin(t1x, t1y), t1z);
         const T tl = fmin(tx, tmax);

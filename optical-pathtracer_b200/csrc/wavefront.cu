@@ -319,10 +319,23 @@ __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kMedium(DeviceSc
     const uint32_t n = q.counts[cur];
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const uint32_t i = q.active[cur][k];
+        const HitRec h = pb.hit[i];
+        {
+            // A segment through a region without absorption or scattering that met a boundary has
+            // no medium event (sampleMedium draws nothing and changes nothing): straight to the
+            // surface queues, without reading or writing the rest of the path's state.
+            const owec_medium& m0 = sc.media[sc.regionMedium[pb.ray[i].region]];
+            if (h.boundary < kNone - 1u && !mediumAbsorbs(m0, sc) && !mediumScatters(m0, sc)) {
+                const int32_t ot = sc.optics[sc.boundaries[h.boundary].optics].type;
+                const bool simple = ot == OWEC_SURF_DIFFUSE || ot == OWEC_SURF_ABSORBER || ot == OWEC_SURF_DETECTOR;
+                warpPush(q.surface, &q.counts[2], !simple, i);
+                warpPush(q.surfaceSimple, &q.counts[6], simple, i);
+                continue;
+            }
+        }
         PathRay<R> ray = pb.ray[i];
         PathSpec<R> sp = pb.spec[i];
         PathAux aux = pb.aux[i];
-        const HitRec h = pb.hit[i];
         Pcg32 rng{aux.rngState, (uint64_t(aux.stream) << 1u) | 1u};
         const bool fault = h.boundary == kNone - 1u;
         const bool found = h.boundary < kNone - 1u;
@@ -463,8 +476,11 @@ __device__ __forceinline__ Interface<R> makeInterface(const DeviceScene& sc, con
 // Simple: the lean instantiation for the simple surface queue (Lambertian, absorbing and detecting
 // boundaries): the other lobes, dispersion and the index models compile out, and with them most of
 // the registers.
+#ifndef OWEC_SIMPLE_MIN_BLOCKS
+#define OWEC_SIMPLE_MIN_BLOCKS 4
+#endif
 template <int M, bool Simple>
-__global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kSurface(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
+__global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SHADING_MIN_BLOCKS) kSurface(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
                                                 int cur, StatCounters* st) {
     using R = RT<M>;
     using Ro = typename Mode<M>::Ro;
