@@ -77,12 +77,22 @@ __device__ SurfacePoint<R> hitGeometry(const DeviceScene& sc, const PathRay<R>& 
     const V3<double> od(ray.o[0], ray.o[1], ray.o[2]);
     const V3<R> d(ray.d[0], ray.d[1], ray.d[2]);
     if (bd.shape == OWEC_SHAPE_MESH) {
-        V3<R> v0, v1, v2;
-        uint32_t b, prim, kind;
-        TriFetch<R>::get(sc, h.slot, v0, v1, v2, b, prim, kind);
-        const double t = sizeof(Rr) == sizeof(double) ? refineTriangleT(sc, h.slot, od, V3<double>(d), h.t) : h.t;
-        sp.p = od + V3<double>(d) * t;
-        sp.n = normalize(triangleNormal(v0, v1, v2));
+        if (sizeof(Rr) == sizeof(double)) {
+            // the FP64 vertices alone: the refined distance and the normal from them
+            const PrimRec64& p = sc.prims64[h.slot];
+            const V3<double> v0(p.v0[0], p.v0[1], p.v0[2]), v1(p.v1[0], p.v1[1], p.v1[2]),
+                v2(p.v2[0], p.v2[1], p.v2[2]);
+            const V3<double> n = triangleNormal(v0, v1, v2);
+            const double t = dot(v0 - od, n) / dot(V3<double>(d), n);
+            sp.p = od + V3<double>(d) * ((t > 0 && fabs(t - h.t) <= 1e-3 * (1 + fabs(h.t))) ? t : h.t);
+            sp.n = V3<R>(normalize(n));
+        } else {
+            V3<R> v0, v1, v2;
+            uint32_t b, prim, kind;
+            TriFetch<R>::get(sc, h.slot, v0, v1, v2, b, prim, kind);
+            sp.p = od + V3<double>(d) * h.t;
+            sp.n = normalize(triangleNormal(v0, v1, v2));
+        }
         sp.pLocal = bd.toLocal.point(sp.p);
         sp.nLocal = bd.toLocal.vector(V3<double>(sp.n));
         return sp;
