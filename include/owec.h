@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define OWEC_ABI_VERSION 2
+#define OWEC_ABI_VERSION 3
 
 /* ------------------------------------------------------------------ status codes */
 #define OWEC_OK 0
@@ -205,6 +205,12 @@ typedef struct owec_scene_desc {
 #define OWEC_PRECISION_FP32 1   /* plain FP32 everywhere (the baseline the mixed mode is measured against) */
 #define OWEC_PRECISION_FP64 2   /* all-FP64 instantiation of the same kernels */
 
+/* Integrators (RenderSettings::integrator, src/owe/scene/scene.hpp:19). */
+#define OWEC_INTEGRATOR_PATH 0   /* "path": camera paths with next-event estimation (Tracer::radiance) */
+#define OWEC_INTEGRATOR_LIGHT 1  /* "light": particles from the emitters, connected to the pinhole at every
+                                  * non-specular vertex, or recorded where they reach a surface sensor (the
+                                  * reference's GPU particle pass, src/owe/backends/gpu/shaders/particle.slang) */
+
 typedef struct owec_settings {
     uint64_t seed;          /* RenderSettings::seed (src/owe/scene/scene.hpp:15-49) */
     int32_t max_depth;      /* RenderSettings::maxDepth */
@@ -214,6 +220,8 @@ typedef struct owec_settings {
     double lambda_min;      /* OWEC_WAVELENGTHS_UNIFORM1 range, nm */
     double lambda_max;
     double fresnel_floor;   /* RenderSettings::fresnelFloor */
+    int32_t integrator;     /* OWEC_INTEGRATOR_* */
+    int32_t pad0;
 } owec_settings;
 
 /* Transport statistics (src/owe/scene/transport_stats.hpp:12-31) plus device counters. */
@@ -255,14 +263,21 @@ int owec_set_settings(owec_ctx* ctx, const owec_settings* settings);
 /* One pass of `spp` samples per pixel (Renderer::pass, src/owe/render/renderer.hpp:63;
  * CpuRenderer::pass, src/owe/backends/cpu/cpu_backend.cpp:52-94). Sample s of the pass draws
  * from the PCG32 stream (hashCombine(seed, pixel), pass_index + s): a 1-spp pass reproduces the
- * reference's per-pixel stream exactly. Synchronous at return. */
+ * reference's per-pixel stream exactly. With OWEC_INTEGRATOR_LIGHT a pass emits width x height x
+ * spp particles (the reference GPU renderer's passParticles, gpu_renderer_passes.cpp:303-311),
+ * particle i drawing from the stream (hashCombine(seed ^ 0x5bd1e995, i), pass_index).
+ * Synchronous at return. */
 int owec_pass(owec_ctx* ctx, int spp);
 /* Resolved image: XYZ per pixel (3 doubles, row-major) and samples per pixel
- * (CpuRenderer::resolve, src/owe/backends/cpu/cpu_backend.cpp:96-107). Either pointer may be NULL. */
+ * (CpuRenderer::resolve, src/owe/backends/cpu/cpu_backend.cpp:96-107). Either pointer may be NULL.
+ * With OWEC_INTEGRATOR_LIGHT the image is the particle splats over the particles emitted
+ * (GpuRenderer::resolve, gpu_renderer_film.cpp:17-21) and `samples` is spp summed over the passes. */
 int owec_resolve(owec_ctx* ctx, double* xyz, double* samples);
 /* The film as sums: the compensated per-pixel XYZ sums (3 doubles, row-major) and the samples per
  * pixel, which the ranks of a multi-GPU render add up before dividing. No counterpart in the
- * reference, which renders on one device. Either pointer may be NULL. */
+ * reference, which renders on one device. Either pointer may be NULL. With OWEC_INTEGRATOR_LIGHT the
+ * sums are the particle splats over width x height and the samples spp summed over the passes, so
+ * that sums / samples is the resolved image there too. */
 int owec_read_film(owec_ctx* ctx, double* xyz_sums, double* samples);
 /* Sets the index of the next pass's first sample stream (the pass index of owec_pass): each rank
  * of a multi-GPU render starts its share of the streams there, so that the ranks together draw

@@ -15,6 +15,7 @@
 
 #include "bvh_build.hpp"
 #include "owec.h"
+#include "particle.hpp"
 #include "spectral.cuh"
 #include "walk.hpp"
 #include "wavefront.hpp"
@@ -221,6 +222,8 @@ struct owec_ctx {
     uint32_t nTriangles = 0, nPrims = 0;
     bool hasNull = false;
     DeviceScene ds{};
+    // particles: the sky's share of the emitted power and the disc distant light leaves from
+    double pSky = 0, discRadius = 1, discCentre[3] = {0, 0, 0};
 
     // scene (device)
     DBuf<owec_spectrum> dSpectra;
@@ -242,10 +245,12 @@ struct owec_ctx {
     bool prims64Ready = false;
 
     // rendering
-    owec_settings settings{1, 64, 6, OWEC_WAVELENGTHS_HERO4, OWEC_PRECISION_MIXED, 380, 780, 0};
+    owec_settings settings{1, 64, 6, OWEC_WAVELENGTHS_HERO4, OWEC_PRECISION_MIXED, 380, 780, 0, OWEC_INTEGRATOR_PATH, 0};
     uint64_t passCount = 0;  // samples per pixel accumulated (the PCG32 stream of the next sample)
     DBuf<double> dFilm, dComp, dSamples;
     DBuf<double> dResolved;  // owec_resolve's per-pixel XYZ, read back in one copy
+    DBuf<unsigned long long> dSplat;  // the light integrator's film: fixed-point splat sums
+    double particles = 0;             // particles emitted into it
     DBuf<uint8_t> dPathRay, dPathSpec, dPathAux, dHit, dShadow;
     DBuf<uint32_t> dQueue0, dQueue1, dQueueSurf, dQueueSurfSimple, dQueueShadow, dCounts;
     DBuf<uint8_t> dShadowVis;  // per shadow-queue entry: 0 blocked, 1 clear, 2 fault
@@ -481,6 +486,20 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
     }
     if (!c.lights.empty()) c.lights.back().cdf = 1.0;
 
+    // Particles: the sky's share of the emitted power (World::computeEnvironmentPower for the
+    // uniform sky, world.cpp:352-368: its mean over 400..700 nm, times pi R^2 4 pi) and the disc the
+    // sun and the sky shine from, about the scene's centre.
+    double skyPower = 0;
+    if (d.env.sky_model == OWEC_SKY_UNIFORM && d.env.sky_radiance >= 0) {
+        double y = 0;
+        for (double l = 400; l <= 700; l += 50) y += evalSpectrumHost(d, d.env.sky_radiance, l);
+        skyPower = std::max(0.0, y / 7) * kPi * sceneRadius * sceneRadius * 4 * kPi;
+    }
+    const double emitted = skyPower + (c.lights.empty() ? 0.0 : total);
+    c.pSky = emitted > 0 ? skyPower / emitted : 0;
+    c.discRadius = sceneRadius * 1.001;
+    for (int k = 0; k < 3; ++k) c.discCentre[k] = center[k];
+
     // Primitives: every mesh triangle (camera-relative FP32, and FP64 for the all-FP64 mode), then
     // every analytic boundary as one primitive of its own world box.
     c.triRecs.clear();
@@ -641,6 +660,8 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
     c.dFilm.release();
     c.dComp.release();
     c.dSamples.release();
+    c.dSplat.release();
+    c.particles = 0;
 }
 
 void ensurePrims64(owec_ctx& c);
@@ -683,6 +704,11 @@ void ensureReady(owec_ctx& c) {
 
 void ensureFilm(owec_ctx& c) {
     const size_t np = size_t(c.ds.det.width) * c.ds.det.height;
+    if (c.settings.integrator == OWEC_INTEGRATOR_LIGHT && c.dSplat.size() != np * kSplatWordsPerPixel) {
+        c.dSplat.resize(np * kSplatWordsPerPixel);
+        OWEC_CUDA(cudaMemsetAsync(c.dSplat.get(), 0, c.dSplat.bytes(), c.stream));
+        c.particles = 0;
+    }
     if (c.dFilm.size() != 3 * np) {
         c.dFilm.resize(3 * np);
         c.dComp.resize(3 * np);
@@ -807,6 +833,48 @@ void runPass(owec_ctx& c, int spp) {
     c.lastIntersectSeconds = travSeconds[0];
     c.lastShadowSeconds = travSeconds[1];
     c.lastIntersectLaunches = intersectLaunches;
+    c.passCount += uint64_t(spp);
+}
+
+// A pass of the light integrator: width x height x spp particles, in launches of up to 2^22.
+void runParticles(owec_ctx& c, int spp) {
+    const DDetector& det = c.ds.det;
+    const uint64_t nPix = uint64_t(det.width) * uint64_t(det.height);
+    const uint64_t total = nPix * uint64_t(spp);
+    ParticleParams P{};
+    P.seed = c.settings.seed;
+    P.stream = c.passCount;
+    P.maxDepth = c.settings.max_depth;
+    P.rrDepth = c.settings.rr_depth;
+    P.wavelengthMode = c.settings.wavelength_mode;
+    P.lambdaMin = float(c.settings.lambda_min);
+    P.lambdaMax = float(c.settings.lambda_max);
+    P.fresnelFloor = float(std::min(0.49, std::max(0.0, c.settings.fresnel_floor)));
+    P.anyHitShadows = c.hasNull ? 0 : 1;
+    P.pSky = c.pSky;
+    P.discRadius = c.discRadius;
+    for (int k = 0; k < 3; ++k) P.discCentre[k] = c.discCentre[k];
+    P.pixelArea = det.kind == OWEC_DETECTOR_OBSERVER ? (2 * det.tanX / det.width) * (2 * det.tanY / det.height)
+                                                     : (2 * det.halfX / det.width) * (2 * det.halfY / det.height);
+    cudaStream_t s = c.stream;
+    OWEC_CUDA(cudaEventRecord(c.passStart, s));
+    // nothing emits: the estimate is zero, but the particles still count
+    if (c.pSky > 0 || !c.lights.empty()) {
+        const uint64_t chunk = 1ull << 22;
+        for (uint64_t first = 0; first < total; first += chunk) {
+            P.first = first;
+            P.n = std::min(chunk, total - first);
+            launchParticles(c.settings.precision, c.ds, P, c.dSplat.get(), c.dStats.get(), c.numSMs * 8, s);
+            checkLaunch();
+        }
+    }
+    OWEC_CUDA(cudaEventRecord(c.passStop, s));
+    OWEC_CUDA(cudaEventSynchronize(c.passStop));
+    float ms = 0;
+    OWEC_CUDA(cudaEventElapsedTime(&ms, c.passStart, c.passStop));
+    c.lastPassSeconds = ms * 1e-3;
+    c.lastIntersectSeconds = c.lastShadowSeconds = c.lastIntersectLaunches = 0;
+    c.particles += double(total);
     c.passCount += uint64_t(spp);
 }
 
@@ -938,6 +1006,8 @@ int owec_set_settings(owec_ctx* ctx, const owec_settings* s) {
         require(s->precision >= OWEC_PRECISION_MIXED && s->precision <= OWEC_PRECISION_FP64, "unknown precision mode");
         require(s->wavelength_mode != OWEC_WAVELENGTHS_UNIFORM1 ||
                     (s->lambda_min > 0 && s->lambda_max > s->lambda_min), "bad wavelength range");
+        require(s->integrator == OWEC_INTEGRATOR_PATH || s->integrator == OWEC_INTEGRATOR_LIGHT,
+                "unknown integrator (expected path or light)", OWEC_E_UNSUPPORTED);
         const bool estimatorChange = std::memcmp(s, &ctx->settings, sizeof(owec_settings)) != 0;
         ctx->settings = *s;
         if (estimatorChange) {
@@ -945,6 +1015,8 @@ int owec_set_settings(owec_ctx* ctx, const owec_settings* s) {
             ctx->dFilm.release();
             ctx->dComp.release();
             ctx->dSamples.release();
+            ctx->dSplat.release();
+            ctx->particles = 0;
         }
     });
 }
@@ -956,6 +1028,10 @@ int owec_pass(owec_ctx* ctx, int spp) {
         OWEC_CUDA(cudaSetDevice(ctx->device));
         ensureReady(*ctx);
         ensureFilm(*ctx);
+        if (ctx->settings.integrator == OWEC_INTEGRATOR_LIGHT) {
+            runParticles(*ctx, spp);
+            return;
+        }
         switch (ctx->settings.precision) {
             case OWEC_PRECISION_MIXED: runPass<OWEC_PRECISION_MIXED>(*ctx, spp); break;
             case OWEC_PRECISION_FP32: runPass<OWEC_PRECISION_FP32>(*ctx, spp); break;
@@ -971,6 +1047,18 @@ int owec_resolve(owec_ctx* ctx, double* xyz, double* samples) {
         OWEC_CUDA(cudaSetDevice(ctx->device));
         ensureFilm(*ctx);
         const size_t np = size_t(ctx->ds.det.width) * ctx->ds.det.height;
+        if (ctx->settings.integrator == OWEC_INTEGRATOR_LIGHT) {
+            if (xyz) {
+                ctx->dResolved.reserve(3 * np);
+                launchResolveSplats(ctx->dSplat.get(), uint32_t(np), ctx->particles > 0 ? 1.0 / ctx->particles : 0.0,
+                                    ctx->dResolved.get(), ctx->stream);
+                checkLaunch();
+                OWEC_CUDA(cudaMemcpyAsync(xyz, ctx->dResolved.get(), 3 * np * 8, cudaMemcpyDeviceToHost, ctx->stream));
+                OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+            }
+            if (samples) std::fill(samples, samples + np, ctx->particles / double(np));
+            return;
+        }
         if (xyz) {
             ctx->dResolved.reserve(3 * np);
             launchResolve(ctx->dFilm.get(), ctx->dComp.get(), ctx->dSamples.get(), uint32_t(np), ctx->dResolved.get(),
@@ -991,6 +1079,18 @@ int owec_read_film(owec_ctx* ctx, double* xyz_sums, double* samples) {
         OWEC_CUDA(cudaSetDevice(ctx->device));
         ensureFilm(*ctx);
         const size_t np = size_t(ctx->ds.det.width) * ctx->ds.det.height;
+        if (ctx->settings.integrator == OWEC_INTEGRATOR_LIGHT) {
+            if (xyz_sums) {
+                ctx->dResolved.reserve(3 * np);
+                launchResolveSplats(ctx->dSplat.get(), uint32_t(np), 1.0 / double(np), ctx->dResolved.get(), ctx->stream);
+                checkLaunch();
+                OWEC_CUDA(cudaMemcpyAsync(xyz_sums, ctx->dResolved.get(), 3 * np * 8, cudaMemcpyDeviceToHost,
+                                          ctx->stream));
+                OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+            }
+            if (samples) std::fill(samples, samples + np, ctx->particles / double(np));
+            return;
+        }
         if (xyz_sums) {
             std::vector<double> film(3 * np), comp(3 * np);
             OWEC_CUDA(cudaMemcpyAsync(film.data(), ctx->dFilm.get(), 3 * np * 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1020,6 +1120,8 @@ int owec_reset_film(owec_ctx* ctx) {
         ctx->dFilm.release();
         ctx->dComp.release();
         ctx->dSamples.release();
+        ctx->dSplat.release();
+        ctx->particles = 0;
         OWEC_CUDA(cudaMemsetAsync(ctx->dStats.get(), 0, sizeof(StatCounters), ctx->stream));
         OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
     });

@@ -289,6 +289,31 @@ __device__ R lightSampleLe(const DeviceScene& sc, const LightSampleD& ls, R lamb
     return ((cosL > 0 && e.front) || (cosL < 0 && e.back)) ? evalSpectrum(sc, e.radiance, lambda) : R(0);
 }
 
+// ------------------------------------------------------------------ interfaces
+// The interface of a boundary at one wavelength (Tracer::makeInterface, transport.cpp:168-185).
+template <class R, bool Lambertian = false>
+__device__ __forceinline__ Interface<R> makeInterface(const DeviceScene& sc, const DBoundary& bd, const V3<R>& n, R lambda,
+                                                      R fresnelFloor) {
+    Interface<R> it;
+    it.o = sc.optics[bd.optics];
+    it.n = n;
+    // a Lambertian interface as a compile-time fact (the lean surface kernel), so that the lobe
+    // switches fold away
+    if (Lambertian) it.o.type = OWEC_SURF_DIFFUSE;
+    // only the dielectric and conductor lobes read the indices (a Lambertian surface, the most
+    // common, skips two index evaluations per wavelength)
+    if (it.o.type == OWEC_SURF_DIELECTRIC || it.o.type == OWEC_SURF_CONDUCTOR) {
+        it.nFront = regionIndex(sc, bd.front, lambda);
+        it.nBack = regionIndex(sc, bd.back, lambda);
+    } else {
+        it.nFront = it.nBack = R(1);
+    }
+    it.lambda = lambda;
+    it.fresnelFloor = fresnelFloor;
+    it.albedo = it.o.reflectance >= 0 ? evalSpectrum(sc, it.o.reflectance, lambda) : R(1);
+    return it;
+}
+
 // Russian roulette against the throughput (CameraPath::survives, transport.cpp:369-374).
 template <class R>
 __device__ __forceinline__ bool survives(PathSpec<R>& sp, Pcg32& rng) {

@@ -450,29 +450,6 @@ __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kMedium(DeviceSc
 }
 
 // ------------------------------------------------------------------ surface
-template <class R, bool Lambertian = false>
-__device__ __forceinline__ Interface<R> makeInterface(const DeviceScene& sc, const DBoundary& bd, const V3<R>& n, R lambda,
-                                                      R fresnelFloor) {
-    Interface<R> it;
-    it.o = sc.optics[bd.optics];
-    it.n = n;
-    // a Lambertian interface as a compile-time fact (the lean surface kernel), so that the lobe
-    // switches fold away
-    if (Lambertian) it.o.type = OWEC_SURF_DIFFUSE;
-    // only the dielectric and conductor lobes read the indices (a Lambertian surface, the most
-    // common, skips two index evaluations per wavelength)
-    if (it.o.type == OWEC_SURF_DIELECTRIC || it.o.type == OWEC_SURF_CONDUCTOR) {
-        it.nFront = regionIndex(sc, bd.front, lambda);
-        it.nBack = regionIndex(sc, bd.back, lambda);
-    } else {
-        it.nFront = it.nBack = R(1);
-    }
-    it.lambda = lambda;
-    it.fresnelFloor = fresnelFloor;
-    it.albedo = it.o.reflectance >= 0 ? evalSpectrum(sc, it.o.reflectance, lambda) : R(1);
-    return it;
-}
-
 // Simple: the lean instantiation for the simple surface queue (Lambertian, absorbing and detecting
 // boundaries): the other lobes, dispersion and the index models compile out, and with them most of
 // the registers.

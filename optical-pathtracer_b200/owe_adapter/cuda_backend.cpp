@@ -249,7 +249,7 @@ std::unique_ptr<Flat> flatten(const Scene& sc, int detectorIndex) {
 class CudaRenderer final : public Renderer {
 public:
     CudaRenderer(const Scene& scene, int detectorIndex, const RenderSettings& settings)
-        : Renderer(scene, detectorIndex, settings, {"path"}), detectorIndex_(detectorIndex) {
+        : Renderer(scene, detectorIndex, settings, {"path", "light"}), detectorIndex_(detectorIndex) {
         check(owec_open(settings.device, &ctx_), "cuda backend");
         upload();
         owec_settings s{};
@@ -261,6 +261,7 @@ public:
         s.lambda_min = 380;
         s.lambda_max = 780;
         s.fresnel_floor = settings.fresnelFloor;
+        s.integrator = settings.integrator == "light" ? OWEC_INTEGRATOR_LIGHT : OWEC_INTEGRATOR_PATH;
         check(owec_set_settings(ctx_, &s), "cuda backend");
     }
     ~CudaRenderer() override { owec_close(ctx_); }
@@ -332,7 +333,7 @@ public:
         owec_close(c);
         return {d};
     }
-    std::vector<std::string> integrators() const override { return {"path"}; }
+    std::vector<std::string> integrators() const override { return {"path", "light"}; }
     std::unique_ptr<Renderer> createRenderer(const Scene& scene, int detectorIndex,
                                              const RenderSettings& settings) const override {
         return std::make_unique<CudaRenderer>(scene, detectorIndex, settings);

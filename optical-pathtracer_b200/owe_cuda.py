@@ -190,7 +190,10 @@ class Context:
 class Renderer:
     """A progressive estimator of one detector's image (owe::Renderer)."""
 
-    def __init__(self, backend, desc, settings, integrator="path", device=-1):
+    def __init__(self, backend, desc, settings, integrator=None, device=-1):
+        if integrator is None:  # RenderSettings::integrator
+            names = {v: k for k, v in A.INTEGRATORS.items()}
+            integrator = names.get(settings.integrator, str(settings.integrator))
         if integrator not in backend.integrators():
             known = ", ".join(backend.integrators())
             raise RuntimeError(f"unknown integrator '{integrator}' (expected {known})")
@@ -198,8 +201,12 @@ class Renderer:
         self.ctx = Context(device)
         self.ctx.upload(desc)
         self.ctx.build_bvh()
+        # the integrator chosen by name, as RenderSettings::integrator (src/owe/scene/scene.hpp:19)
+        settings = A.Settings.from_buffer_copy(settings)
+        settings.integrator = A.INTEGRATORS[integrator]
         self.ctx.set_settings(settings)
         self.settings = settings
+        self.integrator = integrator
         self._passes = 0
         self._spp = 0
         self._seconds = 0.0
@@ -235,7 +242,8 @@ class Renderer:
         name = self.ctx.device_name()
         mode = {A.PRECISION_MIXED: "float32 camera-relative + selective float64",
                 A.PRECISION_FP32: "float32", A.PRECISION_FP64: "float64"}[self.settings.precision]
-        return f"cuda: {name} (sm_100a wavefront; {mode})"
+        kind = "wavefront" if self.integrator == "path" else "particles"
+        return f"cuda: {name} (sm_100a {kind}; {mode})"
 
     def reset_observer(self):
         self.ctx.reset_film()
@@ -275,12 +283,12 @@ class CudaBackend:
             c.close()
 
     def integrators(self):
-        return ["path"]
+        return ["path", "light"]
 
     def supports(self, integrator):
         return integrator in self.integrators()
 
-    def create_renderer(self, desc, settings, integrator="path", device=-1):
+    def create_renderer(self, desc, settings, integrator=None, device=-1):
         return Renderer(self, desc, settings, integrator, device)
 
 

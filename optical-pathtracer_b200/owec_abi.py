@@ -10,7 +10,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libowec.so")
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 OK = 0
 E_INVALID, E_CUDA, E_NOMEM, E_STATE, E_DEVICE_FAULT, E_UNSUPPORTED = -1, -2, -3, -4, -5, -6
@@ -100,8 +100,11 @@ class Settings(ctypes.Structure):
     _fields_ = [("seed", ctypes.c_uint64), ("max_depth", ctypes.c_int32), ("rr_depth", ctypes.c_int32),
                 ("wavelength_mode", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("lambda_min", ctypes.c_double), ("lambda_max", ctypes.c_double),
-                ("fresnel_floor", ctypes.c_double)]
+                ("fresnel_floor", ctypes.c_double), ("integrator", ctypes.c_int32), ("pad0", ctypes.c_int32)]
 
+
+INTEGRATOR_PATH, INTEGRATOR_LIGHT = 0, 1
+INTEGRATORS = {"path": INTEGRATOR_PATH, "light": INTEGRATOR_LIGHT}
 
 SOURCE_POINT, SOURCE_COLLIMATED, SOURCE_COLLIMATED_SQUARE = 0, 1, 2
 WALK_STOCHASTIC, WALK_PRIMARY_TRANSMISSION = 0, 1
@@ -134,9 +137,16 @@ class Stats(ctypes.Structure):
 
 
 def make_settings(seed=1, max_depth=64, rr_depth=6, wavelength_mode=WAVELENGTHS_HERO4,
-                  precision=PRECISION_MIXED, lambda_min=380.0, lambda_max=780.0, fresnel_floor=0.0):
-    """RenderSettings' transport fields (src/owe/scene/scene.hpp:15-49), reference defaults."""
-    return Settings(seed, max_depth, rr_depth, wavelength_mode, precision, lambda_min, lambda_max, fresnel_floor)
+                  precision=PRECISION_MIXED, lambda_min=380.0, lambda_max=780.0, fresnel_floor=0.0,
+                  integrator=INTEGRATOR_PATH):
+    """RenderSettings' transport fields (src/owe/scene/scene.hpp:15-49), reference defaults.
+    `integrator` is INTEGRATOR_PATH or INTEGRATOR_LIGHT, or its name ("path", "light")."""
+    if isinstance(integrator, str):
+        if integrator not in INTEGRATORS:
+            raise RuntimeError(f"unknown integrator '{integrator}' (expected {', '.join(INTEGRATORS)})")
+        integrator = INTEGRATORS[integrator]
+    return Settings(seed, max_depth, rr_depth, wavelength_mode, precision, lambda_min, lambda_max, fresnel_floor,
+                    integrator, 0)
 
 
 _LIB = None

@@ -403,6 +403,68 @@ def invisible_sphere(width=24, height=24):
     return sb
 
 
+def _planck(l_nm, kelvin):
+    """Planck spectral radiance, lambda in nm evaluated in micrometres (the kernels' planck)."""
+    l = np.asarray(l_nm, float) * 1e-3
+    return 1e6 * 1.191042972e8 / (l ** 5 * (np.exp(1.438776877e4 / (l * kelvin)) - 1))
+
+
+def _cie_y(l):
+    """The CIE y-bar multi-lobe fit (the kernels' cieY)."""
+    l = np.asarray(l, float)
+
+    def lobe(mu, s1, s2):
+        t = (l - mu) / np.where(l < mu, s1, s2)
+        return np.exp(-0.5 * t * t)
+    return 0.821 * lobe(568.8, 46.9, 40.5) + 0.286 * lobe(530.9, 16.3, 31.1)
+
+
+def blackbody_scale(kelvin, luminance):
+    """The scale that gives a blackbody spectrum the luminance (Y) `luminance`."""
+    l = np.linspace(360.0, 830.0, 941)
+    y = _cie_y(l)
+    return luminance * np.trapezoid(y, l) / np.trapezoid(_planck(l, kelvin) * y, l)
+
+
+def lamp_over_floor(width=24, height=18):
+    """A 4000 K lamp sphere (luminance 5, black body) over a 4 x 4 m Lambertian floor whose
+    reflectance rises from 0.3 (blue) to 0.9 (red), seen through a pinhole: the scene on which the
+    reference's conformance suite checks light tracing against path tracing
+    (tests/test_backends.cpp:597-614; the floor's rgb(0.9, 0.6, 0.3) is a tabulated ramp here)."""
+    sb = SceneBuilder()
+    floor = sb.optics_(A.SURF_DIFFUSE, sb.spectrum_tabulated([400.0, 500.0, 600.0, 700.0], [0.3, 0.5, 0.75, 0.9]))
+    sb.sheet(2.0, 2.0, pose(), floor)
+    lamp = sb.emission(sb.spectrum_blackbody(4000.0, blackbody_scale(4000.0, 5.0)))
+    sb.sphere_body(0.25, (0.4, -0.2, 1.2), sb.medium_opaque(), sb.absorber(), lamp)
+    sb.observer(width, height, (0.0, -2.2, 1.4), (0.0, 0.0, 0.0), fov_y_deg=40.0)
+    return sb
+
+
+def disk_irradiance(a=0.3, h=0.5, radiance=2.0, half=0.15, screen=False):
+    """A Lambertian disk emitter of radius a (absorbing, emitting downward) at height h over an
+    upward-facing square sensor of half-size `half` with 2 x 2 pixels; with `screen` the sensor is a
+    diffuse screen of reflectance 0.7 that records the incident flux and scatters the rest
+    (tests/analytic.hpp:26-60)."""
+    sb = SceneBuilder()
+    flip = np.diag([1.0, -1.0, -1.0])  # a half turn about x: the disk's front faces down
+    sb.sheet(a, a, pose(flip, (0.0, 0.0, h)), sb.absorber(), sb.emission(sb.spectrum_constant(radiance)), disk=True)
+    optics = sb.diffuse(0.7) if screen else sb.optics_(A.SURF_DETECTOR)
+    b = sb.sheet(half, half, pose(), optics)
+    sb.sensor(2, 2, b, half, half)
+    return sb
+
+
+def disk_irradiance_mean(radiance, a, h, half, n=200):
+    """The mean over the centred square of half-size `half` of the irradiance a Lambertian disk of
+    radius a and radiance L casts on a parallel plane at distance h below its centre:
+    E(r) = pi L / 2 (1 - (h^2 + r^2 - a^2) / sqrt((h^2 + r^2 + a^2)^2 - 4 r^2 a^2))."""
+    x = -half + (np.arange(n) + 0.5) * 2 * half / n
+    r2 = x[:, None] ** 2 + x[None, :] ** 2
+    s = h * h + r2 + a * a
+    e = math.pi * radiance / 2 * (1 - (h * h + r2 - a * a) / np.sqrt(s * s - 4 * r2 * a * a))
+    return float(e.mean())
+
+
 def random_rays(n, seed, lo, hi, target_lo, target_hi):
     """n rays from uniform points of box [lo, hi] toward uniform points of [target_lo, target_hi]
     (seeded numpy PCG64). Unit directions."""

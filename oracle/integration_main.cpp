@@ -29,11 +29,12 @@ void check(bool ok, const char* what, double got, double expected) {
     if (!ok) ++failures;
 }
 
-Image render(const Backend& b, const Scene& sc, int spp, uint64_t seed) {
+Image render(const Backend& b, const Scene& sc, int spp, uint64_t seed, const char* integrator = "path") {
     RenderSettings rs;
     rs.backend = b.name();
     rs.seed = seed;
     rs.spp = spp;
+    rs.integrator = integrator;
     auto r = b.createRenderer(sc, 0, rs);
     r->runPass(spp);
     std::printf("     %s: %lld spp in %.3f s, %llu paths, %llu leaks\n", r->backend().c_str(), r->samplesPerPixel(),
@@ -41,8 +42,9 @@ Image render(const Backend& b, const Scene& sc, int spp, uint64_t seed) {
     return r->resolve();
 }
 
-// tests/test_backends.cpp:349-378: a closed diffuse sphere emitting Le = 1 inward, L = 1 / (1 - rho).
-void whiteFurnace(double rho) {
+// tests/test_backends.cpp:349-378 and :540-574: a closed diffuse sphere emitting Le = 1 inward,
+// L = 1 / (1 - rho), with the path integrator and with the light integrator (particles).
+void whiteFurnace(double rho, const char* integrator) {
     Scene sc;
     SurfaceOptics o;
     o.type = SurfaceType::Diffuse;
@@ -63,8 +65,10 @@ void whiteFurnace(double rho) {
     obs->fovY = radians(70);
     sc.detectors.push_back(std::move(obs));
     sc.build();
-    const double y = render(cudaBackend(), sc, 1024, 1).meanY();
-    check(std::fabs(y - 1 / (1 - rho)) < 0.01 / (1 - rho), "white furnace", y, 1 / (1 - rho));
+    const bool light = std::string(integrator) == "light";
+    const double y = render(cudaBackend(), sc, light ? 4096 : 1024, 1, integrator).meanY();
+    check(std::fabs(y - 1 / (1 - rho)) < (light ? 0.02 : 0.01) / (1 - rho),
+          light ? "white furnace, light integrator" : "white furnace", y, 1 / (1 - rho));
 }
 
 // A glass ball over a floor under the sun, through compareRenderers (compare.cpp:66-119).
@@ -121,7 +125,8 @@ int main() {
         return 2;
     }
     std::printf("cuda backend: %s\n", cudaBackend().summary().c_str());
-    for (double rho : {0.0, 0.5, 0.8}) whiteFurnace(rho);
+    for (double rho : {0.0, 0.5, 0.8}) whiteFurnace(rho, "path");
+    for (double rho : {0.0, 0.5}) whiteFurnace(rho, "light");
     agreesWithReference();
     return failures ? 1 : 0;
 }
