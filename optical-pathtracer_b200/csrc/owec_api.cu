@@ -254,6 +254,7 @@ struct owec_ctx {
     DBuf<uint8_t> dPathRay, dPathSpec, dPathAux, dHit, dShadow;
     DBuf<uint32_t> dQueue0, dQueue1, dQueueSurf, dQueueSurfSimple, dQueueShadow, dCounts;
     DBuf<uint8_t> dShadowVis;  // per shadow-queue entry: 0 blocked, 1 clear, 2 fault
+    DBuf<uint32_t> dShadowPixel;  // light integrator: the pixel of each queued connection
     DBuf<StatCounters> dStats;
     DBuf<unsigned long long> dTravCounters;
     uint32_t capacity = 0;
@@ -719,15 +720,13 @@ void ensureFilm(owec_ctx& c) {
     }
 }
 
+// The path state and queues for `cap` paths in flight (grown, never shrunk).
 template <int M>
-void runPass(owec_ctx& c, int spp) {
+PathBuffers<ModeR<M>> pathState(owec_ctx& c, uint32_t cap, Queues& q) {
     using R = ModeR<M>;
-    const uint32_t nPix = uint32_t(c.ds.det.width) * uint32_t(c.ds.det.height);
-    // Paths in flight: enough to fill the GPU several times over (2M+), within the state budget.
-    const uint32_t target = std::max<uint32_t>(nPix, 1u << 21);
-    uint32_t perBatch = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(spp), target / nPix));
-    const uint32_t cap = perBatch * nPix;
+    // every buffer whose record depends on the precision is checked: a context may switch modes
     if (c.capacity < cap || c.dPathRay.bytes() < size_t(cap) * sizeof(PathRay<R>) ||
+        c.dPathSpec.bytes() < size_t(cap) * sizeof(PathSpec<R>) ||
         c.dShadow.bytes() < size_t(cap) * sizeof(ShadowRay<R>)) {
         c.dPathRay.resize(size_t(cap) * sizeof(PathRay<R>));
         c.dPathSpec.resize(size_t(cap) * sizeof(PathSpec<R>));
@@ -742,11 +741,23 @@ void runPass(owec_ctx& c, int spp) {
         c.dQueueShadow.resize(cap);
         c.capacity = cap;
     }
-    PathBuffers<R> pb{reinterpret_cast<PathRay<R>*>(c.dPathRay.get()), reinterpret_cast<PathSpec<R>*>(c.dPathSpec.get()),
-                      reinterpret_cast<PathAux*>(c.dPathAux.get()), reinterpret_cast<HitRec*>(c.dHit.get()),
-                      reinterpret_cast<ShadowRay<R>*>(c.dShadow.get())};
-    Queues q{{c.dQueue0.get(), c.dQueue1.get()}, c.dQueueSurf.get(), c.dQueueShadow.get(), c.dCounts.get(),
-             c.dQueueSurfSimple.get()};
+    q = Queues{{c.dQueue0.get(), c.dQueue1.get()}, c.dQueueSurf.get(), c.dQueueShadow.get(), c.dCounts.get(),
+               c.dQueueSurfSimple.get()};
+    return PathBuffers<R>{reinterpret_cast<PathRay<R>*>(c.dPathRay.get()), reinterpret_cast<PathSpec<R>*>(c.dPathSpec.get()),
+                          reinterpret_cast<PathAux*>(c.dPathAux.get()), reinterpret_cast<HitRec*>(c.dHit.get()),
+                          reinterpret_cast<ShadowRay<R>*>(c.dShadow.get())};
+}
+
+template <int M>
+void runPass(owec_ctx& c, int spp) {
+    using R = ModeR<M>;
+    const uint32_t nPix = uint32_t(c.ds.det.width) * uint32_t(c.ds.det.height);
+    // Paths in flight: enough to fill the GPU several times over (2M+), within the state budget.
+    const uint32_t target = std::max<uint32_t>(nPix, 1u << 21);
+    uint32_t perBatch = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(spp), target / nPix));
+    const uint32_t cap = perBatch * nPix;
+    Queues q;
+    PathBuffers<R> pb = pathState<M>(c, cap, q);
     PassParams pp{};
     pp.seed = c.settings.seed;
     pp.maxDepth = c.settings.max_depth;
@@ -836,11 +847,19 @@ void runPass(owec_ctx& c, int spp) {
     c.passCount += uint64_t(spp);
 }
 
-// A pass of the light integrator: width x height x spp particles, in launches of up to 2^22.
+// A pass of the light integrator: width x height x spp particles, through the wavefront in batches
+// of up to 2^21 (the particle index, not the batch, keys a particle's stream).
+template <int M>
 void runParticles(owec_ctx& c, int spp) {
+    using R = ModeR<M>;
     const DDetector& det = c.ds.det;
     const uint64_t nPix = uint64_t(det.width) * uint64_t(det.height);
     const uint64_t total = nPix * uint64_t(spp);
+    const uint32_t cap = uint32_t(std::min<uint64_t>(total, 1u << 21));
+    Queues q;
+    PathBuffers<R> pb = pathState<M>(c, cap, q);
+    c.dShadowPixel.reserve(cap);
+    const SplatTarget film{c.dSplat.get(), c.dShadowPixel.get()};
     ParticleParams P{};
     P.seed = c.settings.seed;
     P.stream = c.passCount;
@@ -850,22 +869,45 @@ void runParticles(owec_ctx& c, int spp) {
     P.lambdaMin = float(c.settings.lambda_min);
     P.lambdaMax = float(c.settings.lambda_max);
     P.fresnelFloor = float(std::min(0.49, std::max(0.0, c.settings.fresnel_floor)));
-    P.anyHitShadows = c.hasNull ? 0 : 1;
     P.pSky = c.pSky;
     P.discRadius = c.discRadius;
     for (int k = 0; k < 3; ++k) P.discCentre[k] = c.discCentre[k];
     P.pixelArea = det.kind == OWEC_DETECTOR_OBSERVER ? (2 * det.tanX / det.width) * (2 * det.tanY / det.height)
                                                      : (2 * det.halfX / det.width) * (2 * det.halfY / det.height);
+    PassParams pp{};
+    pp.anyHitShadows = c.hasNull ? 0 : 1;
+    const int grid = c.numSMs * 8;
     cudaStream_t s = c.stream;
+    uint32_t* counts = c.dCounts.get();
     OWEC_CUDA(cudaEventRecord(c.passStart, s));
     // nothing emits: the estimate is zero, but the particles still count
-    if (c.pSky > 0 || !c.lights.empty()) {
-        const uint64_t chunk = 1ull << 22;
-        for (uint64_t first = 0; first < total; first += chunk) {
-            P.first = first;
-            P.n = std::min(chunk, total - first);
-            launchParticles(c.settings.precision, c.ds, P, c.dSplat.get(), c.dStats.get(), c.numSMs * 8, s);
+    const bool emits = c.pSky > 0 || !c.lights.empty();
+    for (uint64_t first = 0; emits && first < total; first += cap) {
+        const uint32_t n = uint32_t(std::min<uint64_t>(cap, total - first));
+        P.first = first;
+        OWEC_CUDA(cudaMemsetAsync(counts, 0, 8 * sizeof(uint32_t), s));
+        launchEmit<M>(c.ds, P, pb, q, c.dStats.get(), film, n, s);
+        launchConnect<M>(c.ds, pp, pb, q, c.dStats.get(), counts + 5, c.dShadowVis.get(), film, grid, s);
+        checkLaunch();
+        int cur = 0;
+        // as the camera paths: bounces queued without a host wait, the queue looked at once the
+        // depth cap is reached and every four bounces after it
+        int nextCheck = P.maxDepth + 1;
+        for (int bounce = 0; bounce < 4 * P.maxDepth + 8; ++bounce) {
+            if (bounce == nextCheck) {
+                OWEC_CUDA(cudaMemcpyAsync(c.hostCounts, counts, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+                OWEC_CUDA(cudaStreamSynchronize(s));
+                if (c.hostCounts[cur] == 0) break;
+                nextCheck = bounce + 4;
+            }
+            OWEC_CUDA(cudaMemsetAsync(counts + (cur ^ 1), 0, sizeof(uint32_t), s));
+            OWEC_CUDA(cudaMemsetAsync(counts + 2, 0, 5 * sizeof(uint32_t), s));  // shadow queue, fetch counters
+            launchIntersect<M>(c.ds, pb, q, cur, c.dStats.get(), counts + 4, grid, s);
+            launchParticleEvent<M>(c.ds, P, pb, q, cur, c.dStats.get(), film, grid, s);
+            launchConnect<M>(c.ds, pp, pb, q, c.dStats.get(), counts + 5, c.dShadowVis.get(), film, grid, s);
             checkLaunch();
+            OWEC_CUDA(cudaMemsetAsync(counts + cur, 0, sizeof(uint32_t), s));
+            cur ^= 1;
         }
     }
     OWEC_CUDA(cudaEventRecord(c.passStop, s));
@@ -1029,7 +1071,11 @@ int owec_pass(owec_ctx* ctx, int spp) {
         ensureReady(*ctx);
         ensureFilm(*ctx);
         if (ctx->settings.integrator == OWEC_INTEGRATOR_LIGHT) {
-            runParticles(*ctx, spp);
+            switch (ctx->settings.precision) {
+                case OWEC_PRECISION_MIXED: runParticles<OWEC_PRECISION_MIXED>(*ctx, spp); break;
+                case OWEC_PRECISION_FP32: runParticles<OWEC_PRECISION_FP32>(*ctx, spp); break;
+                default: runParticles<OWEC_PRECISION_FP64>(*ctx, spp); break;
+            }
             return;
         }
         switch (ctx->settings.precision) {

@@ -13,19 +13,15 @@
 // converges to the same image as the path integrator's wherever a pinhole can see a non-specular
 // surface.
 //
-// One thread walks one particle at a time (grid-stride over the particle indices): a particle's walk
-// is a few segments with one connection ray each, traced with the same wide-BVH traversal as the
-// camera paths. Every particle draws from its own PCG32 stream keyed by (seed, particle index, pass),
-// so a pass gives the same film however it is split into launches.
-//
-// Splats land in exact fixed-point sums: each pixel channel is a 192-bit integer of three 64-bit
-// words, least significant first, whose lowest bit weighs 2^-80. A splat's FP64 significand is
-// shifted to its binary exponent and added with 64-bit atomics, carries propagated word by word.
-// Integer addition does not depend on order, so the particle film is bitwise reproducible even
-// though many threads add to one pixel in no fixed order.
+// The particles run through the same wavefront as the camera paths, in the same path-state slots:
+// kEmit starts a batch, then every bounce is kIntersect (the camera paths' closest-hit kernel),
+// kParticleEvent (free flight, the boundary met, the connection, the scattering sample) and the
+// connection kernels (the shadow rays' visibility kernels, splatting instead of adding radiance).
+// Every particle draws from its own PCG32 stream keyed by (seed, particle index, pass), so a pass
+// gives the same film however it is split into batches, and the splats are exact fixed-point sums
+// (splat.cuh), so it does not depend on their order either.
 #include "particle.hpp"
 #include "transport.cuh"
-#include "wavefront.hpp"
 
 namespace owec {
 
@@ -37,59 +33,9 @@ using RT = typename Mode<M>::R;
 // Keys a particle's stream apart from the camera paths' (hashCombine(seed, pixel)).
 constexpr uint64_t kParticleKey = 0x5bd1e995ULL;
 
-// Adds v to word w of a channel, carrying into the words above it.
-__device__ __forceinline__ void addWord(unsigned long long* acc, int w, unsigned long long v) {
-    const unsigned long long old = atomicAdd(acc + w, v);
-    if (old + v >= old) return;  // no wrap-around
-    for (int k = w + 1; k < kSplatWordsPerChannel; ++k)
-        if (atomicAdd(acc + k, 1ull) != ~0ull) return;
-}
-
-// Adds v exactly to a channel's fixed-point sum. Zero, negative and NaN add nothing; bits below
-// 2^-80 are dropped. False when v does not fit (infinite, or 2^112 and above).
-__device__ bool addFixed(unsigned long long* acc, double v) {
-    if (!(v > 0)) return true;
-    const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(v));
-    const int e = int((bits >> 52) & 0x7FF);
-    if (e == 0x7FF) return false;
-    if (e == 0) return true;  // subnormal: far below the lowest bit
-    unsigned long long mant = (bits & 0xFFFFFFFFFFFFFull) | (1ull << 52);  // v = mant * 2^(e - 1075)
-    int p = e - 1075 - kSplatExp0;  // position of mant's lowest bit in the sum
-    if (p < 0) {
-        if (p <= -53) return true;
-        mant >>= -p;
-        p = 0;
-    }
-    const int w = p >> 6, r = p & 63;
-    if (w >= kSplatWordsPerChannel) return false;
-    const unsigned long long hi = r ? mant >> (64 - r) : 0ull;
-    if (hi && w + 1 >= kSplatWordsPerChannel) return false;
-    addWord(acc, w, mant << r);
-    if (hi) addWord(acc, w + 1, hi);
-    return true;
-}
-
-// A particle's wavelengths (Wavelengths::sample, src/owe/core/wavelengths.hpp:32-44: four hero
-// strata from one uniform), or the one uniform wavelength of OWEC_WAVELENGTHS_UNIFORM1.
-struct Spec {
-    float lambda[NW], pdf[NW];  // pdf 0: a terminated secondary
-};
-__device__ Spec sampleWavelengths(const ParticleParams& P, double u) {
-    Spec s;
-    if (P.wavelengthMode == OWEC_WAVELENGTHS_UNIFORM1) {
-        const double lam = double(P.lambdaMin) + (double(P.lambdaMax) - double(P.lambdaMin)) * u;
-        for (int k = 0; k < NW; ++k) { s.lambda[k] = float(lam); s.pdf[k] = 0.f; }
-        s.pdf[0] = float(1.0 / ((double(P.lambdaMax) - double(P.lambdaMin)) * NW));
-    } else {
-        for (int k = 0; k < NW; ++k) {
-            double up = u + double(k) / NW;
-            if (up >= 1) up -= 1;
-            const double lam = sampleVisibleWavelength(up);
-            s.lambda[k] = float(lam);
-            s.pdf[k] = float(visibleWavelengthPdf(lam));
-        }
-    }
-    return s;
+template <int M>
+__device__ __forceinline__ V3<double> plainPoint(const V3<double>& p) {
+    return Mode<M>::plainOrigin ? V3<double>(V3<float>(p)) : p;
 }
 
 // The concentric map of the unit square onto the unit disk (sampleUniformDiskConcentric,
@@ -126,8 +72,7 @@ struct ObserverLink {
 __device__ bool linkObserver(const DeviceScene& sc, const ParticleParams& P, const V3<double>& x, Pcg32& rng,
                              ObserverLink& k) {
     const DDetector& det = sc.det;
-    const V3<double> eye(det.pos[0], det.pos[1], det.pos[2]);
-    const V3<double> w = x - eye;
+    const V3<double> w = x - V3<double>(det.pos[0], det.pos[1], det.pos[2]);
     const double d2 = dot(w, w);
     if (!(d2 > 0)) return false;
     const double dist = sqrt(d2);
@@ -147,157 +92,115 @@ __device__ bool linkObserver(const DeviceScene& sc, const ParticleParams& P, con
     return true;
 }
 
-// Adds a spectral contribution to a pixel as XYZ (Wavelengths::toXYZ, wavelengths.hpp:71-84).
-template <class R>
-__device__ void deposit(const DeviceScene& sc, unsigned long long* splat, uint32_t pixel, const Spec& s,
-                        const R value[NW], uint32_t& faults) {
-    const double inv = 1.0 / (NW * sc.cieYIntegral);
-    double x = 0, y = 0, z = 0;
-    for (int k = 0; k < NW; ++k) {
-        if (s.pdf[k] == 0.f || value[k] == R(0)) continue;
-        const double w = double(value[k]) / double(s.pdf[k]) * inv;
-        const double l = double(s.lambda[k]);
-        x += w * cieX(l);
-        y += w * cieY(l);
-        z += w * cieZ(l);
-    }
-    if (!isfinite(x + y + z)) return;
-    unsigned long long* px = splat + size_t(pixel) * kSplatWordsPerPixel;
-    bool ok = addFixed(px, x);
-    ok = addFixed(px + kSplatWordsPerChannel, y) && ok;
-    ok = addFixed(px + 2 * kSplatWordsPerChannel, z) && ok;
-    faults += !ok;
-}
-
+// Queues the connection of a particle vertex at x to the eye with its contribution before
+// transmittance (value per wavelength), one atomic per warp. Every lane of the warp that reaches
+// this call takes part (push false: nothing queued).
 template <int M>
-__device__ __forceinline__ V3<double> plainPoint(const V3<double>& p) {
-    return Mode<M>::plainOrigin ? V3<double>(V3<float>(p)) : p;
-}
-
-// The transmittance of the segment from o to a point `dist` along dir that must arrive in region
-// endRegion (Tracer::connectionTransmittance, transport.cpp:237-321): null boundaries are crossed
-// when met from the current region, any other matter blocks, media attenuate by Beer-Lambert.
-template <int M, bool AnyHit>
-__device__ bool connectTransmittance(const DeviceScene& sc, V3<double> o, uint32_t region, uint32_t depB, uint32_t depP,
-                                     float errN, const V3<double>& dir, double dist, uint32_t endRegion,
-                                     const Spec& s, RT<M> Tr[NW], StackEntry* stack, uint32_t& faults) {
+__device__ void queueConnection(const DeviceScene& sc, PathBuffers<RT<M>>& pb, Queues& q, const SplatTarget& film,
+                                uint32_t path, const float pdf[NW], const RT<M> value[NW], const ObserverLink& k,
+                                const V3<double>& x, uint32_t region, uint32_t depB, uint32_t depP, float errN,
+                                bool push) {
     using R = RT<M>;
-    using Ro = typename Mode<M>::Ro;
-    using Rr = typename Mode<M>::Rr;
-    for (int j = 0; j < NW; ++j) Tr[j] = R(1);
-    const V3<R> d(dir);
-    const float errN0 = errN;
-    double remaining = dist;
-    for (int guard = 0;; ++guard) {
-        // stop short of the end point by its error (as the next-event rays do)
-        const double tq = remaining - (4e-6 * remaining + double(errN0) + 1e-9);
-        if (guard >= 256 || tq <= 0) break;
-        RayQuery<R> rq;
-        rq.od = o;
-        rq.o = V3<R>(o);
-        rq.d = d;
-        rq.tmax = R(tq);
-        rq.depB = depB;
-        rq.depP = depP;
-        rq.region = region;
-        rq.errN = R(errN);
-        HitRec h;
-        h.boundary = kNone;
-        h.t = INFINITY;
-        const int st = traceRay<R, Ro, Rr, AnyHit>(sc, rq, stack, blockDim.x, h);
-        if (st == kTraceOverflow) {
-            ++faults;
-            return false;
-        }
-        const bool found = st == kTraceHit;
-        const double seg = found ? fmin(double(h.t), remaining) : remaining;
-        const owec_medium& med = sc.media[sc.regionMedium[region]];
-        if (mediumAbsorbs(med, sc) || mediumScatters(med, sc))
-            for (int j = 0; j < NW; ++j) {
-                const R lam = R(s.lambda[j]);
-                Tr[j] *= exp(-(evalSpectrum(sc, med.absorption, lam) + evalSpectrum(sc, med.scattering, lam)) * R(seg));
-            }
-        if (!found) break;
-        if (AnyHit) return false;
-        const DBoundary& bd = sc.boundaries[h.boundary];
-        if (sc.optics[bd.optics].type != OWEC_SURF_NULL) return false;
-        PathRay<R> tmp;
-        tmp.o[0] = o.x; tmp.o[1] = o.y; tmp.o[2] = o.z;
-        tmp.d[0] = d.x; tmp.d[1] = d.y; tmp.d[2] = d.z;
-        const SurfacePoint<R> gp = hitGeometry<R, Ro, Rr>(sc, tmp, h);
-        const bool ff = dot(d, gp.n) < R(0);
-        if ((ff ? bd.front : bd.back) != region) return false;
-        region = ff ? bd.back : bd.front;
-        o = plainPoint<M>(gp.p);
-        depB = h.boundary;
-        depP = h.prim;
-        errN = anchorError<R>(gp.p);
-        remaining -= double(h.t);
-    }
-    return region == endRegion;
-}
-
-// Counters a thread gathers over its particles, flushed once per warp at the end.
-struct Tally {
-    uint32_t paths = 0, segments = 0, inconsistencies = 0, leaks = 0, connections = 0, faults = 0;
-};
-
-// Connects a particle vertex at x to the observer: f holds the lobe (or phase function) per
-// wavelength toward the eye, cosX the cosine at x.
-template <int M, bool AnyHit>
-__device__ void connectVertex(const DeviceScene& sc, const ParticleParams& P, const V3<double>& x, uint32_t region,
-                              uint32_t depB, uint32_t depP, float errN, const ObserverLink& k, const Spec& s,
-                              const RT<M> value[NW], unsigned long long* splat, StackEntry* stack, Tally& t) {
-    using R = RT<M>;
-    R Tr[NW];
-    ++t.connections;
-    if (!connectTransmittance<M, AnyHit>(sc, x, region, depB, depP, errN, k.dir, k.dist, sc.det.region, s, Tr, stack,
-                                         t.faults))
-        return;
-    R v[NW];
+    float c[NW];
     bool any = false;
-    for (int j = 0; j < NW; ++j) {
-        v[j] = value[j] * Tr[j];
-        any = any || v[j] != R(0);
+    if (push) {
+        const double inv = 1.0 / (NW * sc.cieYIntegral);
+        for (int j = 0; j < NW; ++j) {
+            c[j] = (pdf[j] != 0.f) ? float(double(value[j]) / double(pdf[j]) * inv) : 0.f;
+            any = any || c[j] != 0.f;
+        }
     }
-    if (any) deposit(sc, splat, k.pixel, s, v, t.faults);
+    push = push && any;
+    const unsigned active = __activemask();
+    const unsigned mask = __ballot_sync(active, push);
+    if (mask == 0) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&q.counts[3], uint32_t(__popc(mask)));
+    base = __shfl_sync(active, base, leader);
+    if (!push) return;
+    const uint32_t slot = base + __popc(mask & ((1u << lane) - 1u));
+    ShadowRay<R> sr;
+    sr.o[0] = x.x; sr.o[1] = x.y; sr.o[2] = x.z;
+    sr.d[0] = R(k.dir.x); sr.d[1] = R(k.dir.y); sr.d[2] = R(k.dir.z);
+    sr.tmax = k.dist;
+    sr.region = region;
+    sr.endRegion = sc.det.region;
+    sr.depB = depB;
+    sr.depP = depP;
+    sr.path = path;
+    sr.errN = errN;
+    for (int j = 0; j < NW; ++j) sr.contrib[j] = c[j];
+    pb.shadow[slot] = sr;
+    q.shadow[slot] = slot;
+    film.pixel[slot] = k.pixel;
 }
 
-// One particle: Tracer::traceParticle's emission, walk, connections and sensor hits
-// (particle.slang:356-427; the hybrid integrator's partition is not built).
-template <int M, bool AnyHit>
-__device__ void traceParticle(const DeviceScene& sc, const ParticleParams& P, uint64_t index, StackEntry* stack,
-                              unsigned long long* splat, Tally& t) {
+// ------------------------------------------------------------------ emission
+// Particle P.first + i: its wavelengths, the emitter it leaves (emitParticle,
+// particle.slang:310-338), the emitter point's own connection, and its first ray.
+template <int M>
+__global__ void __launch_bounds__(128) kEmit(DeviceScene sc, ParticleParams P, PathBuffers<RT<M>> pb, Queues q,
+                                             StatCounters* st, SplatTarget film, uint32_t n) {
     using R = RT<M>;
-    using Ro = typename Mode<M>::Ro;
-    using Rr = typename Mode<M>::Rr;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
     const DDetector& det = sc.det;
     const bool observer = det.kind == OWEC_DETECTOR_OBSERVER;
-    Pcg32 rng = Pcg32::seeded(hashCombine(P.seed ^ kParticleKey, index), P.stream);
-    const Spec s = sampleWavelengths(P, rng.uniform());
-    ++t.paths;
-
-    // ---- emission (emitParticle, particle.slang:310-338): the sky, or a light of the table
+    Pcg32 rng = Pcg32::seeded(hashCombine(P.seed ^ kParticleKey, P.first + i), P.stream);
+    // Wavelengths::sample (src/owe/core/wavelengths.hpp:32-44): four hero strata from one uniform
+    PathSpec<R> sp;
+    {
+        const double u = rng.uniform();
+        if (P.wavelengthMode == OWEC_WAVELENGTHS_UNIFORM1) {
+            const double lam = double(P.lambdaMin) + (double(P.lambdaMax) - double(P.lambdaMin)) * u;
+            for (int k = 0; k < NW; ++k) { sp.lambda[k] = float(lam); sp.pdf[k] = 0.f; }
+            sp.pdf[0] = float(1.0 / ((double(P.lambdaMax) - double(P.lambdaMin)) * NW));
+        } else {
+            for (int k = 0; k < NW; ++k) {
+                double up = u + double(k) / NW;
+                if (up >= 1) up -= 1;
+                const double lam = sampleVisibleWavelength(up);
+                sp.lambda[k] = float(lam);
+                sp.pdf[k] = float(visibleWavelengthPdf(lam));
+            }
+        }
+        for (int k = 0; k < NW; ++k) sp.L[k] = 0.f;
+    }
+    // the sky, or a light of the table (World::pickLight: the first cdf above u)
+    bool live = true;
     const bool fromSky = rng.uniform() < P.pSky;
     uint32_t li = 0;
     if (!fromSky) {
-        if (sc.nLights == 0) return;
-        const double u = rng.uniform();
-        uint32_t lo = 0, hi = sc.nLights;  // World::pickLight: the first cdf above u
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (sc.lights[mid].cdf <= u) lo = mid + 1; else hi = mid;
+        if (sc.nLights == 0) {
+            live = false;
+        } else {
+            const double u = rng.uniform();
+            uint32_t lo = 0, hi = sc.nLights;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (sc.lights[mid].cdf <= u) lo = mid + 1; else hi = mid;
+            }
+            li = lo < sc.nLights ? lo : sc.nLights - 1;
         }
-        li = lo < sc.nLights ? lo : sc.nLights - 1;
     }
-    const bool distant = fromSky || sc.lights[li].kind == kLightSun;
-    const double sel = fromSky ? P.pSky : (1 - P.pSky) * sc.lights[li].pdf;
-    if (!(sel > 0)) return;
-    V3<double> o, dir;
-    uint32_t region, depB = kNone, depP = kNone;
-    float errN = 0.f;
-    R beta[NW];
-    if (distant) {
+    const bool distant = live && (fromSky || sc.lights[li].kind == kLightSun);
+    const double sel = !live ? 0.0 : fromSky ? P.pSky : (1 - P.pSky) * sc.lights[li].pdf;
+    live = live && sel > 0;
+    PathRay<R> ray;
+    ray.depB = kNone;
+    ray.depP = kNone;
+    ray.errN = 0.f;
+    ray.region = 0;
+    V3<double> o(0, 0, 0), dir(0, 0, 1);
+    // the emitter point's own connection to the eye (areaEmitterToObserver)
+    bool connect = false;
+    ObserverLink k;
+    R value[NW] = {R(0), R(0), R(0), R(0)};
+    V3<double> cp;
+    uint32_t cRegion = 0, cB = kNone;
+    float cErr = 0.f;
+    if (live && distant) {
         // emitDistant (particle.slang:223-262): a direction, then a point of a disc covering the
         // world, beyond it
         const Draw2<double> u(rng);
@@ -324,17 +227,16 @@ __device__ void traceParticle(const DeviceScene& sc, const ParticleParams& P, ui
         const double Rd = P.discRadius;
         const V3<double> centre(P.discCentre[0], P.discCentre[1], P.discCentre[2]);
         o = centre - dir * (1.01 * Rd) + a1 * (qx * Rd) + a2 * (qy * Rd);
-        region = 0;
-        const double w = 1 / (sel * pdfDir / (kPi * Rd * Rd));
+        const double w = kPi * Rd * Rd / (sel * pdfDir);
         for (int j = 0; j < NW; ++j) {
-            const R lam = R(s.lambda[j]);
+            const R lam = R(sp.lambda[j]);
             const R Le = fromSky ? (sc.skyModel == OWEC_SKY_UNIFORM ? evalSpectrum(sc, sc.skySpectrum, lam) : R(0))
                                  : evalSpectrum(sc, sc.sunSpectrum, lam);
-            beta[j] = Le * R(w);
+            sp.beta[j] = Le * R(w);
         }
-    } else {
-        // emitFromArea (particle.slang:278-306): a point of the emitter, its own connection to the
-        // eye, a side, then a cosine-distributed direction
+    } else if (live) {
+        // emitFromArea (particle.slang:278-306): a point of the emitter, its own connection, a
+        // side, then a cosine-distributed direction
         const DLight L = sc.lights[li];
         const DBoundary& bd = sc.boundaries[L.boundary];
         const owec_emission em = sc.emissions[bd.emission];
@@ -344,18 +246,19 @@ __device__ void traceParticle(const DeviceScene& sc, const ParticleParams& P, ui
         const V3<double> p = bd.toWorld.point(pL), n = normalize(bd.toWorld.vector(nL));
         const double pdfA = 1 / bd.area;
         R Le[NW];
-        for (int j = 0; j < NW; ++j) Le[j] = (j == 0 || s.pdf[j] != 0.f) ? evalSpectrum(sc, em.radiance, R(s.lambda[j])) : R(0);
+        for (int j = 0; j < NW; ++j)
+            Le[j] = (j == 0 || sp.pdf[j] != 0.f) ? evalSpectrum(sc, em.radiance, R(sp.lambda[j])) : R(0);
         const float errP = anchorError<R>(p);
-        ObserverLink k;
         if (observer && linkObserver(sc, P, p, rng, k)) {
-            // the emitter's own point seen by the eye (areaEmitterToObserver)
             const double cosL = dot(n, k.dir);
             if ((cosL > 0 && em.front) || (cosL < 0 && em.back)) {
-                R v[NW];
                 const R f = R(fabs(cosL) * k.factor / (sel * pdfA));
-                for (int j = 0; j < NW; ++j) v[j] = Le[j] * f;
-                connectVertex<M, AnyHit>(sc, P, plainPoint<M>(p), cosL > 0 ? bd.front : bd.back, L.boundary, 0u, errP,
-                                         k, s, v, splat, stack, t);
+                for (int j = 0; j < NW; ++j) value[j] = Le[j] * f;
+                connect = true;
+                cp = plainPoint<M>(p);
+                cRegion = cosL > 0 ? bd.front : bd.back;
+                cB = L.boundary;
+                cErr = errP;
             }
         }
         bool front = em.front != 0;
@@ -369,211 +272,243 @@ __device__ void traceParticle(const DeviceScene& sc, const ParticleParams& P, ui
         concentricDisk(c.u1, c.u2, dx, dy);
         dir = Frame<double>(front ? n : -n).toWorld(V3<double>(dx, dy, sqrt(fmax(0.0, 1 - dx * dx - dy * dy))));
         o = p;
-        region = front ? bd.front : bd.back;
-        depB = L.boundary;
-        depP = 0;
-        errN = errP;
+        ray.region = front ? bd.front : bd.back;
+        ray.depB = L.boundary;
+        ray.depP = 0;
+        ray.errN = errP;
         // beta = Le cos / (sel pdfA sidePdf cos / pi)
         const R w = R(kPi / (sel * pdfA * sidePdf));
-        for (int j = 0; j < NW; ++j) beta[j] = Le[j] * w;
+        for (int j = 0; j < NW; ++j) sp.beta[j] = Le[j] * w;
     }
-    bool live = false;
+    bool any = false;
     for (int j = 0; j < NW; ++j) {
-        if (j > 0 && s.pdf[j] == 0.f) beta[j] = R(0);  // maskTerminated
-        live = live || beta[j] != R(0);
+        if (!live || (j > 0 && sp.pdf[j] == 0.f)) sp.beta[j] = R(0);  // maskTerminated
+        any = any || sp.beta[j] != R(0);
     }
-    if (!live) return;
-    Spec sp = s;  // dispersion may terminate the secondaries on the way
-    o = plainPoint<M>(o);
-    V3<R> d(dir);
+    live = live && any;
+    const V3<double> op = plainPoint<M>(o);
+    ray.o[0] = op.x; ray.o[1] = op.y; ray.o[2] = op.z;
+    ray.d[0] = R(dir.x); ray.d[1] = R(dir.y); ray.d[2] = R(dir.z);
+    PathAux aux;
+    aux.stream = uint32_t(P.stream);
+    aux.pixel = 0;
+    aux.depth = 0;
+    aux.flags = live ? kFlagAlive : 0u;
+    aux.prevPdf = 0.f;
+    aux.weight = 0.f;
+    aux.prevP[0] = aux.prevP[1] = aux.prevP[2] = 0;
+    aux.lastBoundary = kNone;
+    aux.rngState = rng.state;
+    pb.ray[i] = ray;
+    pb.spec[i] = sp;
+    pb.aux[i] = aux;
+    queueConnection<M>(sc, pb, q, film, i, sp.pdf, value, k, cp, cRegion, cB, 0u, cErr, connect);
+    warpCount(&st->paths, true);
+    warpPush(q.active[0], &q.counts[0], live, i);
+}
 
-    // ---- the walk (traceParticle's loop, particle.slang:365-426)
-    for (int depth = 0;; ++depth) {
-        RayQuery<R> rq;
-        rq.od = o;
-        rq.o = V3<R>(o);
-        rq.d = d;
-        rq.tmax = R(INFINITY);
-        rq.depB = depB;
-        rq.depP = depP;
-        rq.region = region;
-        rq.errN = R(errN);
-        HitRec h;
-        h.boundary = kNone;
-        h.t = INFINITY;
-        const int st = traceRay<R, Ro, Rr, false>(sc, rq, stack, blockDim.x, h);
-        ++t.segments;
-        if (st == kTraceOverflow) {
-            ++t.faults;
-            return;
-        }
-        const bool found = st == kTraceHit;
-        // sampleMedium (transport.cpp:95-113): hero-extinction distance sampling
-        const owec_medium med = sc.media[sc.regionMedium[region]];
-        const double seg = found ? double(h.t) : INFINITY;
-        bool scatter = false;
-        double tS = 0;
-        if (mediumScatters(med, sc)) {
-            R sT[NW];
-            for (int j = 0; j < NW; ++j)
-                sT[j] = evalSpectrum(sc, med.absorption, R(sp.lambda[j])) + evalSpectrum(sc, med.scattering, R(sp.lambda[j]));
-            tS = -log(1 - rng.uniform()) / double(sT[0]);
-            if (tS < seg) {
-                const R pdf0 = sT[0] * exp(-sT[0] * R(tS));
+// ------------------------------------------------------------------ one event of every particle
+// What a particle meets after its closest-hit query: free flight through the medium (with a
+// connection at a scattering event), escape, the boundary (null crossing, sensor record,
+// absorption), the connection of a non-delta surface vertex and the importance-transport
+// scattering sample with roulette (traceParticle's loop body, particle.slang:365-426).
+template <int M>
+__global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, ParticleParams P, PathBuffers<RT<M>> pb,
+                                                         Queues q, int cur, StatCounters* st, SplatTarget film) {
+    using R = RT<M>;
+    using Ro = typename Mode<M>::Ro;
+    using Rr = typename Mode<M>::Rr;
+    const int nxt = cur ^ 1;
+    const uint32_t n = q.counts[cur];
+    const DDetector& det = sc.det;
+    const bool observer = det.kind == OWEC_DETECTOR_OBSERVER;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const uint32_t i = q.active[cur][e];
+        const HitRec h = pb.hit[i];
+        PathRay<R> ray = pb.ray[i];
+        PathSpec<R> sp = pb.spec[i];
+        PathAux aux = pb.aux[i];
+        Pcg32 rng{aux.rngState, (uint64_t(aux.stream) << 1u) | 1u};
+        const int depth = int(aux.depth);
+        // a connection goes out with the spectrum it was made with, before a dispersive interface
+        // ends the secondaries
+        float pdfIn[NW];
+        for (int j = 0; j < NW; ++j) pdfIn[j] = sp.pdf[j];
+        const V3<double> o(ray.o[0], ray.o[1], ray.o[2]);
+        const V3<R> d(ray.d[0], ray.d[1], ray.d[2]);
+        const bool fault = h.boundary == kNone - 1u;
+        const bool found = h.boundary < kNone - 1u;
+        bool cont = false, leak = false, inconsistent = false, connect = false, lost = false;
+        ObserverLink k;
+        R value[NW] = {R(0), R(0), R(0), R(0)};
+        V3<double> cp;
+        uint32_t cRegion = 0, cB = kNone, cP = kNone;
+        float cErr = 0.f;
+        if (!fault) {
+            // sampleMedium (transport.cpp:95-113): hero-extinction distance sampling
+            const owec_medium med = sc.media[sc.regionMedium[ray.region]];
+            const double seg = found ? h.t : INFINITY;
+            int event = 0;  // 0 pass, 1 scatter, 2 end
+            double tS = 0;
+            if (mediumScatters(med, sc)) {
+                R sT[NW];
                 for (int j = 0; j < NW; ++j)
-                    beta[j] *= evalSpectrum(sc, med.scattering, R(sp.lambda[j])) * exp(-sT[j] * R(tS)) / pdf0;
-                scatter = true;
-            } else if (isinf(seg)) {
-                return;
-            } else {
-                const R pass0 = exp(-sT[0] * R(seg));
-                for (int j = 0; j < NW; ++j) beta[j] *= exp(-sT[j] * R(seg)) / pass0;
-            }
-        } else if (mediumAbsorbs(med, sc)) {
-            if (isinf(seg)) return;
-            for (int j = 0; j < NW; ++j) beta[j] *= exp(-evalSpectrum(sc, med.absorption, R(sp.lambda[j])) * R(seg));
-        }
-        if (scatter) {
-            const V3<double> x = plainPoint<M>(o + V3<double>(d) * tS);
-            ObserverLink k;
-            if (observer && linkObserver(sc, P, x, rng, k)) {
-                const R ph = hgPhase(dot(-d, V3<R>(k.dir)), R(med.g));
-                R v[NW];
-                for (int j = 0; j < NW; ++j) v[j] = beta[j] * ph * R(k.factor);
-                connectVertex<M, AnyHit>(sc, P, x, region, kNone, kNone, 0.f, k, sp, v, splat, stack, t);
-            }
-            if (depth >= P.maxDepth) return;
-            const Draw2<R> u(rng);
-            V3<R> wi;
-            sampleHg(-d, R(med.g), u.u1, u.u2, wi);
-            o = x;
-            d = wi;
-            depB = kNone;
-            depP = kNone;
-            errN = 0.f;
-            if (depth >= P.rrDepth) {  // a fixed survival probability: any in (0, 1] is unbiased
-                if (rng.uniform() >= 0.95) return;
-                for (int j = 0; j < NW; ++j) beta[j] *= R(1 / 0.95);
-            }
-            continue;
-        }
-        if (!found) {
-            t.leaks += region != 0;
-            return;
-        }
-        // meetBoundary (transport.cpp:121-133)
-        PathRay<R> ray;
-        ray.o[0] = o.x; ray.o[1] = o.y; ray.o[2] = o.z;
-        ray.d[0] = d.x; ray.d[1] = d.y; ray.d[2] = d.z;
-        const DBoundary& bd = sc.boundaries[h.boundary];
-        const SurfacePoint<R> g = hitGeometry<R, Ro, Rr>(sc, ray, h);
-        const bool fromFront = dot(d, g.n) < R(0);
-        const uint32_t inc = fromFront ? bd.front : bd.back, other = fromFront ? bd.back : bd.front;
-        t.inconsistencies += inc != region;
-        region = inc;
-        const owec_optics& op = sc.optics[bd.optics];
-        const V3<double> gp = plainPoint<M>(g.p);
-        const float errG = anchorError<R>(g.p);
-        if (op.type == OWEC_SURF_NULL) {
-            region = other;
-            o = gp;
-            depB = h.boundary;
-            depP = h.prim;
-            errN = errG;
-            if (depth >= 4 * P.maxDepth) return;
-            continue;
-        }
-        // a surface sensor records the flux reaching its front face
-        if (!observer && fromFront && h.boundary == det.boundary) {
-            double fx = (g.pLocal.x / det.halfX + 1) * 0.5 * det.width, fy = (1 - g.pLocal.y / det.halfY) * 0.5 * det.height;
-            filterOffset(det, rng, fx, fy);
-            if (fx >= 0 && fy >= 0 && fx < det.width && fy < det.height) {
-                const uint32_t pixel = uint32_t(min(int(fy), det.height - 1)) * uint32_t(det.width) +
-                                       uint32_t(min(int(fx), det.width - 1));
-                R v[NW];
-                for (int j = 0; j < NW; ++j) v[j] = beta[j] * R(1 / P.pixelArea);
-                deposit(sc, splat, pixel, sp, v, t.faults);
-            }
-        }
-        if (op.type == OWEC_SURF_DETECTOR || op.type == OWEC_SURF_ABSORBER) return;
-        const Interface<R> it = makeInterface(sc, bd, g.n, R(sp.lambda[0]), R(P.fresnelFloor));
-        if (!isDeltaOptics<R>(op) && observer) {
-            ObserverLink k;
-            if (linkObserver(sc, P, gp, rng, k)) {
-                const V3<R> wo(k.dir);
-                R v[NW];
-                bool any = false;
-                for (int j = 0; j < NW; ++j) {
-                    v[j] = R(0);
-                    if (beta[j] == R(0)) continue;
-                    R pdf;
-                    const Interface<R> itj = j == 0 ? it : makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor));
-                    v[j] = beta[j] * evalScatter(sc, itj, d, wo, false, pdf);
-                    any = any || v[j] != R(0);
+                    sT[j] = evalSpectrum(sc, med.absorption, R(sp.lambda[j])) + evalSpectrum(sc, med.scattering, R(sp.lambda[j]));
+                tS = -log(1 - rng.uniform()) / double(sT[0]);
+                if (tS < seg) {
+                    const R pdf0 = sT[0] * exp(-sT[0] * R(tS));
+                    for (int j = 0; j < NW; ++j)
+                        sp.beta[j] *= evalSpectrum(sc, med.scattering, R(sp.lambda[j])) * exp(-sT[j] * R(tS)) / pdf0;
+                    event = 1;
+                } else if (isinf(seg)) {
+                    event = 2;
+                } else {
+                    const R pass0 = exp(-sT[0] * R(seg));
+                    for (int j = 0; j < NW; ++j) sp.beta[j] *= exp(-sT[j] * R(seg)) / pass0;
                 }
-                if (any) {
-                    const R cosX = fabs(dot(wo, g.n));
-                    for (int j = 0; j < NW; ++j) v[j] *= cosX * R(k.factor);
-                    connectVertex<M, AnyHit>(sc, P, gp, dot(wo, g.n) > R(0) ? bd.front : bd.back, h.boundary, h.prim,
-                                             errG, k, sp, v, splat, stack, t);
+            } else if (mediumAbsorbs(med, sc)) {
+                if (isinf(seg)) event = 2;
+                else
+                    for (int j = 0; j < NW; ++j)
+                        sp.beta[j] *= exp(-evalSpectrum(sc, med.absorption, R(sp.lambda[j])) * R(seg));
+            }
+            if (event == 1) {
+                // a scattering event in the medium: its connection, then Henyey-Greenstein
+                const V3<double> x = plainPoint<M>(o + V3<double>(d) * tS);
+                if (observer && linkObserver(sc, P, x, rng, k)) {
+                    const R ph = hgPhase(dot(-d, V3<R>(k.dir)), R(med.g));
+                    for (int j = 0; j < NW; ++j) value[j] = sp.beta[j] * ph * R(k.factor);
+                    connect = true;
+                    cp = x;
+                    cRegion = ray.region;
+                }
+                if (depth < P.maxDepth) {
+                    const Draw2<R> u(rng);
+                    V3<R> wi;
+                    sampleHg(-d, R(med.g), u.u1, u.u2, wi);
+                    ray.o[0] = x.x; ray.o[1] = x.y; ray.o[2] = x.z;
+                    ray.d[0] = wi.x; ray.d[1] = wi.y; ray.d[2] = wi.z;
+                    ray.depB = kNone;
+                    ray.depP = kNone;
+                    ray.errN = 0.f;
+                    cont = true;
+                    if (depth >= P.rrDepth) {  // a fixed survival probability: any in (0, 1] is unbiased
+                        cont = rng.uniform() < 0.95;
+                        for (int j = 0; j < NW; ++j) sp.beta[j] *= R(1 / 0.95);
+                    }
+                }
+            } else if (event == 0 && !found) {
+                leak = ray.region != 0;
+            } else if (event == 0) {
+                // meetBoundary (transport.cpp:121-133)
+                const DBoundary& bd = sc.boundaries[h.boundary];
+                const SurfacePoint<R> g = hitGeometry<R, Ro, Rr>(sc, ray, h);
+                const bool fromFront = dot(d, g.n) < R(0);
+                const uint32_t inc = fromFront ? bd.front : bd.back, other = fromFront ? bd.back : bd.front;
+                inconsistent = inc != ray.region;
+                ray.region = inc;
+                const owec_optics& op = sc.optics[bd.optics];
+                const V3<double> gp = plainPoint<M>(g.p);
+                const float errG = anchorError<R>(g.p);
+                if (op.type == OWEC_SURF_NULL) {
+                    ray.region = other;
+                    ray.o[0] = gp.x; ray.o[1] = gp.y; ray.o[2] = gp.z;
+                    ray.depB = h.boundary;
+                    ray.depP = h.prim;
+                    ray.errN = errG;
+                    cont = depth < 4 * P.maxDepth;
+                } else {
+                    // a surface sensor records the flux reaching its front face
+                    if (!observer && fromFront && h.boundary == det.boundary) {
+                        double fx = (g.pLocal.x / det.halfX + 1) * 0.5 * det.width;
+                        double fy = (1 - g.pLocal.y / det.halfY) * 0.5 * det.height;
+                        filterOffset(det, rng, fx, fy);
+                        if (fx >= 0 && fy >= 0 && fx < det.width && fy < det.height) {
+                            const uint32_t pixel = uint32_t(min(int(fy), det.height - 1)) * uint32_t(det.width) +
+                                                   uint32_t(min(int(fx), det.width - 1));
+                            const double inv = 1.0 / (NW * sc.cieYIntegral * P.pixelArea);
+                            float c[NW];
+                            const R one[NW] = {R(1), R(1), R(1), R(1)};
+                            for (int j = 0; j < NW; ++j)
+                                c[j] = sp.pdf[j] != 0.f ? float(double(sp.beta[j]) / double(sp.pdf[j]) * inv) : 0.f;
+                            lost = !splatXyz(film.words, pixel, sp.lambda, c, one);
+                        }
+                    }
+                    if (op.type != OWEC_SURF_DETECTOR && op.type != OWEC_SURF_ABSORBER) {
+                        const Interface<R> it = makeInterface(sc, bd, g.n, R(sp.lambda[0]), R(P.fresnelFloor));
+                        if (observer && !isDeltaOptics<R>(op) && linkObserver(sc, P, gp, rng, k)) {
+                            const V3<R> wo(k.dir);
+                            bool any = false;
+                            for (int j = 0; j < NW; ++j) {
+                                if (sp.beta[j] == R(0)) continue;
+                                R pdf;
+                                const Interface<R> itj =
+                                    j == 0 ? it : makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor));
+                                value[j] = sp.beta[j] * evalScatter(sc, itj, d, wo, false, pdf);
+                                any = any || value[j] != R(0);
+                            }
+                            if (any) {
+                                const R f = fabs(dot(wo, g.n)) * R(k.factor);
+                                for (int j = 0; j < NW; ++j) value[j] *= f;
+                                connect = true;
+                                cp = gp;
+                                cRegion = dot(wo, g.n) > R(0) ? bd.front : bd.back;
+                                cB = h.boundary;
+                                cP = h.prim;
+                                cErr = errG;
+                            }
+                        }
+                        if (depth < P.maxDepth) {
+                            if (op.type == OWEC_SURF_DIELECTRIC) {  // terminateIfDispersive (transport.cpp:216-225)
+                                for (int j = 1; j < NW; ++j) {
+                                    if (sp.pdf[j] == 0.f) continue;
+                                    if (isDispersive(it, makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor)))) {
+                                        for (int m = 1; m < NW; ++m) { sp.pdf[m] = 0.f; sp.beta[m] = R(0); }
+                                        sp.pdf[0] /= float(NW);
+                                        break;
+                                    }
+                                }
+                            }
+                            // scatterAtSurface in importance transport (transport.cpp:437-471)
+                            const Draw3<R> u(rng);
+                            ScatterSample<R> ss;
+                            if (sampleScatter(sc, it, d, u.u1, u.u2, u.u3, false, ss) && ss.weight > R(0)) {
+                                sp.beta[0] *= ss.weight;
+                                for (int j = 1; j < NW; ++j) {
+                                    if (sp.pdf[j] == 0.f) continue;
+                                    const Interface<R> itj = makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor));
+                                    sp.beta[j] *= secondaryScatterWeight(sc, itj, d, ss, false);
+                                }
+                                if (ss.transmitted) ray.region = other;
+                                ray.o[0] = gp.x; ray.o[1] = gp.y; ray.o[2] = gp.z;
+                                ray.d[0] = ss.wi.x; ray.d[1] = ss.wi.y; ray.d[2] = ss.wi.z;
+                                ray.depB = h.boundary;
+                                ray.depP = h.prim;
+                                ray.errN = errG;
+                                cont = true;
+                                // particles carry flux: roulette against the event's own weight
+                                if (depth >= P.rrDepth && ss.weight < R(1)) {
+                                    cont = rng.uniform() < double(ss.weight);
+                                    for (int j = 0; j < NW; ++j) sp.beta[j] *= R(1) / ss.weight;
+                                }
+                            }
+                        }
+                    }
                 }
             }
         }
-        if (depth >= P.maxDepth) return;
-        if (op.type == OWEC_SURF_DIELECTRIC) {  // terminateIfDispersive (transport.cpp:216-225)
-            for (int j = 1; j < NW; ++j) {
-                if (sp.pdf[j] == 0.f) continue;
-                if (isDispersive(it, makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor)))) {
-                    for (int m = 1; m < NW; ++m) { sp.pdf[m] = 0.f; beta[m] = R(0); }
-                    sp.pdf[0] /= float(NW);
-                    break;
-                }
-            }
-        }
-        // scatterAtSurface in importance transport (transport.cpp:437-471)
-        const Draw3<R> u(rng);
-        ScatterSample<R> ss;
-        if (!sampleScatter(sc, it, d, u.u1, u.u2, u.u3, false, ss) || !(ss.weight > R(0))) return;
-        beta[0] *= ss.weight;
-        for (int j = 1; j < NW; ++j) {
-            if (sp.pdf[j] == 0.f) continue;
-            const Interface<R> itj = makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor));
-            beta[j] *= secondaryScatterWeight(sc, itj, d, ss, false);
-        }
-        if (ss.transmitted) region = other;
-        o = gp;
-        d = ss.wi;
-        depB = h.boundary;
-        depP = h.prim;
-        errN = errG;
-        // particles carry flux: roulette against the event's own weight
-        if (depth >= P.rrDepth && ss.weight < R(1)) {
-            if (rng.uniform() >= double(ss.weight)) return;
-            for (int j = 0; j < NW; ++j) beta[j] *= R(1) / ss.weight;
-        }
+        queueConnection<M>(sc, pb, q, film, i, pdfIn, value, k, cp, cRegion, cB, cP, cErr, connect);
+        if (cont) aux.depth += 1;
+        else aux.flags &= ~kFlagAlive;
+        aux.rngState = rng.state;
+        pb.ray[i] = ray;
+        pb.spec[i] = sp;
+        pb.aux[i] = aux;
+        warpCount(&st->leaks, leak);
+        warpCount(&st->inconsistencies, inconsistent);
+        warpCount(&st->faults, lost);
+        warpPush(q.active[nxt], &q.counts[nxt], cont, i);
     }
-}
-
-// Adds a per-lane count to a counter, one atomic per warp (all lanes of the warp present).
-__device__ __forceinline__ void warpFlush(unsigned long long* counter, uint32_t v) {
-    const uint32_t sum = __reduce_add_sync(0xFFFFFFFFu, v);
-    if ((threadIdx.x & 31u) == 0 && sum) atomicAdd(counter, (unsigned long long)sum);
-}
-
-template <int M, bool AnyHit>
-__global__ void __launch_bounds__(128) kParticle(DeviceScene sc, ParticleParams P, unsigned long long* splat,
-                                                 StatCounters* st) {
-    extern __shared__ StackEntry stackMem[];
-    StackEntry* stack = stackMem + threadIdx.x;
-    Tally t;
-    for (uint64_t k = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; k < P.n; k += uint64_t(gridDim.x) * blockDim.x)
-        traceParticle<M, AnyHit>(sc, P, P.first + k, stack, splat, t);
-    warpFlush(&st->paths, t.paths);
-    warpFlush(&st->segments, t.segments);
-    warpFlush(&st->inconsistencies, t.inconsistencies);
-    warpFlush(&st->leaks, t.leaks);
-    warpFlush(&st->shadowRays, t.connections);
-    warpFlush(&st->faults, t.faults);
 }
 
 __global__ void __launch_bounds__(256) kResolveSplats(const unsigned long long* splat, uint32_t nPixels, double scale,
@@ -587,31 +522,30 @@ __global__ void __launch_bounds__(256) kResolveSplats(const unsigned long long* 
     xyz[i] = v * scale;
 }
 
-template <int M, bool AnyHit>
-void launchOne(const DeviceScene& sc, const ParticleParams& P, unsigned long long* splat, StatCounters* st, int grid,
-               cudaStream_t s) {
-    kParticle<M, AnyHit><<<grid, 128, traversalSharedBytes(128), s>>>(sc, P, splat, st);
-}
-
 }  // namespace
 
-void launchParticles(int mode, const DeviceScene& sc, const ParticleParams& P, unsigned long long* splat,
-                     StatCounters* st, int grid, cudaStream_t s) {
-    const bool any = P.anyHitShadows != 0;
-    if (mode == OWEC_PRECISION_FP64) {
-        if (any) launchOne<OWEC_PRECISION_FP64, true>(sc, P, splat, st, grid, s);
-        else launchOne<OWEC_PRECISION_FP64, false>(sc, P, splat, st, grid, s);
-    } else if (mode == OWEC_PRECISION_FP32) {
-        if (any) launchOne<OWEC_PRECISION_FP32, true>(sc, P, splat, st, grid, s);
-        else launchOne<OWEC_PRECISION_FP32, false>(sc, P, splat, st, grid, s);
-    } else {
-        if (any) launchOne<OWEC_PRECISION_MIXED, true>(sc, P, splat, st, grid, s);
-        else launchOne<OWEC_PRECISION_MIXED, false>(sc, P, splat, st, grid, s);
-    }
+template <int M>
+void launchEmit(const DeviceScene& sc, const ParticleParams& P, const PathBuffers<ModeR<M>>& pb, const Queues& q,
+                StatCounters* st, const SplatTarget& film, uint32_t n, cudaStream_t s) {
+    kEmit<M><<<(n + 127) / 128, 128, 0, s>>>(sc, P, pb, q, st, film, n);
 }
-
+template <int M>
+void launchParticleEvent(const DeviceScene& sc, const ParticleParams& P, const PathBuffers<ModeR<M>>& pb,
+                         const Queues& q, int cur, StatCounters* st, const SplatTarget& film, int grid, cudaStream_t s) {
+    kParticleEvent<M><<<grid, 128, 0, s>>>(sc, P, pb, q, cur, st, film);
+}
 void launchResolveSplats(const unsigned long long* splat, uint32_t nPixels, double scale, double* xyz, cudaStream_t s) {
     kResolveSplats<<<(3 * nPixels + 255) / 256, 256, 0, s>>>(splat, nPixels, scale, xyz);
 }
+
+#define OWEC_INSTANTIATE_PARTICLES(M)                                                                              \
+    template void launchEmit<M>(const DeviceScene&, const ParticleParams&, const PathBuffers<ModeR<M>>&,          \
+                                const Queues&, StatCounters*, const SplatTarget&, uint32_t, cudaStream_t);         \
+    template void launchParticleEvent<M>(const DeviceScene&, const ParticleParams&, const PathBuffers<ModeR<M>>&, \
+                                         const Queues&, int, StatCounters*, const SplatTarget&, int, cudaStream_t);
+
+OWEC_INSTANTIATE_PARTICLES(0)
+OWEC_INSTANTIATE_PARTICLES(1)
+OWEC_INSTANTIATE_PARTICLES(2)
 
 }  // namespace owec

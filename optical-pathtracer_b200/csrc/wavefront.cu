@@ -17,6 +17,7 @@
 //
 // Each path draws from its own PCG32 stream in the reference's order, so for a one-sample pass
 // a device path makes the CPU path's decisions until rounding changes one of them.
+#include "splat.cuh"
 #include "transport.cuh"
 #include "wavefront.hpp"
 
@@ -607,10 +608,11 @@ __global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SH
 //
 // Persistent like kIntersect: a lane's job is one shadow ray, walked segment by segment through
 // null boundaries; its traversal advances a few visits per round and a finished lane takes the
-// next job.
-template <int M, bool AnyHit, bool Count>
+// next job. Splat: the rays are the light integrator's connections to the eye, whose
+// contributions land in the film's pixels instead of the paths' radiance.
+template <int M, bool AnyHit, bool Count, bool Splat = false>
 __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
-                                               StatCounters* st, uint32_t* fetch) {
+                                               StatCounters* st, uint32_t* fetch, SplatTarget film) {
     using R = RT<M>;
     using Ro = typename Mode<M>::Ro;
     using Rr = typename Mode<M>::Rr;
@@ -731,7 +733,9 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
             bool clear = outcome == 1;
             const ShadowRay<R>& sr = pb.shadow[job];
             if (clear && finite && region != sr.endRegion) clear = false;
-            if (clear) {
+            if (clear && Splat) {
+                faults += !splatXyz(film.words, film.pixel[job], pb.spec[path].lambda, sr.contrib, Tr);
+            } else if (clear) {
                 float* L = pb.spec[path].L;
                 for (int j = 0; j < NW; ++j) L[j] += float(R(sr.contrib[j]) * Tr[j]);
             }
@@ -805,13 +809,13 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadowVis(DeviceScene sc, PathBuffers<RT<
     }
 }
 
-template <int M>
+template <int M, bool Splat = false>
 __global__ void __launch_bounds__(256) kShadowApply(DeviceScene sc, PathBuffers<RT<M>> pb, Queues q, const uint8_t* vis,
-                                                    StatCounters* st) {
+                                                    StatCounters* st, SplatTarget film) {
     using R = RT<M>;
     const uint32_t n = q.counts[3];
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const uint8_t v = vis[k];
+        uint8_t v = vis[k];
         bool clear = v == 1;
         if (clear) {
             const ShadowRay<R> sr = pb.shadow[k];
@@ -833,7 +837,9 @@ __global__ void __launch_bounds__(256) kShadowApply(DeviceScene sc, PathBuffers<
             }
             if (!finite && sr.region != 0) clear = false;
             if (finite && sr.region != sr.endRegion) clear = false;
-            if (clear) {
+            if (clear && Splat) {
+                if (!splatXyz(film.words, film.pixel[k], pb.spec[sr.path].lambda, sr.contrib, Tr)) v = 2;
+            } else if (clear) {
                 float* L = pb.spec[sr.path].L;
                 for (int j = 0; j < NW; ++j) L[j] += float(R(sr.contrib[j]) * Tr[j]);
             }
@@ -1010,10 +1016,21 @@ void launchShadow(const DeviceScene& sc, const PassParams& pp, const PathBuffers
     if (pp.anyHitShadows) {
         if (sc.travCounters) kShadowVis<M, true><<<grid, 128, smem, s>>>(sc, pb, q, vis, fetch);
         else kShadowVis<M, false><<<grid, 128, smem, s>>>(sc, pb, q, vis, fetch);
-        kShadowApply<M><<<grid, 256, 0, s>>>(sc, pb, q, vis, st);
+        kShadowApply<M><<<grid, 256, 0, s>>>(sc, pb, q, vis, st, SplatTarget{});
     } else {
-        if (sc.travCounters) kShadow<M, false, true><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch);
-        else kShadow<M, false, false><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch);
+        if (sc.travCounters) kShadow<M, false, true><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch, SplatTarget{});
+        else kShadow<M, false, false><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch, SplatTarget{});
+    }
+}
+template <int M>
+void launchConnect(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q,
+                   StatCounters* st, uint32_t* fetch, uint8_t* vis, const SplatTarget& film, int grid, cudaStream_t s) {
+    const size_t smem = traversalSharedBytes(128);
+    if (pp.anyHitShadows) {
+        kShadowVis<M, false><<<grid, 128, smem, s>>>(sc, pb, q, vis, fetch);
+        kShadowApply<M, true><<<grid, 256, 0, s>>>(sc, pb, q, vis, st, film);
+    } else {
+        kShadow<M, false, false, true><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch, film);
     }
 }
 template <int M>
@@ -1059,6 +1076,8 @@ void configureKernels() {
                                    int, StatCounters*, int, cudaStream_t);                                          \
     template void launchShadow<M>(const DeviceScene&, const PassParams&, const PathBuffers<RT<M>>&, const Queues&,   \
                                   StatCounters*, uint32_t*, uint8_t*, int, cudaStream_t);                                                \
+    template void launchConnect<M>(const DeviceScene&, const PassParams&, const PathBuffers<RT<M>>&, const Queues&,  \
+                                   StatCounters*, uint32_t*, uint8_t*, const SplatTarget&, int, cudaStream_t);      \
     template void launchFilm<M>(const DeviceScene&, const PassParams&, const PathBuffers<RT<M>>&, double*, double*,  \
                                 double*, uint32_t, cudaStream_t);                                                   \
     template void launchCastRays<M>(const DeviceScene&, uint64_t, const double*, const double*, uint32_t*,          \

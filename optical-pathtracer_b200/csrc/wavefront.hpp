@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include "path_state.cuh"
+#include "splat.cuh"
 
 namespace owec {
 
@@ -28,6 +29,10 @@ void launchSurface(const DeviceScene&, const PassParams&, const PathBuffers<Mode
 template <int M>
 void launchShadow(const DeviceScene&, const PassParams&, const PathBuffers<ModeR<M>>&, const Queues&, StatCounters*,
                   uint32_t* fetch, uint8_t* vis, int grid, cudaStream_t);
+// The light integrator's connections to the eye: their visibility, transmittance and splats.
+template <int M>
+void launchConnect(const DeviceScene&, const PassParams&, const PathBuffers<ModeR<M>>&, const Queues&, StatCounters*,
+                   uint32_t* fetch, uint8_t* vis, const SplatTarget& film, int grid, cudaStream_t);
 void launchResolve(const double* film, const double* comp, const double* samples, uint32_t nPixels, double* xyz,
                    cudaStream_t);
 template <int M>

@@ -168,3 +168,22 @@ def test_film_is_deterministic_and_passes_accumulate():
         b, n2 = c.resolve()
     assert np.array_equal(n, n2) and n.max() == 3
     assert np.array_equal(a, b), "a pass split into sub-passes must give the same film, bit for bit"
+
+
+@pytest.mark.parametrize("integrator", ["path", "light"])
+def test_switching_precision_in_one_context_matches_a_fresh_context(integrator):
+    """The path state is sized per precision mode: an FP64 pass after a mixed one in the same
+    context renders exactly what a fresh FP64 context renders (the FP64 records are larger)."""
+    desc = scenes.lamp_over_floor(64, 48).desc()
+    s64 = A.make_settings(seed=21, precision=A.PRECISION_FP64, integrator=integrator)
+    with _ctx(desc) as c:
+        c.set_settings(A.make_settings(seed=20, precision=A.PRECISION_MIXED, integrator=integrator))
+        c.run_pass(700)  # 2M+ paths in flight, the most the mixed mode allocates
+        c.set_settings(s64)
+        c.run_pass(700)
+        switched = c.resolve()[0]
+        assert c.stats()["device_faults"] == 0
+    with _ctx(desc, s64) as c:
+        c.run_pass(700)
+        fresh = c.resolve()[0]
+    assert np.array_equal(switched, fresh)
