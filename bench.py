@@ -117,9 +117,12 @@ PRECISIONS = {"mixed": A.PRECISION_MIXED, "fp32": A.PRECISION_FP32, "fp64": A.PR
 PRECISION = "mixed"
 
 
+INTEGRATOR = "path"
+
+
 def settings_for(rank):
     return A.make_settings(seed=rank, max_depth=MAX_DEPTH, rr_depth=RR_DEPTH, wavelength_mode=A.WAVELENGTHS_HERO4,
-                           precision=PRECISIONS[PRECISION])
+                           precision=PRECISIONS[PRECISION], integrator=INTEGRATOR)
 
 
 def cpu_reference_rate(desc, seconds_target=12.0, threads=0):
@@ -275,6 +278,35 @@ def configs_study(device):
     return out
 
 
+def light_study(device, passes=8):
+    """The light integrator (particles from the area light, connected to the pinhole at every
+    non-specular vertex) on the bench's own scene at 1920 x 1080: particles/s over one-particle-per-
+    pixel passes, and its image mean against the path integrator's on the same scene."""
+    import owe_cuda
+    out = {}
+    with owe_cuda.Context(device) as c:
+        c.upload(scenes.bvh_stress_room(WIDTH, HEIGHT).desc())
+        c.build_bvh()
+        means = {}
+        for integrator in ("light", "path"):
+            c.set_settings(A.make_settings(seed=5, max_depth=12, rr_depth=6, integrator=integrator))
+            c.run_pass(1)
+            c.reset_film()
+            seconds = 0.0
+            for _ in range(passes):
+                c.run_pass(1)
+                seconds += c.last_pass_timing()[0]
+            means[integrator] = float(c.resolve()[0][:, :, 1].mean())
+            out[f"{integrator}_per_s"] = WIDTH * HEIGHT * passes / seconds
+            if integrator == "light":
+                st = c.stats()
+                out["light_connections_per_particle"] = st["shadow_rays"] / max(1, st["paths"])
+                out["light_faults"] = st["device_faults"]
+        out["mean_y_light_over_path"] = means["light"] / means["path"]
+    out["unit"] = "particles/s (light), paths/s (path)"
+    return out
+
+
 def run_cuda(args):
     import torch
     world, rank, local = dist_env()
@@ -370,17 +402,22 @@ def run_cuda(args):
             pass
         clk = clocks.summary()
         cpu_rate, cores, sample = (None, None, "skipped")
-        if not args.no_cpu_baseline:
+        if INTEGRATOR == "light":
+            sample = "none: the reference has no CPU light integrator"
+        elif not args.no_cpu_baseline:
             try:
                 cpu_rate, cores, sample = cpu_reference_rate(desc)
             except BaseException as e:  # pytest.skip when the oracle was not built
                 sample = f"unavailable: {e}"
+        light = INTEGRATOR == "light"
         line = {
-            "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
+            "metric": "spectral particles/s" if light else METRIC, "value": value,
+            "unit": "particles/s" if light else "paths/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * device_seconds / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": {"mixed": "f32+f64", "fp32": "f32", "fp64": "f64"}[PRECISION], "data": "synthetic",
-            "config": {"workload": WORKLOAD, "paths_per_step": n_pix, "triangles": info["triangles"],
+            "config": {"workload": WORKLOAD + (", light integrator (particles)" if light else ""),
+                       "paths_per_step": n_pix, "triangles": info["triangles"],
                        "precision": {"mixed": "fp32 camera-relative + selective fp64", "fp32": "plain fp32",
                                      "fp64": "all fp64"}[PRECISION], "l2": "flushed between steps (512 MB write)",
                        "parallelism": f"replicated scene, dp{world} over sample streams"},
@@ -405,13 +442,16 @@ def run_cuda(args):
                     "resolve_ms": [round(1e3 * b, 2) for _, b in split], "note": "pass + resolved image read back into pinned host memory per step through owe_cuda.Renderer"},
             "faults": stats1["device_faults"],
         }
-        if not args.no_extras and world == 1:
+        if not args.no_extras and world == 1 and not light:
             line["precision_study"] = precision_study(local)
             line["adjoint_study"] = adjoint_study(local)
             line["configs_study"] = configs_study(local)
+            line["light_study"] = light_study(local)
         # our own kernel launches in the timed region: intersect, medium, two surface kernels, the
-        # shadow visibility and its contributions per bounce, and generate + film per step
-        line["gpu_launches"] = int(6 * launches + 2 * args.steps)
+        # shadow visibility and its contributions per bounce, and generate + film per step; for
+        # particles intersect, event, visibility and splats per bounce, and emit with the emitters'
+        # own connections (visibility and splats) per step
+        line["gpu_launches"] = int(4 * launches + 3 * args.steps) if light else int(6 * launches + 2 * args.steps)
         print(json.dumps(line))
     renderer.close()
     if world > 1:
@@ -433,9 +473,13 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=sorted(PRECISIONS),
                     help="mixed: FP32 camera-relative + selective FP64 (the product); fp64: the all-FP64 "
                          "instantiation of the same kernels it is compared with")
+    ap.add_argument("--integrator", default="path", choices=["path", "light"],
+                    help="path: the headline camera-path integrator; light: particles from the emitters, "
+                         "measured in particles/s on the same scene")
     args = ap.parse_args()
     globals()["WIDTH"], globals()["HEIGHT"] = args.width, args.height
     globals()["PRECISION"] = args.precision
+    globals()["INTEGRATOR"] = args.integrator
     if args.impl == "reference":
         return run_reference(args)
     return run_cuda(args)

@@ -879,6 +879,8 @@ void runParticles(owec_ctx& c, int spp) {
     const int grid = c.numSMs * 8;
     cudaStream_t s = c.stream;
     uint32_t* counts = c.dCounts.get();
+    double travSeconds[2] = {0, 0};
+    int intersectLaunches = 0, evUsed = 0;
     OWEC_CUDA(cudaEventRecord(c.passStart, s));
     // nothing emits: the estimate is zero, but the particles still count
     const bool emits = c.pSky > 0 || !c.lights.empty();
@@ -902,20 +904,48 @@ void runParticles(owec_ctx& c, int spp) {
             }
             OWEC_CUDA(cudaMemsetAsync(counts + (cur ^ 1), 0, sizeof(uint32_t), s));
             OWEC_CUDA(cudaMemsetAsync(counts + 2, 0, 5 * sizeof(uint32_t), s));  // shadow queue, fetch counters
+            if (size_t(evUsed + 4) > c.travEvents.size())
+                for (int k = 0; k < 4; ++k) {
+                    cudaEvent_t e;
+                    OWEC_CUDA(cudaEventCreate(&e));
+                    c.travEvents.push_back(e);
+                }
+            OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed], s));
             launchIntersect<M>(c.ds, pb, q, cur, c.dStats.get(), counts + 4, grid, s);
+            ++intersectLaunches;
+            OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 1], s));
             launchParticleEvent<M>(c.ds, P, pb, q, cur, c.dStats.get(), film, grid, s);
+            OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 2], s));
             launchConnect<M>(c.ds, pp, pb, q, c.dStats.get(), counts + 5, c.dShadowVis.get(), film, grid, s);
+            OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 3], s));
             checkLaunch();
+            evUsed += 4;
             OWEC_CUDA(cudaMemsetAsync(counts + cur, 0, sizeof(uint32_t), s));
             cur ^= 1;
+            if (evUsed >= 256) {  // fold the timings in before reusing the events
+                OWEC_CUDA(cudaStreamSynchronize(s));
+                for (int e = 0; e < evUsed; e += 2) {
+                    float ms = 0;
+                    OWEC_CUDA(cudaEventElapsedTime(&ms, c.travEvents[e], c.travEvents[e + 1]));
+                    travSeconds[(e >> 1) & 1] += ms * 1e-3;
+                }
+                evUsed = 0;
+            }
         }
     }
     OWEC_CUDA(cudaEventRecord(c.passStop, s));
     OWEC_CUDA(cudaEventSynchronize(c.passStop));
+    for (int e = 0; e < evUsed; e += 2) {
+        float ms = 0;
+        OWEC_CUDA(cudaEventElapsedTime(&ms, c.travEvents[e], c.travEvents[e + 1]));
+        travSeconds[(e >> 1) & 1] += ms * 1e-3;  // pairs alternate: intersect, connections
+    }
     float ms = 0;
     OWEC_CUDA(cudaEventElapsedTime(&ms, c.passStart, c.passStop));
     c.lastPassSeconds = ms * 1e-3;
-    c.lastIntersectSeconds = c.lastShadowSeconds = c.lastIntersectLaunches = 0;
+    c.lastIntersectSeconds = travSeconds[0];
+    c.lastShadowSeconds = travSeconds[1];
+    c.lastIntersectLaunches = intersectLaunches;
     c.particles += double(total);
     c.passCount += uint64_t(spp);
 }

@@ -1027,10 +1027,12 @@ void launchConnect(const DeviceScene& sc, const PassParams& pp, const PathBuffer
                    StatCounters* st, uint32_t* fetch, uint8_t* vis, const SplatTarget& film, int grid, cudaStream_t s) {
     const size_t smem = traversalSharedBytes(128);
     if (pp.anyHitShadows) {
-        kShadowVis<M, false><<<grid, 128, smem, s>>>(sc, pb, q, vis, fetch);
+        if (sc.travCounters) kShadowVis<M, true><<<grid, 128, smem, s>>>(sc, pb, q, vis, fetch);
+        else kShadowVis<M, false><<<grid, 128, smem, s>>>(sc, pb, q, vis, fetch);
         kShadowApply<M, true><<<grid, 256, 0, s>>>(sc, pb, q, vis, st, film);
     } else {
-        kShadow<M, false, false, true><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch, film);
+        if (sc.travCounters) kShadow<M, false, true, true><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch, film);
+        else kShadow<M, false, false, true><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch, film);
     }
 }
 template <int M>
