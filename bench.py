@@ -434,9 +434,9 @@ def run_cuda(args):
                          "per_query": {"nodes": nodes / max(1, q), "prims": prims / max(1, q)},
                          "queries_per_pass": q, "launches_per_pass": launches_prof},
             "clocks": clk,
-            "cpu_baseline": {"value": cpu_rate, "unit": "paths/s", "cores": cores, "kind": "reference",
+            "cpu_baseline": {"value": cpu_rate, "unit": "particles/s" if light else "paths/s", "cores": cores, "kind": "reference",
                              "sample": sample},
-            "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
+            "e2e": {"value": e2e_value, "unit": "particles/s" if light else "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
                     "value_at_median_step": n_pix * world / statistics.median(a + b for a, b in split),
                     "steps": e2e_steps, "pass_ms": [round(1e3 * a, 2) for a, _ in split],
                     "resolve_ms": [round(1e3 * b, 2) for _, b in split], "note": "pass + resolved image read back into pinned host memory per step through owe_cuda.Renderer"},

@@ -110,16 +110,28 @@ typedef struct owec_emission {
     int32_t pad0;
 } owec_emission;
 
-/* Shapes (src/owe/scene/geometry.hpp), in their own frames. */
+/* Shapes (src/owe/scene/geometry.hpp), in their own frames. "Data" is the boundary's run of
+ * owec_scene_desc.shape_data (data_offset, data_count). */
 #define OWEC_SHAPE_SPHERE 0   /* params: R                                        */
-#define OWEC_SHAPE_SAG 1      /* params: c (1/R), k (conic), rMax, rMin; quadric form, vertex at 0, +z normal */
-#define OWEC_SHAPE_PLANE 2    /* params: aperture (0 disk, 1 rect, 2 ellipse), a, b */
+#define OWEC_SHAPE_SAG 1      /* params: c (1/R), k (conic), rMax, rMin; vertex at 0, +z normal. Data: the even
+                               * asphere terms A4, A6, ... (none: a conic, solved as a quadric; otherwise the
+                               * sag is crossed numerically, SagSurface::intersectNumeric) */
+#define OWEC_SHAPE_PLANE 2    /* params: aperture (OWEC_APERTURE_*), a, b         */
 #define OWEC_SHAPE_CYLINDER 3 /* params: R, z0, z1                                */
 #define OWEC_SHAPE_MESH 4     /* mesh: index into owec_scene_desc.meshes           */
+#define OWEC_SHAPE_CONE 5     /* params: r0, z0, r1, z1: the frustum revolving the segment (r0, z0)-(r1, z1)
+                               * about z (ConeShape; z0 != z1), normal away from the axis */
+#define OWEC_SHAPE_TORUS 6    /* params: R, zc, rho, a0; data: a1. The arc of radius rho about (R, zc) in the
+                               * (r, z) half-plane for angles a0..a1, revolved about z (TorusPatchShape) */
+#define OWEC_SHAPE_ROUND_WALL 7 /* params: R, H; data: openings as (azimuth, width, sill, top) quadruples: an
+                                 * open cylinder from z = 0 to H with rectangular openings (RoundWallShape) */
+#define OWEC_SHAPE_DOME 8     /* params: R, slit azimuth, slit width, slit top elevation: the hemisphere
+                               * z >= 0 with an observing slit (DomeShape) */
 
 #define OWEC_APERTURE_DISK 0 /* a = rMax, b = rMin */
 #define OWEC_APERTURE_RECT 1 /* a = halfX, b = halfY */
 #define OWEC_APERTURE_ELLIPSE 2
+#define OWEC_APERTURE_DISK_HOLE 3 /* a = rMax, b = the hole's radius; data: the hole's centre (hx, hy) */
 
 #define OWEC_REGION_OUTSIDE 0xFFFFFFFFu /* placeholder resolved by the engine before flattening */
 
@@ -132,6 +144,8 @@ typedef struct owec_boundary {
     int32_t emission;   /* -1 = none */
     double to_world[12];/* rigid transform shape -> world: row-major [R | t], 3 rows of 4 */
     double params[4];
+    uint32_t data_offset; /* first value of the shape's data in owec_scene_desc.shape_data */
+    uint32_t data_count;  /* its number of values (0: none) */
 } owec_boundary;
 
 typedef struct owec_mesh {
@@ -194,6 +208,8 @@ typedef struct owec_scene_desc {
     int32_t frame_origin_set;
     int32_t pad0;
     double frame_origin[3];
+    uint64_t n_shape_data;
+    const double* shape_data;      /* the shapes' data (asphere terms, wall openings, ...) */
 } owec_scene_desc;
 
 /* ------------------------------------------------------------------ pass settings */

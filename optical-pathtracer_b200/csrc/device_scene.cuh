@@ -36,6 +36,11 @@ struct DBoundary {
     double params[4];
     double area;          // emitter area (planes, spheres, flat sags, cylinders)
     double scale;         // size of the frame (error model of anchors)
+    // what the numeric crossings need beyond params: an asphere's z slab (zMin, zMax); a torus
+    // patch's rMax, zMin, zMax and its arc's end a1
+    double ext[4];
+    uint32_t dataOffset;  // the shape's data in DeviceScene::shapeData (asphere terms, openings, ...)
+    uint32_t dataCount;
 };
 
 struct DLight {
@@ -83,6 +88,8 @@ struct DeviceScene {
     const owec_emission* emissions;
     const DBoundary* boundaries;
     const DLight* lights;
+    const double* shapeData;  // the shapes' data, addressed by DBoundary::dataOffset
+    int32_t fullShapes;       // 1: shapes beyond spheres, conic sags, plain apertures and cylinders
     uint32_t nRegions, nBoundaries, nLights, nMedia;
     const WideNode* nodes;
     const PrimRec* prims;

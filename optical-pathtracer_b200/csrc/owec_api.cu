@@ -81,21 +81,47 @@ void xfPoint(const double m[12], const double p[3], double out[3]) {
     for (int i = 0; i < 3; ++i) out[i] = m[4 * i] * p[0] + m[4 * i + 1] * p[1] + m[4 * i + 2] * p[2] + m[4 * i + 3];
 }
 
-// The conic sag's z range over the aperture (SagSurface's constructor, geometry.cpp:74-90).
-void sagZRange(double c, double k, double rMax, double rMin, double& zMin, double& zMax) {
+// The sag's z range over the aperture (SagSurface's constructor, geometry.cpp:70-88); A: the even
+// asphere terms A4, A6, ...
+void sagZRange(double c, double k, double rMax, double rMin, const double* A, uint32_t nA, double& zMin, double& zMax) {
     zMin = INFINITY;
     zMax = -INFINITY;
     const int N = 512;
     for (int i = 0; i <= N; ++i) {
         const double r = rMin + (rMax - rMin) * i / N;
         const double r2 = r * r;
-        const double z = c * r2 / (1 + std::sqrt(std::max(0.0, 1 - (1 + k) * c * c * r2)));
+        double z = c * r2 / (1 + std::sqrt(std::max(0.0, 1 - (1 + k) * c * c * r2)));
+        double rp = r2 * r2;
+        for (uint32_t j = 0; j < nA; ++j) { z += A[j] * rp; rp *= r2; }
         zMin = std::min(zMin, z);
         zMax = std::max(zMax, z);
     }
     const double pad = 1e-9 + 1e-3 * (zMax - zMin);
     zMin -= pad;
     zMax += pad;
+}
+
+// A torus patch's extent (TorusPatchShape's constructor, geometry.cpp:557-577): ext = rMax, zMin,
+// zMax of the arc a0..a1 of radius rho about (R, zc), and the arc's upper end.
+void torusExtent(double R, double zc, double rho, double a0, double a1, double ext[4]) {
+    const double lo = std::min(a0, a1), hi = std::max(a0, a1);
+    double rMax = -INFINITY, zMin = INFINITY, zMax = -INFINITY;
+    auto add = [&](double a) {
+        rMax = std::max(rMax, R + rho * std::cos(a));
+        const double z = zc + rho * std::sin(a);
+        zMin = std::min(zMin, z);
+        zMax = std::max(zMax, z);
+    };
+    add(lo);
+    add(hi);
+    for (int k = -4; k <= 4; ++k) {  // the extremes of cos and sin inside the range
+        const double a = k * kPi / 2;
+        if (a > lo && a < hi) add(a);
+    }
+    ext[0] = rMax;
+    ext[1] = zMin;
+    ext[2] = zMax;
+    ext[3] = hi;
 }
 
 // A shape's bounds in its frame (Shape::bounds of the reference's shapes).
@@ -111,12 +137,26 @@ Box localBounds(const owec_scene_desc& d, const owec_boundary& b) {
         case OWEC_SHAPE_SPHERE: put(-P[0], -P[0], -P[0], P[0], P[0], P[0]); break;
         case OWEC_SHAPE_SAG: {
             double zMin, zMax;
-            sagZRange(P[0], P[1], P[2], P[3], zMin, zMax);
+            sagZRange(P[0], P[1], P[2], P[3], d.shape_data + b.data_offset, b.data_count, zMin, zMax);
             put(-P[2], -P[2], zMin, P[2], P[2], zMax);
             break;
         }
+        case OWEC_SHAPE_CONE: {
+            const double R = std::max(P[0], P[2]);
+            put(-R, -R, std::min(P[1], P[3]), R, R, std::max(P[1], P[3]));
+            break;
+        }
+        case OWEC_SHAPE_TORUS: {
+            double ext[4];
+            torusExtent(P[0], P[1], P[2], P[3], d.shape_data[b.data_offset], ext);
+            put(-ext[0], -ext[0], ext[1], ext[0], ext[0], ext[2]);
+            break;
+        }
+        case OWEC_SHAPE_ROUND_WALL: put(-P[0], -P[0], 0, P[0], P[0], P[1]); break;
+        case OWEC_SHAPE_DOME: put(-P[0], -P[0], 0, P[0], P[0], P[0]); break;
         case OWEC_SHAPE_PLANE: {
-            const double ex = P[1], ey = int(P[0]) == OWEC_APERTURE_DISK ? P[1] : P[2];
+            const int ap = int(P[0]);
+            const double ex = P[1], ey = (ap == OWEC_APERTURE_DISK || ap == OWEC_APERTURE_DISK_HOLE) ? P[1] : P[2];
             const double pad = 1e-9 * (1 + std::max(ex, ey));
             put(-ex, -ey, -pad, ex, ey, pad);
             break;
@@ -159,12 +199,16 @@ double shapeArea(const owec_scene_desc& d, const owec_boundary& b, bool& canSamp
         case OWEC_SHAPE_SPHERE: return 4 * kPi * P[0] * P[0];
         case OWEC_SHAPE_PLANE: {
             const int ap = int(P[0]);
+            if (ap == OWEC_APERTURE_DISK_HOLE) {  // no area sampler (PlaneShape::canSample)
+                canSample = false;
+                return kPi * (P[1] * P[1] - P[2] * P[2]);
+            }
             if (ap == OWEC_APERTURE_DISK) return kPi * (P[1] * P[1] - P[2] * P[2]);
             if (ap == OWEC_APERTURE_RECT) return 4 * P[1] * P[2];
             return kPi * P[1] * P[2];
         }
         case OWEC_SHAPE_SAG:
-            canSample = P[0] == 0;  // only a flat sag has an area sampler
+            canSample = P[0] == 0 && b.data_count == 0;  // only a flat sag has an area sampler
             return kPi * (P[2] * P[2] - P[3] * P[3]);
         case OWEC_SHAPE_CYLINDER: return 2 * kPi * P[0] * std::fabs(P[2] - P[1]);
         default: canSample = false; return 0;  // emitting meshes are not sampled by next-event estimation here
@@ -234,6 +278,7 @@ struct owec_ctx {
     DBuf<owec_emission> dEmissions;
     DBuf<DBoundary> dBoundaries;
     DBuf<DLight> dLights;
+    DBuf<double> dShapeData;
     DBuf<float4> dPrimLo, dPrimHi, dTri;
     DBuf<double> dTri64;
     BvhScratch scratch;
@@ -340,7 +385,40 @@ void validateDesc(const owec_scene_desc& d) {
                                                           "emission needs a radiance spectrum");
     for (uint32_t i = 0; i < d.n_boundaries; ++i) {
         const owec_boundary& b = d.boundaries[i];
-        require(b.shape >= OWEC_SHAPE_SPHERE && b.shape <= OWEC_SHAPE_MESH, "unknown shape");
+        require(b.shape >= OWEC_SHAPE_SPHERE && b.shape <= OWEC_SHAPE_DOME, "unknown shape");
+        require(b.data_count == 0 || (d.shape_data && uint64_t(b.data_offset) + b.data_count <= d.n_shape_data),
+                "shape data out of range");
+        const double* P = b.params;
+        const double* D = b.data_count ? d.shape_data + b.data_offset : nullptr;
+        switch (b.shape) {
+            case OWEC_SHAPE_SPHERE: require(P[0] > 0, "sphere: radius must be positive"); break;
+            case OWEC_SHAPE_PLANE:
+                require(P[0] >= OWEC_APERTURE_DISK && P[0] <= OWEC_APERTURE_DISK_HOLE, "plane: unknown aperture");
+                if (int(P[0]) == OWEC_APERTURE_DISK_HOLE)
+                    require(b.data_count == 2 && P[1] > 0 && P[2] > 0 && std::hypot(D[0], D[1]) + P[2] < P[1],
+                            "disk with hole: the hole must lie inside the disk");
+                break;
+            case OWEC_SHAPE_CONE:
+                require(std::fabs(P[3] - P[1]) > 0 && P[0] >= 0 && P[2] >= 0, "cone: needs z0 != z1 and radii >= 0");
+                break;
+            case OWEC_SHAPE_TORUS: {
+                require(b.data_count == 1, "torus patch: its data is the arc's end angle");
+                require(P[2] > 0 && std::fabs(D[0] - P[3]) <= kPi + 1e-12, "torus patch: invalid arc");
+                double rMin = INFINITY;
+                for (double a : {std::min(P[3], D[0]), std::max(P[3], D[0])}) rMin = std::min(rMin, P[0] + P[2] * std::cos(a));
+                for (int k = -4; k <= 4; ++k) {
+                    const double a = k * kPi / 2;
+                    if (a > std::min(P[3], D[0]) && a < std::max(P[3], D[0])) rMin = std::min(rMin, P[0] + P[2] * std::cos(a));
+                }
+                require(rMin >= -1e-12 * P[2], "torus patch: the arc crosses the axis");
+                break;
+            }
+            case OWEC_SHAPE_ROUND_WALL:
+                require(P[0] > 0 && P[1] > 0 && b.data_count % 4 == 0, "round wall: radius, height and openings");
+                break;
+            case OWEC_SHAPE_DOME: require(P[0] > 0, "dome: radius must be positive"); break;
+            default: break;
+        }
         require(b.front < d.n_regions && b.back < d.n_regions, "boundary region out of range");
         require(b.optics < d.n_optics, "boundary optics out of range");
         require(b.emission < 0 || uint32_t(b.emission) < d.n_emissions, "boundary emission out of range");
@@ -421,6 +499,16 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
         db.toWorld.m[11] -= origin[2];
         invertRigid(db.toWorld.m, db.toLocal.m);
         for (int k = 0; k < 4; ++k) db.params[k] = b.params[k];
+        db.dataOffset = b.data_offset;
+        db.dataCount = b.data_count;
+        for (double& e : db.ext) e = 0;
+        if (b.shape == OWEC_SHAPE_SAG && b.data_count) {
+            sagZRange(b.params[0], b.params[1], b.params[2], b.params[3], d.shape_data + b.data_offset, b.data_count,
+                      db.ext[0], db.ext[1]);
+        } else if (b.shape == OWEC_SHAPE_TORUS) {
+            torusExtent(b.params[0], b.params[1], b.params[2], b.params[3], d.shape_data[b.data_offset], db.ext);
+            db.params[3] = std::min(b.params[3], d.shape_data[b.data_offset]);
+        }
         bool canSample = false;
         db.area = shapeArea(d, b, canSample);
         if (!canSample) db.area = 0;
@@ -616,6 +704,7 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
     c.dEmissions.upload(c.emissions.data(), c.emissions.size(), s);
     c.dBoundaries.upload(c.boundaries.data(), c.boundaries.size(), s);
     c.dLights.upload(c.lights.data(), c.lights.size(), s);
+    c.dShapeData.upload(d.shape_data, d.n_shape_data, s);
     c.dPrimLo.upload(c.primLo.data(), c.primLo.size(), s);
     c.dPrimHi.upload(c.primHi.data(), c.primHi.size(), s);
     c.dTri.upload(c.triRecs.data(), c.triRecs.size(), s);
@@ -631,6 +720,15 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
     ds.emissions = c.dEmissions.get();
     ds.boundaries = c.dBoundaries.get();
     ds.lights = c.dLights.get();
+    ds.shapeData = c.dShapeData.get();
+    ds.fullShapes = 0;
+    for (uint32_t i = 0; i < d.n_boundaries; ++i) {
+        const owec_boundary& b = d.boundaries[i];
+        if (b.shape == OWEC_SHAPE_CONE || b.shape == OWEC_SHAPE_TORUS || b.shape == OWEC_SHAPE_ROUND_WALL ||
+            b.shape == OWEC_SHAPE_DOME || (b.shape == OWEC_SHAPE_SAG && b.data_count > 0) ||
+            (b.shape == OWEC_SHAPE_PLANE && int(b.params[0]) == OWEC_APERTURE_DISK_HOLE))
+            ds.fullShapes = 1;
+    }
     ds.nRegions = d.n_regions;
     ds.nBoundaries = d.n_boundaries;
     ds.nLights = uint32_t(c.lights.size());

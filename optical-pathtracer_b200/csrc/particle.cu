@@ -312,7 +312,7 @@ __global__ void __launch_bounds__(128) kEmit(DeviceScene sc, ParticleParams P, P
 // connection at a scattering event), escape, the boundary (null crossing, sensor record,
 // absorption), the connection of a non-delta surface vertex and the importance-transport
 // scattering sample with roulette (traceParticle's loop body, particle.slang:365-426).
-template <int M>
+template <int M, bool Full>
 __global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, ParticleParams P, PathBuffers<RT<M>> pb,
                                                          Queues q, int cur, StatCounters* st, SplatTarget film) {
     using R = RT<M>;
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, Particl
             } else if (event == 0) {
                 // meetBoundary (transport.cpp:121-133)
                 const DBoundary& bd = sc.boundaries[h.boundary];
-                const SurfacePoint<R> g = hitGeometry<R, Ro, Rr>(sc, ray, h);
+                const SurfacePoint<R> g = hitGeometry<R, Ro, Rr, Full>(sc, ray, h);
                 const bool fromFront = dot(d, g.n) < R(0);
                 const uint32_t inc = fromFront ? bd.front : bd.back, other = fromFront ? bd.back : bd.front;
                 inconsistent = inc != ray.region;
@@ -532,7 +532,8 @@ void launchEmit(const DeviceScene& sc, const ParticleParams& P, const PathBuffer
 template <int M>
 void launchParticleEvent(const DeviceScene& sc, const ParticleParams& P, const PathBuffers<ModeR<M>>& pb,
                          const Queues& q, int cur, StatCounters* st, const SplatTarget& film, int grid, cudaStream_t s) {
-    kParticleEvent<M><<<grid, 128, 0, s>>>(sc, P, pb, q, cur, st, film);
+    if (sc.fullShapes) kParticleEvent<M, true><<<grid, 128, 0, s>>>(sc, P, pb, q, cur, st, film);
+    else kParticleEvent<M, false><<<grid, 128, 0, s>>>(sc, P, pb, q, cur, st, film);
 }
 void launchResolveSplats(const unsigned long long* splat, uint32_t nPixels, double scale, double* xyz, cudaStream_t s) {
     kResolveSplats<<<(3 * nPixels + 255) / 256, 256, 0, s>>>(splat, nPixels, scale, xyz);

@@ -1,8 +1,10 @@
-// Analytic surfaces in their own frames: spheres, conic sags, planes with apertures and cylinders.
-// Roots come from the numerically stable quadratic in precision R and are refined by re-solving
-// from the approximate hit in precision Rr (src/owe/core/shared/surfaces.hpp:13-137): with
-// R = float and Rr = double this is the selective FP64 step that keeps large-radius lens surfaces
-// exact; with R = Rr = float it is the plain FP32 baseline.
+// Analytic surfaces in their own frames: spheres, conic and aspheric sags, planes with apertures,
+// cylinders, cones, torus patches, round walls and domes (src/owe/scene/geometry.cpp). Quadric roots
+// come from the numerically stable quadratic in precision R and are refined by re-solving from the
+// approximate hit in precision Rr (src/owe/core/shared/surfaces.hpp:13-137): with R = float and
+// Rr = double this is the selective FP64 step that keeps large-radius lens surfaces exact; with
+// R = Rr = float it is the plain FP32 baseline. Aspheres and torus patches have no closed form:
+// their crossings are bracketed by sampling along the clipped ray and bisected, in precision Rr.
 #pragma once
 
 #include "device_scene.cuh"
@@ -11,10 +13,14 @@ namespace owec {
 
 template <class T> struct Tol;
 template <> struct Tol<float> {
-    static constexpr float refine = 1e-3f, relTol = 1e-6f, tiny = 1e-30f;
+    static constexpr float refine = 1e-3f, relTol = 1e-6f, tiny = 1e-30f, bisect = 2e-7f, angle = 1e-5f,
+                           eps = 1.1920929e-7f;
+    static constexpr int bisectSteps = 40;
 };
 template <> struct Tol<double> {
-    static constexpr double refine = 1e-6, relTol = 1e-9, tiny = 1e-300;
+    static constexpr double refine = 1e-6, relTol = 1e-9, tiny = 1e-300, bisect = 1e-15, angle = 1e-9,
+                            eps = 2.220446049250313e-16;
+    static constexpr int bisectSteps = 80;
 };
 
 // Real roots of a t^2 + b t + c = 0, ascending; returns their count (surfaces.hpp:13-33).
@@ -35,11 +41,19 @@ OWEC_HD int solveQuadratic(T a, T b, T c, T& t0, T& t1) {
     return 2;
 }
 
-constexpr int kQuadSag = 0, kQuadSphere = 1, kQuadCylinder = 2;
+constexpr int kQuadSag = 0, kQuadSphere = 1, kQuadCylinder = 2, kQuadCone = 3;
 
+// The coefficients of a quadric along o + t d: a sag c (x^2 + y^2) + c (1 + k) z^2 - 2 z
+// (qa = c, qb = c (1 + k)), a sphere or an infinite cylinder of radius^2 qa, or a cone
+// x^2 + y^2 = (r0 + k (z - z0))^2 (qa = r0, qb = z0, qc = k) (surfaces.hpp:34-72).
 template <class T>
-OWEC_HD void quadricCoeffs(int kind, T qa, T qb, const V3<T>& o, const V3<T>& d, T& A, T& B, T& C) {
-    if (kind == kQuadSag) {
+OWEC_HD void quadricCoeffs(int kind, T qa, T qb, T qc, const V3<T>& o, const V3<T>& d, T& A, T& B, T& C) {
+    if (kind == kQuadCone) {
+        const T rho = qa + qc * (o.z - qb);
+        A = d.x * d.x + d.y * d.y - qc * qc * d.z * d.z;
+        B = T(2) * (o.x * d.x + o.y * d.y - qc * rho * d.z);
+        C = o.x * o.x + o.y * o.y - rho * rho;
+    } else if (kind == kQuadSag) {
         A = qa * (d.x * d.x + d.y * d.y) + qb * d.z * d.z;
         B = T(2) * (qa * (o.x * d.x + o.y * d.y) + qb * o.z * d.z - d.z);
         C = qa * (o.x * o.x + o.y * o.y) + qb * o.z * o.z - T(2) * o.z;
@@ -57,12 +71,13 @@ OWEC_HD void quadricCoeffs(int kind, T qa, T qb, const V3<T>& o, const V3<T>& d,
 // The root t (from precision R) refined in precision Rr, if it may lie in (tmin, tmax) and does
 // once refined (refineRoot / mayLieIn / refinedRootIn, surfaces.hpp:75-101).
 template <class R, class Rr>
-OWEC_HD bool refinedRootIn(int kind, Rr qa, Rr qb, const V3<Rr>& o, const V3<Rr>& d, Rr t, Rr tmin, Rr tmax, Rr& tr) {
+OWEC_HD bool refinedRootIn(int kind, Rr qa, Rr qb, const V3<Rr>& o, const V3<Rr>& d, Rr t, Rr tmin, Rr tmax, Rr& tr,
+                           Rr qc = Rr(0)) {
     tr = t;
     const Rr m = Rr(Tol<R>::refine) * (Rr(1) + fabs(t));
     if (t + m <= tmin || t - m >= tmax) return false;
     Rr A, B, C, u0, u1;
-    quadricCoeffs(kind, qa, qb, o + d * t, d, A, B, C);
+    quadricCoeffs(kind, qa, qb, qc, o + d * t, d, A, B, C);
     if (solveQuadratic(A, B, C, u0, u1) != 0) {
         const Rr du = fabs(u0) < fabs(u1) ? u0 : u1;
         if (fabs(du) < m) tr = t + du;
@@ -130,10 +145,121 @@ template <class T> OWEC_HD T conicSlope(T c, T k, T r) {
     return root > T(0) ? c * r / root : (c != T(0) ? T(INFINITY) : T(0));
 }
 
-// Up to two crossings of boundary b's shape by the local ray (o, d) in (tmin, tmax), ascending,
-// each inside the shape's trim. Returns how many.
+// An even asphere's sag z(r) = conic + sum A_{2m} r^{2m} (m >= 2) and its slope dz/dr
+// (SagSurface::sag, dsag, src/owe/scene/geometry.cpp:90-103). A: A4, A6, ...
+template <class T>
+OWEC_HD T asphereSag(T c, T k, const double* A, int nA, T r) {
+    const T r2 = r * r;
+    T z = conicSag(c, k, r2), rp = r2 * r2;
+    for (int i = 0; i < nA; ++i) { z += T(A[i]) * rp; rp *= r2; }
+    return z;
+}
+template <class T>
+OWEC_HD T asphereSlope(T c, T k, const double* A, int nA, T r) {
+    T s = conicSlope(c, k, r), m = T(4), rp = r * r * r;
+    for (int i = 0; i < nA; ++i) { s += T(A[i]) * m * rp; rp *= r * r; m += T(2); }
+    return s;
+}
+// The unit normal (toward +z) of a sag of slope s at radius r of point p (sagNormal, surfaces.hpp:168).
+template <class T>
+OWEC_HD V3<T> sagNormal(const V3<T>& p, T r, T s) {
+    if (r < Tol<T>::tiny) return V3<T>(0, 0, 1);
+    return normalize(V3<T>(-s * p.x / r, -s * p.y / r, T(1)));
+}
+
+// Clips (ta, tb) to the slab lo <= o + t d <= hi along one axis, and to the infinite cylinder of
+// radius R about z; false when nothing remains (clipSlab, clipCylinder, surfaces.hpp:140-157).
+template <class T>
+OWEC_HD bool clipSlab(T o, T d, T lo, T hi, T& ta, T& tb) {
+    if (fabs(d) < Tol<T>::tiny) return o >= lo && o <= hi && ta < tb;
+    const T s0 = (lo - o) / d, s1 = (hi - o) / d;
+    ta = fmax(ta, fmin(s0, s1));
+    tb = fmin(tb, fmax(s0, s1));
+    return ta < tb;
+}
+template <class T>
+OWEC_HD bool clipCylinder(const V3<T>& o, const V3<T>& d, T R, T& ta, T& tb) {
+    const T a = d.x * d.x + d.y * d.y;
+    if (a < Tol<T>::tiny) return o.x * o.x + o.y * o.y <= R * R && ta < tb;
+    T q0, q1;
+    if (solveQuadratic(a, T(2) * (o.x * d.x + o.y * d.y), o.x * o.x + o.y * o.y - R * R, q0, q1) < 2) return false;
+    ta = fmax(ta, q0);
+    tb = fmin(tb, q1);
+    return ta < tb;
+}
+
+// Bisects a sign change of f in [lo, hi] (f(lo) = flo) to the precision's bracket width
+// (geometry.cpp:50-64).
+template <class T, class F>
+OWEC_HD T bisectRoot(const F& f, T lo, T hi, T flo, int steps) {
+    for (int it = 0; it < steps && hi - lo > T(Tol<T>::bisect) * (T(1) + fabs(hi)); ++it) {
+        const T mid = T(0.5) * (lo + hi);
+        const T fm = f(mid);
+        if ((fm <= T(0)) == (flo <= T(0))) {
+            lo = mid;
+            flo = fm;
+        } else {
+            hi = mid;
+        }
+    }
+    return T(0.5) * (lo + hi);
+}
+
+// Torus patch: F < 0 inside the tube, the arc test and the normal away from the arc's centre
+// (torusF, torusOnArc, torusNormal, surfaces.hpp:209-225).
+template <class T>
+OWEC_HD T torusF(T R, T zc, T rho, const V3<T>& p) {
+    return sqr(sqrt(p.x * p.x + p.y * p.y) - R) + sqr(p.z - zc) - rho * rho;
+}
+template <class T>
+OWEC_HD bool torusOnArc(T R, T zc, T a0, T a1, const V3<T>& p) {
+    const T a = atan2(p.z - zc, sqrt(p.x * p.x + p.y * p.y) - R);
+    for (int k = -1; k <= 1; ++k) {
+        const T w = a + T(k) * T(2 * kPi);
+        if (w >= a0 - T(Tol<T>::angle) && w <= a1 + T(Tol<T>::angle)) return true;
+    }
+    return false;
+}
+template <class T>
+OWEC_HD V3<T> torusNormal(T R, T zc, const V3<T>& p) {
+    const T rho = sqrt(p.x * p.x + p.y * p.y);
+    const V3<T> c = rho > T(0) ? V3<T>(p.x * R / rho, p.y * R / rho, zc) : V3<T>(0, 0, zc);
+    return normalize(p - c);
+}
+
+// Trims: a plane aperture, a round wall's rectangular opening (centred on an azimuth from +y toward
+// +x, `width` along the wall, between sill and top) and a dome's slit of constant linear width
+// (inPlaneAperture, inWallOpening, domeSolid, surfaces.hpp:232-262).
+template <class T>
+OWEC_HD bool inPlaneAperture(int kind, T a, T b, T hx, T hy, const V3<T>& p) {
+    if (kind == OWEC_APERTURE_DISK) {
+        const T r2 = p.x * p.x + p.y * p.y;
+        return r2 <= a * a && r2 >= b * b;
+    }
+    if (kind == OWEC_APERTURE_RECT) return fabs(p.x) <= a && fabs(p.y) <= b;
+    if (kind == OWEC_APERTURE_ELLIPSE) return sqr(p.x / a) + sqr(p.y / b) <= T(1);
+    return p.x * p.x + p.y * p.y <= a * a && sqr(p.x - hx) + sqr(p.y - hy) >= b * b;
+}
+template <class T>
+OWEC_HD bool inWallOpening(T R, T azimuth, T width, T sill, T top, const V3<T>& p) {
+    const T dAz = remainder(atan2(p.x, p.y) - azimuth, T(2 * kPi));
+    return fabs(dAz) * R < width / T(2) && p.z > sill && p.z < top;
+}
+template <class T>
+OWEC_HD bool domeSolid(T R, T azimuth, T width, T top, const V3<T>& p) {
+    if (p.z < T(0)) return false;
+    if (width <= T(0)) return true;
+    const T el = asin(fmin(T(1), fmax(T(-1), p.z / R)));
+    if (el >= top) return true;
+    const T dAz = remainder(atan2(p.x, p.y) - azimuth, T(2 * kPi));
+    return fabs(sin(dAz)) * R * cos(el) >= width / T(2) || cos(dAz) < T(0);
+}
+
+// The crossings of the shapes every scene had before the trimmed, lathe and aspheric ones: spheres,
+// conic sags, disk, rectangle and ellipse apertures and cylinders (the lean traversal's
+// analyticCrossings; see there).
 template <class R, class Rr>
-OWEC_HD int analyticCrossings(const DBoundary& b, const V3<Rr>& o, const V3<Rr>& d, Rr tmin, Rr tmax, AHits<Rr>& out) {
+OWEC_HD int classicCrossings(const DBoundary& b, const V3<Rr>& o, const V3<Rr>& d, Rr tmin, Rr tmax, AHits<Rr>& out) {
     out.n = 0;
     const double* P = b.params;
     switch (b.shape) {
@@ -173,7 +299,7 @@ OWEC_HD int analyticCrossings(const DBoundary& b, const V3<Rr>& o, const V3<Rr>&
                 break;
             }
             R A, B, C, t0, t1;
-            quadricCoeffs(kQuadSag, R(c), R(c * (Rr(1) + k)), V3<R>(o), V3<R>(d), A, B, C);
+            quadricCoeffs(kQuadSag, R(c), R(c * (Rr(1) + k)), R(0), V3<R>(o), V3<R>(d), A, B, C);
             if (solveQuadratic(A, B, C, t0, t1) <= 0) return 0;
             const R ts[2] = {t0, t1};
             for (int i = 0; i < 2; ++i) {
@@ -225,6 +351,245 @@ OWEC_HD int analyticCrossings(const DBoundary& b, const V3<Rr>& o, const V3<Rr>&
     }
     if (out.n == 2 && out.h1.t < out.h0.t) { const AHit<Rr> tmp = out.h0; out.h0 = out.h1; out.h1 = tmp; }
     return out.n;
+}
+
+// Up to two crossings found numerically, ascending. The root finders below are out of line and
+// return by value: they need many registers and run only for the rare aspheres and torus patches,
+// so they must not raise the register count of the traversal that inlines analyticCrossings.
+template <class Rr>
+struct NumericRoots {
+    Rr t[2];
+    int n;
+};
+
+// SagSurface::intersectNumeric (geometry.cpp:138-166): the first sign changes of sag(r) - z over 96
+// samples of the ray clipped to the surface's cylinder and z slab, bisected; up to two, each within
+// the aperture.
+template <class Rr>
+__device__ __noinline__ NumericRoots<Rr> asphereRoots(Rr c, Rr k, Rr rMax, Rr rMin, Rr zMin, Rr zMax, const double* A,
+                                                      int nA, V3<Rr> o, V3<Rr> d, Rr tmin, Rr tmax) {
+    NumericRoots<Rr> r{{Rr(0), Rr(0)}, 0};
+    Rr ta = tmin, tb = tmax;
+    if (!clipCylinder(o, d, rMax, ta, tb) || !clipSlab(o.z, d.z, zMin, zMax, ta, tb)) return r;
+    auto f = [&](Rr t) {
+        const V3<Rr> p = o + d * t;
+        return asphereSag(c, k, A, nA, sqrt(p.x * p.x + p.y * p.y)) - p.z;
+    };
+    constexpr int N = 96;
+    Rr tPrev = ta, fPrev = f(ta);
+    for (int i = 1; i <= N && r.n < 2; ++i) {
+        const Rr tCur = ta + (tb - ta) * Rr(i) / Rr(N);
+        const Rr fCur = f(tCur);
+        if (((fPrev <= Rr(0) && fCur >= Rr(0)) || (fPrev >= Rr(0) && fCur <= Rr(0))) && !(fPrev == Rr(0) && tPrev <= tmin)) {
+            const Rr t = bisectRoot(f, tPrev, tCur, fPrev, Tol<Rr>::bisectSteps);
+            const V3<Rr> p = o + d * t;
+            const Rr r2 = p.x * p.x + p.y * p.y;
+            if (t > tmin && t < tmax && r2 <= rMax * rMax && r2 >= rMin * rMin) r.t[r.n++] = t;
+        }
+        tPrev = tCur;
+        fPrev = fCur;
+    }
+    return r;
+}
+
+// TorusPatchShape::intersect (geometry.cpp:581-618): the ray clipped to the patch's slab and
+// cylinder, F sampled at 64 steps for sign changes and bisected; a ray leaving the patch starts
+// with geometrically growing steps so that its own root and a nearby grazing one fall in different
+// brackets. Up to two crossings on the arc a0..a1.
+template <class Rr>
+__device__ __noinline__ NumericRoots<Rr> torusRoots(Rr R0, Rr zc, Rr rho, Rr a0, Rr a1, Rr rMax, Rr zMin, Rr zMax, V3<Rr> o,
+                                                    V3<Rr> d, Rr tmin, Rr tmax, bool departed) {
+    NumericRoots<Rr> r{{Rr(0), Rr(0)}, 0};
+    Rr ta = tmin, tb = tmax;
+    const Rr pad = Rr(1e-9) * (Rr(1) + rMax + fabs(zMax));
+    if (!clipSlab(o.z, d.z, zMin - pad, zMax + pad, ta, tb) || !clipCylinder(o, d, rMax + pad, ta, tb)) return r;
+    auto F = [&](Rr t) { return torusF(R0, zc, rho, o + d * t); };
+    constexpr int N = 64;
+    Rr tPrev = ta, fPrev = F(ta);
+    int sample = 1;
+    Rr firstStep = !departed ? tb - ta
+                             : fmin((tb - ta) / Rr(N), fmax(ldexp((tb - ta) / Rr(N), -60),
+                                                            Rr(64) * Rr(Tol<Rr>::eps) * (Rr(1) + fabs(ta))));
+    for (int guard = 0; sample <= N && guard < N + 64 && r.n < 2; ++guard) {
+        const Rr uniform = ta + (tb - ta) * Rr(sample) / Rr(N);
+        const Rr tCur = fmin(uniform, ta + firstStep);
+        if (tCur == uniform) ++sample;
+        else firstStep = fmin(tb - ta, firstStep * Rr(2));
+        const Rr fCur = F(tCur);
+        if ((fPrev <= Rr(0)) != (fCur <= Rr(0)) || fCur == Rr(0)) {
+            const Rr t = bisectRoot(F, tPrev, tCur, fPrev, 100);
+            if (t > tmin && t < tmax && torusOnArc(R0, zc, a0, a1, o + d * t)) r.t[r.n++] = t;
+        }
+        tPrev = tCur;
+        fPrev = fCur;
+    }
+    return r;
+}
+
+// The quadric crossings of a shape: roots t0 <= t1 in precision R, each refined in precision Rr and
+// kept when it lies in (tmin, tmax) and solid(p) accepts it (firstRefinedHit, geometry.cpp:32-48,
+// for both roots).
+template <class R, class Rr, bool SkipDouble = false, class Solid, class Normal>
+OWEC_HD void quadricHits(int kind, Rr qa, Rr qb, Rr qc, const V3<Rr>& o, const V3<Rr>& d, R t0, R t1, Rr tmin, Rr tmax,
+                         const Solid& solid, const Normal& normal, AHits<Rr>& out) {
+    const R ts[2] = {t0, t1};
+    for (int i = 0; i < 2; ++i) {
+        if (SkipDouble && i == 1 && t1 == t0) break;  // a sag's double root counts once
+        Rr tr;
+        if (!refinedRootIn<R, Rr>(kind, qa, qb, o, d, Rr(ts[i]), tmin, tmax, tr, qc)) continue;
+        const V3<Rr> p = o + d * tr;
+        if (!solid(p)) continue;
+        out.add({tr, p, normal(p)});
+    }
+}
+
+// The crossings of every shape (analyticCrossings with Full).
+template <class R, class Rr>
+OWEC_HD int fullCrossings(const DBoundary& b, const double* data, const V3<Rr>& o, const V3<Rr>& d, Rr tmin, Rr tmax,
+                          bool departed, AHits<Rr>& out) {
+    out.n = 0;
+    const double* P = b.params;
+    switch (b.shape) {
+        case OWEC_SHAPE_SPHERE: {
+            const Rr Rad = Rr(P[0]);
+            R t0, t1;
+            if (!sphereRoots(V3<R>(o), V3<R>(d), R(P[0]), t0, t1)) return 0;
+            quadricHits<R, Rr>(kQuadSphere, Rad * Rad, Rr(0), Rr(0), o, d, t0, t1, tmin, tmax,
+                               [](const V3<Rr>&) { return true; }, [&](const V3<Rr>& p) { return normalize(p / Rad); },
+                               out);
+            break;
+        }
+        case OWEC_SHAPE_DOME: {
+            const Rr Rad = Rr(P[0]), az = Rr(P[1]), w = Rr(P[2]), top = Rr(P[3]);
+            R t0, t1;
+            if (!sphereRoots(V3<R>(o), V3<R>(d), R(P[0]), t0, t1)) return 0;
+            quadricHits<R, Rr>(kQuadSphere, Rad * Rad, Rr(0), Rr(0), o, d, t0, t1, tmin, tmax,
+                               [&](const V3<Rr>& p) { return domeSolid(Rad, az, w, top, p); },
+                               [](const V3<Rr>& p) { return normalize(p); }, out);
+            break;
+        }
+        case OWEC_SHAPE_SAG: {
+            const Rr c = Rr(P[0]), k = Rr(P[1]), rMax = Rr(P[2]), rMin = Rr(P[3]);
+            const int nA = int(b.dataCount);
+            auto accept = [&](const V3<Rr>& p) {
+                const Rr r2 = p.x * p.x + p.y * p.y;
+                return r2 <= rMax * rMax && r2 >= rMin * rMin;
+            };
+            auto normal = [&](const V3<Rr>& p) {
+                const Rr r = sqrt(p.x * p.x + p.y * p.y);
+                return sagNormal(p, r, nA ? asphereSlope(c, k, data, nA, r) : conicSlope(c, k, r));
+            };
+            if (nA > 0) {
+                const NumericRoots<Rr> r = asphereRoots<Rr>(c, k, rMax, rMin, Rr(b.ext[0]), Rr(b.ext[1]), data, nA, o, d, tmin, tmax);
+                for (int i = 0; i < r.n; ++i) {
+                    const V3<Rr> p = o + d * r.t[i];
+                    out.add({r.t[i], p, normal(p)});
+                }
+                break;
+            }
+            auto solid = [&](const V3<Rr>& p) {
+                return accept(p) && (c == Rr(0) || (Rr(1) + k) * c * p.z <= Rr(1) + Rr(Tol<R>::relTol));
+            };
+            if (c == Rr(0)) {
+                if (d.z == Rr(0)) return 0;
+                const Rr t = -o.z / d.z;
+                if (t <= tmin || t >= tmax) return 0;
+                const V3<Rr> p = o + d * t;
+                if (!solid(p)) return 0;
+                out.add({t, p, normal(p)});
+                break;
+            }
+            R A, B, C, t0, t1;
+            quadricCoeffs(kQuadSag, R(c), R(c * (Rr(1) + k)), R(0), V3<R>(o), V3<R>(d), A, B, C);
+            if (solveQuadratic(A, B, C, t0, t1) <= 0) return 0;
+            quadricHits<R, Rr, true>(kQuadSag, c, c * (Rr(1) + k), Rr(0), o, d, t0, t1, tmin, tmax, solid, normal, out);
+            break;
+        }
+        case OWEC_SHAPE_PLANE: {
+            if (d.z == Rr(0)) return 0;
+            const Rr t = -o.z / d.z;
+            if (t <= tmin || t >= tmax) return 0;
+            V3<Rr> p = o + d * t;
+            p.z = Rr(0);
+            const int ap = int(P[0]);
+            const bool hole = ap == OWEC_APERTURE_DISK_HOLE && b.dataCount >= 2;
+            if (!inPlaneAperture(ap, Rr(P[1]), Rr(P[2]), hole ? Rr(data[0]) : Rr(0), hole ? Rr(data[1]) : Rr(0), p))
+                return 0;
+            out.add({t, p, V3<Rr>(0, 0, 1)});
+            break;
+        }
+        case OWEC_SHAPE_CYLINDER:
+        case OWEC_SHAPE_ROUND_WALL: {
+            const bool wall = b.shape == OWEC_SHAPE_ROUND_WALL;
+            const Rr Rad = Rr(P[0]), z0 = wall ? Rr(0) : Rr(P[1]), z1 = wall ? Rr(P[1]) : Rr(P[2]);
+            const int openings = wall ? int(b.dataCount / 4) : 0;
+            R t0, t1;
+            if (!cylinderRoots(V3<R>(o), V3<R>(d), R(P[0]), t0, t1)) return 0;
+            auto solid = [&](const V3<Rr>& p) {
+                if (p.z < z0 || p.z > z1) return false;
+                for (int i = 0; i < openings; ++i)
+                    if (inWallOpening(Rad, Rr(data[4 * i]), Rr(data[4 * i + 1]), Rr(data[4 * i + 2]), Rr(data[4 * i + 3]), p))
+                        return false;
+                return true;
+            };
+            quadricHits<R, Rr>(kQuadCylinder, Rad * Rad, Rr(0), Rr(0), o, d, t0, t1, tmin, tmax, solid,
+                               [](const V3<Rr>& p) { return normalize(V3<Rr>(p.x, p.y, Rr(0))); }, out);
+            break;
+        }
+        case OWEC_SHAPE_CONE: {
+            // x^2 + y^2 = (r0 + k (z - z0))^2 on the nappe where r0 + k (z - z0) >= 0 (ConeShape,
+            // geometry.cpp:519-538), z0 < z1 after ordering the ends
+            const bool swap = P[1] > P[3];
+            const Rr r0 = Rr(swap ? P[2] : P[0]), z0 = Rr(swap ? P[3] : P[1]);
+            const Rr r1 = Rr(swap ? P[0] : P[2]), z1 = Rr(swap ? P[1] : P[3]);
+            const Rr k = (r1 - r0) / (z1 - z0);
+            R A, B, C, t0, t1;
+            quadricCoeffs(kQuadCone, R(r0), R(z0), R(k), V3<R>(o), V3<R>(d), A, B, C);
+            if (solveQuadratic(A, B, C, t0, t1) <= 0) return 0;
+            quadricHits<R, Rr>(kQuadCone, r0, z0, k, o, d, t0, t1, tmin, tmax,
+                               [&](const V3<Rr>& p) { return p.z >= z0 && p.z <= z1 && r0 + k * (p.z - z0) >= Rr(0); },
+                               [&](const V3<Rr>& p) { return normalize(V3<Rr>(p.x, p.y, -(r0 + k * (p.z - z0)) * k)); },
+                               out);
+            break;
+        }
+        case OWEC_SHAPE_TORUS: {
+            const NumericRoots<Rr> r = torusRoots<Rr>(Rr(P[0]), Rr(P[1]), Rr(P[2]), Rr(P[3]), Rr(b.ext[3]), Rr(b.ext[0]),
+                                                      Rr(b.ext[1]), Rr(b.ext[2]), o, d, tmin, tmax, departed);
+            for (int i = 0; i < r.n; ++i) {
+                const V3<Rr> p = o + d * r.t[i];
+                out.add({r.t[i], p, torusNormal(Rr(P[0]), Rr(P[1]), p)});
+            }
+            break;
+        }
+        default: break;
+    }
+    if (out.n == 2 && out.h1.t < out.h0.t) { const AHit<Rr> tmp = out.h0; out.h0 = out.h1; out.h1 = tmp; }
+    return out.n;
+}
+
+// Up to two crossings of boundary b's shape by the local ray (o, d) in (tmin, tmax), ascending,
+// each inside the shape's trim. data: the shape's run of the scene's shape data. departed: the ray
+// leaves this boundary (a torus patch then resolves the start of its bracket finely). Returns how
+// many. Full = false compiles only the spheres, conic sags, plain apertures and cylinders: the
+// kernels of a scene without the other shapes keep the registers they need for those alone.
+template <class R, class Rr, bool Full>
+OWEC_HD int analyticCrossings(const DBoundary& b, const double* data, const V3<Rr>& o, const V3<Rr>& d, Rr tmin, Rr tmax,
+                              bool departed, AHits<Rr>& out) {
+    if constexpr (Full) return fullCrossings<R, Rr>(b, data, o, d, tmin, tmax, departed, out);
+    else return classicCrossings<R, Rr>(b, o, d, tmin, tmax, out);
+}
+
+// The unit normal of a shape found by a numeric crossing (aspheres, torus patches) at local point p.
+template <class Rr>
+OWEC_HD V3<Rr> numericNormal(const DBoundary& b, const double* data, const V3<Rr>& p) {
+    const double* P = b.params;
+    if (b.shape == OWEC_SHAPE_TORUS) return torusNormal(Rr(P[0]), Rr(P[1]), p);
+    const Rr r = sqrt(p.x * p.x + p.y * p.y);
+    return sagNormal(p, r, asphereSlope(Rr(P[0]), Rr(P[1]), data, int(b.dataCount), r));
+}
+// Whether boundary b's crossings are found numerically (no closed form).
+OWEC_HD bool numericShape(const DBoundary& b) {
+    return b.shape == OWEC_SHAPE_TORUS || (b.shape == OWEC_SHAPE_SAG && b.dataCount > 0);
 }
 
 // Watertight line-triangle crossing test (Woop, Benthin and Wald 2013), edges included, as the

@@ -70,7 +70,9 @@ __device__ __forceinline__ double refineTriangleT(const DeviceScene& sc, uint32_
     return (t > 0 && fabs(t - t32) <= 1e-3 * (1 + fabs(t32))) ? t : t32;
 }
 
-template <class R, class Ro, class Rr>
+// Full: the scene may hold shapes beyond spheres, conic sags, plain apertures and cylinders
+// (analyticCrossings).
+template <class R, class Ro, class Rr, bool Full>
 __device__ SurfacePoint<R> hitGeometry(const DeviceScene& sc, const PathRay<R>& ray, const HitRec& h) {
     SurfacePoint<R> sp;
     const DBoundary& bd = sc.boundaries[h.boundary];
@@ -99,10 +101,20 @@ __device__ SurfacePoint<R> hitGeometry(const DeviceScene& sc, const PathRay<R>& 
     }
     const V3<Rr> lo = bd.toLocal.point(V3<Rr>(od));
     const V3<Rr> ld = bd.toLocal.vector(V3<Rr>(d));
-    AHits<Rr> hits;
     const Rr t = Rr(h.t);
+    const double* data = Full ? sc.shapeData + bd.dataOffset : nullptr;
+    if (Full && numericShape(bd)) {
+        // a bisected crossing is already as precise as its arithmetic: the point on the ray
+        const V3<Rr> pl = lo + ld * t;
+        sp.pLocal = V3<double>(pl);
+        sp.nLocal = V3<double>(numericNormal(bd, data, pl));
+        sp.p = bd.toWorld.point(sp.pLocal);
+        sp.n = V3<R>(normalize(bd.toWorld.vector(sp.nLocal)));
+        return sp;
+    }
+    AHits<Rr> hits;
     const Rr slack = Rr(1e-6) * (Rr(1) + fabs(t));
-    const int n = analyticCrossings<Ro, Rr>(bd, lo, ld, Rr(0), t + slack, hits);
+    const int n = analyticCrossings<Ro, Rr, Full>(bd, data, lo, ld, Rr(0), t + slack, ray.depB == h.boundary, hits);
     const AHit<Rr>& hb = (n == 2 && fabs(hits.h1.t - t) < fabs(hits.h0.t - t)) ? hits.h1 : hits.h0;
     if (n == 0) {  // not found again (rounding at a trim edge): the point on the ray
         sp.p = od + V3<double>(d) * h.t;

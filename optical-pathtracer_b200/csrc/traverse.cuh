@@ -91,13 +91,15 @@ template <> __device__ __forceinline__ float farWiden<float>() { return 4e-7f; }
 template <> __device__ __forceinline__ double farWiden<double>() { return 4e-16; }
 
 // The analytic boundary b's first acceptable crossing in (0, best); FP64 refinement when Rr = double.
-template <class R, class Rr, class T>
+template <class R, class Rr, class T, bool Full>
 __device__ __forceinline__ bool analyticCandidate(const DeviceScene& sc, const RayQuery<T>& q, uint32_t b, T best, Rr& tOut) {
     const DBoundary& bd = sc.boundaries[b];
     const V3<Rr> lo = bd.toLocal.point(V3<Rr>(q.od));
     const V3<Rr> ld = bd.toLocal.vector(V3<Rr>(q.d));
     AHits<Rr> hits;
-    const int n = analyticCrossings<R, Rr>(bd, lo, ld, Rr(0), Rr(best), hits);
+    int n;
+    if constexpr (Full) n = analyticCrossings<R, Rr, true>(bd, sc.shapeData + bd.dataOffset, lo, ld, Rr(0), Rr(best), b == q.depB, hits);
+    else n = analyticCrossings<R, Rr, false>(bd, nullptr, lo, ld, Rr(0), Rr(best), false, hits);
     // Leaving this boundary, the anchor lies on it to the precision of the refinement, not of FP32:
     // with the FP32 window a grazing ray's far crossing of the same sphere (at t = 2 R cos) fell
     // inside it and was rejected as the departure, and the path leaked.
@@ -123,7 +125,7 @@ struct AnalyticResult {
     Rr t;
     bool ok;
 };
-template <class T, class R, class Rr>
+template <class T, class R, class Rr, bool Full>
 __device__ __noinline__ AnalyticResult<Rr> analyticHit(const DeviceScene& sc, uint32_t b, V3<double> od, V3<T> d, T best,
                                                         uint32_t depB, uint32_t region, T errN) {
     RayQuery<T> q;
@@ -137,7 +139,7 @@ __device__ __noinline__ AnalyticResult<Rr> analyticHit(const DeviceScene& sc, ui
     q.errN = errN;
     AnalyticResult<Rr> r;
     r.t = Rr(0);
-    r.ok = analyticCandidate<R, Rr, T>(sc, q, b, best, r.t);
+    r.ok = analyticCandidate<R, Rr, T, Full>(sc, q, b, best, r.t);
     return r;
 }
 
@@ -285,7 +287,9 @@ __device__ __forceinline__ uint32_t permuteSlots(uint32_t m, uint32_t x) {
 // machine that a persistent kernel can advance a few visits at a time and then hand the thread a
 // new query when this one ends. R / Rr: precision of analytic roots and of their refinement.
 // Count: keep the per-query visit and test counts (the counting pass; the timed kernels leave them out).
-template <class T, class R, class Rr, bool AnyHit, class Stack = SharedStack, bool Count = true>
+// Full: the scene has shapes beyond spheres, conic sags, plain apertures and cylinders
+// (analyticCrossings).
+template <class T, class R, class Rr, bool AnyHit, class Stack = SharedStack, bool Count = true, bool Full = false>
 struct Traversal {
     RayQuery<T> q;
     V3<T> inv, oinv;
@@ -386,7 +390,7 @@ struct Traversal {
             hit.t = double(t);
             hit.prim = prim;
         } else {
-            const AnalyticResult<Rr> ar = analyticHit<T, R, Rr>(sc, b, q.od, q.d, best, q.depB, q.region, q.errN);
+            const AnalyticResult<Rr> ar = analyticHit<T, R, Rr, Full>(sc, b, q.od, q.d, best, q.depB, q.region, q.errN);
             if (!ar.ok) return false;
             best = T(ar.t);
             hit.t = double(ar.t);
@@ -407,9 +411,9 @@ struct DeepResult {
     int status;
     uint32_t visits, tests;
 };
-template <class T, class R, class Rr, bool AnyHit>
+template <class T, class R, class Rr, bool AnyHit, bool Full = false>
 __device__ __noinline__ DeepResult traceRayDeep(const DeviceScene& sc, RayQuery<T> q, HitRec hitIn) {
-    Traversal<T, R, Rr, AnyHit, LocalStack> tr;
+    Traversal<T, R, Rr, AnyHit, LocalStack, true, Full> tr;
     tr.begin(q, nullptr, 0);
     tr.hit = hitIn;
     int s;
@@ -425,10 +429,10 @@ __device__ __noinline__ DeepResult traceRayDeep(const DeviceScene& sc, RayQuery<
 }
 
 // The whole query in one call (cast rays, forward walks and the adjoint's replay).
-template <class T, class R, class Rr, bool AnyHit>
+template <class T, class R, class Rr, bool AnyHit, bool Full = false>
 __device__ __forceinline__ int traceRay(const DeviceScene& sc, const RayQuery<T>& q, StackEntry* stack, int stride, HitRec& hit,
                                         uint32_t* visits = nullptr, uint32_t* tests = nullptr) {
-    Traversal<T, R, Rr, AnyHit> tr;
+    Traversal<T, R, Rr, AnyHit, SharedStack, true, Full> tr;
     tr.begin(q, stack, stride);
     tr.hit = hit;
     int s;
@@ -437,7 +441,7 @@ __device__ __forceinline__ int traceRay(const DeviceScene& sc, const RayQuery<T>
     } while (s == kTraceRunning);
     uint32_t nv = tr.nodeVisits, nt = tr.primTests;
     if (s == kTraceOverflow) {
-        const DeepResult d = traceRayDeep<T, R, Rr, AnyHit>(sc, q, hit);
+        const DeepResult d = traceRayDeep<T, R, Rr, AnyHit, Full>(sc, q, hit);
         s = d.status;
         hit = d.hit;
         nv += d.visits;

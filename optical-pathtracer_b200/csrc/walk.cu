@@ -94,7 +94,7 @@ __device__ void fresnelWithDerivative(double c, double eta, double& R, double& d
     dRdc = sgn * (rp * drp + rs * drs);
 }
 
-template <int M, bool ADJ>
+template <int M, bool ADJ, bool Full>
 __device__ void walkOne(const DeviceScene& sc, const WalkParams& P, uint64_t walkIndex, StackEntry* stack, int stride,
                         unsigned long long* bins, unsigned long long* stats, const double* g, double* dH) {
     using R = typename Mode<M>::R;
@@ -154,12 +154,12 @@ __device__ void walkOne(const DeviceScene& sc, const WalkParams& P, uint64_t wal
         rq.region = ray.region;
         rq.errN = R(ray.errN);
         HitRec h;
-        const int s = traceRay<R, Ro, Rr, false>(sc, rq, stack, stride, h);
+        const int s = traceRay<R, Ro, Rr, false, Full>(sc, rq, stack, stride, h);
         if (s == kTraceOverflow) { fault = true; break; }
         if (s != kTraceHit) { escaped = true; break; }
         const owec_medium med = sc.media[sc.regionMedium[ray.region]];
         const DBoundary bd = sc.boundaries[h.boundary];
-        const SurfacePoint<R> gp = hitGeometry<R, Ro, Rr>(sc, ray, h);
+        const SurfacePoint<R> gp = hitGeometry<R, Ro, Rr, Full>(sc, ray, h);
         const V3<R> d(ray.d[0], ray.d[1], ray.d[2]);
         const R betaBefore = beta;
         R atten = R(1);
@@ -349,13 +349,22 @@ __device__ void walkOne(const DeviceScene& sc, const WalkParams& P, uint64_t wal
     }
 }
 
-template <int M, bool ADJ>
+template <int M, bool ADJ, bool Full>
 __global__ void __launch_bounds__(128) kWalk(DeviceScene sc, WalkParams P, unsigned long long* bins,
                                              unsigned long long* stats, const double* g, double* dH) {
     extern __shared__ StackEntry stackMem[];
     StackEntry* stack = stackMem + threadIdx.x;
     for (uint64_t k = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; k < P.n; k += uint64_t(gridDim.x) * blockDim.x)
-        walkOne<M, ADJ>(sc, P, P.first + k, stack, blockDim.x, bins, stats, g, dH);
+        walkOne<M, ADJ, Full>(sc, P, P.first + k, stack, blockDim.x, bins, stats, g, dH);
+}
+
+// kWalk for the scene's shapes (the lean traversal unless the scene needs the full set).
+template <int M, bool ADJ>
+void walkKernel(const DeviceScene& sc, const WalkParams& P, unsigned long long* bins, unsigned long long* stats,
+                const double* g, double* dH, int grid, cudaStream_t s) {
+    const size_t smem = traversalSharedBytes(128);
+    if (sc.fullShapes) kWalk<M, ADJ, true><<<grid, 128, smem, s>>>(sc, P, bins, stats, g, dH);
+    else kWalk<M, ADJ, false><<<grid, 128, smem, s>>>(sc, P, bins, stats, g, dH);
 }
 
 WalkParams makeParams(const owec_walk_desc& w, const Xform& targetToLocal, uint64_t first, uint64_t n, double scale,
@@ -384,20 +393,18 @@ void launchWalk(int mode, const DeviceScene& sc, const owec_walk_desc& w, const 
     HeightfieldParams hf{};
     hf.boundary = kNone;
     const WalkParams P = makeParams(w, targetToLocal, first, n, 1.0, hf);
-    const size_t smem = traversalSharedBytes(128);
-    if (mode == OWEC_PRECISION_FP64) kWalk<OWEC_PRECISION_FP64, false><<<grid, 128, smem, s>>>(sc, P, bins, stats, nullptr, nullptr);
-    else if (mode == OWEC_PRECISION_FP32) kWalk<OWEC_PRECISION_FP32, false><<<grid, 128, smem, s>>>(sc, P, bins, stats, nullptr, nullptr);
-    else kWalk<OWEC_PRECISION_MIXED, false><<<grid, 128, smem, s>>>(sc, P, bins, stats, nullptr, nullptr);
+    if (mode == OWEC_PRECISION_FP64) walkKernel<OWEC_PRECISION_FP64, false>(sc, P, bins, stats, nullptr, nullptr, grid, s);
+    else if (mode == OWEC_PRECISION_FP32) walkKernel<OWEC_PRECISION_FP32, false>(sc, P, bins, stats, nullptr, nullptr, grid, s);
+    else walkKernel<OWEC_PRECISION_MIXED, false>(sc, P, bins, stats, nullptr, nullptr, grid, s);
 }
 
 void launchWalkAdjoint(int mode, const DeviceScene& sc, const owec_walk_desc& w, const Xform& targetToLocal,
                        const HeightfieldParams& hf, uint64_t first, uint64_t n, double scale, const double* g,
                        double* dH, unsigned long long* stats, int grid, cudaStream_t s) {
     const WalkParams P = makeParams(w, targetToLocal, first, n, scale, hf);
-    const size_t smem = traversalSharedBytes(128);
-    if (mode == OWEC_PRECISION_FP64) kWalk<OWEC_PRECISION_FP64, true><<<grid, 128, smem, s>>>(sc, P, nullptr, stats, g, dH);
-    else if (mode == OWEC_PRECISION_FP32) kWalk<OWEC_PRECISION_FP32, true><<<grid, 128, smem, s>>>(sc, P, nullptr, stats, g, dH);
-    else kWalk<OWEC_PRECISION_MIXED, true><<<grid, 128, smem, s>>>(sc, P, nullptr, stats, g, dH);
+    if (mode == OWEC_PRECISION_FP64) walkKernel<OWEC_PRECISION_FP64, true>(sc, P, nullptr, stats, g, dH, grid, s);
+    else if (mode == OWEC_PRECISION_FP32) walkKernel<OWEC_PRECISION_FP32, true>(sc, P, nullptr, stats, g, dH, grid, s);
+    else walkKernel<OWEC_PRECISION_MIXED, true>(sc, P, nullptr, stats, g, dH, grid, s);
 }
 
 }  // namespace owec

@@ -206,14 +206,14 @@ __device__ __forceinline__ void warpFlush(unsigned long long* counter, uint32_t 
 // Closest crossing of every active path's ray. Persistent: each lane advances its query a few
 // visits at a time and, when it ends, takes the next query of the queue, so that lanes whose rays
 // finish early do not idle until the warp's longest ray is done.
-template <int M, bool Count>
+template <int M, bool Count, bool Full>
 __global__ void OWEC_TRAVERSAL_BOUNDS kIntersect(DeviceScene sc, PathBuffers<RT<M>> pb, Queues q, int cur,
                                                   StatCounters* st, uint32_t* fetch) {
     using R = RT<M>;
     extern __shared__ StackEntry stackMem[];
     StackEntry* stack = stackMem + threadIdx.x;
     const uint32_t n = q.counts[cur];
-    Traversal<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false, SharedStack, Count> tr;
+    Traversal<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false, SharedStack, Count, Full> tr;
     uint32_t path = 0, segments = 0, faults = 0;
     bool alive = false, exhausted = false;
     for (;;) {
@@ -242,7 +242,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kIntersect(DeviceScene sc, PathBuffers<RT<
                 if (s == kTraceOverflow) {
                     h.boundary = kNone;
                     h.t = INFINITY;
-                    const DeepResult d = traceRayDeep<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false>(sc, tr.q, h);
+                    const DeepResult d = traceRayDeep<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false, Full>(sc, tr.q, h);
                     s = d.status;
                     h = d.hit;
                     nv += d.visits;
@@ -457,7 +457,7 @@ __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kMedium(DeviceSc
 #ifndef OWEC_SIMPLE_MIN_BLOCKS
 #define OWEC_SIMPLE_MIN_BLOCKS 4
 #endif
-template <int M, bool Simple>
+template <int M, bool Simple, bool Full>
 __global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SHADING_MIN_BLOCKS) kSurface(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
                                                 int cur, StatCounters* st) {
     using R = RT<M>;
@@ -474,7 +474,7 @@ __global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SH
         const HitRec h = pb.hit[i];
         Pcg32 rng{aux.rngState, (uint64_t(aux.stream) << 1u) | 1u};
         const DBoundary& bd = sc.boundaries[h.boundary];
-        const SurfacePoint<R> g = hitGeometry<R, Ro, Rr>(sc, ray, h);
+        const SurfacePoint<R> g = hitGeometry<R, Ro, Rr, Full>(sc, ray, h);
         const V3<R> d = rayDir(ray);
         // meetBoundary (transport.cpp:121-133)
         const bool fromFront = dot(d, g.n) < R(0);
@@ -610,7 +610,7 @@ __global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SH
 // null boundaries; its traversal advances a few visits per round and a finished lane takes the
 // next job. Splat: the rays are the light integrator's connections to the eye, whose
 // contributions land in the film's pixels instead of the paths' radiance.
-template <int M, bool AnyHit, bool Count, bool Splat = false>
+template <int M, bool AnyHit, bool Count, bool Splat, bool Full>
 __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
                                                StatCounters* st, uint32_t* fetch, SplatTarget film) {
     using R = RT<M>;
@@ -619,7 +619,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
     extern __shared__ StackEntry stackMem[];
     StackEntry* stack = stackMem + threadIdx.x;
     const uint32_t n = q.counts[3];
-    Traversal<R, Ro, Rr, AnyHit, SharedStack, Count> tr;
+    Traversal<R, Ro, Rr, AnyHit, SharedStack, Count, Full> tr;
     R Tr[NW];
     double remaining = 0;
     uint32_t job = 0, path = 0, region = 0, guard = 0, rays = 0, faults = 0;
@@ -658,7 +658,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
             uint32_t nv = tr.nodeVisits, nt = tr.primTests;
             if (s == kTraceOverflow) {
                 h.boundary = kNone;
-                const DeepResult d = traceRayDeep<R, Ro, Rr, AnyHit>(sc, tr.q, h);
+                const DeepResult d = traceRayDeep<R, Ro, Rr, AnyHit, Full>(sc, tr.q, h);
                 s = d.status;
                 h = d.hit;
                 nv += d.visits;
@@ -697,7 +697,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
                             PathRay<R> tmp;
                             tmp.o[0] = tr.q.od.x; tmp.o[1] = tr.q.od.y; tmp.o[2] = tr.q.od.z;
                             tmp.d[0] = tr.q.d.x; tmp.d[1] = tr.q.d.y; tmp.d[2] = tr.q.d.z;
-                            const SurfacePoint<R> gp = hitGeometry<R, Ro, Rr>(sc, tmp, h);
+                            const SurfacePoint<R> gp = hitGeometry<R, Ro, Rr, Full>(sc, tmp, h);
                             const bool ff = dot(tr.q.d, gp.n) < R(0);
                             if ((ff ? bd.front : bd.back) != region) {
                                 outcome = 2;
@@ -753,7 +753,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
 // runs the queries alone, persistent like kIntersect, and records one visibility byte per shadow ray
 // (0 blocked, 1 clear, 2 fault); kShadowApply then adds the contributions in one coalesced pass,
 // so the bookkeeping does not run divergently inside the traversal loop.
-template <int M, bool Count>
+template <int M, bool Count, bool Full>
 __global__ void OWEC_TRAVERSAL_BOUNDS kShadowVis(DeviceScene sc, PathBuffers<RT<M>> pb, Queues q, uint8_t* vis,
                                                   uint32_t* fetch) {
     using R = RT<M>;
@@ -762,7 +762,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadowVis(DeviceScene sc, PathBuffers<RT<
     extern __shared__ StackEntry stackMem[];
     StackEntry* stack = stackMem + threadIdx.x;
     const uint32_t n = q.counts[3];
-    Traversal<R, Ro, Rr, true, SharedStack, Count> tr;
+    Traversal<R, Ro, Rr, true, SharedStack, Count, Full> tr;
     uint32_t job = 0;
     bool alive = false, exhausted = false;
     for (;;) {
@@ -798,7 +798,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadowVis(DeviceScene sc, PathBuffers<RT<
         if (s == kTraceOverflow) {
             HitRec h = tr.hit;
             h.boundary = kNone;
-            const DeepResult d = traceRayDeep<R, Ro, Rr, true>(sc, tr.q, h);
+            const DeepResult d = traceRayDeep<R, Ro, Rr, true, Full>(sc, tr.q, h);
             s = d.status;
             nv += d.visits;
             nt += d.tests;
@@ -891,7 +891,7 @@ __global__ void __launch_bounds__(256) kFilm(DeviceScene sc, PassParams pp, Path
 }
 
 // ------------------------------------------------------------------ ray casts
-template <int M>
+template <int M, bool Full>
 __global__ void __launch_bounds__(128) kCastRays(DeviceScene sc, uint64_t n, const double* o, const double* d,
                                                  uint32_t* boundary, uint32_t* prim, double* t) {
     using R = RT<M>;
@@ -908,7 +908,7 @@ __global__ void __launch_bounds__(128) kCastRays(DeviceScene sc, uint64_t n, con
         rq.region = kNone;
         rq.errN = R(0);
         HitRec h;
-        const int s = traceRay<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false>(sc, rq, stack, blockDim.x, h);
+        const int s = traceRay<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false, Full>(sc, rq, stack, blockDim.x, h);
         if (s == kTraceHit) {
             boundary[i] = h.boundary;
             prim[i] = h.prim;
@@ -923,6 +923,7 @@ __global__ void __launch_bounds__(128) kCastRays(DeviceScene sc, uint64_t n, con
 }
 
 // Device-resident FP32 camera-relative rays (the benchmark's ray-cast workload).
+template <bool Full>
 __global__ void __launch_bounds__(128) kCastRaysF(DeviceScene sc, uint64_t n, const float* o, const float* d,
                                                   uint32_t* boundary, uint32_t* prim, float* t) {
     extern __shared__ StackEntry stackMem[];
@@ -937,7 +938,7 @@ __global__ void __launch_bounds__(128) kCastRaysF(DeviceScene sc, uint64_t n, co
         rq.region = kNone;
         rq.errN = 0.f;
         HitRec h;
-        const int s = traceRay<float, float, double, false>(sc, rq, stack, blockDim.x, h);
+        const int s = traceRay<float, float, double, false, Full>(sc, rq, stack, blockDim.x, h);
         boundary[i] = s == kTraceHit ? h.boundary : (s == kTraceOverflow ? kNone - 1u : kNone);
         prim[i] = s == kTraceHit ? h.prim : 0u;
         t[i] = s == kTraceHit ? float(h.t) : INFINITY;
@@ -993,10 +994,14 @@ void launchGenerate(const DeviceScene& sc, const PassParams& pp, const PathBuffe
 template <int M>
 void launchIntersect(const DeviceScene& sc, const PathBuffers<RT<M>>& pb, const Queues& q, int cur, StatCounters* st,
                      uint32_t* fetch, int grid, cudaStream_t s) {
-    if (sc.travCounters)
-        kIntersect<M, true><<<grid, 128, traversalSharedBytes(128), s>>>(sc, pb, q, cur, st, fetch);
-    else
-        kIntersect<M, false><<<grid, 128, traversalSharedBytes(128), s>>>(sc, pb, q, cur, st, fetch);
+    const size_t smem = traversalSharedBytes(128);
+    if (sc.fullShapes) {
+        if (sc.travCounters) kIntersect<M, true, true><<<grid, 128, smem, s>>>(sc, pb, q, cur, st, fetch);
+        else kIntersect<M, false, true><<<grid, 128, smem, s>>>(sc, pb, q, cur, st, fetch);
+    } else {
+        if (sc.travCounters) kIntersect<M, true, false><<<grid, 128, smem, s>>>(sc, pb, q, cur, st, fetch);
+        else kIntersect<M, false, false><<<grid, 128, smem, s>>>(sc, pb, q, cur, st, fetch);
+    }
 }
 template <int M>
 void launchMedium(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q, int cur,
@@ -1006,34 +1011,48 @@ void launchMedium(const DeviceScene& sc, const PassParams& pp, const PathBuffers
 template <int M>
 void launchSurface(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q, int cur,
                    StatCounters* st, int grid, cudaStream_t s) {
-    kSurface<M, true><<<grid, 128, 0, s>>>(sc, pp, pb, q, cur, st);
-    kSurface<M, false><<<grid, 128, 0, s>>>(sc, pp, pb, q, cur, st);
+    if (sc.fullShapes) {
+        kSurface<M, true, true><<<grid, 128, 0, s>>>(sc, pp, pb, q, cur, st);
+        kSurface<M, false, true><<<grid, 128, 0, s>>>(sc, pp, pb, q, cur, st);
+    } else {
+        kSurface<M, true, false><<<grid, 128, 0, s>>>(sc, pp, pb, q, cur, st);
+        kSurface<M, false, false><<<grid, 128, 0, s>>>(sc, pp, pb, q, cur, st);
+    }
 }
+// The shadow-ray kernels of a bounce: visibility then contributions without null boundaries, the
+// ordered walk with them; instantiated for the counting passes and for the scene's shapes.
+template <int M, bool Splat, bool Count, bool Full>
+void shadowKernelsOf(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q,
+                     StatCounters* st, uint32_t* fetch, uint8_t* vis, const SplatTarget& film, int grid, cudaStream_t s) {
+    const size_t smem = traversalSharedBytes(128);
+    if (pp.anyHitShadows) {
+        kShadowVis<M, Count, Full><<<grid, 128, smem, s>>>(sc, pb, q, vis, fetch);
+        kShadowApply<M, Splat><<<grid, 256, 0, s>>>(sc, pb, q, vis, st, film);
+    } else {
+        kShadow<M, false, Count, Splat, Full><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch, film);
+    }
+}
+template <int M, bool Splat>
+void shadowKernels(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q,
+                   StatCounters* st, uint32_t* fetch, uint8_t* vis, const SplatTarget& film, int grid, cudaStream_t s) {
+    if (sc.fullShapes) {
+        if (sc.travCounters) shadowKernelsOf<M, Splat, true, true>(sc, pp, pb, q, st, fetch, vis, film, grid, s);
+        else shadowKernelsOf<M, Splat, false, true>(sc, pp, pb, q, st, fetch, vis, film, grid, s);
+    } else {
+        if (sc.travCounters) shadowKernelsOf<M, Splat, true, false>(sc, pp, pb, q, st, fetch, vis, film, grid, s);
+        else shadowKernelsOf<M, Splat, false, false>(sc, pp, pb, q, st, fetch, vis, film, grid, s);
+    }
+}
+
 template <int M>
 void launchShadow(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q,
                   StatCounters* st, uint32_t* fetch, uint8_t* vis, int grid, cudaStream_t s) {
-    const size_t smem = traversalSharedBytes(128);
-    if (pp.anyHitShadows) {
-        if (sc.travCounters) kShadowVis<M, true><<<grid, 128, smem, s>>>(sc, pb, q, vis, fetch);
-        else kShadowVis<M, false><<<grid, 128, smem, s>>>(sc, pb, q, vis, fetch);
-        kShadowApply<M><<<grid, 256, 0, s>>>(sc, pb, q, vis, st, SplatTarget{});
-    } else {
-        if (sc.travCounters) kShadow<M, false, true><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch, SplatTarget{});
-        else kShadow<M, false, false><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch, SplatTarget{});
-    }
+    shadowKernels<M, false>(sc, pp, pb, q, st, fetch, vis, SplatTarget{}, grid, s);
 }
 template <int M>
 void launchConnect(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q,
                    StatCounters* st, uint32_t* fetch, uint8_t* vis, const SplatTarget& film, int grid, cudaStream_t s) {
-    const size_t smem = traversalSharedBytes(128);
-    if (pp.anyHitShadows) {
-        if (sc.travCounters) kShadowVis<M, true><<<grid, 128, smem, s>>>(sc, pb, q, vis, fetch);
-        else kShadowVis<M, false><<<grid, 128, smem, s>>>(sc, pb, q, vis, fetch);
-        kShadowApply<M, true><<<grid, 256, 0, s>>>(sc, pb, q, vis, st, film);
-    } else {
-        if (sc.travCounters) kShadow<M, false, true, true><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch, film);
-        else kShadow<M, false, false, true><<<grid, 128, smem, s>>>(sc, pp, pb, q, st, fetch, film);
-    }
+    shadowKernels<M, true>(sc, pp, pb, q, st, fetch, vis, film, grid, s);
 }
 template <int M>
 void launchFilm(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, double* film, double* comp,
@@ -1043,11 +1062,13 @@ void launchFilm(const DeviceScene& sc, const PassParams& pp, const PathBuffers<R
 template <int M>
 void launchCastRays(const DeviceScene& sc, uint64_t n, const double* o, const double* d, uint32_t* b, uint32_t* p,
                     double* t, int grid, cudaStream_t s) {
-    kCastRays<M><<<grid, 128, traversalSharedBytes(128), s>>>(sc, n, o, d, b, p, t);
+    if (sc.fullShapes) kCastRays<M, true><<<grid, 128, traversalSharedBytes(128), s>>>(sc, n, o, d, b, p, t);
+    else kCastRays<M, false><<<grid, 128, traversalSharedBytes(128), s>>>(sc, n, o, d, b, p, t);
 }
 void launchCastRaysF(const DeviceScene& sc, uint64_t n, const float* o, const float* d, uint32_t* b, uint32_t* p,
                      float* t, int grid, cudaStream_t s) {
-    kCastRaysF<<<grid, 128, traversalSharedBytes(128), s>>>(sc, n, o, d, b, p, t);
+    if (sc.fullShapes) kCastRaysF<true><<<grid, 128, traversalSharedBytes(128), s>>>(sc, n, o, d, b, p, t);
+    else kCastRaysF<false><<<grid, 128, traversalSharedBytes(128), s>>>(sc, n, o, d, b, p, t);
 }
 void launchResolve(const double* film, const double* comp, const double* samples, uint32_t nPixels, double* xyz,
                    cudaStream_t s) {
@@ -1059,12 +1080,12 @@ void launchMaterialize(const uint32_t* leafOrder, uint32_t n, const float4* tri,
 }
 void configureKernels() {
     const int smem = int(traversalSharedBytes(128));
-    cudaFuncSetAttribute(kIntersect<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(kIntersect<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(kIntersect<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(kIntersect<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(kIntersect<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(kIntersect<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kIntersect<0, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kIntersect<1, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kIntersect<2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kIntersect<0, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kIntersect<1, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kIntersect<2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
 #define OWEC_INSTANTIATE(M)                                                                                         \

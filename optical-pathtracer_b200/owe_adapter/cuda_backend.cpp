@@ -4,12 +4,13 @@
 // This file belongs in the engine's tree as src/owe/backends/cuda/cuda_backend.cpp, beside the cpu
 // and gpu backends; the registry lists it (src/owe/backends/registry.cpp:10-13) and the layering
 // rule allows it core/, scene/, render/ and backends/cuda/ (not transport/). It flattens the world
-// model into owec_scene_desc: media, regions, optics, emitters, boundaries with their rigid frames,
-// the sun and sky, and the detector. Scenes using features the CUDA backend does not implement
-// (textures, environment maps, aspheres, lathe and wave shapes, thin-lens observers, aim guides)
-// are refused with std::runtime_error, as Backend::createRenderer does for unsupported settings
+// model into owec_scene_desc: media, regions, optics, emitters, boundaries with their rigid frames
+// and shape data, the sun and sky, and the detector. Scenes using features the CUDA backend does not
+// implement (textures, environment maps, wave surfaces, thin-lens observers, aim guides) are refused
+// with std::runtime_error, as Backend::createRenderer does for unsupported settings
 // (src/owe/render/backend.hpp:44).
 #include <cstring>
+#include <initializer_list>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -39,7 +40,15 @@ struct Flat {
     std::vector<owec_mesh> meshes;
     std::vector<double> vertices;
     std::vector<uint32_t> triangles;
+    std::vector<double> shapeData;
     owec_scene_desc desc{};
+
+    // Appends a shape's data run and records it in the boundary.
+    void data(owec_boundary& b, std::initializer_list<double> values) {
+        b.data_offset = uint32_t(shapeData.size());
+        b.data_count = uint32_t(values.size());
+        shapeData.insert(shapeData.end(), values.begin(), values.end());
+    }
 
     int32_t spectrum(const Spectrum& s) {
         owec_spectrum o{};
@@ -153,18 +162,25 @@ std::unique_ptr<Flat> flatten(const Scene& sc, int detectorIndex) {
             o.shape = OWEC_SHAPE_SPHERE;
             o.params[0] = sp->radius();
         } else if (auto* sg = dynamic_cast<const SagSurface*>(s)) {
-            if (!sg->asphere().empty()) throw std::runtime_error("boundary '" + b.name + "': aspheres are not rendered by the cuda backend");
             o.shape = OWEC_SHAPE_SAG;
             o.params[0] = sg->curvature();
             o.params[1] = sg->conic();
             o.params[2] = sg->rMax();
             o.params[3] = sg->rMin();
+            o.data_offset = uint32_t(f->shapeData.size());
+            o.data_count = uint32_t(sg->asphere().size());
+            f->shapeData.insert(f->shapeData.end(), sg->asphere().begin(), sg->asphere().end());
         } else if (auto* pl = dynamic_cast<const PlaneShape*>(s)) {
-            if (pl->aperture() == PlaneShape::Aperture::DiskHole)
-                throw std::runtime_error("boundary '" + b.name + "': holed disks are not rendered by the cuda backend");
             o.shape = OWEC_SHAPE_PLANE;
-            o.params[0] = pl->aperture() == PlaneShape::Aperture::Disk ? OWEC_APERTURE_DISK
-                          : pl->aperture() == PlaneShape::Aperture::Rect ? OWEC_APERTURE_RECT : OWEC_APERTURE_ELLIPSE;
+            switch (pl->aperture()) {
+                case PlaneShape::Aperture::Disk: o.params[0] = OWEC_APERTURE_DISK; break;
+                case PlaneShape::Aperture::Rect: o.params[0] = OWEC_APERTURE_RECT; break;
+                case PlaneShape::Aperture::Ellipse: o.params[0] = OWEC_APERTURE_ELLIPSE; break;
+                case PlaneShape::Aperture::DiskHole:
+                    o.params[0] = OWEC_APERTURE_DISK_HOLE;
+                    f->data(o, {pl->holeX(), pl->holeY()});
+                    break;
+            }
             o.params[1] = pl->a();
             o.params[2] = pl->b();
         } else if (auto* cy = dynamic_cast<const CylinderShape*>(s)) {
@@ -172,6 +188,33 @@ std::unique_ptr<Flat> flatten(const Scene& sc, int detectorIndex) {
             o.params[0] = cy->radius();
             o.params[1] = cy->z0();
             o.params[2] = cy->z1();
+        } else if (auto* co = dynamic_cast<const ConeShape*>(s)) {
+            o.shape = OWEC_SHAPE_CONE;
+            o.params[0] = co->r0();
+            o.params[1] = co->z0();
+            o.params[2] = co->r1();
+            o.params[3] = co->z1();
+        } else if (auto* to = dynamic_cast<const TorusPatchShape*>(s)) {
+            o.shape = OWEC_SHAPE_TORUS;
+            o.params[0] = to->majorRadius();
+            o.params[1] = to->zc();
+            o.params[2] = to->rho();
+            o.params[3] = to->a0();
+            f->data(o, {to->a1()});
+        } else if (auto* rw = dynamic_cast<const RoundWallShape*>(s)) {
+            o.shape = OWEC_SHAPE_ROUND_WALL;
+            o.params[0] = rw->radius();
+            o.params[1] = rw->height();
+            o.data_offset = uint32_t(f->shapeData.size());
+            o.data_count = uint32_t(4 * rw->openings().size());
+            for (const auto& op : rw->openings())
+                f->shapeData.insert(f->shapeData.end(), {op.azimuth, op.width, op.sill, op.top});
+        } else if (auto* dm = dynamic_cast<const DomeShape*>(s)) {
+            o.shape = OWEC_SHAPE_DOME;
+            o.params[0] = dm->radius();
+            o.params[1] = dm->slitAzimuth();
+            o.params[2] = dm->slitWidth();
+            o.params[3] = dm->slitTop();
         } else if (auto* me = dynamic_cast<const MeshShape*>(s)) {
             o.shape = OWEC_SHAPE_MESH;
             o.mesh = int32_t(f->meshes.size());
@@ -243,6 +286,8 @@ std::unique_ptr<Flat> flatten(const Scene& sc, int detectorIndex) {
     d.meshes = f->meshes.data();
     d.vertices = f->vertices.data();
     d.triangles = f->triangles.data();
+    d.n_shape_data = f->shapeData.size();
+    d.shape_data = f->shapeData.data();
     return f;
 }
 

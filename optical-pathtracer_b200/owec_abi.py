@@ -18,8 +18,9 @@ E_INVALID, E_CUDA, E_NOMEM, E_STATE, E_DEVICE_FAULT, E_UNSUPPORTED = -1, -2, -3,
 SPEC_CONSTANT, SPEC_TABULATED, SPEC_BLACKBODY = 0, 1, 2
 INDEX_CONSTANT, INDEX_CAUCHY, INDEX_SELLMEIER, INDEX_CIDDOR, INDEX_TABULATED = 0, 1, 2, 3, 4
 SURF_NULL, SURF_DIELECTRIC, SURF_DIFFUSE, SURF_CONDUCTOR, SURF_MIRROR, SURF_ABSORBER, SURF_DETECTOR = range(7)
-SHAPE_SPHERE, SHAPE_SAG, SHAPE_PLANE, SHAPE_CYLINDER, SHAPE_MESH = range(5)
-APERTURE_DISK, APERTURE_RECT, APERTURE_ELLIPSE = 0, 1, 2
+SHAPE_SPHERE, SHAPE_SAG, SHAPE_PLANE, SHAPE_CYLINDER, SHAPE_MESH, SHAPE_CONE, SHAPE_TORUS, SHAPE_ROUND_WALL, \
+    SHAPE_DOME = range(9)
+APERTURE_DISK, APERTURE_RECT, APERTURE_ELLIPSE, APERTURE_DISK_HOLE = 0, 1, 2, 3
 SKY_NONE, SKY_UNIFORM = 0, 1
 DETECTOR_OBSERVER, DETECTOR_SENSOR = 0, 1
 WAVELENGTHS_HERO4, WAVELENGTHS_UNIFORM1 = 0, 1
@@ -58,7 +59,8 @@ class Emission(ctypes.Structure):
 class Boundary(ctypes.Structure):
     _fields_ = [("shape", ctypes.c_int32), ("mesh", ctypes.c_int32), ("front", ctypes.c_uint32),
                 ("back", ctypes.c_uint32), ("optics", ctypes.c_uint32), ("emission", ctypes.c_int32),
-                ("to_world", ctypes.c_double * 12), ("params", ctypes.c_double * 4)]
+                ("to_world", ctypes.c_double * 12), ("params", ctypes.c_double * 4),
+                ("data_offset", ctypes.c_uint32), ("data_count", ctypes.c_uint32)]
 
 
 class Mesh(ctypes.Structure):
@@ -93,7 +95,8 @@ class SceneDesc(ctypes.Structure):
                 ("vertices", c_double_p), ("triangles", c_u32_p),
                 ("env", Environment), ("detector", Detector),
                 ("frame_origin_set", ctypes.c_int32), ("pad0", ctypes.c_int32),
-                ("frame_origin", ctypes.c_double * 3)]
+                ("frame_origin", ctypes.c_double * 3),
+                ("n_shape_data", ctypes.c_uint64), ("shape_data", c_double_p)]
 
 
 class Settings(ctypes.Structure):

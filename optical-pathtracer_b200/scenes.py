@@ -61,6 +61,7 @@ class SceneBuilder:
         self.optics, self.emissions, self.boundaries, self.meshes = [], [], [], []
         self.vertices, self.triangles = [], []
         self.n_vertices = self.n_triangles = 0
+        self.shape_data = []
         self.env = A.Environment(A.SKY_NONE, -1, 0, -1, (0, 0, 1), math.radians(0.2665), 0.0)
         self.detector = None
         air = self.medium_ciddor_air()
@@ -125,11 +126,16 @@ class SceneBuilder:
         return len(self.emissions) - 1
 
     # ---------------------------------------------------------- boundaries
-    def boundary(self, shape, params, xf, front, back, optics, emission=-1, mesh=-1):
+    def boundary(self, shape, params, xf, front, back, optics, emission=-1, mesh=-1, data=()):
+        """A boundary; `data`: the shape's run of shape data (asphere terms, a torus arc's end,
+        wall openings, a hole's centre)."""
         xf = np.asarray(xf, float).reshape(3, 4)
         p = list(params) + [0.0] * (4 - len(params))
+        offset = len(self.shape_data)
+        self.shape_data += [float(v) for v in data]
         self.boundaries.append(A.Boundary(shape, mesh, front, back, optics, emission,
-                                          (ctypes.c_double * 12)(*xf.ravel()), (ctypes.c_double * 4)(*p)))
+                                          (ctypes.c_double * 12)(*xf.ravel()), (ctypes.c_double * 4)(*p),
+                                          offset, len(data)))
         return len(self.boundaries) - 1
 
     def mesh(self, vertices, triangles):
@@ -208,6 +214,7 @@ class SceneBuilder:
             "meshes": _arr(A.Mesh, self.meshes),
             "verts": verts,
             "tris": tris,
+            "shape_data": _arr(ctypes.c_double, self.shape_data),
         }
         d = A.SceneDesc()
         d.abi_version = A.ABI_VERSION
@@ -225,6 +232,8 @@ class SceneBuilder:
         d.triangles = tris.ctypes.data_as(A.c_u32_p)
         d.env = self.env
         d.detector = self.detector
+        d.n_shape_data = len(self.shape_data)
+        d.shape_data = keep["shape_data"]
         d._keep = keep  # the pointed-to arrays live as long as the description
         return d
 
@@ -463,6 +472,53 @@ def disk_irradiance_mean(radiance, a, h, half, n=200):
     s = h * h + r2 + a * a
     e = math.pi * radiance / 2 * (1 - (h * h + r2 - a * a) / np.sqrt(s * s - 4 * r2 * a * a))
     return float(e.mean())
+
+
+def shape_gallery(width=48, height=36, sun=True):
+    """One of every trimmed and lathe shape beside the conic ones, as two-sided Lambertian sheets on a
+    floor under the sun and a uniform sky: a cone frustum, a torus patch (a vessel's fillet), a round
+    wall with two openings, an observatory dome with its slit, a disk with an off-centre hole and an
+    even asphere (src/owe/scene/geometry.hpp:51-300)."""
+    sb = SceneBuilder()
+    sb.sheet(3.0, 3.0, pose(), sb.diffuse(0.5))
+    grey, white = sb.diffuse(0.6), sb.diffuse(0.85)
+    sb.boundary(A.SHAPE_CONE, [0.35, 0.0, 0.1, 0.6], translate(-1.1, 0.2, 0.0), 0, 0, white)
+    sb.boundary(A.SHAPE_TORUS, [0.3, 0.25, 0.2, -math.pi / 2], translate(1.1, 0.2, 0.0), 0, 0, grey,
+                data=[math.pi / 2])
+    sb.boundary(A.SHAPE_ROUND_WALL, [0.45, 0.7], translate(0.0, 1.2, 0.0), 0, 0, white,
+                data=[0.0, 0.35, 0.1, 0.45, math.pi, 0.25, 0.2, 0.6])
+    sb.boundary(A.SHAPE_DOME, [0.5, 0.6, 0.25, 1.2], translate(0.0, -0.4, 0.0), 0, 0, grey)
+    sb.boundary(A.SHAPE_PLANE, [A.APERTURE_DISK_HOLE, 0.4, 0.12], pose(rotate_to((0, 0, 1), (0, -1, 0.3)), (1.2, -1.0, 0.5)),
+                0, 0, white, data=[0.12, 0.05])
+    sb.boundary(A.SHAPE_SAG, [1 / 0.6, -0.6, 0.35, 0.0], pose(rotate_to((0, 0, 1), (0.2, -1, 0.4)), (-1.2, -1.0, 0.45)),
+                0, 0, white, data=[0.4, -0.6, 0.3])
+    if sun:
+        sb.sun((0.4, -0.5, 0.75), 3.0e4)
+    sb.uniform_sky(0.4)
+    sb.observer(width, height, (0.0, -4.2, 2.6), (0.0, 0.1, 0.3), fov_y_deg=42.0)
+    return sb
+
+
+def asphere_lens(width=48, height=48):
+    """A biconvex N-BK7 lens with even-aspheric faces (A4, A6) and a cylindrical rim over a
+    Lambertian floor under the sun: light through two numerically crossed surfaces."""
+    sb = SceneBuilder()
+    bk7 = sb.medium_sellmeier(*NBK7, rel_air=True)
+    glass = sb.region(bk7)
+    opt = sb.dielectric()
+    r, t = 0.3, 0.12
+    # front face: vertex at z = t / 2, bulging up (+z normal outward)
+    sb.boundary(A.SHAPE_SAG, [-1 / 0.9, -1.2, r, 0.0], translate(0, 0, 1.0 + t / 2), 0, glass, opt, data=[-0.08, 0.02])
+    # back face: vertex at z = -t / 2, bulging down; its +z normal points into the glass
+    sb.boundary(A.SHAPE_SAG, [-1 / 0.9, -1.2, r, 0.0], pose(np.diag([1.0, -1.0, -1.0]), (0, 0, 1.0 - t / 2)), 0, glass,
+                opt, data=[-0.08, 0.02])
+    sag_edge = float(-(1 / 0.9) * r * r / (1 + math.sqrt(1 - (1 - 1.2) * (1 / 0.9) ** 2 * r * r))
+                     - 0.08 * r ** 4 + 0.02 * r ** 6)
+    sb.boundary(A.SHAPE_CYLINDER, [r, -(t / 2 + sag_edge), t / 2 + sag_edge], translate(0, 0, 1.0), 0, glass, sb.absorber())
+    sb.sheet(4.0, 4.0, pose(), sb.diffuse(0.8))
+    sb.sun((0.1, -0.15, 1.0), 2.0e4)
+    sb.observer(width, height, (0.0, -2.6, 2.4), (0.0, 0.0, 0.6), fov_y_deg=40.0)
+    return sb
 
 
 def random_rays(n, seed, lo, hi, target_lo, target_hi):

@@ -87,14 +87,33 @@ IndexModel makeIndex(const owec_scene_desc& d, const owec_medium& m) {
 
 std::shared_ptr<const Shape> makeShape(const owec_scene_desc& d, const owec_boundary& b) {
     const double* p = b.params;
+    if (b.data_count && (!d.shape_data || uint64_t(b.data_offset) + b.data_count > d.n_shape_data))
+        throw std::runtime_error("shape data out of range");
+    const double* data = b.data_count ? d.shape_data + b.data_offset : nullptr;
     switch (b.shape) {
         case OWEC_SHAPE_SPHERE: return std::make_shared<SphereShape>(p[0]);
-        case OWEC_SHAPE_SAG: return std::make_shared<SagSurface>(p[0], p[1], std::vector<double>{}, p[2], p[3]);
+        case OWEC_SHAPE_SAG:
+            return std::make_shared<SagSurface>(p[0], p[1], std::vector<double>(data, data + b.data_count), p[2], p[3]);
         case OWEC_SHAPE_PLANE:
             if (int(p[0]) == OWEC_APERTURE_DISK) return PlaneShape::disk(p[1], p[2]);
             if (int(p[0]) == OWEC_APERTURE_RECT) return PlaneShape::rect(p[1], p[2]);
+            if (int(p[0]) == OWEC_APERTURE_DISK_HOLE) {
+                if (b.data_count != 2) throw std::runtime_error("disk with hole: its data is the hole's centre");
+                return PlaneShape::diskWithHole(p[1], p[2], data[0], data[1]);
+            }
             return PlaneShape::ellipse(p[1], p[2]);
         case OWEC_SHAPE_CYLINDER: return std::make_shared<CylinderShape>(p[0], p[1], p[2]);
+        case OWEC_SHAPE_CONE: return std::make_shared<ConeShape>(p[0], p[1], p[2], p[3]);
+        case OWEC_SHAPE_TORUS:
+            if (b.data_count != 1) throw std::runtime_error("torus patch: its data is the arc's end angle");
+            return std::make_shared<TorusPatchShape>(p[0], p[1], p[2], p[3], data[0]);
+        case OWEC_SHAPE_ROUND_WALL: {
+            std::vector<RoundWallShape::Opening> open;
+            for (uint32_t i = 0; i + 3 < b.data_count; i += 4)
+                open.push_back({data[i], data[i + 1], data[i + 2], data[i + 3]});
+            return std::make_shared<RoundWallShape>(p[0], p[1], std::move(open));
+        }
+        case OWEC_SHAPE_DOME: return std::make_shared<DomeShape>(p[0], p[1], p[2], p[3]);
         case OWEC_SHAPE_MESH: {
             if (b.mesh < 0 || uint32_t(b.mesh) >= d.n_meshes) throw std::runtime_error("mesh index out of range");
             const owec_mesh& m = d.meshes[b.mesh];
