@@ -168,8 +168,8 @@ typedef struct owec_environment {
     double sun_nee_share;     /* fraction of NEE light selections given to the sun (0 = by power) */
 } owec_environment;
 
-#define OWEC_DETECTOR_OBSERVER 0 /* IdealObserver, pinhole (src/owe/scene/detector.hpp:77-123) */
-#define OWEC_DETECTOR_SENSOR 1   /* SurfaceSensor, hemispherical (src/owe/scene/detector.hpp:125-158) */
+#define OWEC_DETECTOR_OBSERVER 0 /* IdealObserver: pinhole or thin lens (src/owe/scene/detector.hpp:75-123) */
+#define OWEC_DETECTOR_SENSOR 1   /* SurfaceSensor: hemispherical or aimed (src/owe/scene/detector.hpp:125-158) */
 
 typedef struct owec_detector {
     int32_t kind;
@@ -184,6 +184,20 @@ typedef struct owec_detector {
     uint32_t boundary;        /* sensor: its detector boundary */
     int32_t pad0;
     double half_x, half_y;    /* sensor: half sizes in the boundary's plane */
+    /* Observer: a thin lens (IdealObserver::pupilRadius, focusDistance; pupil 0: a pinhole; focus 0
+     * or infinite: focused at infinity) and its pupil guide toward an instrument's exit pupil
+     * (IdealObserver::guide; radius 0: none). */
+    double pupil_radius, focus_distance;
+    double guide_center[3];
+    double guide_radius, guide_share;
+    /* Sensor: the readout flips and the aimed direction sampling (SurfaceSensor flipX, flipY,
+     * hasAim, aimCenter, aimNormal, aimRadius, aimShare, focusCenter, focusRadius, focusShare). */
+    int32_t flip_x, flip_y;
+    int32_t has_aim, pad1;
+    double aim_center[3], aim_normal[3];
+    double aim_radius, aim_share;
+    double focus_center[3];
+    double focus_radius, focus_share;
 } owec_detector;
 
 typedef struct owec_scene_desc {

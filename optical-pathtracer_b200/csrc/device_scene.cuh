@@ -62,6 +62,16 @@ struct DDetector {
     uint32_t boundary;    // sensor
     double halfX, halfY;
     double normal[3];
+    // observer: thin lens (pupil 0: a pinhole; focus INFINITY: at infinity) and its pupil guide
+    double pupil, focus;
+    double guideC[3];     // camera-relative
+    double guideR, guideShare;
+    // sensor: readout flips and the aimed direction mixture (aimR 0: hemispherical)
+    int32_t flipX, flipY;
+    double aimC[3], aimN[3];  // camera-relative centre, unit normal
+    double aimR, aimShare;
+    double focusC[3];
+    double focusR, focusShare;
 };
 
 // An 8-wide BVH node with children quantised to 8 bits against the node's box (80 bytes, five

@@ -450,6 +450,8 @@ void validateDesc(const owec_scene_desc& d) {
     } else {
         require(det.region < d.n_regions, "observer region out of range (the engine locates it before flattening)");
         require(det.fov_y > 0 && det.fov_y < kPi, "observer field of view out of range");
+        require(det.pupil_radius >= 0 && !(det.focus_distance < 0) && det.guide_radius >= 0 && det.guide_share >= 0 &&
+                    det.guide_share < 1, "observer: pupil, focus or guide out of range");
     }
     require(d.env.sky_model == OWEC_SKY_NONE || d.env.sky_model == OWEC_SKY_UNIFORM, "unknown sky model");
     require(specOk(d.env.sky_radiance) && specOk(d.env.sun_radiance), "environment spectrum out of range");
@@ -681,6 +683,11 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
         det.tanY = std::tan(0.5 * dd.fov_y);
         det.tanX = det.tanY * double(dd.width) / double(dd.height);
         det.region = dd.region;
+        det.pupil = dd.pupil_radius;
+        det.focus = dd.focus_distance > 0 && std::isfinite(dd.focus_distance) ? dd.focus_distance : INFINITY;
+        det.guideR = dd.pupil_radius > 0 ? dd.guide_radius : 0;
+        det.guideShare = dd.guide_share;
+        for (int k = 0; k < 3; ++k) det.guideC[k] = dd.guide_center[k] - origin[k];
     } else {
         const owec_boundary& b = d.boundaries[dd.boundary];
         require(d.optics[b.optics].type == OWEC_SURF_DETECTOR || d.optics[b.optics].type == OWEC_SURF_DIFFUSE,
@@ -692,6 +699,25 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
         const double nl = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
         for (int k = 0; k < 3; ++k) det.normal[k] = nrm[k] / nl;
         det.region = b.front;
+        det.flipX = dd.flip_x != 0;
+        det.flipY = dd.flip_y != 0;
+        if (dd.has_aim) {
+            const double al = std::sqrt(dd.aim_normal[0] * dd.aim_normal[0] + dd.aim_normal[1] * dd.aim_normal[1] +
+                                        dd.aim_normal[2] * dd.aim_normal[2]);
+            require(al > 0 && dd.aim_radius > 0 && dd.aim_share > 0 && dd.aim_share <= 1,
+                    "sensor aim: needs a normal, a radius and a share in (0, 1]");
+            require(dd.focus_share >= 0 && dd.focus_share < 1 && (dd.focus_share == 0 || dd.focus_radius > 0),
+                    "sensor aim: focus share in [0, 1) with a radius");
+            det.aimR = dd.aim_radius;
+            det.aimShare = dd.aim_share;
+            det.focusR = dd.focus_radius;
+            det.focusShare = dd.focus_share;
+            for (int k = 0; k < 3; ++k) {
+                det.aimC[k] = dd.aim_center[k] - origin[k];
+                det.aimN[k] = dd.aim_normal[k] / al;
+                det.focusC[k] = dd.focus_center[k] - origin[k];
+            }
+        }
     }
 
     // Upload.

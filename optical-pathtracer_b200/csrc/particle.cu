@@ -38,19 +38,6 @@ __device__ __forceinline__ V3<double> plainPoint(const V3<double>& p) {
     return Mode<M>::plainOrigin ? V3<double>(V3<float>(p)) : p;
 }
 
-// The concentric map of the unit square onto the unit disk (sampleUniformDiskConcentric,
-// src/owe/core/shared/warps.hpp:45-60).
-__device__ __forceinline__ void concentricDisk(double u1, double u2, double& x, double& y) {
-    const double a = 2 * u1 - 1, b = 2 * u2 - 1;
-    x = y = 0;
-    if (a == 0 && b == 0) return;
-    double r, phi;
-    if (fabs(a) > fabs(b)) { r = a; phi = (kPi / 4) * (b / a); }
-    else { r = b; phi = kPi / 2 - (kPi / 4) * (a / b); }
-    x = r * cos(phi);
-    y = r * sin(phi);
-}
-
 // The Gaussian pixel response as an offset in pixels (Detector::filterOffset,
 // src/owe/scene/detector.hpp:57-62); nothing is drawn without one.
 __device__ __forceinline__ void filterOffset(const DDetector& det, Pcg32& rng, double& fx, double& fy) {
@@ -61,26 +48,45 @@ __device__ __forceinline__ void filterOffset(const DDetector& det, Pcg32& rng, d
     fy += r * sin(phi) * det.sigma;
 }
 
-// A connection of point x to the pinhole (IdealObserver::connect): the pixel, the direction and
-// distance from x to the eye, and the factor 1 / (d^2 * pixel area * cos^3) of the observer's
-// importance. False when x lies behind the eye or outside the field.
+// A connection of point x to the observer (IdealObserver::connect; particle.slang:48-84): a point q
+// of the pupil (the eye itself for a pinhole), the pixel, the direction and distance from x to q,
+// and the factor 1 / (d^2 * pixel area * cos^3) of the observer's importance (for a thin lens the
+// pupil's area cancels against the density of q). False when x lies behind the eye or outside the
+// field.
 struct ObserverLink {
-    V3<double> dir;
+    V3<double> q, dir;
     double dist, factor;
     uint32_t pixel;
 };
 __device__ bool linkObserver(const DeviceScene& sc, const ParticleParams& P, const V3<double>& x, Pcg32& rng,
                              ObserverLink& k) {
     const DDetector& det = sc.det;
-    const V3<double> w = x - V3<double>(det.pos[0], det.pos[1], det.pos[2]);
+    const V3<double> eye(det.pos[0], det.pos[1], det.pos[2]);
+    const V3<double> R3(det.right[0], det.right[1], det.right[2]), U3(det.up[0], det.up[1], det.up[2]);
+    k.q = eye;
+    if (det.pupil > 0) {
+        const Draw2<double> u(rng);
+        double dx, dy;
+        concentricDisk(u.u1, u.u2, dx, dy);
+        k.q = eye + (R3 * dx + U3 * dy) * det.pupil;
+    }
+    const V3<double> w = x - k.q;
     const double d2 = dot(w, w);
     if (!(d2 > 0)) return false;
     const double dist = sqrt(d2);
     const V3<double> om = w / dist;
     const double c = dot(om, V3<double>(det.fwd[0], det.fwd[1], det.fwd[2]));
     if (c <= 1e-9) return false;
-    const double sx = dot(om, V3<double>(det.right[0], det.right[1], det.right[2])) / c;
-    const double sy = dot(om, V3<double>(det.up[0], det.up[1], det.up[2])) / c;
+    double sx, sy;
+    if (det.pupil > 0 && isfinite(det.focus)) {
+        // where the line from q through x meets the plane in focus, seen from the eye
+        const V3<double> F = k.q + om * (det.focus / c) - eye;
+        sx = dot(F, R3) / det.focus;
+        sy = dot(F, U3) / det.focus;
+    } else {
+        sx = dot(om, R3) / c;
+        sy = dot(om, U3) / c;
+    }
     double fx = (sx / det.tanX + 1) * 0.5 * det.width, fy = (1 - sy / det.tanY) * 0.5 * det.height;
     filterOffset(det, rng, fx, fy);
     if (!(fx >= 0 && fy >= 0 && fx < det.width && fy < det.height)) return false;
@@ -420,8 +426,11 @@ __global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, Particl
                 } else {
                     // a surface sensor records the flux reaching its front face
                     if (!observer && fromFront && h.boundary == det.boundary) {
+                        // SurfaceSensor::pixelOfHit (particle.slang:88-104)
                         double fx = (g.pLocal.x / det.halfX + 1) * 0.5 * det.width;
                         double fy = (1 - g.pLocal.y / det.halfY) * 0.5 * det.height;
+                        if (det.flipX) fx = det.width - fx;
+                        if (det.flipY) fy = det.height - fy;
                         filterOffset(det, rng, fx, fy);
                         if (fx >= 0 && fy >= 0 && fx < det.width && fy < det.height) {
                             const uint32_t pixel = uint32_t(min(int(fy), det.height - 1)) * uint32_t(det.width) +

@@ -130,6 +130,34 @@ __device__ SurfacePoint<R> hitGeometry(const DeviceScene& sc, const PathRay<R>& 
     return sp;
 }
 
+// ------------------------------------------------------------------ sampling
+// The concentric map of the unit square onto the unit disk (sampleUniformDiskConcentric,
+// src/owe/core/shared/warps.hpp:45-60).
+__device__ __forceinline__ void concentricDisk(double u1, double u2, double& x, double& y) {
+    const double a = 2 * u1 - 1, b = 2 * u2 - 1;
+    x = y = 0;
+    if (a == 0 && b == 0) return;
+    double r, phi;
+    if (fabs(a) > fabs(b)) { r = a; phi = (kPi / 4) * (b / a); }
+    else { r = b; phi = kPi / 2 - (kPi / 4) * (a / b); }
+    x = r * cos(phi);
+    y = r * sin(phi);
+}
+
+// The solid-angle density at p of directions toward a uniform point of the disk (centre, unit
+// normal, radius). generatingDisk: the direction is known to come from that disk, which is then
+// not tested again (diskAimPdf, src/owe/core/shared/optics.hpp:244-255).
+__device__ __forceinline__ double diskAimPdf(const V3<double>& p, const V3<double>& wi, const V3<double>& center,
+                                             const V3<double>& normal, double radius, bool generatingDisk) {
+    if (!(radius > 0)) return 0;
+    const double dn = dot(wi, normal);
+    if (fabs(dn) < 1e-12) return 0;
+    const double t = dot(center - p, normal) / dn;
+    const V3<double> delta = p + wi * t - center;
+    if (t <= 0 || (!generatingDisk && dot(delta, delta) > radius * radius)) return 0;
+    return t * t / (fabs(dn) * kPi * radius * radius);
+}
+
 // ------------------------------------------------------------------ emitters
 // The solid-angle density at ref of a point p (normal n) drawn uniformly from an area
 // (areaToSolidAngle, src/owe/core/shared/warps.hpp:103-113); 0 when seen edge-on.

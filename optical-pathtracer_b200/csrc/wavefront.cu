@@ -94,36 +94,90 @@ __global__ void __launch_bounds__(256) kGenerate(DeviceScene sc, PassParams pp, 
     double weight = 0;
     V3<double> o, dir;
     if (det.kind == OWEC_DETECTOR_OBSERVER) {
-        // IdealObserver::generate, pinhole (detector.cpp:61-91)
+        // IdealObserver::generate (detector.cpp:61-91): a pinhole, or a thin lens whose pupil point
+        // is drawn uniformly or, when a guide is set, from the guide's disk with its share
         const double sx = (2 * px / det.width - 1) * det.tanX;
         const double sy = (1 - 2 * py / det.height) * det.tanY;
         const V3<double> R3(det.right[0], det.right[1], det.right[2]), U3(det.up[0], det.up[1], det.up[2]),
             F3(det.fwd[0], det.fwd[1], det.fwd[2]);
+        const V3<double> eye(det.pos[0], det.pos[1], det.pos[2]);
         dir = normalize(R3 * sx + U3 * sy + F3);
-        o = V3<double>(det.pos[0], det.pos[1], det.pos[2]);
+        o = eye;
         weight = 1;
+        if (det.pupil > 0) {
+            V3<double> c;
+            bool guided = false;
+            if (det.guideR > 0) {  // IdealObserver::guideCenter (detector.cpp:29-34)
+                const double dn = dot(dir, F3);
+                if (dn > 0) {
+                    const V3<double> gc(det.guideC[0], det.guideC[1], det.guideC[2]);
+                    c = gc - dir * (dot(gc - eye, F3) / dn);
+                    guided = dot(c - eye, c - eye) < sqr(det.pupil + det.guideR);
+                }
+            }
+            const bool fromGuide = guided && rng.uniform() < det.guideShare;
+            const Draw2<double> u(rng);
+            double dx, dy;
+            concentricDisk(u.u1, u.u2, dx, dy);
+            o = fromGuide ? c + (R3 * dx + U3 * dy) * det.guideR : eye + (R3 * dx + U3 * dy) * det.pupil;
+            if (guided) {
+                // radiance averaged over the eye's pupil: (1 / A_eye) / p(q), nothing outside the eye
+                if (fromGuide && dot(o - eye, o - eye) > sqr(det.pupil)) {
+                    weight = 0;
+                } else {
+                    const double pEye = 1 / (kPi * sqr(det.pupil));
+                    const bool inGuide = fromGuide || dot(o - c, o - c) <= sqr(det.guideR);
+                    const double pGuide = inGuide ? 1 / (kPi * sqr(det.guideR)) : 0;
+                    weight = pEye / ((1 - det.guideShare) * pEye + det.guideShare * pGuide);
+                }
+            }
+            if (isfinite(det.focus)) dir = normalize(eye + (R3 * sx + U3 * sy + F3) * det.focus - o);
+        }
         ray.region = det.region;
         ray.depB = kNone;
         ray.depP = kNone;
         ray.errN = 0.f;
     } else if (!(px < 0 || py < 0 || px >= det.width || py >= det.height)) {
-        // SurfaceSensor::generate, hemispherical (detector.cpp:113-148)
+        // SurfaceSensor::generate (detector.cpp:113-148): hemispherical, or aimed at a disk (and a
+        // focus disk) with cosine support kept by the remaining share
+        if (det.flipX) px = det.width - px;
+        if (det.flipY) py = det.height - py;
         const DBoundary& bd = sc.boundaries[det.boundary];
         const V3<double> pl((2 * px / det.width - 1) * det.halfX, (1 - 2 * py / det.height) * det.halfY, 0);
         o = bd.toWorld.point(pl);
         const V3<double> nrm(det.normal[0], det.normal[1], det.normal[2]);
-        const Draw2<double> g(rng);
-        const double a = 2 * g.u1 - 1, b = 2 * g.u2 - 1;
-        double dx = 0, dy = 0;
-        if (!(a == 0 && b == 0)) {
-            double r, phi;
-            if (fabs(a) > fabs(b)) { r = a; phi = (kPi / 4) * (b / a); }
-            else { r = b; phi = kPi / 2 - (kPi / 4) * (a / b); }
-            dx = r * cos(phi);
-            dy = r * sin(phi);
-        }
-        dir = Frame<double>(nrm).toWorld(V3<double>(dx, dy, sqrt(fmax(0.0, 1 - dx * dx - dy * dy))));
         weight = kPi;
+        if (det.aimR > 0) {
+            const V3<double> aN(det.aimN[0], det.aimN[1], det.aimN[2]), aC(det.aimC[0], det.aimC[1], det.aimC[2]);
+            const V3<double> fC(det.focusC[0], det.focusC[1], det.focusC[2]);
+            V3<double> a1, a2;
+            basis(aN, a1, a2);
+            const bool useAim = det.aimShare >= 1 || rng.uniform() < det.aimShare;
+            const bool useFocus = det.focusShare > 0 && rng.uniform() < det.focusShare;
+            const Draw2<double> u(rng);
+            double dx, dy;
+            concentricDisk(u.u1, u.u2, dx, dy);
+            const V3<double> w = (useFocus ? fC : aC) + (a1 * dx + a2 * dy) * (useFocus ? det.focusR : det.aimR) - o;
+            dir = w / length(w);
+            if (!useAim) {
+                double hx, hy;
+                concentricDisk(u.u1, u.u2, hx, hy);
+                dir = Frame<double>(nrm).toWorld(V3<double>(hx, hy, sqrt(fmax(0.0, 1 - hx * hx - hy * hy))));
+            }
+            const double cosS = dot(dir, nrm);
+            double pdfW = 0;
+            if (cosS > 0) {
+                pdfW = (1 - det.focusShare) * diskAimPdf(o, dir, aC, aN, det.aimR, useAim && !useFocus);
+                if (det.focusShare > 0) pdfW += det.focusShare * diskAimPdf(o, dir, fC, aN, det.focusR, useAim && useFocus);
+                pdfW = det.aimShare * pdfW + (1 - det.aimShare) * cosS * kInvPi;
+            }
+            weight = cosS > 0 && pdfW > 0 ? cosS / pdfW : 0.0;
+        } else {
+            const Draw2<double> g(rng);
+            double dx, dy;
+            concentricDisk(g.u1, g.u2, dx, dy);
+            dir = Frame<double>(nrm).toWorld(V3<double>(dx, dy, sqrt(fmax(0.0, 1 - dx * dx - dy * dy))));
+        }
         ray.region = det.region;
         ray.depB = det.boundary;
         ray.depP = 0;

@@ -6,9 +6,10 @@
 // rule allows it core/, scene/, render/ and backends/cuda/ (not transport/). It flattens the world
 // model into owec_scene_desc: media, regions, optics, emitters, boundaries with their rigid frames
 // and shape data, the sun and sky, and the detector. Scenes using features the CUDA backend does not
-// implement (textures, environment maps, wave surfaces, thin-lens observers, aim guides) are refused
-// with std::runtime_error, as Backend::createRenderer does for unsupported settings
+// implement (textures, environment maps, wave surfaces, materials' aim guides) are refused with
+// std::runtime_error, as Backend::createRenderer does for unsupported settings
 // (src/owe/render/backend.hpp:44).
+#include <cmath>
 #include <cstring>
 #include <initializer_list>
 #include <memory>
@@ -249,20 +250,35 @@ std::unique_ptr<Flat> flatten(const Scene& sc, int detectorIndex) {
     d.detector.pixel_sigma = det.pixelSigma;
     d.detector.region = det.region;
     if (auto* eye = dynamic_cast<const IdealObserver*>(&det)) {
-        if (eye->pupilRadius > 0) throw std::runtime_error("the cuda backend renders pinhole observers only");
         d.detector.kind = OWEC_DETECTOR_OBSERVER;
         for (int k = 0; k < 3; ++k) {
             d.detector.position[k] = eye->position[k];
             d.detector.look_at[k] = eye->lookAt[k];
             d.detector.up[k] = eye->up[k];
+            d.detector.guide_center[k] = eye->guide.center[k];
         }
         d.detector.fov_y = eye->fovY;
+        d.detector.pupil_radius = eye->pupilRadius;
+        d.detector.focus_distance = std::isfinite(eye->focusDistance) ? eye->focusDistance : 0;
+        d.detector.guide_radius = eye->guide.radius;
+        d.detector.guide_share = eye->guide.share;
     } else if (auto* sen = dynamic_cast<const SurfaceSensor*>(&det)) {
-        if (sen->hasAim || sen->flipX || sen->flipY) throw std::runtime_error("the cuda backend renders unaimed, unflipped sensors only");
         d.detector.kind = OWEC_DETECTOR_SENSOR;
         d.detector.boundary = sen->boundaryIndex;
         d.detector.half_x = sen->halfX;
         d.detector.half_y = sen->halfY;
+        d.detector.flip_x = sen->flipX;
+        d.detector.flip_y = sen->flipY;
+        d.detector.has_aim = sen->hasAim;
+        for (int k = 0; k < 3; ++k) {
+            d.detector.aim_center[k] = sen->aimCenter[k];
+            d.detector.aim_normal[k] = sen->aimNormal[k];
+            d.detector.focus_center[k] = sen->focusCenter[k];
+        }
+        d.detector.aim_radius = sen->aimRadius;
+        d.detector.aim_share = sen->aimShare;
+        d.detector.focus_radius = sen->focusRadius;
+        d.detector.focus_share = sen->focusShare;
     } else {
         throw std::runtime_error("unknown detector type");
     }

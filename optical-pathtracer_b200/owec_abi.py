@@ -79,7 +79,13 @@ class Detector(ctypes.Structure):
                 ("region", ctypes.c_uint32), ("position", ctypes.c_double * 3), ("look_at", ctypes.c_double * 3),
                 ("up", ctypes.c_double * 3), ("fov_y", ctypes.c_double), ("pixel_sigma", ctypes.c_double),
                 ("boundary", ctypes.c_uint32), ("pad0", ctypes.c_int32), ("half_x", ctypes.c_double),
-                ("half_y", ctypes.c_double)]
+                ("half_y", ctypes.c_double), ("pupil_radius", ctypes.c_double), ("focus_distance", ctypes.c_double),
+                ("guide_center", ctypes.c_double * 3), ("guide_radius", ctypes.c_double),
+                ("guide_share", ctypes.c_double), ("flip_x", ctypes.c_int32), ("flip_y", ctypes.c_int32),
+                ("has_aim", ctypes.c_int32), ("pad1", ctypes.c_int32), ("aim_center", ctypes.c_double * 3),
+                ("aim_normal", ctypes.c_double * 3), ("aim_radius", ctypes.c_double), ("aim_share", ctypes.c_double),
+                ("focus_center", ctypes.c_double * 3), ("focus_radius", ctypes.c_double),
+                ("focus_share", ctypes.c_double)]
 
 
 class SceneDesc(ctypes.Structure):

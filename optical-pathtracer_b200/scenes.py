@@ -179,20 +179,42 @@ class SceneBuilder:
         self.env.sky_model = A.SKY_UNIFORM
         self.env.sky_radiance = self.spectrum_constant(radiance)
 
-    def observer(self, width, height, position, look_at, up=(0, 0, 1), fov_y_deg=40.0, pixel_sigma=0.0, region=0):
-        self.detector = A.Detector(A.DETECTOR_OBSERVER, width, height, region, (ctypes.c_double * 3)(*position),
-                                   (ctypes.c_double * 3)(*look_at), (ctypes.c_double * 3)(*up),
-                                   math.radians(fov_y_deg), float(pixel_sigma), 0, 0, 0.0, 0.0)
+    def observer(self, width, height, position, look_at, up=(0, 0, 1), fov_y_deg=40.0, pixel_sigma=0.0, region=0,
+                 pupil=0.0, focus=0.0, guide=None):
+        """An IdealObserver; pupil > 0 makes it a thin lens focused at `focus` (0: at infinity);
+        guide = (centre, radius, share) draws that share of the pupil samples from a disk."""
+        d = A.Detector(A.DETECTOR_OBSERVER, width, height, region, (ctypes.c_double * 3)(*position),
+                       (ctypes.c_double * 3)(*look_at), (ctypes.c_double * 3)(*up),
+                       math.radians(fov_y_deg), float(pixel_sigma), 0, 0, 0.0, 0.0)
+        d.pupil_radius, d.focus_distance = float(pupil), float(focus)
+        if guide is not None:
+            d.guide_center = (ctypes.c_double * 3)(*guide[0])
+            d.guide_radius, d.guide_share = float(guide[1]), float(guide[2])
+        self.detector = d
 
     def frame_origin(self, point):
         """Put the origin of the device's camera-relative FP32 frame at `point` (default: the
         observer's position)."""
         self.origin = tuple(float(x) for x in point)
 
-    def sensor(self, width, height, boundary, half_x, half_y, pixel_sigma=0.0):
-        self.detector = A.Detector(A.DETECTOR_SENSOR, width, height, A.REGION_OUTSIDE, (ctypes.c_double * 3)(),
-                                   (ctypes.c_double * 3)(), (ctypes.c_double * 3)(), 0.0, float(pixel_sigma),
-                                   boundary, 0, float(half_x), float(half_y))
+    def sensor(self, width, height, boundary, half_x, half_y, pixel_sigma=0.0, flip=(False, False), aim=None,
+               focus=None):
+        """A SurfaceSensor; aim = (centre, normal, radius, share) samples that share of the directions
+        toward a disk, focus = (centre, radius, share) a share of those toward a second disk."""
+        d = A.Detector(A.DETECTOR_SENSOR, width, height, A.REGION_OUTSIDE, (ctypes.c_double * 3)(),
+                       (ctypes.c_double * 3)(), (ctypes.c_double * 3)(), 0.0, float(pixel_sigma),
+                       boundary, 0, float(half_x), float(half_y))
+        d.flip_x, d.flip_y = int(flip[0]), int(flip[1])
+        if aim is not None:
+            d.has_aim = 1
+            d.aim_center = (ctypes.c_double * 3)(*aim[0])
+            n = np.asarray(aim[1], float)
+            d.aim_normal = (ctypes.c_double * 3)(*(n / np.linalg.norm(n)))
+            d.aim_radius, d.aim_share = float(aim[2]), float(aim[3])
+            if focus is not None:
+                d.focus_center = (ctypes.c_double * 3)(*focus[0])
+                d.focus_radius, d.focus_share = float(focus[1]), float(focus[2])
+        self.detector = d
 
     # ---------------------------------------------------------- the description
     def desc(self):

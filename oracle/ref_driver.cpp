@@ -175,6 +175,10 @@ std::unique_ptr<RefScene> buildScene(const owec_scene_desc& d) {
         if (o.conductor_n >= 0) so.conductor.n = makeSpectrum(d, o.conductor_n);
         if (o.conductor_k >= 0) so.conductor.k = makeSpectrum(d, o.conductor_k);
         if (so.type == SurfaceType::Detector) so.detector = 0;
+        // a diffuse measurement screen: the sensor's own boundary with Lambertian optics
+        if (so.type == SurfaceType::Diffuse && d.detector.kind == OWEC_DETECTOR_SENSOR &&
+            d.detector.boundary < d.n_boundaries && d.boundaries[d.detector.boundary].optics == i)
+            so.detector = 0;
         opticsMap[i] = w.addOptics(so);
     }
     std::vector<int> emissionMap(d.n_emissions);
@@ -214,6 +218,8 @@ std::unique_ptr<RefScene> buildScene(const owec_scene_desc& d) {
         eye->up = {dd.up[0], dd.up[1], dd.up[2]};
         eye->fovY = dd.fov_y;
         eye->pixelSigma = dd.pixel_sigma;
+        eye->pupilRadius = dd.pupil_radius;
+        eye->focusDistance = dd.focus_distance > 0 && std::isfinite(dd.focus_distance) ? dd.focus_distance : Inf;
         rs->scene.detectors.push_back(std::move(eye));
     } else {
         auto s = std::make_unique<SurfaceSensor>();
@@ -224,11 +230,28 @@ std::unique_ptr<RefScene> buildScene(const owec_scene_desc& d) {
         s->halfX = dd.half_x;
         s->halfY = dd.half_y;
         s->pixelSigma = dd.pixel_sigma;
+        s->flipX = dd.flip_x != 0;
+        s->flipY = dd.flip_y != 0;
+        s->hasAim = dd.has_aim != 0;
+        s->aimCenter = {dd.aim_center[0], dd.aim_center[1], dd.aim_center[2]};
+        s->aimNormal = {dd.aim_normal[0], dd.aim_normal[1], dd.aim_normal[2]};
+        s->aimRadius = dd.aim_radius;
+        s->aimShare = dd.aim_share;
+        s->focusCenter = {dd.focus_center[0], dd.focus_center[1], dd.focus_center[2]};
+        s->focusRadius = dd.focus_radius;
+        s->focusShare = dd.focus_share;
         rs->scene.detectors.push_back(std::move(s));
     }
     rs->scene.build();
     if (dd.kind == OWEC_DETECTOR_OBSERVER && dd.region != OWEC_REGION_OUTSIDE)
         rs->scene.detectors[0]->region = rs->regionMap.at(dd.region);
+    if (dd.kind == OWEC_DETECTOR_OBSERVER && dd.guide_radius > 0) {
+        // a pupil guide as IdealObserver::prepare would set for an instrument's exit pupil
+        auto* eye = static_cast<IdealObserver*>(rs->scene.detectors[0].get());
+        eye->guide.center = {dd.guide_center[0], dd.guide_center[1], dd.guide_center[2]};
+        eye->guide.radius = dd.guide_radius;
+        eye->guide.share = dd.guide_share;
+    }
     return rs;
 }
 
