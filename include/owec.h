@@ -91,14 +91,30 @@ typedef struct owec_medium {
 #define OWEC_SURF_ABSORBER 5
 #define OWEC_SURF_DETECTOR 6
 
+/* Procedural textures of a Lambertian surface's albedo (Texture::Kind, src/owe/scene/world.hpp:29-49,
+ * and their patterns, src/owe/core/shared/textures.hpp): mixing weights of the spectra a (the
+ * optics' reflectance), b and c at the boundary-local hit point and normal. */
+#define OWEC_TEXTURE_NONE 0
+#define OWEC_TEXTURE_CHECKER 1
+#define OWEC_TEXTURE_NOISE 2
+#define OWEC_TEXTURE_RINGS 3
+#define OWEC_TEXTURE_TERRAIN 4
+#define OWEC_TEXTURE_BANDS 5
+#define OWEC_TEXTURE_RADIAL 6
+#define OWEC_TEXTURE_MARBLE 7
+
 typedef struct owec_optics {
     int32_t type;
     int32_t back_absorbs;  /* thin opaque sheet with a black back */
     int32_t reflectance;   /* spectrum index (diffuse albedo / mirror reflectance / conductor tint), -1 = 1 */
     int32_t conductor_n;   /* spectrum index of the metal's n, -1 = none */
     int32_t conductor_k;   /* spectrum index of the metal's k, -1 = none */
-    int32_t pad0;
+    int32_t texture;       /* OWEC_TEXTURE_* of a diffuse albedo */
     double roughness;      /* GGX alpha; below 1e-3 the surface is smooth (a delta) */
+    int32_t texture_b;     /* spectrum indices of the texture's second and third spectra */
+    int32_t texture_c;
+    double texture_scale;  /* cell or feature size, metres */
+    double texture_param;  /* terrain: snow line height; rings, bands, marble: turbulence */
 } owec_optics;
 
 typedef struct owec_emission {

@@ -99,7 +99,8 @@ struct DeviceScene {
     const DBoundary* boundaries;
     const DLight* lights;
     const double* shapeData;  // the shapes' data, addressed by DBoundary::dataOffset
-    int32_t fullShapes;       // 1: shapes beyond spheres, conic sags, plain apertures and cylinders
+    int32_t fullFeatures;     // 1: shapes beyond spheres, conic sags, plain apertures and cylinders, or
+                              // textured materials (the kernels' Full instantiations)
     uint32_t nRegions, nBoundaries, nLights, nMedia;
     const WideNode* nodes;
     const PrimRec* prims;

@@ -380,6 +380,11 @@ void validateDesc(const owec_scene_desc& d) {
         const owec_optics& o = d.optics[i];
         require(o.type >= OWEC_SURF_NULL && o.type <= OWEC_SURF_DETECTOR, "unknown surface type");
         require(specOk(o.reflectance) && specOk(o.conductor_n) && specOk(o.conductor_k), "optics spectrum out of range");
+        require(o.texture >= OWEC_TEXTURE_NONE && o.texture <= OWEC_TEXTURE_MARBLE, "unknown texture");
+        require(o.texture == OWEC_TEXTURE_NONE ||
+                    (o.type == OWEC_SURF_DIFFUSE && o.reflectance >= 0 && o.texture_b >= 0 && specOk(o.texture_b) &&
+                     o.texture_c >= 0 && specOk(o.texture_c) && o.texture_scale > 0),
+                "a texture needs a Lambertian surface, its three spectra and a positive scale");
     }
     for (uint32_t i = 0; i < d.n_emissions; ++i) require(specOk(d.emissions[i].radiance) && d.emissions[i].radiance >= 0,
                                                           "emission needs a radiance spectrum");
@@ -747,14 +752,16 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
     ds.boundaries = c.dBoundaries.get();
     ds.lights = c.dLights.get();
     ds.shapeData = c.dShapeData.get();
-    ds.fullShapes = 0;
+    ds.fullFeatures = 0;
     for (uint32_t i = 0; i < d.n_boundaries; ++i) {
         const owec_boundary& b = d.boundaries[i];
         if (b.shape == OWEC_SHAPE_CONE || b.shape == OWEC_SHAPE_TORUS || b.shape == OWEC_SHAPE_ROUND_WALL ||
             b.shape == OWEC_SHAPE_DOME || (b.shape == OWEC_SHAPE_SAG && b.data_count > 0) ||
             (b.shape == OWEC_SHAPE_PLANE && int(b.params[0]) == OWEC_APERTURE_DISK_HOLE))
-            ds.fullShapes = 1;
+            ds.fullFeatures = 1;
     }
+    for (uint32_t i = 0; i < d.n_optics; ++i)
+        if (d.optics[i].texture != OWEC_TEXTURE_NONE) ds.fullFeatures = 1;
     ds.nRegions = d.n_regions;
     ds.nBoundaries = d.n_boundaries;
     ds.nLights = uint32_t(c.lights.size());

@@ -444,7 +444,9 @@ __global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, Particl
                         }
                     }
                     if (op.type != OWEC_SURF_DETECTOR && op.type != OWEC_SURF_ABSORBER) {
-                        const Interface<R> it = makeInterface(sc, bd, g.n, R(sp.lambda[0]), R(P.fresnelFloor));
+                        V3<double> texW;
+                        const V3<double>* tex = hitTexture<Full>(sc, bd, g.pLocal, g.nLocal, texW);
+                        const Interface<R> it = makeInterface(sc, bd, g.n, R(sp.lambda[0]), R(P.fresnelFloor), tex);
                         if (observer && !isDeltaOptics<R>(op) && linkObserver(sc, P, gp, rng, k)) {
                             const V3<R> wo(k.dir);
                             bool any = false;
@@ -452,7 +454,7 @@ __global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, Particl
                                 if (sp.beta[j] == R(0)) continue;
                                 R pdf;
                                 const Interface<R> itj =
-                                    j == 0 ? it : makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor));
+                                    j == 0 ? it : makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor), tex);
                                 value[j] = sp.beta[j] * evalScatter(sc, itj, d, wo, false, pdf);
                                 any = any || value[j] != R(0);
                             }
@@ -471,7 +473,7 @@ __global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, Particl
                             if (op.type == OWEC_SURF_DIELECTRIC) {  // terminateIfDispersive (transport.cpp:216-225)
                                 for (int j = 1; j < NW; ++j) {
                                     if (sp.pdf[j] == 0.f) continue;
-                                    if (isDispersive(it, makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor)))) {
+                                    if (isDispersive(it, makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor), tex))) {
                                         for (int m = 1; m < NW; ++m) { sp.pdf[m] = 0.f; sp.beta[m] = R(0); }
                                         sp.pdf[0] /= float(NW);
                                         break;
@@ -485,7 +487,7 @@ __global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, Particl
                                 sp.beta[0] *= ss.weight;
                                 for (int j = 1; j < NW; ++j) {
                                     if (sp.pdf[j] == 0.f) continue;
-                                    const Interface<R> itj = makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor));
+                                    const Interface<R> itj = makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor), tex);
                                     sp.beta[j] *= secondaryScatterWeight(sc, itj, d, ss, false);
                                 }
                                 if (ss.transmitted) ray.region = other;
@@ -541,7 +543,7 @@ void launchEmit(const DeviceScene& sc, const ParticleParams& P, const PathBuffer
 template <int M>
 void launchParticleEvent(const DeviceScene& sc, const ParticleParams& P, const PathBuffers<ModeR<M>>& pb,
                          const Queues& q, int cur, StatCounters* st, const SplatTarget& film, int grid, cudaStream_t s) {
-    if (sc.fullShapes) kParticleEvent<M, true><<<grid, 128, 0, s>>>(sc, P, pb, q, cur, st, film);
+    if (sc.fullFeatures) kParticleEvent<M, true><<<grid, 128, 0, s>>>(sc, P, pb, q, cur, st, film);
     else kParticleEvent<M, false><<<grid, 128, 0, s>>>(sc, P, pb, q, cur, st, film);
 }
 void launchResolveSplats(const unsigned long long* splat, uint32_t nPixels, double scale, double* xyz, cudaStream_t s) {

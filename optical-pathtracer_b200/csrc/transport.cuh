@@ -6,6 +6,7 @@
 
 #include "optics.cuh"
 #include "path_state.cuh"
+#include "textures.cuh"
 
 namespace owec {
 
@@ -330,10 +331,12 @@ __device__ R lightSampleLe(const DeviceScene& sc, const LightSampleD& ls, R lamb
 }
 
 // ------------------------------------------------------------------ interfaces
-// The interface of a boundary at one wavelength (Tracer::makeInterface, transport.cpp:168-185).
+// The interface of a boundary at one wavelength (Tracer::makeInterface, transport.cpp:168-185). tex:
+// the hit's texture weights when its Lambertian albedo is textured (surfaceAlbedo,
+// src/owe/transport/scattering.cpp:190-195), else null.
 template <class R, bool Lambertian = false>
 __device__ __forceinline__ Interface<R> makeInterface(const DeviceScene& sc, const DBoundary& bd, const V3<R>& n, R lambda,
-                                                      R fresnelFloor) {
+                                                      R fresnelFloor, const V3<double>* tex = nullptr) {
     Interface<R> it;
     it.o = sc.optics[bd.optics];
     it.n = n;
@@ -351,7 +354,28 @@ __device__ __forceinline__ Interface<R> makeInterface(const DeviceScene& sc, con
     it.lambda = lambda;
     it.fresnelFloor = fresnelFloor;
     it.albedo = it.o.reflectance >= 0 ? evalSpectrum(sc, it.o.reflectance, lambda) : R(1);
+    if (tex && it.o.type == OWEC_SURF_DIFFUSE) {
+        R a = it.albedo * R(tex->x);
+        if (tex->y != 0) a += R(tex->y) * evalSpectrum(sc, it.o.texture_b, lambda);
+        if (tex->z != 0) a += R(tex->z) * evalSpectrum(sc, it.o.texture_c, lambda);
+        it.albedo = a;
+    }
     return it;
+}
+
+// The texture weights of a hit on boundary bd at local point pl with local normal nl, or null when
+// its optics are not textured (or the kernel is the lean instantiation: Full false).
+template <bool Full>
+__device__ __forceinline__ const V3<double>* hitTexture(const DeviceScene& sc, const DBoundary& bd, const V3<double>& pl,
+                                                        const V3<double>& nl, V3<double>& storage) {
+    if constexpr (Full) {
+        const owec_optics& o = sc.optics[bd.optics];
+        if (o.texture == OWEC_TEXTURE_NONE || o.type != OWEC_SURF_DIFFUSE) return nullptr;
+        storage = textureWeights(o.texture, o.texture_scale, o.texture_param, pl, nl);
+        return &storage;
+    } else {
+        return nullptr;
+    }
 }
 
 // Russian roulette against the throughput (CameraPath::survives, transport.cpp:369-374).

@@ -273,6 +273,16 @@ __device__ void walkOne(const DeviceScene& sc, const WalkParams& P, uint64_t wal
         it.lambda = R(lambda);
         it.fresnelFloor = R(0);
         it.albedo = op.reflectance >= 0 ? evalSpectrum(sc, op.reflectance, R(lambda)) : R(1);
+        {
+            V3<double> texW;
+            const V3<double>* tex = hitTexture<Full>(sc, bd, gp.pLocal, gp.nLocal, texW);
+            if (tex) {
+                R a = it.albedo * R(tex->x);
+                if (tex->y != 0) a += R(tex->y) * evalSpectrum(sc, op.texture_b, R(lambda));
+                if (tex->z != 0) a += R(tex->z) * evalSpectrum(sc, op.texture_c, R(lambda));
+                it.albedo = a;
+            }
+        }
         ScatterSample<R> ss;
         bool ok;
         if (w.mode == OWEC_WALK_PRIMARY_TRANSMISSION && op.type == OWEC_SURF_DIELECTRIC) {
@@ -363,7 +373,7 @@ template <int M, bool ADJ>
 void walkKernel(const DeviceScene& sc, const WalkParams& P, unsigned long long* bins, unsigned long long* stats,
                 const double* g, double* dH, int grid, cudaStream_t s) {
     const size_t smem = traversalSharedBytes(128);
-    if (sc.fullShapes) kWalk<M, ADJ, true><<<grid, 128, smem, s>>>(sc, P, bins, stats, g, dH);
+    if (sc.fullFeatures) kWalk<M, ADJ, true><<<grid, 128, smem, s>>>(sc, P, bins, stats, g, dH);
     else kWalk<M, ADJ, false><<<grid, 128, smem, s>>>(sc, P, bins, stats, g, dH);
 }
 

@@ -571,14 +571,16 @@ __global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SH
                    int(aux.depth) < pp.maxDepth) {
             // scatterAtSurface (transport.cpp:437-471)
             const R hero = R(sp.lambda[0]);
-            const Interface<R> it = makeInterface<R, Simple>(sc, bd, g.n, hero, R(pp.fresnelFloor));
+            V3<double> texW;
+            const V3<double>* tex = hitTexture<Full>(sc, bd, g.pLocal, g.nLocal, texW);
+            const Interface<R> it = makeInterface<R, Simple>(sc, bd, g.n, hero, R(pp.fresnelFloor), tex);
             if (!Simple && o.type == OWEC_SURF_DIELECTRIC) {  // terminateIfDispersive
                 bool alive2 = false;
                 for (int j = 1; j < NW; ++j) alive2 = alive2 || sp.pdf[j] != 0.f;
                 if (alive2) {
                     for (int j = 1; j < NW; ++j) {
                         if (sp.pdf[j] == 0.f) continue;
-                        const Interface<R> it2 = makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(pp.fresnelFloor));
+                        const Interface<R> it2 = makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(pp.fresnelFloor), tex);
                         if (isDispersive(it, it2)) {
                             for (int m = 1; m < NW; ++m) sp.pdf[m] = 0.f;
                             sp.pdf[0] /= float(NW);
@@ -602,7 +604,7 @@ __global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SH
                             if (sp.pdf[j] == 0.f) continue;
                             R pdf;
                             const Interface<R> itj =
-                                j == 0 ? it : makeInterface<R, Simple>(sc, bd, g.n, R(sp.lambda[j]), R(pp.fresnelFloor));
+                                j == 0 ? it : makeInterface<R, Simple>(sc, bd, g.n, R(sp.lambda[j]), R(pp.fresnelFloor), tex);
                             fN[j] = evalScatter(sc, itj, d, wi, true, pdf);
                             if (j == 0) pdfS = pdf;
                             if (fN[j] != R(0)) fZero = false;
@@ -623,7 +625,7 @@ __global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SH
                 sp.beta[0] *= s.weight;
                 for (int j = 1; j < NW; ++j) {
                     if (sp.pdf[j] == 0.f) continue;
-                    const Interface<R> itj = makeInterface<R, Simple>(sc, bd, g.n, R(sp.lambda[j]), R(pp.fresnelFloor));
+                    const Interface<R> itj = makeInterface<R, Simple>(sc, bd, g.n, R(sp.lambda[j]), R(pp.fresnelFloor), tex);
                     sp.beta[j] *= secondaryScatterWeight(sc, itj, d, s, true);
                 }
                 if (s.transmitted) ray.region = other;
@@ -1049,7 +1051,7 @@ template <int M>
 void launchIntersect(const DeviceScene& sc, const PathBuffers<RT<M>>& pb, const Queues& q, int cur, StatCounters* st,
                      uint32_t* fetch, int grid, cudaStream_t s) {
     const size_t smem = traversalSharedBytes(128);
-    if (sc.fullShapes) {
+    if (sc.fullFeatures) {
         if (sc.travCounters) kIntersect<M, true, true><<<grid, 128, smem, s>>>(sc, pb, q, cur, st, fetch);
         else kIntersect<M, false, true><<<grid, 128, smem, s>>>(sc, pb, q, cur, st, fetch);
     } else {
@@ -1065,7 +1067,7 @@ void launchMedium(const DeviceScene& sc, const PassParams& pp, const PathBuffers
 template <int M>
 void launchSurface(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q, int cur,
                    StatCounters* st, int grid, cudaStream_t s) {
-    if (sc.fullShapes) {
+    if (sc.fullFeatures) {
         kSurface<M, true, true><<<grid, 128, 0, s>>>(sc, pp, pb, q, cur, st);
         kSurface<M, false, true><<<grid, 128, 0, s>>>(sc, pp, pb, q, cur, st);
     } else {
@@ -1089,7 +1091,7 @@ void shadowKernelsOf(const DeviceScene& sc, const PassParams& pp, const PathBuff
 template <int M, bool Splat>
 void shadowKernels(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q,
                    StatCounters* st, uint32_t* fetch, uint8_t* vis, const SplatTarget& film, int grid, cudaStream_t s) {
-    if (sc.fullShapes) {
+    if (sc.fullFeatures) {
         if (sc.travCounters) shadowKernelsOf<M, Splat, true, true>(sc, pp, pb, q, st, fetch, vis, film, grid, s);
         else shadowKernelsOf<M, Splat, false, true>(sc, pp, pb, q, st, fetch, vis, film, grid, s);
     } else {
@@ -1116,12 +1118,12 @@ void launchFilm(const DeviceScene& sc, const PassParams& pp, const PathBuffers<R
 template <int M>
 void launchCastRays(const DeviceScene& sc, uint64_t n, const double* o, const double* d, uint32_t* b, uint32_t* p,
                     double* t, int grid, cudaStream_t s) {
-    if (sc.fullShapes) kCastRays<M, true><<<grid, 128, traversalSharedBytes(128), s>>>(sc, n, o, d, b, p, t);
+    if (sc.fullFeatures) kCastRays<M, true><<<grid, 128, traversalSharedBytes(128), s>>>(sc, n, o, d, b, p, t);
     else kCastRays<M, false><<<grid, 128, traversalSharedBytes(128), s>>>(sc, n, o, d, b, p, t);
 }
 void launchCastRaysF(const DeviceScene& sc, uint64_t n, const float* o, const float* d, uint32_t* b, uint32_t* p,
                      float* t, int grid, cudaStream_t s) {
-    if (sc.fullShapes) kCastRaysF<true><<<grid, 128, traversalSharedBytes(128), s>>>(sc, n, o, d, b, p, t);
+    if (sc.fullFeatures) kCastRaysF<true><<<grid, 128, traversalSharedBytes(128), s>>>(sc, n, o, d, b, p, t);
     else kCastRaysF<false><<<grid, 128, traversalSharedBytes(128), s>>>(sc, n, o, d, b, p, t);
 }
 void launchResolve(const double* film, const double* comp, const double* samples, uint32_t nPixels, double* xyz,

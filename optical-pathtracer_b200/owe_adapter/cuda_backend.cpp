@@ -6,7 +6,7 @@
 // rule allows it core/, scene/, render/ and backends/cuda/ (not transport/). It flattens the world
 // model into owec_scene_desc: media, regions, optics, emitters, boundaries with their rigid frames
 // and shape data, the sun and sky, and the detector. Scenes using features the CUDA backend does not
-// implement (textures, environment maps, wave surfaces, materials' aim guides) are refused with
+// implement (image textures, environment maps, wave surfaces, materials' aim guides) are refused with
 // std::runtime_error, as Backend::createRenderer does for unsupported settings
 // (src/owe/render/backend.hpp:44).
 #include <cmath>
@@ -125,9 +125,9 @@ std::unique_ptr<Flat> flatten(const Scene& sc, int detectorIndex) {
     }
     for (const Region& r : w.regions()) f->regionMedium.push_back(r.medium);
     for (const SurfaceOptics& so : w.optics()) {
-        if (so.texture.kind != Texture::Kind::None || so.sampleAimShare > 0 || !so.roughnessMap.empty() ||
+        if (so.texture.kind == Texture::Kind::Image || so.sampleAimShare > 0 || !so.roughnessMap.empty() ||
             so.reliefDepth != 0 || so.normalImage.image || so.roughnessImage.image)
-            throw std::runtime_error("material '" + so.name + "' uses textures, maps or aim guides, which the cuda backend does not render");
+            throw std::runtime_error("material '" + so.name + "' uses image textures, maps or aim guides, which the cuda backend does not render");
         if (so.type == SurfaceType::StainedGlass) throw std::runtime_error("stained glass is not rendered by the cuda backend");
         owec_optics o{};
         o.type = int32_t(so.type);
@@ -136,6 +136,16 @@ std::unique_ptr<Flat> flatten(const Scene& sc, int detectorIndex) {
         o.reflectance = f->spectrum(so.reflectance);
         o.conductor_n = so.type == SurfaceType::Conductor ? f->spectrum(so.conductor.n) : -1;
         o.conductor_k = so.type == SurfaceType::Conductor ? f->spectrum(so.conductor.k) : -1;
+        if (so.texture.kind != Texture::Kind::None && so.type == SurfaceType::Diffuse) {
+            // only a Lambertian albedo reads a texture, whose spectrum a takes the reflectance's place
+            // (surfaceAlbedo, scattering.cpp:190-195)
+            o.texture = int32_t(so.texture.kind);
+            o.reflectance = f->spectrum(so.texture.a);
+            o.texture_b = f->spectrum(so.texture.b);
+            o.texture_c = f->spectrum(so.texture.c);
+            o.texture_scale = so.texture.scale;
+            o.texture_param = so.texture.param;
+        }
         f->optics.push_back(o);
     }
     for (const Emission& e : w.emissions()) {

@@ -47,8 +47,13 @@ class Medium(ctypes.Structure):
 
 class Optics(ctypes.Structure):
     _fields_ = [("type", ctypes.c_int32), ("back_absorbs", ctypes.c_int32), ("reflectance", ctypes.c_int32),
-                ("conductor_n", ctypes.c_int32), ("conductor_k", ctypes.c_int32), ("pad0", ctypes.c_int32),
-                ("roughness", ctypes.c_double)]
+                ("conductor_n", ctypes.c_int32), ("conductor_k", ctypes.c_int32), ("texture", ctypes.c_int32),
+                ("roughness", ctypes.c_double), ("texture_b", ctypes.c_int32), ("texture_c", ctypes.c_int32),
+                ("texture_scale", ctypes.c_double), ("texture_param", ctypes.c_double)]
+
+
+TEXTURE_NONE, TEXTURE_CHECKER, TEXTURE_NOISE, TEXTURE_RINGS, TEXTURE_TERRAIN, TEXTURE_BANDS, TEXTURE_RADIAL, \
+    TEXTURE_MARBLE = range(8)
 
 
 class Emission(ctypes.Structure):

@@ -115,6 +115,14 @@ class SceneBuilder:
     def diffuse(self, albedo, **kw):
         return self.optics_(A.SURF_DIFFUSE, self.spectrum_constant(albedo), **kw)
 
+    def textured(self, kind, a, b, c=0.9, scale=1.0, param=0.0, **kw):
+        """A Lambertian surface whose albedo mixes the constants a, b, c by a procedural texture."""
+        o = self.optics_(A.SURF_DIFFUSE, self.spectrum_constant(a), **kw)
+        opt = self.optics[o]
+        opt.texture, opt.texture_b, opt.texture_c = kind, self.spectrum_constant(b), self.spectrum_constant(c)
+        opt.texture_scale, opt.texture_param = float(scale), float(param)
+        return o
+
     def dielectric(self, roughness=0.0):
         return self.optics_(A.SURF_DIELECTRIC, roughness=roughness)
 
@@ -518,6 +526,24 @@ def shape_gallery(width=48, height=36, sun=True):
         sb.sun((0.4, -0.5, 0.75), 3.0e4)
     sb.uniform_sky(0.4)
     sb.observer(width, height, (0.0, -4.2, 2.6), (0.0, 0.1, 0.3), fov_y_deg=42.0)
+    return sb
+
+
+def texture_gallery(width=64, height=40):
+    """Every procedural texture on Lambertian albedos: a checker floor and six spheres (noise,
+    rings, terrain, bands, radial, marble) under the sun and a uniform sky
+    (src/owe/core/shared/textures.hpp:93-138)."""
+    sb = SceneBuilder()
+    sb.sheet(10.0, 10.0, pose(), sb.textured(A.TEXTURE_CHECKER, 0.8, 0.15, scale=0.4))
+    opaque = sb.medium_opaque()
+    kinds = [(A.TEXTURE_NOISE, 0.15, 0.0), (A.TEXTURE_RINGS, 0.1, 0.8), (A.TEXTURE_TERRAIN, 0.2, 0.25),
+             (A.TEXTURE_BANDS, 0.12, 0.6), (A.TEXTURE_RADIAL, 0.3, 0.0), (A.TEXTURE_MARBLE, 0.25, 0.7)]
+    for i, (kind, scale, param) in enumerate(kinds):
+        x, y = -1.0 + 1.0 * (i % 3), -0.5 + 1.0 * (i // 3)
+        sb.sphere_body(0.35, (x, y, 0.35), opaque, sb.textured(kind, 0.85, 0.1, 0.5, scale=scale, param=param))
+    sb.sun((0.3, -0.4, 0.85), 2.0e4)
+    sb.uniform_sky(0.5)
+    sb.observer(width, height, (0.0, -2.6, 3.2), (0.0, 0.2, 0.2), fov_y_deg=45.0)  # sees no sky
     return sb
 
 

@@ -174,6 +174,14 @@ std::unique_ptr<RefScene> buildScene(const owec_scene_desc& d) {
         so.reflectance = o.reflectance >= 0 ? makeSpectrum(d, o.reflectance) : Spectrum::constant(1.0);
         if (o.conductor_n >= 0) so.conductor.n = makeSpectrum(d, o.conductor_n);
         if (o.conductor_k >= 0) so.conductor.k = makeSpectrum(d, o.conductor_k);
+        if (o.texture != OWEC_TEXTURE_NONE) {
+            so.texture.kind = Texture::Kind(o.texture);
+            so.texture.a = so.reflectance;
+            so.texture.b = makeSpectrum(d, o.texture_b);
+            so.texture.c = makeSpectrum(d, o.texture_c);
+            so.texture.scale = o.texture_scale;
+            so.texture.param = o.texture_param;
+        }
         if (so.type == SurfaceType::Detector) so.detector = 0;
         // a diffuse measurement screen: the sensor's own boundary with Lambertian optics
         if (so.type == SurfaceType::Diffuse && d.detector.kind == OWEC_DETECTOR_SENSOR &&

@@ -79,3 +79,38 @@ def test_shapes_render_like_the_reference(name):
     assert st["device_faults"] == 0 and st["leaks"] == 0, st
     ok, rep = block_z_test(runs_ref, runs_gpu)
     assert ok, rep
+
+
+def test_textures_follow_the_reference_paths():
+    """Procedural albedos (checker, noise, rings, terrain, bands, radial, marble): with one-sample
+    passes the device paths read the CPU paths' albedos at the same points (the same lattice hash
+    and FP64 noise) and make the same decisions."""
+    desc = scenes.texture_gallery().desc()
+    ref = ReferenceEngine(desc)
+    s = A.make_settings(seed=9, max_depth=8, rr_depth=4, wavelength_mode=A.WAVELENGTHS_UNIFORM1)
+    img_ref, _ = ref.render(s, 1, passes=1)
+    with _ctx(desc, s) as c:
+        c.run_pass(1)
+        img_gpu = c.resolve()[0]
+    a, b = img_ref[:, :, 1].ravel(), img_gpu[:, :, 1].ravel()
+    close = np.abs(a - b) <= 1e-4 * np.maximum(np.abs(a), 1e-3)
+    assert close.mean() > 0.97, f"only {close.mean():.3f} of paths agree"
+
+
+@pytest.mark.parametrize("integrator", ["path", "light"])
+def test_textures_render_like_the_reference(integrator):
+    desc = scenes.texture_gallery(48, 30).desc()
+    ref = ReferenceEngine(desc)
+    runs_ref, runs_gpu = [], []
+    with _ctx(desc) as c:
+        for k in range(12):
+            img, _, _ = ref.render_backend(A.make_settings(seed=300 + k), 64)
+            runs_ref.append(img)
+            c.set_settings(A.make_settings(seed=400 + k, integrator=integrator))
+            c.reset_film()
+            c.run_pass(64 if integrator == "path" else 512)
+            runs_gpu.append(c.resolve()[0])
+        assert c.stats()["device_faults"] == 0
+    save_artifact(f"textures_{integrator}", ref=np.array(runs_ref), gpu=np.array(runs_gpu))
+    ok, rep = block_z_test(runs_ref, runs_gpu)
+    assert ok, rep
