@@ -172,7 +172,10 @@ typedef struct owec_mesh {
 } owec_mesh;
 
 #define OWEC_SKY_NONE 0
-#define OWEC_SKY_UNIFORM 1
+#define OWEC_SKY_UNIFORM 1   /* sky_radiance in every direction */
+#define OWEC_SKY_GRADIENT 2  /* Environment::sky's gradient (src/owe/scene/world.cpp:60-65): below the
+                              * horizon sky_ground, above it horizon (1 - t) + zenith t, t = cos^0.45
+                              * from sky_up; sky_radiance is the zenith */
 
 typedef struct owec_environment {
     int32_t sky_model;
@@ -182,6 +185,9 @@ typedef struct owec_environment {
     double sun_dir[3];        /* unit vector toward the sun */
     double sun_angular_radius;/* radians; the reference default is 0.2665 degrees */
     double sun_nee_share;     /* fraction of NEE light selections given to the sun (0 = by power) */
+    int32_t sky_horizon;      /* OWEC_SKY_GRADIENT: spectrum indices of the horizon and the ground */
+    int32_t sky_ground;
+    double sky_up[3];         /* OWEC_SKY_GRADIENT: the zenith direction */
 } owec_environment;
 
 #define OWEC_DETECTOR_OBSERVER 0 /* IdealObserver: pinhole or thin lens (src/owe/scene/detector.hpp:75-123) */

@@ -90,6 +90,10 @@ struct alignas(16) WideNode {
 static_assert(sizeof(WideNode) == 80, "wide node must stay 80 bytes");
 
 struct DeviceScene {
+    // This description's own copy in device memory: the out-of-line traversal functions read the
+    // scene through it, so that a kernel need not copy its by-value scene parameter to local memory
+    // to pass its address.
+    const DeviceScene* self;
     const owec_spectrum* spectra;
     const double* table;
     const owec_medium* media;
@@ -107,7 +111,9 @@ struct DeviceScene {
     const PrimRec64* prims64;
     uint32_t nNodes, nPrims;
     // environment
-    int32_t skyModel, skySpectrum;
+    int32_t skyModel, skySpectrum;      // skySpectrum: the uniform sky, or the gradient's zenith
+    int32_t skyHorizon, skyGround;      // the gradient's horizon and ground spectra
+    double skyUp[3];
     int32_t hasSun, sunSpectrum;
     double sunDir[3];
     double sunCosMax, sunSolidAngle;

@@ -266,6 +266,7 @@ struct owec_ctx {
     uint32_t nTriangles = 0, nPrims = 0;
     bool hasNull = false;
     DeviceScene ds{};
+    DBuf<DeviceScene> dScene;  // ds's copy on the device (DeviceScene::self), allocated when the context opens
     // particles: the sky's share of the emitted power and the disc distant light leaves from
     double pSky = 0, discRadius = 1, discCentre[3] = {0, 0, 0};
 
@@ -458,7 +459,12 @@ void validateDesc(const owec_scene_desc& d) {
         require(det.pupil_radius >= 0 && !(det.focus_distance < 0) && det.guide_radius >= 0 && det.guide_share >= 0 &&
                     det.guide_share < 1, "observer: pupil, focus or guide out of range");
     }
-    require(d.env.sky_model == OWEC_SKY_NONE || d.env.sky_model == OWEC_SKY_UNIFORM, "unknown sky model");
+    require(d.env.sky_model == OWEC_SKY_NONE || d.env.sky_model == OWEC_SKY_UNIFORM || d.env.sky_model == OWEC_SKY_GRADIENT,
+            "unknown sky model");
+    require(d.env.sky_model != OWEC_SKY_GRADIENT ||
+                (d.env.sky_radiance >= 0 && d.env.sky_horizon >= 0 && specOk(d.env.sky_horizon) && d.env.sky_ground >= 0 &&
+                 specOk(d.env.sky_ground)),
+            "a gradient sky needs its zenith, horizon and ground spectra");
     require(specOk(d.env.sky_radiance) && specOk(d.env.sun_radiance), "environment spectrum out of range");
 }
 
@@ -586,10 +592,31 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
     // uniform sky, world.cpp:352-368: its mean over 400..700 nm, times pi R^2 4 pi) and the disc the
     // sun and the sky shine from, about the scene's centre.
     double skyPower = 0;
-    if (d.env.sky_model == OWEC_SKY_UNIFORM && d.env.sky_radiance >= 0) {
-        double y = 0;
-        for (double l = 400; l <= 700; l += 50) y += evalSpectrumHost(d, d.env.sky_radiance, l);
-        skyPower = std::max(0.0, y / 7) * kPi * sceneRadius * sceneRadius * 4 * kPi;
+    if (d.env.sky_model != OWEC_SKY_NONE && d.env.sky_radiance >= 0) {
+        // the sky's mean over 16 x 32 directions and 400..700 nm (computeEnvironmentPower)
+        double upv[3] = {d.env.sky_up[0], d.env.sky_up[1], d.env.sky_up[2]};
+        const double ul = std::sqrt(upv[0] * upv[0] + upv[1] * upv[1] + upv[2] * upv[2]);
+        for (int k = 0; k < 3; ++k) upv[k] = ul > 0 ? upv[k] / ul : (k == 2 ? 1.0 : 0.0);
+        auto sky = [&](const double dir[3], double l) {
+            if (d.env.sky_model == OWEC_SKY_UNIFORM) return evalSpectrumHost(d, d.env.sky_radiance, l);
+            const double c = dir[0] * upv[0] + dir[1] * upv[1] + dir[2] * upv[2];
+            if (c < 0) return evalSpectrumHost(d, d.env.sky_ground, l);
+            const double t = std::pow(c, 0.45);
+            return evalSpectrumHost(d, d.env.sky_horizon, l) * (1 - t) + evalSpectrumHost(d, d.env.sky_radiance, l) * t;
+        };
+        double sum = 0;
+        int n = 0;
+        for (int i = 0; i < 16; ++i)
+            for (int j = 0; j < 32; ++j) {
+                const double z = 1 - 2 * (i + 0.5) / 16, r = std::sqrt(std::max(0.0, 1 - z * z));
+                const double phi = 2 * kPi * (j + 0.5) / 32;
+                const double dir[3] = {r * std::cos(phi), r * std::sin(phi), z};
+                double y = 0;
+                for (double l = 400; l <= 700; l += 50) y += sky(dir, l);
+                sum += y / 7;
+                ++n;
+            }
+        skyPower = std::max(0.0, sum / n) * kPi * sceneRadius * sceneRadius * 4 * kPi;
     }
     const double emitted = skyPower + (c.lights.empty() ? 0.0 : total);
     c.pSky = emitted > 0 ? skyPower / emitted : 0;
@@ -768,6 +795,13 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
     ds.nMedia = d.n_media;
     ds.skyModel = d.env.sky_model;
     ds.skySpectrum = d.env.sky_radiance;
+    ds.skyHorizon = d.env.sky_horizon;
+    ds.skyGround = d.env.sky_ground;
+    {
+        const double* u = d.env.sky_up;
+        double ul = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        for (int k = 0; k < 3; ++k) ds.skyUp[k] = ul > 0 ? u[k] / ul : (k == 2 ? 1.0 : 0.0);
+    }
     ds.hasSun = d.env.has_sun;
     ds.sunSpectrum = d.env.sun_radiance;
     double sl = std::sqrt(d.env.sun_dir[0] * d.env.sun_dir[0] + d.env.sun_dir[1] * d.env.sun_dir[1] +
@@ -827,11 +861,20 @@ void ensurePrims64(owec_ctx& c) {
     c.prims64Ready = true;
 }
 
+// Copies the scene description to its device copy, which the out-of-line traversal functions read
+// (DeviceScene::self); every launch follows one. A copy from pageable memory: ds may change as soon
+// as this returns.
+void publishScene(owec_ctx& c) {
+    c.ds.self = c.dScene.get();
+    OWEC_CUDA(cudaMemcpyAsync(c.dScene.get(), &c.ds, sizeof(DeviceScene), cudaMemcpyHostToDevice, c.stream));
+}
+
 void ensureReady(owec_ctx& c) {
     require(c.hasScene, "no scene uploaded", OWEC_E_STATE);
     if (c.bvhDirty) buildBvh(c);
     // FP64 vertices: the traversal's in the FP64 mode, the refined triangle distances in the mixed one
     if (c.settings.precision != OWEC_PRECISION_FP32) ensurePrims64(c);
+    publishScene(c);
 }
 
 void ensureFilm(owec_ctx& c) {
@@ -1142,6 +1185,7 @@ int owec_open(int device, owec_ctx** out) {
         OWEC_CUDA(cudaMallocHost(&c->hostCounts, 8 * sizeof(uint32_t)));
         c->dCounts.resize(8);
         c->dStats.resize(1);
+        c->dScene.resize(1);
         OWEC_CUDA(cudaMemsetAsync(c->dStats.get(), 0, sizeof(StatCounters), c->stream));
         configureKernels();
         OWEC_CUDA(cudaStreamSynchronize(c->stream));
@@ -1619,6 +1663,7 @@ int owec_walk_adjoint_noalloc(owec_ctx* ctx, const owec_walk_desc* w, uint64_t f
         else if (w->source_kind == OWEC_SOURCE_COLLIMATED) measure = kPi * w->extent * w->extent;
         else measure = 4 * w->extent * w->extent;
         const double binArea = (2 * w->half_x / w->width) * (2 * w->half_y / w->height);
+        publishScene(*ctx);  // a copy into the context's own scene buffer: no allocation
         OWEC_CUDA(cudaEventRecord(ctx->passStart, ctx->stream));
         launchWalkAdjoint(ctx->settings.precision, ctx->ds, *w, ctx->boundaries[w->target].toLocal, ctx->hf, first, n,
                           measure / (double(n) * binArea), dG, dDH, st, ctx->numSMs * 8, ctx->stream);

@@ -236,8 +236,7 @@ __global__ void __launch_bounds__(128) kEmit(DeviceScene sc, ParticleParams P, P
         const double w = kPi * Rd * Rd / (sel * pdfDir);
         for (int j = 0; j < NW; ++j) {
             const R lam = R(sp.lambda[j]);
-            const R Le = fromSky ? (sc.skyModel == OWEC_SKY_UNIFORM ? evalSpectrum(sc, sc.skySpectrum, lam) : R(0))
-                                 : evalSpectrum(sc, sc.sunSpectrum, lam);
+            const R Le = fromSky ? skyRadiance(sc, toward, lam) : evalSpectrum(sc, sc.sunSpectrum, lam);
             sp.beta[j] = Le * R(w);
         }
     } else if (live) {

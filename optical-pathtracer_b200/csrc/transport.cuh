@@ -159,6 +159,20 @@ __device__ __forceinline__ double diskAimPdf(const V3<double>& p, const V3<doubl
     return t * t / (fabs(dn) * kPi * radius * radius);
 }
 
+// ------------------------------------------------------------------ sky
+// The sky's radiance toward direction dir at wavelength lambda (Environment::sky,
+// src/owe/scene/world.cpp:56-73): none, uniform, or the gradient from the ground through the
+// horizon to the zenith.
+template <class R>
+__device__ __forceinline__ R skyRadiance(const DeviceScene& sc, const V3<double>& dir, R lambda) {
+    if (sc.skyModel == OWEC_SKY_UNIFORM) return evalSpectrum(sc, sc.skySpectrum, lambda);
+    if (sc.skyModel != OWEC_SKY_GRADIENT) return R(0);
+    const double c = dir.x * sc.skyUp[0] + dir.y * sc.skyUp[1] + dir.z * sc.skyUp[2];
+    if (c < 0) return evalSpectrum(sc, sc.skyGround, lambda);
+    const R t = R(pow(c, 0.45));
+    return evalSpectrum(sc, sc.skyHorizon, lambda) * (R(1) - t) + evalSpectrum(sc, sc.skySpectrum, lambda) * t;
+}
+
 // ------------------------------------------------------------------ emitters
 // The solid-angle density at ref of a point p (normal n) drawn uniformly from an area
 // (areaToSolidAngle, src/owe/core/shared/warps.hpp:103-113); 0 when seen edge-on.

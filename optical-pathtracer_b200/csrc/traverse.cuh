@@ -126,7 +126,7 @@ struct AnalyticResult {
     bool ok;
 };
 template <class T, class R, class Rr, bool Full>
-__device__ __noinline__ AnalyticResult<Rr> analyticHit(const DeviceScene& sc, uint32_t b, V3<double> od, V3<T> d, T best,
+__device__ __noinline__ AnalyticResult<Rr> analyticHit(const DeviceScene* scp, uint32_t b, V3<double> od, V3<T> d, T best,
                                                         uint32_t depB, uint32_t region, T errN) {
     RayQuery<T> q;
     q.od = od;
@@ -139,7 +139,7 @@ __device__ __noinline__ AnalyticResult<Rr> analyticHit(const DeviceScene& sc, ui
     q.errN = errN;
     AnalyticResult<Rr> r;
     r.t = Rr(0);
-    r.ok = analyticCandidate<R, Rr, T, Full>(sc, q, b, best, r.t);
+    r.ok = analyticCandidate<R, Rr, T, Full>(*scp, q, b, best, r.t);
     return r;
 }
 
@@ -390,7 +390,7 @@ struct Traversal {
             hit.t = double(t);
             hit.prim = prim;
         } else {
-            const AnalyticResult<Rr> ar = analyticHit<T, R, Rr, Full>(sc, b, q.od, q.d, best, q.depB, q.region, q.errN);
+            const AnalyticResult<Rr> ar = analyticHit<T, R, Rr, Full>(sc.self, b, q.od, q.d, best, q.depB, q.region, q.errN);
             if (!ar.ok) return false;
             best = T(ar.t);
             hit.t = double(ar.t);
@@ -412,7 +412,8 @@ struct DeepResult {
     uint32_t visits, tests;
 };
 template <class T, class R, class Rr, bool AnyHit, bool Full = false>
-__device__ __noinline__ DeepResult traceRayDeep(const DeviceScene& sc, RayQuery<T> q, HitRec hitIn) {
+__device__ __noinline__ DeepResult traceRayDeep(const DeviceScene* scp, RayQuery<T> q, HitRec hitIn) {
+    const DeviceScene& sc = *scp;
     Traversal<T, R, Rr, AnyHit, LocalStack, true, Full> tr;
     tr.begin(q, nullptr, 0);
     tr.hit = hitIn;
@@ -441,7 +442,7 @@ __device__ __forceinline__ int traceRay(const DeviceScene& sc, const RayQuery<T>
     } while (s == kTraceRunning);
     uint32_t nv = tr.nodeVisits, nt = tr.primTests;
     if (s == kTraceOverflow) {
-        const DeepResult d = traceRayDeep<T, R, Rr, AnyHit, Full>(sc, q, hit);
+        const DeepResult d = traceRayDeep<T, R, Rr, AnyHit, Full>(sc.self, q, hit);
         s = d.status;
         hit = d.hit;
         nv += d.visits;

@@ -296,7 +296,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kIntersect(DeviceScene sc, PathBuffers<RT<
                 if (s == kTraceOverflow) {
                     h.boundary = kNone;
                     h.t = INFINITY;
-                    const DeepResult d = traceRayDeep<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false, Full>(sc, tr.q, h);
+                    const DeepResult d = traceRayDeep<R, typename Mode<M>::Ro, typename Mode<M>::Rr, false, Full>(sc.self, tr.q, h);
                     s = d.status;
                     h = d.hit;
                     nv += d.visits;
@@ -473,7 +473,7 @@ __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kMedium(DeviceSc
                     if (!spec && inSun) w = powerHeuristic(R(aux.prevPdf), R(sc.sunSelectPdf / sc.sunSolidAngle));
                     for (int j = 0; j < NW; ++j) {
                         const R lam = R(sp.lambda[j]);
-                        const R sky = sc.skyModel == OWEC_SKY_UNIFORM ? evalSpectrum(sc, sc.skySpectrum, lam) : R(0);
+                        const R sky = skyRadiance(sc, dd, lam);
                         const R sun = inSun ? evalSpectrum(sc, sc.sunSpectrum, lam) : R(0);
                         sp.L[j] += float(sp.beta[j] * (sky + sun * w));
                     }
@@ -714,7 +714,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
             uint32_t nv = tr.nodeVisits, nt = tr.primTests;
             if (s == kTraceOverflow) {
                 h.boundary = kNone;
-                const DeepResult d = traceRayDeep<R, Ro, Rr, AnyHit, Full>(sc, tr.q, h);
+                const DeepResult d = traceRayDeep<R, Ro, Rr, AnyHit, Full>(sc.self, tr.q, h);
                 s = d.status;
                 h = d.hit;
                 nv += d.visits;
@@ -854,7 +854,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadowVis(DeviceScene sc, PathBuffers<RT<
         if (s == kTraceOverflow) {
             HitRec h = tr.hit;
             h.boundary = kNone;
-            const DeepResult d = traceRayDeep<R, Ro, Rr, true, Full>(sc, tr.q, h);
+            const DeepResult d = traceRayDeep<R, Ro, Rr, true, Full>(sc.self, tr.q, h);
             s = d.status;
             nv += d.visits;
             nt += d.tests;

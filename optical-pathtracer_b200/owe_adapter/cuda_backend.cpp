@@ -245,10 +245,15 @@ std::unique_ptr<Flat> flatten(const Scene& sc, int detectorIndex) {
     owec_scene_desc& d = f->desc;
     d.abi_version = OWEC_ABI_VERSION;
     const Environment& env = w.env;
-    if (env.skyModel != Environment::Sky::None && env.skyModel != Environment::Sky::Uniform)
-        throw std::runtime_error("the cuda backend renders no sky but a uniform one");
-    d.env.sky_model = env.skyModel == Environment::Sky::Uniform ? OWEC_SKY_UNIFORM : OWEC_SKY_NONE;
-    d.env.sky_radiance = d.env.sky_model == OWEC_SKY_UNIFORM ? f->spectrum(env.zenith) : -1;
+    if (env.skyModel == Environment::Sky::Map)
+        throw std::runtime_error("the cuda backend renders uniform and gradient skies, not environment maps");
+    d.env.sky_model = env.skyModel == Environment::Sky::Uniform    ? OWEC_SKY_UNIFORM
+                      : env.skyModel == Environment::Sky::Gradient ? OWEC_SKY_GRADIENT
+                                                                   : OWEC_SKY_NONE;
+    d.env.sky_radiance = d.env.sky_model != OWEC_SKY_NONE ? f->spectrum(env.zenith) : -1;
+    d.env.sky_horizon = d.env.sky_model == OWEC_SKY_GRADIENT ? f->spectrum(env.horizon) : -1;
+    d.env.sky_ground = d.env.sky_model == OWEC_SKY_GRADIENT ? f->spectrum(env.ground) : -1;
+    for (int k = 0; k < 3; ++k) d.env.sky_up[k] = env.up[k];
     d.env.has_sun = env.hasSun;
     d.env.sun_radiance = env.hasSun ? f->spectrum(env.sunRadiance) : -1;
     for (int k = 0; k < 3; ++k) d.env.sun_dir[k] = env.sunDir[k];

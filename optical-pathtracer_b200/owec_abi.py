@@ -21,7 +21,7 @@ SURF_NULL, SURF_DIELECTRIC, SURF_DIFFUSE, SURF_CONDUCTOR, SURF_MIRROR, SURF_ABSO
 SHAPE_SPHERE, SHAPE_SAG, SHAPE_PLANE, SHAPE_CYLINDER, SHAPE_MESH, SHAPE_CONE, SHAPE_TORUS, SHAPE_ROUND_WALL, \
     SHAPE_DOME = range(9)
 APERTURE_DISK, APERTURE_RECT, APERTURE_ELLIPSE, APERTURE_DISK_HOLE = 0, 1, 2, 3
-SKY_NONE, SKY_UNIFORM = 0, 1
+SKY_NONE, SKY_UNIFORM, SKY_GRADIENT = 0, 1, 2
 DETECTOR_OBSERVER, DETECTOR_SENSOR = 0, 1
 WAVELENGTHS_HERO4, WAVELENGTHS_UNIFORM1 = 0, 1
 PRECISION_MIXED, PRECISION_FP32, PRECISION_FP64 = 0, 1, 2
@@ -76,7 +76,8 @@ class Mesh(ctypes.Structure):
 class Environment(ctypes.Structure):
     _fields_ = [("sky_model", ctypes.c_int32), ("sky_radiance", ctypes.c_int32), ("has_sun", ctypes.c_int32),
                 ("sun_radiance", ctypes.c_int32), ("sun_dir", ctypes.c_double * 3),
-                ("sun_angular_radius", ctypes.c_double), ("sun_nee_share", ctypes.c_double)]
+                ("sun_angular_radius", ctypes.c_double), ("sun_nee_share", ctypes.c_double),
+                ("sky_horizon", ctypes.c_int32), ("sky_ground", ctypes.c_int32), ("sky_up", ctypes.c_double * 3)]
 
 
 class Detector(ctypes.Structure):

@@ -187,6 +187,15 @@ class SceneBuilder:
         self.env.sky_model = A.SKY_UNIFORM
         self.env.sky_radiance = self.spectrum_constant(radiance)
 
+    def gradient_sky(self, zenith, horizon, ground, up=(0.0, 0.0, 1.0)):
+        """Environment::sky's gradient: ground below the horizon, horizon blending into zenith above."""
+        self.env.sky_model = A.SKY_GRADIENT
+        self.env.sky_radiance = self.spectrum_constant(zenith)
+        self.env.sky_horizon = self.spectrum_constant(horizon)
+        self.env.sky_ground = self.spectrum_constant(ground)
+        u = np.asarray(up, float)
+        self.env.sky_up = (ctypes.c_double * 3)(*(u / np.linalg.norm(u)))
+
     def observer(self, width, height, position, look_at, up=(0, 0, 1), fov_y_deg=40.0, pixel_sigma=0.0, region=0,
                  pupil=0.0, focus=0.0, guide=None):
         """An IdealObserver; pupil > 0 makes it a thin lens focused at `focus` (0: at infinity);
@@ -544,6 +553,20 @@ def texture_gallery(width=64, height=40):
     sb.sun((0.3, -0.4, 0.85), 2.0e4)
     sb.uniform_sky(0.5)
     sb.observer(width, height, (0.0, -2.6, 3.2), (0.0, 0.2, 0.2), fov_y_deg=45.0)  # sees no sky
+    return sb
+
+
+def gradient_sky_scene(width=48, height=36):
+    """A glass sphere and a Lambertian block on a floor under a gradient sky (ground, horizon,
+    zenith; Environment::Sky::Gradient) tilted off the z axis, no sun: the sky seen directly,
+    through the glass, and as the only light."""
+    sb = SceneBuilder()
+    bk7 = sb.medium_sellmeier(*NBK7, rel_air=True)
+    sb.sphere_body(0.5, (-0.4, 0.3, 0.5), bk7, sb.dielectric())
+    sb.sphere_body(0.35, (0.7, -0.2, 0.35), sb.medium_opaque(), sb.diffuse(0.7))
+    sb.sheet(2.5, 2.5, pose(), sb.diffuse(0.6))
+    sb.gradient_sky(1.2, 0.4, 0.1, up=(0.1, 0.0, 1.0))
+    sb.observer(width, height, (0.0, -3.5, 1.6), (0.0, 0.0, 0.4), fov_y_deg=45.0)
     return sb
 
 

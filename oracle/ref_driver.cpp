@@ -207,8 +207,15 @@ std::unique_ptr<RefScene> buildScene(const owec_scene_desc& d) {
                       b.emission >= 0 ? emissionMap.at(b.emission) : -1);
     }
     Environment& env = w.env;
-    env.skyModel = d.env.sky_model == OWEC_SKY_UNIFORM ? Environment::Sky::Uniform : Environment::Sky::None;
+    env.skyModel = d.env.sky_model == OWEC_SKY_UNIFORM    ? Environment::Sky::Uniform
+                   : d.env.sky_model == OWEC_SKY_GRADIENT ? Environment::Sky::Gradient
+                                                          : Environment::Sky::None;
     if (d.env.sky_radiance >= 0) env.zenith = makeSpectrum(d, d.env.sky_radiance);
+    if (d.env.sky_model == OWEC_SKY_GRADIENT) {
+        env.horizon = makeSpectrum(d, d.env.sky_horizon);
+        env.ground = makeSpectrum(d, d.env.sky_ground);
+        env.up = normalize(Vec3(d.env.sky_up[0], d.env.sky_up[1], d.env.sky_up[2]));
+    }
     env.hasSun = d.env.has_sun != 0;
     env.sunDir = normalize(Vec3(d.env.sun_dir[0], d.env.sun_dir[1], d.env.sun_dir[2]));
     env.sunAngularRadius = d.env.sun_angular_radius;
