@@ -230,6 +230,81 @@ void padPrimBox(const double lo[3], const double hi[3], float4& flo, float4& fhi
                       std::nextafter(float(hi[2] + pad), INFINITY), 0.f);
 }
 
+// Whether the scene has contacts the lean traversal would resolve differently from the reference:
+// faces of two boundaries in one plane (bodies that touch, a sheet under a box), or parallel faces
+// closer than the FP32 anchor error `tol` (plates thinner than it). Mesh triangles and plane shapes
+// are keyed by their world plane (the normal, signed so its largest component is positive, rounded
+// to 1e-6, then the offset); neighbours in key order with the same normal are compared.
+bool hasContacts(const owec_scene_desc& d, double tol) {
+    struct Plane {
+        int64_t k[3];
+        double off;
+        uint32_t boundary;
+        bool flipped;  // the face's normal points against the key's
+    };
+    std::vector<Plane> planes;
+    auto add = [&](double n[3], const double p[3], uint32_t b) {
+        const double l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        if (!(l > 0)) return;
+        int big = 0;
+        for (int k = 1; k < 3; ++k)
+            if (std::fabs(n[k]) > std::fabs(n[big])) big = k;
+        const double s = (n[big] < 0 ? -1.0 : 1.0) / l;
+        Plane pl;
+        for (int k = 0; k < 3; ++k) pl.k[k] = int64_t(std::llround(n[k] * s * 1e6));
+        pl.off = (n[0] * p[0] + n[1] * p[1] + n[2] * p[2]) * s;
+        pl.boundary = b;
+        pl.flipped = n[big] < 0;
+        planes.push_back(pl);
+    };
+    std::vector<double> sphere;  // centre and radius of every sphere, with its boundary
+    for (uint32_t i = 0; i < d.n_boundaries; ++i) {
+        const owec_boundary& b = d.boundaries[i];
+        const double* m = b.to_world;
+        if (b.shape == OWEC_SHAPE_MESH) {
+            const owec_mesh& me = d.meshes[b.mesh];
+            for (uint64_t t = 0; t < me.tri_count; ++t) {
+                const uint32_t* tri = d.triangles + 3 * (me.tri_offset + t);
+                double w[3][3];
+                for (int k = 0; k < 3; ++k) xfPoint(m, d.vertices + 3 * (me.vertex_offset + tri[k]), w[k]);
+                const double e1[3] = {w[1][0] - w[0][0], w[1][1] - w[0][1], w[1][2] - w[0][2]};
+                const double e2[3] = {w[2][0] - w[0][0], w[2][1] - w[0][1], w[2][2] - w[0][2]};
+                double n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+                add(n, w[0], i);
+            }
+        } else if (b.shape == OWEC_SHAPE_PLANE) {
+            double n[3] = {m[2], m[6], m[10]};
+            const double c[3] = {m[3], m[7], m[11]};
+            add(n, c, i);
+        } else if (b.shape == OWEC_SHAPE_SPHERE) {
+            sphere.insert(sphere.end(), {m[3], m[7], m[11], b.params[0], double(i)});
+        }
+    }
+    std::sort(planes.begin(), planes.end(), [](const Plane& a, const Plane& b) {
+        if (a.k[0] != b.k[0]) return a.k[0] < b.k[0];
+        if (a.k[1] != b.k[1]) return a.k[1] < b.k[1];
+        if (a.k[2] != b.k[2]) return a.k[2] < b.k[2];
+        return a.off < b.off;
+    });
+    for (size_t i = 1; i < planes.size(); ++i) {
+        const Plane &a = planes[i - 1], &b = planes[i];
+        if (a.k[0] != b.k[0] || a.k[1] != b.k[1] || a.k[2] != b.k[2]) continue;
+        const double gap = b.off - a.off;
+        if (gap > tol) continue;
+        if (a.boundary != b.boundary) return true;  // two bodies' faces in one plane
+        // a body thinner than the anchor error: its two faces, facing apart (adjacent faces of a
+        // smooth mesh that are nearly coplanar face the same way)
+        if (a.flipped != b.flipped && gap > 1e-12 * (1 + std::fabs(a.off))) return true;
+    }
+    for (size_t i = 0; i < sphere.size(); i += 5)
+        for (size_t j = i + 5; j < sphere.size(); j += 5) {
+            const double dc = std::sqrt(sqr(sphere[i] - sphere[j]) + sqr(sphere[i + 1] - sphere[j + 1]) +
+                                        sqr(sphere[i + 2] - sphere[j + 2]));
+            if (std::fabs(sphere[i + 3] - sphere[j + 3]) <= tol && dc <= tol) return true;  // one sphere twice
+        }
+    return false;
+}
+
 void invertRigid(const double m[12], double out[12]) {
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) out[4 * i + j] = m[4 * j + i];
@@ -267,6 +342,7 @@ struct owec_ctx {
     bool hasNull = false;
     DeviceScene ds{};
     DBuf<DeviceScene> dScene;  // ds's copy on the device (DeviceScene::self), allocated when the context opens
+    bool contacts = false;  // touching bodies or plates thinner than the FP32 anchor error
     // particles: the sky's share of the emitted power and the disc distant light leaves from
     double pSky = 0, discRadius = 1, discCentre[3] = {0, 0, 0};
 
@@ -789,6 +865,10 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
     }
     for (uint32_t i = 0; i < d.n_optics; ++i)
         if (d.optics[i].texture != OWEC_TEXTURE_NONE) ds.fullFeatures = 1;
+    // contacts: resolved as the reference does by the contact-resolving instantiation; the tolerance
+    // is the FP32 anchor error over the scene's extent
+    c.contacts = hasContacts(d, 1e-5 * std::max(2 * sceneRadius, 1e-3));
+    if (c.contacts) ds.fullFeatures = 1;
     ds.nRegions = d.n_regions;
     ds.nBoundaries = d.n_boundaries;
     ds.nLights = uint32_t(c.lights.size());

@@ -410,12 +410,15 @@ __global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, Particl
                 const SurfacePoint<R> g = hitGeometry<R, Ro, Rr, Full>(sc, ray, h);
                 const bool fromFront = dot(d, g.n) < R(0);
                 const uint32_t inc = fromFront ? bd.front : bd.back, other = fromFront ? bd.back : bd.front;
-                inconsistent = inc != ray.region;
+                // an undecided contact counts as inconsistent and ends the particle
+                const bool ambiguous = Full && (h.flags & kHitAmbiguous);
+                inconsistent = inc != ray.region || ambiguous;
                 ray.region = inc;
                 const owec_optics& op = sc.optics[bd.optics];
                 const V3<double> gp = plainPoint<M>(g.p);
                 const float errG = anchorError<R>(g.p);
-                if (op.type == OWEC_SURF_NULL) {
+                if (ambiguous) {
+                } else if (op.type == OWEC_SURF_NULL) {
                     ray.region = other;
                     ray.o[0] = gp.x; ray.o[1] = gp.y; ray.o[2] = gp.z;
                     ray.depB = h.boundary;

@@ -66,11 +66,32 @@ struct HitRec {
     uint32_t boundary;
     uint32_t prim;        // triangle index within its mesh; 0 for analytic shapes
     uint32_t slot;        // leaf-order primitive slot
-    uint32_t pad;
+    uint32_t flags;       // kHitFront, kHitAmbiguous (kept by the contact-resolving traversal only)
 };
-
-// The acceptance rule of a candidate crossing at distance t with (unnormalised) normal n.
+// The crossing was met from its boundary's front side; it tied with another boundary's crossing that
+// the ray's region matches as well, which leaves their order undecided (NearestCrossing::offer,
+// src/owe/scene/world.cpp:515-550): the reference ends such a path.
+constexpr uint32_t kHitFront = 1u, kHitAmbiguous = 2u;
+// Crossings of two boundaries closer than this relative distance are the same contact: coincident
+// faces' FP32 distances, computed from different vertices, differ by a few ulps of the coordinates.
+// The contact-resolving traversal culls nodes with the closest distance widened by it.
+template <class T> __device__ __forceinline__ T tieWindow();
+template <> __device__ __forceinline__ float tieWindow<float>() { return 4e-6f; }
+template <> __device__ __forceinline__ double tieWindow<double>() { return 3e-16; }
+// How far behind its origin a crossing of another boundary through the anchor may fall by the
+// rounding of the origin and of its distance: a few ulps of the origin's magnitude. (The reference
+// searches from minus the anchor's error for every boundary but a departed mesh, world.cpp:473-476.)
 template <class T>
+__device__ __forceinline__ T behindWindow(const V3<T>& o) {
+    return T(sizeof(T) == 4 ? 5e-7 : 1e-15) * fmax(fmax(fabs(o.x), fabs(o.y)), fmax(fabs(o.z), T(1e-3)));
+}
+
+// The acceptance rule of a candidate crossing at distance t with (unnormalised) normal n. Near the
+// anchor the departed boundary is excluded, and a crossing counts only if it is met from the ray's
+// region. Contacts (the contact-resolving instantiation): of a departed mesh only the departed
+// triangle is excluded, so the far face of a plate thinner than the anchor's error is still met
+// (World::intersect's mesh departure, src/owe/scene/world.cpp:463-471; MeshShape::intersect).
+template <class T, bool Contacts = false>
 __device__ __forceinline__ bool acceptCrossing(const DeviceScene& sc, const RayQuery<T>& q, uint32_t b, uint32_t prim, bool mesh, T t,
                             const V3<T>& n) {
     if (mesh && b == q.depB && prim == q.depP) return false;
@@ -78,7 +99,7 @@ __device__ __forceinline__ bool acceptCrossing(const DeviceScene& sc, const RayQ
     const T nl = sqrt(dot(n, n));
     const bool near = fabs(t * dn) <= q.errN * nl;
     if (!near) return true;
-    if (b == q.depB) return false;
+    if (b == q.depB && !(Contacts && mesh)) return false;
     if (q.region == kNone) return true;
     const DBoundary& bd = sc.boundaries[b];
     const uint32_t incident = dn < T(0) ? bd.front : bd.back;
@@ -92,13 +113,18 @@ template <> __device__ __forceinline__ double farWiden<double>() { return 4e-16;
 
 // The analytic boundary b's first acceptable crossing in (0, best); FP64 refinement when Rr = double.
 template <class R, class Rr, class T, bool Full>
-__device__ __forceinline__ bool analyticCandidate(const DeviceScene& sc, const RayQuery<T>& q, uint32_t b, T best, Rr& tOut) {
+__device__ __forceinline__ bool analyticCandidate(const DeviceScene& sc, const RayQuery<T>& q, uint32_t b, T best, Rr& tOut,
+                                                  bool& frontOut) {
     const DBoundary& bd = sc.boundaries[b];
     const V3<Rr> lo = bd.toLocal.point(V3<Rr>(q.od));
     const V3<Rr> ld = bd.toLocal.vector(V3<Rr>(q.d));
     AHits<Rr> hits;
     int n;
-    if constexpr (Full) n = analyticCrossings<R, Rr, true>(bd, sc.shapeData + bd.dataOffset, lo, ld, Rr(0), Rr(best), b == q.depB, hits);
+    // contacts: another surface through the anchor may lie just behind it (world.cpp:473-476); such
+    // roots must lie within the rounding of the origin along the surface normal (checked below)
+    if constexpr (Full)
+        n = analyticCrossings<R, Rr, true>(bd, sc.shapeData + bd.dataOffset, lo, ld, -Rr(64) * Rr(q.errN), Rr(best),
+                                           b == q.depB, hits);
     else n = analyticCrossings<R, Rr, false>(bd, nullptr, lo, ld, Rr(0), Rr(best), false, hits);
     // Leaving this boundary, the anchor lies on it to the precision of the refinement, not of FP32:
     // with the FP32 window a grazing ray's far crossing of the same sphere (at t = 2 R cos) fell
@@ -110,8 +136,10 @@ __device__ __forceinline__ bool analyticCandidate(const DeviceScene& sc, const R
         if (i >= n) break;
         const AHit<Rr>& h = hits.get(i);
         const V3<T> nw = V3<T>(bd.toWorld.vector(h.n));
-        if (!acceptCrossing(sc, qs, b, 0u, false, T(h.t), nw)) continue;
+        if (Full && !(h.t > Rr(0)) && (b == q.depB || !(fabs(T(h.t) * dot(q.d, nw)) <= behindWindow(q.o)))) continue;
+        if (!acceptCrossing<T, Full>(sc, qs, b, 0u, false, T(h.t), nw)) continue;
         tOut = h.t;
+        frontOut = dot(q.d, nw) < T(0);
         return true;
     }
     return false;
@@ -124,6 +152,7 @@ template <class Rr>
 struct AnalyticResult {
     Rr t;
     bool ok;
+    bool front;  // met from the boundary's front side
 };
 template <class T, class R, class Rr, bool Full>
 __device__ __noinline__ AnalyticResult<Rr> analyticHit(const DeviceScene* scp, uint32_t b, V3<double> od, V3<T> d, T best,
@@ -139,7 +168,8 @@ __device__ __noinline__ AnalyticResult<Rr> analyticHit(const DeviceScene* scp, u
     q.errN = errN;
     AnalyticResult<Rr> r;
     r.t = Rr(0);
-    r.ok = analyticCandidate<R, Rr, T, Full>(*scp, q, b, best, r.t);
+    r.front = false;
+    r.ok = analyticCandidate<R, Rr, T, Full>(*scp, q, b, best, r.t, r.front);
     return r;
 }
 
@@ -357,7 +387,7 @@ struct Traversal {
             NodeWords nd;
             loadNode(sc.nodes, node, nd);
             if (Count) ++nodeVisits;
-            const uint32_t mask = intersectChildren(nd, inv, oinv, T(0), best);
+            const uint32_t mask = intersectChildren(nd, inv, oinv, T(0), Full ? best * (T(1) + tieWindow<T>()) : best);
             const uint32_t inner = nd.a.w >> 24;
             nodeBase = nd.b.x;
             nodeBits = permuteSlots(mask & inner, first) | (inner << 8);
@@ -374,28 +404,82 @@ struct Traversal {
         return kTraceRunning;
     }
 
+    // Whether boundary b's crossing at t, met from its front side when `front`, replaces the current
+    // closest (the contact-resolving instantiation; NearestCrossing::offer,
+    // src/owe/scene/world.cpp:515-550). Crossings of different boundaries within the tie window are
+    // one contact: the one met from the ray's region wins, matter wins over a zero-thickness
+    // readout, then the lower boundary index; two that both match leave the order undecided
+    // (kHitAmbiguous). `flags` receives the winner's flags.
+    __device__ __forceinline__ bool winsContact(const DeviceScene& sc, uint32_t b, T t, bool front, uint32_t& flags) {
+        const uint32_t frontFlag = front ? kHitFront : 0u;
+        if (!found || t < best * (T(1) - tieWindow<T>()) || b == hit.boundary) {
+            flags = frontFlag;
+            return !found || t < best;
+        }
+        const bool hinted = q.region != kNone;
+        auto incident = [&](uint32_t bb, bool fr) {
+            const DBoundary& bd = sc.boundaries[bb];
+            return fr ? bd.front : bd.back;
+        };
+        auto readout = [&](uint32_t bb) {
+            const DBoundary& bd = sc.boundaries[bb];
+            return sc.optics[bd.optics].type == OWEC_SURF_DETECTOR && bd.front == bd.back;
+        };
+        const bool mNew = !hinted || incident(b, front) == q.region;
+        const bool mOld = !hinted || incident(hit.boundary, hit.flags & kHitFront) == q.region;
+        const bool rNew = readout(b), rOld = readout(hit.boundary);
+        bool ambiguous = hit.flags & kHitAmbiguous;
+        if (mNew && mOld && rNew != rOld) {
+            if (rNew) return false;  // physical matter precedes a coincident readout
+            ambiguous = false;
+        } else if (hinted && mNew && mOld) {
+            ambiguous = true;
+        }
+        const bool replace = mNew != mOld ? mNew : (rNew != rOld ? rOld : b < hit.boundary);
+        if (!replace) {
+            hit.flags = (hit.flags & ~kHitAmbiguous) | (ambiguous ? kHitAmbiguous : 0u);
+            return false;
+        }
+        flags = frontFlag | (ambiguous ? kHitAmbiguous : 0u);
+        return true;
+    }
+
     // Tests primitive slot i; true when its crossing was accepted as the new closest.
     __device__ __forceinline__ bool testPrim(const DeviceScene& sc, uint32_t i) {
         V3<T> v0, v1, v2;
         uint32_t b, prim, kind;
         TriFetch<T>::get(sc, i, v0, v1, v2, b, prim, kind);
+        // the contact-resolving instantiation looks a tie window beyond the closest so far
+        const T limit = Full ? best * (T(1) + tieWindow<T>()) : best;
+        uint32_t flags = 0;
         if (kind == kPrimTriangle) {
             const V3<T> a = v0 - q.o, bb = v1 - q.o, c = v2 - q.o;
             if (!lineCrossesTriangle(sh, a, bb, c)) return false;
             const V3<T> n = triangleNormal(v0, v1, v2);
-            const T t = -dot(q.o - v0, n) / dot(q.d, n);
-            if (!(t > T(0) && t < best)) return false;
-            if (!acceptCrossing(sc, q, b, prim, true, t, n)) return false;
+            const T dn = dot(q.d, n);
+            const T t = -dot(q.o - v0, n) / dn;
+            // contacts: another boundary's face through the anchor may fall just behind it
+            if (!((Full ? t > T(0) || (b != q.depB && fabs(t * dn) <= behindWindow(q.o) * sqrt(dot(n, n))) : t > T(0)) &&
+                  t < limit))
+                return false;
+            if (!acceptCrossing<T, Full>(sc, q, b, prim, true, t, n)) return false;
+            if constexpr (Full) {
+                if (!winsContact(sc, b, t, dn < T(0), flags)) return false;
+            }
             best = t;
             hit.t = double(t);
             hit.prim = prim;
         } else {
-            const AnalyticResult<Rr> ar = analyticHit<T, R, Rr, Full>(sc.self, b, q.od, q.d, best, q.depB, q.region, q.errN);
+            const AnalyticResult<Rr> ar = analyticHit<T, R, Rr, Full>(sc.self, b, q.od, q.d, limit, q.depB, q.region, q.errN);
             if (!ar.ok) return false;
+            if constexpr (Full) {
+                if (!winsContact(sc, b, T(ar.t), ar.front, flags)) return false;
+            }
             best = T(ar.t);
             hit.t = double(ar.t);
             hit.prim = 0;
         }
+        if constexpr (Full) hit.flags = flags;
         hit.boundary = b;
         hit.slot = i;
         found = true;

@@ -534,12 +534,14 @@ __global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SH
         const bool fromFront = dot(d, g.n) < R(0);
         const uint32_t inc = fromFront ? bd.front : bd.back;
         const uint32_t other = fromFront ? bd.back : bd.front;
-        const bool inconsistent = inc != ray.region;
+        // an undecided contact counts as inconsistent and ends the path (transport.cpp:503)
+        const bool ambiguous = Full && (h.flags & kHitAmbiguous);
+        const bool inconsistent = inc != ray.region || ambiguous;
         ray.region = inc;
         aux.lastBoundary = h.boundary;
         const bool specular = aux.flags & kFlagSpecular;
         // emissionMet (transport.cpp:420-433)
-        if (bd.emission >= 0) {
+        if (bd.emission >= 0 && !ambiguous) {
             const owec_emission e = sc.emissions[bd.emission];
             if (fromFront ? e.front : e.back) {
                 R w = R(1);
@@ -560,7 +562,8 @@ __global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SH
         R betaNee[NW] = {R(0), R(0), R(0), R(0)};
         R pdfS = R(0), cosF = R(0);
         uint32_t neeRegion = ray.region;
-        if (!Simple && o.type == OWEC_SURF_NULL) {
+        if (ambiguous) {
+        } else if (!Simple && o.type == OWEC_SURF_NULL) {
             ray.region = other;
             setOrigin<M>(ray.o, g.p);
             ray.depB = h.boundary;
@@ -746,7 +749,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
                         outcome = 2;
                     } else {
                         const DBoundary& bd = sc.boundaries[h.boundary];
-                        if (sc.optics[bd.optics].type != OWEC_SURF_NULL) {
+                        if (sc.optics[bd.optics].type != OWEC_SURF_NULL || (Full && (h.flags & kHitAmbiguous))) {
                             outcome = 2;
                         } else {
                             // pass the null boundary, if met from this region

@@ -570,6 +570,36 @@ def gradient_sky_scene(width=48, height=36):
     return sb
 
 
+def box_mesh(lo, hi):
+    """An axis-aligned box as a closed triangle mesh, counter-clockwise seen from outside."""
+    (x0, y0, z0), (x1, y1, z1) = lo, hi
+    v = np.array([(x0, y0, z0), (x1, y0, z0), (x1, y1, z0), (x0, y1, z0),
+                  (x0, y0, z1), (x1, y0, z1), (x1, y1, z1), (x0, y1, z1)], float)
+    t = np.array([(0, 2, 1), (0, 3, 2), (4, 5, 6), (4, 6, 7), (0, 1, 5), (0, 5, 4),
+                  (1, 2, 6), (1, 6, 5), (2, 3, 7), (2, 7, 6), (3, 0, 4), (3, 4, 7)], np.uint32)
+    return v, t
+
+
+def touching_glass(width=48, height=36, thickness=0.2, gap=0.0):
+    """Two N-BK7 blocks side by side (touching when gap = 0: coincident faces of two boundaries) and
+    a thin glass plate of the given thickness over a Lambertian floor under the sun: contacts the
+    reference resolves by its region rule (src/owe/scene/world.cpp:440-582)."""
+    sb = SceneBuilder()
+    bk7 = sb.medium_sellmeier(*NBK7, rel_air=True)
+    glass = sb.dielectric()
+    v, t = box_mesh((-0.6, -0.3, 0.0), (0.0, 0.3, 0.5))
+    sb.mesh_body(v, t, bk7, glass)
+    v, t = box_mesh((gap, -0.3, 0.0), (0.6, 0.3, 0.5))
+    sb.mesh_body(v, t, bk7, glass)
+    v, t = box_mesh((-0.5, -0.9, 0.3), (0.5, -0.45, 0.3 + thickness))
+    sb.mesh_body(v, t, bk7, glass)
+    sb.sheet(3.0, 3.0, pose(), sb.diffuse(0.7))
+    sb.sun((0.35, -0.3, 0.9), 2.0e4)
+    sb.uniform_sky(0.3)
+    sb.observer(width, height, (0.2, -2.8, 1.9), (0.0, -0.2, 0.25), fov_y_deg=40.0)
+    return sb
+
+
 def asphere_lens(width=48, height=48):
     """A biconvex N-BK7 lens with even-aspheric faces (A4, A6) and a cylindrical rim over a
     Lambertian floor under the sun: light through two numerically crossed surfaces."""

@@ -1,0 +1,47 @@
+"""Contacts on a GPU: touching bodies (coincident faces of two boundaries) and thin plates, whose
+crossings the reference resolves with its departure and region rules (World::intersect,
+src/owe/scene/world.cpp:440-582). The device paths must neither leak nor meet inconsistent regions
+where the reference's do not, and the images must agree."""
+import numpy as np
+import pytest
+
+import owec_abi as A
+import owe_cuda
+import scenes
+from conftest import save_artifact
+from oracle_ref import ReferenceEngine, block_z_test
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("thickness", [0.2, 1e-4, 1e-6])
+def test_touching_blocks_and_thin_plates_like_the_reference(thickness):
+    desc = scenes.touching_glass(thickness=thickness).desc()
+    ref = ReferenceEngine(desc)
+    runs_ref, runs_gpu = [], []
+    ref_stats = {"inconsistencies": 0, "leaks": 0, "paths": 0}
+    st = {"inconsistencies": 0, "leaks": 0, "paths": 0, "device_faults": 0}
+    with owe_cuda.Context() as c:
+        c.upload(desc)
+        c.build_bvh()
+        for k in range(8):
+            img, rs, _ = ref.render_backend(A.make_settings(seed=10 + k, max_depth=24), 64)
+            runs_ref.append(img)
+            for key in ref_stats:
+                ref_stats[key] += rs[key]
+            c.set_settings(A.make_settings(seed=20 + k, max_depth=24))
+            c.reset_film()
+            c.run_pass(64)
+            runs_gpu.append(c.resolve()[0])
+            gs = c.stats()
+            for key in st:
+                st[key] += gs[key]
+    save_artifact(f"contacts_{thickness:g}", ref=np.array(runs_ref), gpu=np.array(runs_gpu))
+    # The reference's paths meet no inconsistent region. On the device a few in 10^4 still do (grazing
+    # crossings of the coincident faces, whose FP32 distances differ by more than the tie window):
+    # the bound is one path in 10^3. Before contacts were resolved one path in ten did.
+    assert ref_stats["inconsistencies"] == 0 and ref_stats["leaks"] == 0, ref_stats
+    assert st["inconsistencies"] + st["leaks"] <= 1e-3 * st["paths"], st
+    assert st["device_faults"] == 0, st
+    ok, rep = block_z_test(runs_ref, runs_gpu)
+    assert ok, rep
