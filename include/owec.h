@@ -143,6 +143,11 @@ typedef struct owec_emission {
                                  * open cylinder from z = 0 to H with rectangular openings (RoundWallShape) */
 #define OWEC_SHAPE_DOME 8     /* params: R, slit azimuth, slit width, slit top elevation: the hemisphere
                                * z >= 0 with an observing slit (DomeShape) */
+#define OWEC_SHAPE_WAVES 9    /* params: halfX, halfY, margin; data: nodes_x, nodes_y, then the plane waves as
+                               * (amplitude, kx, ky, phase): the liquid surface z = w(x) w(y) sum a sin(kx x + ky y
+                               * + phase) over the rectangle, tapered to 0 within margin of its edges, +z normal
+                               * (WaveSurface). nodes_x = nodes_y = 0: the analytic sum; otherwise the sum
+                               * sampled at nodes_x x nodes_y nodes (2..4096 each) as a bicubic Hermite spline */
 
 #define OWEC_APERTURE_DISK 0 /* a = rMax, b = rMin */
 #define OWEC_APERTURE_RECT 1 /* a = halfX, b = halfY */

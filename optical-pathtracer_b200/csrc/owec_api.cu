@@ -124,6 +124,47 @@ void torusExtent(double R, double zc, double rho, double a0, double a1, double e
     ext[3] = hi;
 }
 
+// A wave surface's derived record (WaveSurface's constructor, geometry.cpp:190-221): the margin
+// clamped to the half sizes, the amplitude bound (the sum of |a|), the slope bound (the sum of |a| k,
+// plus the taper's share), and, for a sampled surface, the node spacings, the nodes (h, dh/dx,
+// dh/dy, d2h/dxdy, row by row) and the slope bound tightened to the nodes' largest slope plus the
+// curvature bound over half a cell diagonal. P: halfX, halfY, margin; D: nodes x, nodes y, waves.
+struct WaveSetup {
+    double margin = 0, amp = 0, slope = 0, dx = 0, dy = 0;
+    std::vector<double> nodes;
+};
+WaveSetup waveSetup(const double* P, const double* D, uint32_t count) {
+    WaveSetup w;
+    const double hx = P[0], hy = P[1];
+    w.margin = std::max(0.0, std::min({P[2], hx, hy}));
+    const int nW = int((count - 2) / 4);
+    const double* waves = D + 2;
+    double slope = 0, curvature = 0;
+    for (int i = 0; i < nW; ++i) {
+        const double a = std::fabs(waves[4 * i]), k = std::hypot(waves[4 * i + 1], waves[4 * i + 2]);
+        w.amp += a;
+        slope += a * k;
+        curvature += a * k * k;
+    }
+    const double taper = w.margin > 0 ? 1.5 * std::sqrt(2.0) / w.margin : 0;
+    w.slope = slope + w.amp * taper;
+    const int nx = int(D[0]), ny = int(D[1]);
+    if (nx == 0) return w;
+    w.dx = 2 * hx / (nx - 1);
+    w.dy = 2 * hy / (ny - 1);
+    w.nodes.resize(size_t(4) * nx * ny);
+    double nodeSlope = 0;
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            double* n = w.nodes.data() + 4 * (size_t(j) * nx + i);
+            waveAnalytic<double>(waves, nW, hx, hy, w.margin, -hx + i * w.dx, -hy + j * w.dy, n[0], n[1], n[2], n[3]);
+            nodeSlope = std::max(nodeSlope, std::hypot(n[1], n[2]));
+        }
+    const double hessian = curvature + 2 * taper * slope + (w.margin > 0 ? 6 * w.amp / (w.margin * w.margin) : 0);
+    w.slope = std::min(w.slope, 1.05 * (nodeSlope + hessian * 0.5 * std::hypot(w.dx, w.dy)));
+    return w;
+}
+
 // A shape's bounds in its frame (Shape::bounds of the reference's shapes).
 Box localBounds(const owec_scene_desc& d, const owec_boundary& b) {
     Box bx;
@@ -154,6 +195,12 @@ Box localBounds(const owec_scene_desc& d, const owec_boundary& b) {
         }
         case OWEC_SHAPE_ROUND_WALL: put(-P[0], -P[0], 0, P[0], P[0], P[1]); break;
         case OWEC_SHAPE_DOME: put(-P[0], -P[0], 0, P[0], P[0], P[0]); break;
+        case OWEC_SHAPE_WAVES: {
+            double amp = 0;
+            for (uint32_t i = 2; i + 3 < b.data_count; i += 4) amp += std::fabs(d.shape_data[b.data_offset + i]);
+            put(-P[0], -P[1], -amp, P[0], P[1], amp);
+            break;
+        }
         case OWEC_SHAPE_PLANE: {
             const int ap = int(P[0]);
             const double ex = P[1], ey = (ap == OWEC_APERTURE_DISK || ap == OWEC_APERTURE_DISK_HOLE) ? P[1] : P[2];
@@ -355,6 +402,7 @@ struct owec_ctx {
     DBuf<owec_emission> dEmissions;
     DBuf<DBoundary> dBoundaries;
     DBuf<DLight> dLights;
+    std::vector<double> shapeData;  // the scene's shape data, then the nodes of sampled wave surfaces
     DBuf<double> dShapeData;
     DBuf<float4> dPrimLo, dPrimHi, dTri;
     DBuf<double> dTri64;
@@ -467,7 +515,7 @@ void validateDesc(const owec_scene_desc& d) {
                                                           "emission needs a radiance spectrum");
     for (uint32_t i = 0; i < d.n_boundaries; ++i) {
         const owec_boundary& b = d.boundaries[i];
-        require(b.shape >= OWEC_SHAPE_SPHERE && b.shape <= OWEC_SHAPE_DOME, "unknown shape");
+        require(b.shape >= OWEC_SHAPE_SPHERE && b.shape <= OWEC_SHAPE_WAVES, "unknown shape");
         require(b.data_count == 0 || (d.shape_data && uint64_t(b.data_offset) + b.data_count <= d.n_shape_data),
                 "shape data out of range");
         const double* P = b.params;
@@ -499,6 +547,19 @@ void validateDesc(const owec_scene_desc& d) {
                 require(P[0] > 0 && P[1] > 0 && b.data_count % 4 == 0, "round wall: radius, height and openings");
                 break;
             case OWEC_SHAPE_DOME: require(P[0] > 0, "dome: radius must be positive"); break;
+            case OWEC_SHAPE_WAVES: {
+                require(P[0] > 0 && P[1] > 0 && std::isfinite(P[0]) && std::isfinite(P[1]) && P[2] >= 0,
+                        "wave surface: positive half sizes and a margin >= 0");
+                require(b.data_count >= 2 && (b.data_count - 2) % 4 == 0,
+                        "wave surface: its data is the node counts and (amplitude, kx, ky, phase) per wave");
+                const double nx = D[0], ny = D[1];
+                const bool analytic = nx == 0 && ny == 0;
+                const bool sampled = nx == std::floor(nx) && ny == std::floor(ny) && nx >= 2 && ny >= 2 && nx <= 4096 &&
+                                     ny <= 4096;
+                require(analytic || sampled, "wave surface: node counts are 0 (analytic) or 2..4096");
+                for (uint32_t k = 2; k < b.data_count; ++k) require(std::isfinite(D[k]), "wave surface: waves must be finite");
+                break;
+            }
             default: break;
         }
         require(b.front < d.n_regions && b.back < d.n_regions, "boundary region out of range");
@@ -553,6 +614,7 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
     c.regionMedium.assign(d.region_medium, d.region_medium + d.n_regions);
     c.optics.assign(d.optics, d.optics + d.n_optics);
     c.emissions.assign(d.emissions, d.emissions + d.n_emissions);
+    c.shapeData.assign(d.shape_data, d.shape_data + (d.shape_data ? d.n_shape_data : 0));
 
     // The camera-relative origin: the one given, the observer's position, or the sensor's centre.
     double origin[3];
@@ -597,6 +659,21 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
         } else if (b.shape == OWEC_SHAPE_TORUS) {
             torusExtent(b.params[0], b.params[1], b.params[2], b.params[3], d.shape_data[b.data_offset], db.ext);
             db.params[3] = std::min(b.params[3], d.shape_data[b.data_offset]);
+        } else if (b.shape == OWEC_SHAPE_WAVES) {
+            const WaveSetup w = waveSetup(b.params, d.shape_data + b.data_offset, b.data_count);
+            db.params[2] = w.margin;
+            db.params[3] = double((b.data_count - 2) / 4);
+            db.ext[0] = w.amp;
+            db.ext[1] = w.slope;
+            db.ext[2] = w.dx;
+            db.ext[3] = w.dy;
+            if (!w.nodes.empty()) {  // the record and its nodes, appended to the device copy of the data
+                require(c.shapeData.size() + b.data_count + w.nodes.size() < (1ull << 32), "wave surface: too many nodes");
+                db.dataOffset = uint32_t(c.shapeData.size());
+                db.dataCount = uint32_t(b.data_count + w.nodes.size());
+                c.shapeData.insert(c.shapeData.end(), d.shape_data + b.data_offset, d.shape_data + b.data_offset + b.data_count);
+                c.shapeData.insert(c.shapeData.end(), w.nodes.begin(), w.nodes.end());
+            }
         }
         bool canSample = false;
         db.area = shapeArea(d, b, canSample);
@@ -838,7 +915,7 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
     c.dEmissions.upload(c.emissions.data(), c.emissions.size(), s);
     c.dBoundaries.upload(c.boundaries.data(), c.boundaries.size(), s);
     c.dLights.upload(c.lights.data(), c.lights.size(), s);
-    c.dShapeData.upload(d.shape_data, d.n_shape_data, s);
+    c.dShapeData.upload(c.shapeData.data(), c.shapeData.size(), s);
     c.dPrimLo.upload(c.primLo.data(), c.primLo.size(), s);
     c.dPrimHi.upload(c.primHi.data(), c.primHi.size(), s);
     c.dTri.upload(c.triRecs.data(), c.triRecs.size(), s);
@@ -859,7 +936,7 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
     for (uint32_t i = 0; i < d.n_boundaries; ++i) {
         const owec_boundary& b = d.boundaries[i];
         if (b.shape == OWEC_SHAPE_CONE || b.shape == OWEC_SHAPE_TORUS || b.shape == OWEC_SHAPE_ROUND_WALL ||
-            b.shape == OWEC_SHAPE_DOME || (b.shape == OWEC_SHAPE_SAG && b.data_count > 0) ||
+            b.shape == OWEC_SHAPE_DOME || b.shape == OWEC_SHAPE_WAVES || (b.shape == OWEC_SHAPE_SAG && b.data_count > 0) ||
             (b.shape == OWEC_SHAPE_PLANE && int(b.params[0]) == OWEC_APERTURE_DISK_HOLE))
             ds.fullFeatures = 1;
     }

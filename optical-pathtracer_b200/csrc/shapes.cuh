@@ -1,10 +1,11 @@
 // Analytic surfaces in their own frames: spheres, conic and aspheric sags, planes with apertures,
-// cylinders, cones, torus patches, round walls and domes (src/owe/scene/geometry.cpp). Quadric roots
+// cylinders, cones, torus patches, round walls, domes and wave surfaces (src/owe/scene/geometry.cpp). Quadric roots
 // come from the numerically stable quadratic in precision R and are refined by re-solving from the
 // approximate hit in precision Rr (src/owe/core/shared/surfaces.hpp:13-137): with R = float and
 // Rr = double this is the selective FP64 step that keeps large-radius lens surfaces exact; with
-// R = Rr = float it is the plain FP32 baseline. Aspheres and torus patches have no closed form:
-// their crossings are bracketed by sampling along the clipped ray and bisected, in precision Rr.
+// R = Rr = float it is the plain FP32 baseline. Aspheres, torus patches and wave surfaces have no
+// closed form: their crossings are bracketed along the clipped ray and bisected (or, near a wave
+// surface, converged on by Newton's method), in precision Rr.
 #pragma once
 
 #include "device_scene.cuh"
@@ -426,6 +427,187 @@ __device__ __noinline__ NumericRoots<Rr> torusRoots(Rr R0, Rr zc, Rr rho, Rr a0,
     return r;
 }
 
+// ------------------------------------------------------------------ liquid waves
+// A wave surface z = h(x, y) (WaveSurface, src/owe/scene/geometry.hpp:90-140): h = w(x) w(y) sum of
+// a_i sin(k_i . (x, y) + phase_i) over |x| <= halfX, |y| <= halfY, w a smoothstep taper to zero
+// within `margin` of the edges; or that sum sampled at nodes as a bicubic Hermite spline. The
+// device record: params = halfX, halfY, margin (clamped to the half sizes), the number of waves;
+// ext = the amplitude bound, the slope bound, the node spacings in x and y (0: the analytic sum);
+// data = the node counts in x and y, the waves as (amplitude, kx, ky, phase), then the nodes row by
+// row from (-halfX, -halfY), each (h, dh/dx, dh/dy, d2h/dxdy).
+
+// The taper w(u) toward the edges at +-half within `margin`, and dw/du (waveTaper,
+// src/owe/core/shared/surfaces.hpp:177-192).
+template <class T>
+OWEC_HD void waveTaper(T u, T half, T margin, T& w, T& dw) {
+    w = T(1);
+    dw = T(0);
+    if (!(margin > T(0))) return;
+    const T e = half - fabs(u);
+    if (e >= margin) return;
+    if (e <= T(0)) {
+        w = T(0);
+        return;
+    }
+    const T s = e / margin;
+    w = s * s * (T(3) - T(2) * s);
+    dw = (u < T(0) ? T(6) : T(-6)) * s * (T(1) - s) / margin;
+}
+
+// The tapered wave sum at (x, y) with its derivatives dh/dx, dh/dy and d2h/dxdy; zero outside the
+// rectangle (WaveSurface::analytic, geometry.cpp:223-242). waves: nW (amplitude, kx, ky, phase).
+template <class T>
+OWEC_HD void waveAnalytic(const double* waves, int nW, T hx, T hy, T margin, T x, T y, T& h, T& gx, T& gy, T& gxy) {
+    h = gx = gy = gxy = T(0);
+    if (fabs(x) > hx || fabs(y) > hy) return;
+    T g = T(0), sx = T(0), sy = T(0), sxy = T(0);
+    for (int i = 0; i < nW; ++i) {
+        const T a = T(waves[4 * i]), kx = T(waves[4 * i + 1]), ky = T(waves[4 * i + 2]);
+        const T arg = kx * x + ky * y + T(waves[4 * i + 3]);
+        const T s = sin(arg), c = cos(arg);
+        g += a * s;
+        sx += a * c * kx;
+        sy += a * c * ky;
+        sxy -= a * s * kx * ky;
+    }
+    T wx, dwx, wy, dwy;
+    waveTaper(x, hx, margin, wx, dwx);
+    waveTaper(y, hy, margin, wy, dwy);
+    h = wx * wy * g;
+    gx = dwx * wy * g + wx * wy * sx;
+    gy = wx * dwy * g + wx * wy * sy;
+    gxy = dwx * dwy * g + dwx * wy * sy + wx * dwy * sx + wx * wy * sxy;
+}
+
+// The cubic Hermite bases on [0, 1] at u: value bases p0, p1 and slope bases q0, q1 of the two ends,
+// and their derivatives.
+template <class T>
+OWEC_HD void hermiteBasis(T u, T p[2], T q[2], T dp[2], T dq[2]) {
+    const T u2 = u * u, u3 = u2 * u;
+    p[0] = T(2) * u3 - T(3) * u2 + T(1);
+    p[1] = T(3) * u2 - T(2) * u3;
+    q[0] = u3 - T(2) * u2 + u;
+    q[1] = u3 - u2;
+    dp[0] = T(6) * u2 - T(6) * u;
+    dp[1] = T(6) * u - T(6) * u2;
+    dq[0] = T(3) * u2 - T(4) * u + T(1);
+    dq[1] = T(3) * u2 - T(2) * u;
+}
+
+// The wave surface's height and gradient at local (x, y), zero outside its rectangle
+// (WaveSurface::height, geometry.cpp:244-270).
+template <class T>
+OWEC_HD void waveHeight(const DBoundary& b, const double* data, T x, T y, T& h, T& gx, T& gy) {
+    const T hx = T(b.params[0]), hy = T(b.params[1]);
+    const int nW = int(b.params[3]);
+    if (b.ext[2] == 0) {
+        T gxy;
+        waveAnalytic(data + 2, nW, hx, hy, T(b.params[2]), x, y, h, gx, gy, gxy);
+        return;
+    }
+    h = gx = gy = T(0);
+    if (fabs(x) > hx || fabs(y) > hy) return;
+    const int nx = int(data[0]), ny = int(data[1]);
+    const double* nodes = data + 2 + 4 * nW;
+    const T dx = T(b.ext[2]), dy = T(b.ext[3]);
+    const T fx = (x + hx) / dx, fy = (y + hy) / dy;
+    const int i = min(max(int(fx), 0), nx - 2), j = min(max(int(fy), 0), ny - 2);
+    T P[2], Q[2], dP[2], dQ[2], Pv[2], Qv[2], dPv[2], dQv[2];
+    hermiteBasis(fx - T(i), P, Q, dP, dQ);
+    hermiteBasis(fy - T(j), Pv, Qv, dPv, dQv);
+    T f = T(0), fu = T(0), fv = T(0);
+    for (int bj = 0; bj < 2; ++bj)
+        for (int ai = 0; ai < 2; ++ai) {
+            const double* n = nodes + 4 * (size_t(j + bj) * nx + (i + ai));
+            const T c0 = T(n[0]), cu = T(n[1]) * dx, cv = T(n[2]) * dy, cuv = T(n[3]) * dx * dy;
+            f += c0 * P[ai] * Pv[bj] + cu * Q[ai] * Pv[bj] + cv * P[ai] * Qv[bj] + cuv * Q[ai] * Qv[bj];
+            fu += c0 * dP[ai] * Pv[bj] + cu * dQ[ai] * Pv[bj] + cv * dP[ai] * Qv[bj] + cuv * dQ[ai] * Qv[bj];
+            fv += c0 * P[ai] * dPv[bj] + cu * Q[ai] * dPv[bj] + cv * P[ai] * dQv[bj] + cuv * Q[ai] * dQv[bj];
+        }
+    h = f;
+    gx = fu / dx;
+    gy = fv / dy;
+}
+
+template <class T>
+OWEC_HD V3<T> waveNormal(const DBoundary& b, const double* data, const V3<T>& p) {
+    T h, gx, gy;
+    waveHeight(b, data, p.x, p.y, h, gx, gy);
+    return normalize(V3<T>(-gx, -gy, T(1)));
+}
+
+// WaveSurface::intersect (geometry.cpp:278-344): the ray clipped to the surface's box is marched in
+// steps |f| / L, f = z - h along the ray and L its Lipschitz bound along the ray, so that no crossing
+// is stepped over; near the surface Newton's method converges on the crossing being approached; a
+// sign change within a minimum step is bisected. A crossing within depWindow (plus its own error)
+// along the normal of a ray leaving this surface is the departure and skipped. The first accepted
+// crossing is returned, and a second only when the first lies within nearWindow of the origin along
+// its normal, where the caller's region rule may still reject it.
+template <class Rr>
+__device__ __noinline__ NumericRoots<Rr> waveRoots(const DBoundary& b, const double* data, V3<Rr> o, V3<Rr> d, Rr tmin,
+                                                   Rr tmax, Rr depWindow, Rr nearWindow) {
+    NumericRoots<Rr> r{{Rr(0), Rr(0)}, 0};
+    const Rr hx = Rr(b.params[0]), hy = Rr(b.params[1]), amp = Rr(b.ext[0]), slope = Rr(b.ext[1]);
+    Rr ta = tmin, tb = tmax;
+    if (!clipSlab(o.x, d.x, -hx, hx, ta, tb) || !clipSlab(o.y, d.y, -hy, hy, ta, tb) || !clipSlab(o.z, d.z, -amp, amp, ta, tb))
+        return r;
+    const Rr L = fabs(d.z) + slope * sqrt(d.x * d.x + d.y * d.y);
+    const Rr tol = Rr(sizeof(Rr) == 8 ? 1e-12 : 1e-6) * (Rr(1) + fmax(fmax(hx, hy), amp));
+    auto f = [&](Rr t, Rr& dfdt) {
+        const V3<Rr> p = o + d * t;
+        Rr h, gx, gy;
+        waveHeight(b, data, p.x, p.y, h, gx, gy);
+        dfdt = d.z - gx * d.x - gy * d.y;
+        return p.z - h;
+    };
+    auto value = [&](Rr t) {
+        Rr dfdt;
+        return f(t, dfdt);
+    };
+    Rr t = ta, dfdt;
+    Rr ft = f(t, dfdt);
+    if (t <= tmin && fabs(ft) < tol) {  // starting on the surface it leaves
+        t = tmin + tol / fmax(L, Rr(1e-30));
+        ft = f(t, dfdt);
+    }
+    const Rr minStep = Rr(1e-7) * (tb - ta), nearSurface = Rr(1e-6) * (amp + tol);
+    // Records crossing tr; true when the search is over.
+    auto record = [&](Rr tr) {
+        const V3<Rr> p = o + d * tr;
+        if (!(tr > tmin && tr < tmax) || fabs(p.x) > hx || fabs(p.y) > hy) return false;
+        Rr h, gx, gy;
+        waveHeight(b, data, p.x, p.y, h, gx, gy);
+        const Rr gl = sqrt(Rr(1) + gx * gx + gy * gy);
+        const Rr along = fabs(tr * (d.z - gx * d.x - gy * d.y)) / gl;  // |t d.n|
+        if (depWindow > Rr(0) && along <= depWindow + fabs(p.z - h) / gl) return false;
+        if (r.n == 1 && fabs(tr - r.t[0]) <= Rr(1e3) * tol) return false;  // the same crossing again
+        r.t[r.n++] = tr;
+        return r.n == 2 || along > nearWindow;
+    };
+    for (int i = 0; i < 4096 && t < tb; ++i) {
+        Rr step = fmax(fabs(ft) / L, minStep);
+        if (fabs(ft) < nearSurface) {
+            Rr tn = t;
+            for (int k = 0; k < 8; ++k) {
+                const Rr fn = f(tn, dfdt);
+                const V3<Rr> p = o + d * tn;
+                const Rr arithmeticTol = Rr(8) * Rr(Tol<Rr>::eps) *
+                                         fmax(fmax(Rr(1e-12), amp), fmax(fmax(fabs(p.x), fabs(p.y)), fabs(p.z)));
+                if (fabs(fn) < arithmeticTol || fabs(dfdt) < Rr(1e-12)) break;
+                tn -= fn / dfdt;
+            }
+            if (tn >= t - Rr(1e3) * tol && fabs(value(tn)) < Rr(1e3) * tol && record(tn)) return r;
+            step = fmax(minStep, Rr(2) * fabs(ft) / L);  // a grazing approach: move past it
+        }
+        const Rr tn = fmin(t + step, tb);
+        const Rr fn = f(tn, dfdt);
+        if ((fn < Rr(0)) != (ft < Rr(0)) && record(bisectRoot(value, t, tn, ft, Tol<Rr>::bisectSteps))) return r;
+        t = tn;
+        ft = fn;
+    }
+    return r;
+}
+
 // The quadric crossings of a shape: roots t0 <= t1 in precision R, each refined in precision Rr and
 // kept when it lies in (tmin, tmax) and solid(p) accepts it (firstRefinedHit, geometry.cpp:32-48,
 // for both roots).
@@ -446,7 +628,7 @@ OWEC_HD void quadricHits(int kind, Rr qa, Rr qb, Rr qc, const V3<Rr>& o, const V
 // The crossings of every shape (analyticCrossings with Full).
 template <class R, class Rr>
 OWEC_HD int fullCrossings(const DBoundary& b, const double* data, const V3<Rr>& o, const V3<Rr>& d, Rr tmin, Rr tmax,
-                          bool departed, AHits<Rr>& out) {
+                          bool departed, AHits<Rr>& out, Rr depWindow, Rr nearWindow) {
     out.n = 0;
     const double* P = b.params;
     switch (b.shape) {
@@ -561,6 +743,14 @@ OWEC_HD int fullCrossings(const DBoundary& b, const double* data, const V3<Rr>& 
             }
             break;
         }
+        case OWEC_SHAPE_WAVES: {
+            const NumericRoots<Rr> r = waveRoots<Rr>(b, data, o, d, tmin, tmax, departed ? depWindow : Rr(0), nearWindow);
+            for (int i = 0; i < r.n; ++i) {
+                const V3<Rr> p = o + d * r.t[i];
+                out.add({r.t[i], p, waveNormal(b, data, p)});
+            }
+            break;
+        }
         default: break;
     }
     if (out.n == 2 && out.h1.t < out.h0.t) { const AHit<Rr> tmp = out.h0; out.h0 = out.h1; out.h1 = tmp; }
@@ -569,27 +759,32 @@ OWEC_HD int fullCrossings(const DBoundary& b, const double* data, const V3<Rr>& 
 
 // Up to two crossings of boundary b's shape by the local ray (o, d) in (tmin, tmax), ascending,
 // each inside the shape's trim. data: the shape's run of the scene's shape data. departed: the ray
-// leaves this boundary (a torus patch then resolves the start of its bracket finely). Returns how
-// many. Full = false compiles only the spheres, conic sags, plain apertures and cylinders: the
-// kernels of a scene without the other shapes keep the registers they need for those alone.
+// leaves this boundary (a torus patch then resolves the start of its bracket finely; a wave surface
+// skips the crossings within depWindow of the origin along their normal). nearWindow: the origin's
+// error along a surface normal (a wave surface looks for a second crossing only behind a first one
+// within it). Returns how many. Full = false compiles only the spheres, conic sags, plain apertures
+// and cylinders: the kernels of a scene without the other shapes keep the registers they need for
+// those alone.
 template <class R, class Rr, bool Full>
 OWEC_HD int analyticCrossings(const DBoundary& b, const double* data, const V3<Rr>& o, const V3<Rr>& d, Rr tmin, Rr tmax,
-                              bool departed, AHits<Rr>& out) {
-    if constexpr (Full) return fullCrossings<R, Rr>(b, data, o, d, tmin, tmax, departed, out);
+                              bool departed, AHits<Rr>& out, Rr depWindow = Rr(0), Rr nearWindow = Rr(0)) {
+    if constexpr (Full) return fullCrossings<R, Rr>(b, data, o, d, tmin, tmax, departed, out, depWindow, nearWindow);
     else return classicCrossings<R, Rr>(b, o, d, tmin, tmax, out);
 }
 
-// The unit normal of a shape found by a numeric crossing (aspheres, torus patches) at local point p.
+// The unit normal of a shape found by a numeric crossing (aspheres, torus patches, wave surfaces) at
+// local point p.
 template <class Rr>
 OWEC_HD V3<Rr> numericNormal(const DBoundary& b, const double* data, const V3<Rr>& p) {
     const double* P = b.params;
     if (b.shape == OWEC_SHAPE_TORUS) return torusNormal(Rr(P[0]), Rr(P[1]), p);
+    if (b.shape == OWEC_SHAPE_WAVES) return waveNormal(b, data, p);
     const Rr r = sqrt(p.x * p.x + p.y * p.y);
     return sagNormal(p, r, asphereSlope(Rr(P[0]), Rr(P[1]), data, int(b.dataCount), r));
 }
 // Whether boundary b's crossings are found numerically (no closed form).
 OWEC_HD bool numericShape(const DBoundary& b) {
-    return b.shape == OWEC_SHAPE_TORUS || (b.shape == OWEC_SHAPE_SAG && b.dataCount > 0);
+    return b.shape == OWEC_SHAPE_TORUS || b.shape == OWEC_SHAPE_WAVES || (b.shape == OWEC_SHAPE_SAG && b.dataCount > 0);
 }
 
 // Watertight line-triangle crossing test (Woop, Benthin and Wald 2013), edges included, as the

@@ -118,19 +118,19 @@ __device__ __forceinline__ bool analyticCandidate(const DeviceScene& sc, const R
     const DBoundary& bd = sc.boundaries[b];
     const V3<Rr> lo = bd.toLocal.point(V3<Rr>(q.od));
     const V3<Rr> ld = bd.toLocal.vector(V3<Rr>(q.d));
+    // Leaving this boundary, the anchor lies on it to the precision of the refinement, not of FP32:
+    // with the FP32 window a grazing ray's far crossing of the same sphere (at t = 2 R cos) fell
+    // inside it and was rejected as the departure, and the path leaked.
+    RayQuery<T> qs = q;
+    if (b == q.depB && sizeof(Rr) > sizeof(R)) qs.errN = q.errN * T(2.5e-7);
     AHits<Rr> hits;
     int n;
     // contacts: another surface through the anchor may lie just behind it (world.cpp:473-476); such
     // roots must lie within the rounding of the origin along the surface normal (checked below)
     if constexpr (Full)
         n = analyticCrossings<R, Rr, true>(bd, sc.shapeData + bd.dataOffset, lo, ld, -Rr(64) * Rr(q.errN), Rr(best),
-                                           b == q.depB, hits);
+                                           b == q.depB, hits, Rr(qs.errN), Rr(q.errN));
     else n = analyticCrossings<R, Rr, false>(bd, nullptr, lo, ld, Rr(0), Rr(best), false, hits);
-    // Leaving this boundary, the anchor lies on it to the precision of the refinement, not of FP32:
-    // with the FP32 window a grazing ray's far crossing of the same sphere (at t = 2 R cos) fell
-    // inside it and was rejected as the departure, and the path leaked.
-    RayQuery<T> qs = q;
-    if (b == q.depB && sizeof(Rr) > sizeof(R)) qs.errN = q.errN * T(2.5e-7);
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
         if (i >= n) break;

@@ -6,7 +6,7 @@
 // rule allows it core/, scene/, render/ and backends/cuda/ (not transport/). It flattens the world
 // model into owec_scene_desc: media, regions, optics, emitters, boundaries with their rigid frames
 // and shape data, the sun and sky, and the detector. Scenes using features the CUDA backend does not
-// implement (image textures, environment maps, wave surfaces, materials' aim guides) are refused with
+// implement (image textures, environment maps, stained glass, materials' aim guides) are refused with
 // std::runtime_error, as Backend::createRenderer does for unsupported settings
 // (src/owe/render/backend.hpp:44).
 #include <cmath>
@@ -45,7 +45,8 @@ struct Flat {
     owec_scene_desc desc{};
 
     // Appends a shape's data run and records it in the boundary.
-    void data(owec_boundary& b, std::initializer_list<double> values) {
+    void data(owec_boundary& b, std::initializer_list<double> values) { data(b, std::vector<double>(values)); }
+    void data(owec_boundary& b, const std::vector<double>& values) {
         b.data_offset = uint32_t(shapeData.size());
         b.data_count = uint32_t(values.size());
         shapeData.insert(shapeData.end(), values.begin(), values.end());
@@ -226,6 +227,14 @@ std::unique_ptr<Flat> flatten(const Scene& sc, int detectorIndex) {
             o.params[1] = dm->slitAzimuth();
             o.params[2] = dm->slitWidth();
             o.params[3] = dm->slitTop();
+        } else if (auto* ws = dynamic_cast<const WaveSurface*>(s)) {
+            o.shape = OWEC_SHAPE_WAVES;
+            o.params[0] = ws->halfX();
+            o.params[1] = ws->halfY();
+            o.params[2] = ws->margin();
+            std::vector<double> data = {double(ws->sampled() ? ws->nodesX() : 0), double(ws->sampled() ? ws->nodesY() : 0)};
+            for (const PlaneWave& w : ws->waves()) data.insert(data.end(), {w.amplitude, w.kx, w.ky, w.phase});
+            f->data(o, data);
         } else if (auto* me = dynamic_cast<const MeshShape*>(s)) {
             o.shape = OWEC_SHAPE_MESH;
             o.mesh = int32_t(f->meshes.size());

@@ -19,7 +19,7 @@ SPEC_CONSTANT, SPEC_TABULATED, SPEC_BLACKBODY = 0, 1, 2
 INDEX_CONSTANT, INDEX_CAUCHY, INDEX_SELLMEIER, INDEX_CIDDOR, INDEX_TABULATED = 0, 1, 2, 3, 4
 SURF_NULL, SURF_DIELECTRIC, SURF_DIFFUSE, SURF_CONDUCTOR, SURF_MIRROR, SURF_ABSORBER, SURF_DETECTOR = range(7)
 SHAPE_SPHERE, SHAPE_SAG, SHAPE_PLANE, SHAPE_CYLINDER, SHAPE_MESH, SHAPE_CONE, SHAPE_TORUS, SHAPE_ROUND_WALL, \
-    SHAPE_DOME = range(9)
+    SHAPE_DOME, SHAPE_WAVES = range(10)
 APERTURE_DISK, APERTURE_RECT, APERTURE_ELLIPSE, APERTURE_DISK_HOLE = 0, 1, 2, 3
 SKY_NONE, SKY_UNIFORM, SKY_GRADIENT = 0, 1, 2
 DETECTOR_OBSERVER, DETECTOR_SENSOR = 0, 1

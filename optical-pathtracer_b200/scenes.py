@@ -45,6 +45,78 @@ def rotate_to(frm, to):
     return np.eye(3) + math.sin(angle) * K + (1 - math.cos(angle)) * K @ K
 
 
+_M64 = (1 << 64) - 1
+
+
+class Pcg32:
+    """O'Neill's PCG32 as the reference's Rng (src/owe/core/sampling.hpp:11-30,
+    src/owe/core/shared/warps.hpp:24-30): a stream per (seed, stream id), 53-bit uniforms from two
+    outputs."""
+
+    def __init__(self, seed, stream):
+        self.state, self.inc = 0, ((stream << 1) | 1) & _M64
+        self.next_u32()
+        self.state = (self.state + seed) & _M64
+        self.next_u32()
+
+    def next_u32(self):
+        old = self.state
+        self.state = (old * 6364136223846793005 + self.inc) & _M64
+        x = (((old >> 18) ^ old) >> 27) & 0xFFFFFFFF
+        r = old >> 59
+        return ((x >> r) | (x << ((-r) & 31))) & 0xFFFFFFFF
+
+    def uniform(self):
+        a, b = self.next_u32() >> 5, self.next_u32() >> 6
+        return (a * 67108864.0 + b) * (1.0 / 9007199254740992.0)
+
+
+def align_z(axis, up=(0.0, 1.0, 0.0)):
+    """The rotation whose z column is `axis` and whose y column lies toward `up` (Transform::alignZ,
+    src/owe/core/math.hpp:123-132)."""
+    z = np.asarray(axis, float) / np.linalg.norm(axis)
+    u = np.asarray(up, float)
+    if abs(np.dot(u / np.linalg.norm(u), z)) > 0.999:
+        u = np.array([1.0, 0, 0]) if abs(z[0]) < 0.9 else np.array([0, 0, 1.0])
+    x = np.cross(u, z)
+    x /= np.linalg.norm(x)
+    return np.column_stack([x, np.cross(z, x), z])
+
+
+def wave_nodes(half_x, half_y, waves, spacing=-1.0):
+    """The node counts of a wave surface (WaveSurface's constructor, src/owe/scene/geometry.cpp:190-207):
+    (0, 0), the analytic sum, for spacing 0 or, by default, for up to six waves; otherwise nodes about
+    `spacing` apart (by default a twelfth of the shortest wavelength), 2 to 4096 per axis."""
+    k_max = max((math.hypot(w[1], w[2]) for w in waves), default=0.0)
+    if spacing < 0:
+        spacing = 0.0 if len(waves) <= 6 or k_max == 0 else (2 * math.pi / k_max) / 12
+    if not spacing > 0:
+        return 0, 0
+    return (min(max(math.ceil(2 * half_x / spacing) + 1, 2), 4096), min(max(math.ceil(2 * half_y / spacing) + 1, 2), 4096))
+
+
+def plane_wave(amplitude, wavelength, direction=0.0, phase=0.0):
+    """(amplitude, kx, ky, phase) of a wave(...) in a waves body (Loader::wavesBody,
+    src/owe/loader/loader_bodies.cpp:357-366)."""
+    k = 2 * math.pi / wavelength
+    return (amplitude, k * math.cos(direction), k * math.sin(direction), phase)
+
+
+def ripple_field(count, seed, min_wavelength, max_wavelength, slope=0.1, direction=0.0, spread=math.radians(90)):
+    """rippleField (src/owe/scene/builders.cpp:445-461): `count` waves with log-uniform wavelengths,
+    directions spread about `direction` and amplitudes slope / (k sqrt(count)), drawn from the
+    reference's PCG32 stream (seed, 0x7269707063)."""
+    rng = Pcg32(seed, 0x7269707063)
+    waves = []
+    for _ in range(count):
+        u1, u2, u3 = rng.uniform(), rng.uniform(), rng.uniform()
+        lam = min_wavelength * (max_wavelength / min_wavelength) ** u1
+        k = 2 * math.pi / lam
+        theta = direction + (u2 - 0.5) * spread
+        waves.append((slope / (k * math.sqrt(count)), k * math.cos(theta), k * math.sin(theta), 2 * math.pi * u3))
+    return waves
+
+
 def pose(R=None, t=(0, 0, 0)):
     m = np.zeros((3, 4))
     m[:, :3] = np.eye(3) if R is None else R
@@ -145,6 +217,62 @@ class SceneBuilder:
                                           (ctypes.c_double * 12)(*xf.ravel()), (ctypes.c_double * 4)(*p),
                                           offset, len(data)))
         return len(self.boundaries) - 1
+
+    def wave_surface(self, half_x, half_y, margin, waves, xf, front, back, optics, spacing=-1.0):
+        """A WaveSurface boundary: waves as (amplitude, kx, ky, phase); sampled at nodes as the
+        reference samples it (wave_nodes)."""
+        nx, ny = wave_nodes(half_x, half_y, waves, spacing)
+        data = [nx, ny] + [float(v) for w in waves for v in w]
+        return self.boundary(A.SHAPE_WAVES, [half_x, half_y, margin], xf, front, back, optics, data=data)
+
+    def water_pool(self, half_x, half_y, depth, margin, waves, medium, spacing=-1.0, bottom=None, walls=None, rim=None,
+                   base=None):
+        """buildWater (src/owe/scene/builders.cpp:402-443): a liquid region under a wave surface, closed by
+        a floor and four walls facing the liquid. Without `bottom` and `walls` (optics) those are smooth
+        dielectric interfaces to the ambient region; with them they are that matter, the basin an
+        opaque region cut into a block whose rim (default a quarter of the larger half size wide),
+        outer sides and underside (`base`, default a quarter of the depth, below the floor) face the
+        air. Returns the liquid's region."""
+        liquid = self.region(medium)
+        iface = self.dielectric()
+        basin = self.region(self.medium_opaque()) if bottom is not None or walls is not None else 0
+        self.wave_surface(half_x, half_y, margin, waves, pose(), 0, liquid, iface, spacing)
+        side = (lambda o: (basin, o) if o is not None else (0, iface))
+        floor_back, floor_optics = side(bottom)
+        self.boundary(A.SHAPE_PLANE, [A.APERTURE_RECT, half_x, half_y], translate(0.0, 0.0, -depth), liquid, floor_back,
+                      floor_optics)
+        wall_back, wall_optics = side(walls)
+        hz = depth / 2
+        for at, inward, half in (((half_x, 0.0, -hz), (-1, 0, 0), half_y), ((-half_x, 0.0, -hz), (1, 0, 0), half_y),
+                                 ((0.0, half_y, -hz), (0, -1, 0), half_x), ((0.0, -half_y, -hz), (0, 1, 0), half_x)):
+            self.boundary(A.SHAPE_PLANE, [A.APERTURE_RECT, half, hz], pose(align_z(inward, (0, 0, 1)), at), liquid,
+                          wall_back, wall_optics)
+        if basin:
+            ground = walls if walls is not None else bottom
+            rim = 0.25 * max(half_x, half_y) if rim is None else rim
+            base = 0.25 * depth if base is None else base
+            ox, oy, zb = half_x + rim, half_y + rim, -depth - base
+            oz = -zb / 2
+            for cx, cy, hx, hy in ((0.0, (oy + half_y) / 2, ox, (oy - half_y) / 2), (0.0, -(oy + half_y) / 2, ox, (oy - half_y) / 2),
+                                   ((ox + half_x) / 2, 0.0, (ox - half_x) / 2, half_y),
+                                   (-(ox + half_x) / 2, 0.0, (ox - half_x) / 2, half_y)):
+                self.boundary(A.SHAPE_PLANE, [A.APERTURE_RECT, hx, hy], translate(cx, cy, 0.0), 0, basin, ground)
+            for at, outward, half in (((ox, 0.0, zb / 2), (1, 0, 0), oy), ((-ox, 0.0, zb / 2), (-1, 0, 0), oy),
+                                      ((0.0, oy, zb / 2), (0, 1, 0), ox), ((0.0, -oy, zb / 2), (0, -1, 0), ox)):
+                self.boundary(A.SHAPE_PLANE, [A.APERTURE_RECT, half, oz], pose(align_z(outward, (0, 0, 1)), at), 0, basin,
+                              ground)
+            self.boundary(A.SHAPE_PLANE, [A.APERTURE_RECT, ox, oy], pose(align_z((0, 0, -1)), (0.0, 0.0, zb)), 0, basin,
+                          ground)
+        return liquid
+
+    def medium_water(self):
+        """The catalogue's water (src/owe/core/medium.cpp:136-142): Daimon and Masumura's Sellmeier
+        index at 20 C, absorption after Pope and Fry (1/m)."""
+        absorption = self.spectrum_tabulated([380, 400, 450, 500, 550, 600, 650, 700, 750, 800],
+                                             [0.0114, 0.00663, 0.0092, 0.0204, 0.0565, 0.2224, 0.34, 0.65, 2.47, 2.07])
+        return self.medium_sellmeier((5.684027565e-1, 1.726177391e-1, 2.086189578e-2, 1.130748688e-1),
+                                     (5.101829712e-3, 1.821153936e-2, 2.620722293e-2, 1.069792721e1),
+                                     absorption=absorption)
 
     def mesh(self, vertices, triangles):
         v = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 3)
@@ -619,6 +747,35 @@ def asphere_lens(width=48, height=48):
     sb.sheet(4.0, 4.0, pose(), sb.diffuse(0.8))
     sb.sun((0.1, -0.15, 1.0), 2.0e4)
     sb.observer(width, height, (0.0, -2.6, 2.4), (0.0, 0.0, 0.6), fov_y_deg=40.0)
+    return sb
+
+
+def ripple_caustics(amplitude=0.0005, wavelength=0.02, depth=0.08, gap=0.001):
+    """Sunlight through water rippled by one plane wave h = a sin(k x) onto the flat bottom of a layer,
+    and out into a 160 x 4-pixel sensor just below it (tests/test_references.cpp:322-345): an
+    overhead sun of unit radiance, a 0.24 m pool with a 0.03 m margin and dielectric floor and walls."""
+    sb = SceneBuilder()
+    sb.sun((0.0, 0.0, 1.0), 1.0)
+    sb.water_pool(0.06, 0.06, depth, 0.03, [plane_wave(amplitude, wavelength)], sb.medium_water())
+    b = sb.sheet(0.02, 0.01, translate(0.0, 0.0, -depth - gap), sb.optics_(A.SURF_DETECTOR))
+    sb.sensor(160, 4, b, 0.02, 0.01)
+    return sb
+
+
+def wave_pool(width=48, height=32, sampled=False, sun_radius_deg=4.0):
+    """A pool of water in a Lambertian basin (benchmarks/caustic_water_surface.owe's body, smaller and
+    shallower waves): three analytic plane waves, or 24 ripples sampled as a bicubic spline, under a
+    sun widened to `sun_radius_deg` and a uniform sky, seen obliquely through a pinhole."""
+    sb = SceneBuilder()
+    if sampled:
+        waves = ripple_field(24, 3, 0.01, 0.05, slope=0.15)
+    else:
+        waves = [plane_wave(0.002, 0.03, 0.3), plane_wave(0.0012, 0.021, 1.9, 1.0), plane_wave(0.0008, 0.013, -0.7, 2.0)]
+    tile = sb.diffuse(0.8)
+    sb.water_pool(0.15, 0.15, 0.08, 0.05, waves, sb.medium_water(), bottom=tile, walls=tile)
+    sb.sun((0.3, -0.2, 1.0), 150.0, angular_radius=math.radians(sun_radius_deg))
+    sb.uniform_sky(0.3)
+    sb.observer(width, height, (0.0, -0.26, 0.26), (0.0, 0.0, -0.06), fov_y_deg=45.0)
     return sb
 
 

@@ -9,6 +9,7 @@
 //     mode the reference lacks (the pattern of tests/test_transport.cpp:185-186);
 //   - oweref_render_backend: the same through the reference's own `cpu` Backend, unchanged;
 //   - oweref_cast_rays: World::intersect (src/owe/scene/world.cpp:553-582) for hit-ID parity.
+#include <algorithm>
 #include <array>
 #include <atomic>
 #include <cmath>
@@ -114,6 +115,24 @@ std::shared_ptr<const Shape> makeShape(const owec_scene_desc& d, const owec_boun
             return std::make_shared<RoundWallShape>(p[0], p[1], std::move(open));
         }
         case OWEC_SHAPE_DOME: return std::make_shared<DomeShape>(p[0], p[1], p[2], p[3]);
+        case OWEC_SHAPE_WAVES: {
+            if (b.data_count < 2 || (b.data_count - 2) % 4)
+                throw std::runtime_error("wave surface: its data is the node counts and four values per wave");
+            std::vector<PlaneWave> waves;
+            for (uint32_t i = 2; i + 3 < b.data_count; i += 4) waves.push_back({data[i], data[i + 1], data[i + 2], data[i + 3]});
+            const int nx = int(data[0]), ny = int(data[1]);
+            // WaveSurface takes a node spacing: find one that its constructor turns into these counts
+            double spacing = 0;
+            if (nx > 0) {
+                auto count = [](double half, double s) { return std::clamp(int(std::ceil(2 * half / s)) + 1, 2, 4096); };
+                spacing = std::max(2 * p[0] / (nx - 1), 2 * p[1] / (ny - 1));
+                for (int k = 0; k < 8 && (count(p[0], spacing) != nx || count(p[1], spacing) != ny); ++k)
+                    spacing = std::nextafter(spacing, INFINITY);
+                if (count(p[0], spacing) != nx || count(p[1], spacing) != ny)
+                    throw std::runtime_error("wave surface: no node spacing gives these node counts");
+            }
+            return std::make_shared<WaveSurface>(std::move(waves), p[0], p[1], p[2], spacing);
+        }
         case OWEC_SHAPE_MESH: {
             if (b.mesh < 0 || uint32_t(b.mesh) >= d.n_meshes) throw std::runtime_error("mesh index out of range");
             const owec_mesh& m = d.meshes[b.mesh];
