@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define OWEC_ABI_VERSION 3
+#define OWEC_ABI_VERSION 4
 
 /* ------------------------------------------------------------------ status codes */
 #define OWEC_OK 0
@@ -115,6 +115,13 @@ typedef struct owec_optics {
     int32_t texture_c;
     double texture_scale;  /* cell or feature size, metres */
     double texture_param;  /* terrain: snow line height; rings, bands, marble: turbulence */
+    /* A Lambertian surface's aim guide (SurfaceOptics::sampleAim*, src/owe/scene/world.hpp:113-114):
+     * in radiance transport from the front, aim_share of the scattered directions are drawn toward
+     * the disk (aim_center, aim_normal, aim_radius), world coordinates; 0 = none */
+    double aim_center[3];
+    double aim_normal[3];
+    double aim_radius;
+    double aim_share;
 } owec_optics;
 
 typedef struct owec_emission {

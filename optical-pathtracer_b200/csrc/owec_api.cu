@@ -510,6 +510,13 @@ void validateDesc(const owec_scene_desc& d) {
                     (o.type == OWEC_SURF_DIFFUSE && o.reflectance >= 0 && o.texture_b >= 0 && specOk(o.texture_b) &&
                      o.texture_c >= 0 && specOk(o.texture_c) && o.texture_scale > 0),
                 "a texture needs a Lambertian surface, its three spectra and a positive scale");
+        if (o.aim_share != 0) {
+            const double nl = std::sqrt(o.aim_normal[0] * o.aim_normal[0] + o.aim_normal[1] * o.aim_normal[1] +
+                                        o.aim_normal[2] * o.aim_normal[2]);
+            require(o.type == OWEC_SURF_DIFFUSE && o.aim_share > 0 && o.aim_share <= 1 && o.aim_radius > 0 && nl > 0 &&
+                        std::isfinite(o.aim_center[0] + o.aim_center[1] + o.aim_center[2]),
+                    "an aim guide needs a Lambertian surface, a share in (0, 1], a disk radius and a normal");
+        }
     }
     for (uint32_t i = 0; i < d.n_emissions; ++i) require(specOk(d.emissions[i].radiance) && d.emissions[i].radiance >= 0,
                                                           "emission needs a radiance spectrum");
@@ -905,6 +912,17 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
         }
     }
 
+    // Aim guides in the camera-relative frame, with unit normals.
+    for (owec_optics& o : c.optics) {
+        if (!(o.aim_share > 0)) continue;
+        const double nl = std::sqrt(o.aim_normal[0] * o.aim_normal[0] + o.aim_normal[1] * o.aim_normal[1] +
+                                    o.aim_normal[2] * o.aim_normal[2]);
+        for (int k = 0; k < 3; ++k) {
+            o.aim_center[k] -= origin[k];
+            o.aim_normal[k] /= nl;
+        }
+    }
+
     // Upload.
     c.dSpectra.upload(c.spectra.data(), c.spectra.size(), s);
     if (c.table.empty()) c.table.assign(2, 0.0);  // never empty, so its device pointer is valid
@@ -941,7 +959,7 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
             ds.fullFeatures = 1;
     }
     for (uint32_t i = 0; i < d.n_optics; ++i)
-        if (d.optics[i].texture != OWEC_TEXTURE_NONE) ds.fullFeatures = 1;
+        if (d.optics[i].texture != OWEC_TEXTURE_NONE || d.optics[i].aim_share > 0) ds.fullFeatures = 1;
     // contacts: resolved as the reference does by the contact-resolving instantiation; the tolerance
     // is the FP32 anchor error over the scene's extent
     c.contacts = hasContacts(d, 1e-5 * std::max(2 * sceneRadius, 1e-3));

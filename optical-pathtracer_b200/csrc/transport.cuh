@@ -159,6 +159,42 @@ __device__ __forceinline__ double diskAimPdf(const V3<double>& p, const V3<doubl
     return t * t / (fabs(dn) * kPi * radius * radius);
 }
 
+// A Lambertian surface's aim guide (sampleScatter and evalScatter's diffuse mixture,
+// src/owe/transport/scattering.cpp:120-131, 173-174): in radiance transport met from the front, the
+// uniform uc below the share draws the direction toward the guide's disk (the disk point from u1, u2
+// by the concentric map) instead of from the cosine lobe (s, already drawn from u1, u2), and the pdf
+// becomes the mixture. p: the camera-relative hit point; n: the normal toward the front.
+template <class R>
+__device__ __forceinline__ bool aimDiffuse(const owec_optics& o, const V3<double>& p, const V3<R>& n, R albedo, R uc,
+                                           R u1, R u2, ScatterSample<R>& s) {
+    const double share = o.aim_share;
+    const V3<double> c(o.aim_center[0], o.aim_center[1], o.aim_center[2]);
+    const V3<double> an(o.aim_normal[0], o.aim_normal[1], o.aim_normal[2]);
+    const bool toDisk = double(uc) < share;
+    V3<double> wi(s.wi);
+    if (toDisk) {
+        V3<double> a, b;
+        basis(an, a, b);
+        double dx, dy;
+        concentricDisk(double(u1), double(u2), dx, dy);
+        wi = normalize(c + (a * dx + b * dy) * o.aim_radius - p);
+    }
+    const double cs = dot(wi, V3<double>(n));
+    if (cs <= 0) return false;
+    const double pdf = (1 - share) * cs * kInvPi + share * diskAimPdf(p, wi, c, an, o.aim_radius, toDisk);
+    s.wi = V3<R>(wi);
+    s.pdf = R(pdf);
+    s.weight = R(double(albedo) * cs * kInvPi / pdf);
+    return pdf > 0;
+}
+// The mixture pdf of direction wi at a guided Lambertian surface, given its cosine-lobe pdf.
+__device__ __forceinline__ double aimDiffusePdf(const owec_optics& o, const V3<double>& p, const V3<double>& wi,
+                                                double cosinePdf) {
+    const V3<double> c(o.aim_center[0], o.aim_center[1], o.aim_center[2]);
+    const V3<double> an(o.aim_normal[0], o.aim_normal[1], o.aim_normal[2]);
+    return (1 - o.aim_share) * cosinePdf + o.aim_share * diskAimPdf(p, wi, c, an, o.aim_radius, false);
+}
+
 // ------------------------------------------------------------------ sky
 // The sky's radiance toward direction dir at wavelength lambda (Environment::sky,
 // src/owe/scene/world.cpp:56-73): none, uniform, or the gradient from the ground through the

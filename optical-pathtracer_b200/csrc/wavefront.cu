@@ -610,6 +610,8 @@ __global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SH
                                 j == 0 ? it : makeInterface<R, Simple>(sc, bd, g.n, R(sp.lambda[j]), R(pp.fresnelFloor), tex);
                             fN[j] = evalScatter(sc, itj, d, wi, true, pdf);
                             if (j == 0) pdfS = pdf;
+                            if (Full && j == 0 && pdf > R(0) && o.type == OWEC_SURF_DIFFUSE && fromFront && o.aim_share > 0)
+                                pdfS = R(aimDiffusePdf(o, g.p, ls.wi, double(pdf)));
                             if (fN[j] != R(0)) fZero = false;
                         }
                         if (!fZero) {
@@ -622,7 +624,9 @@ __global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SH
             }
             const Draw3<R> u(rng);
             ScatterSample<R> s;
-            const bool ok = sampleScatter(sc, it, d, u.u1, u.u2, u.u3, true, s);
+            bool ok = sampleScatter(sc, it, d, u.u1, u.u2, u.u3, true, s);
+            if (Full && ok && o.type == OWEC_SURF_DIFFUSE && fromFront && o.aim_share > 0)
+                ok = aimDiffuse(o, g.p, g.n, it.albedo, u.u1, u.u2, u.u3, s);
             if (ok && s.weight > R(0)) {
                 // weighScatter (transport.cpp:227-233)
                 sp.beta[0] *= s.weight;

@@ -6,7 +6,7 @@
 // rule allows it core/, scene/, render/ and backends/cuda/ (not transport/). It flattens the world
 // model into owec_scene_desc: media, regions, optics, emitters, boundaries with their rigid frames
 // and shape data, the sun and sky, and the detector. Scenes using features the CUDA backend does not
-// implement (image textures, environment maps, stained glass, materials' aim guides) are refused with
+// implement (image textures and maps, environment maps, stained glass) are refused with
 // std::runtime_error, as Backend::createRenderer does for unsupported settings
 // (src/owe/render/backend.hpp:44).
 #include <cmath>
@@ -126,9 +126,9 @@ std::unique_ptr<Flat> flatten(const Scene& sc, int detectorIndex) {
     }
     for (const Region& r : w.regions()) f->regionMedium.push_back(r.medium);
     for (const SurfaceOptics& so : w.optics()) {
-        if (so.texture.kind == Texture::Kind::Image || so.sampleAimShare > 0 || !so.roughnessMap.empty() ||
-            so.reliefDepth != 0 || so.normalImage.image || so.roughnessImage.image)
-            throw std::runtime_error("material '" + so.name + "' uses image textures, maps or aim guides, which the cuda backend does not render");
+        if (so.texture.kind == Texture::Kind::Image || !so.roughnessMap.empty() || so.reliefDepth != 0 ||
+            so.normalImage.image || so.roughnessImage.image)
+            throw std::runtime_error("material '" + so.name + "' uses image textures or maps, which the cuda backend does not render");
         if (so.type == SurfaceType::StainedGlass) throw std::runtime_error("stained glass is not rendered by the cuda backend");
         owec_optics o{};
         o.type = int32_t(so.type);
@@ -146,6 +146,15 @@ std::unique_ptr<Flat> flatten(const Scene& sc, int detectorIndex) {
             o.texture_c = f->spectrum(so.texture.c);
             o.texture_scale = so.texture.scale;
             o.texture_param = so.texture.param;
+        }
+        if (so.sampleAimShare > 0 && so.type == SurfaceType::Diffuse) {
+            // a measurement screen's or the indirect guide's aim (sampleScatter, scattering.cpp:120-131)
+            for (int k = 0; k < 3; ++k) {
+                o.aim_center[k] = so.sampleAimCenter[k];
+                o.aim_normal[k] = so.sampleAimNormal[k];
+            }
+            o.aim_radius = so.sampleAimRadius;
+            o.aim_share = so.sampleAimShare;
         }
         f->optics.push_back(o);
     }

@@ -10,7 +10,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libowec.so")
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 OK = 0
 E_INVALID, E_CUDA, E_NOMEM, E_STATE, E_DEVICE_FAULT, E_UNSUPPORTED = -1, -2, -3, -4, -5, -6
@@ -49,7 +49,9 @@ class Optics(ctypes.Structure):
     _fields_ = [("type", ctypes.c_int32), ("back_absorbs", ctypes.c_int32), ("reflectance", ctypes.c_int32),
                 ("conductor_n", ctypes.c_int32), ("conductor_k", ctypes.c_int32), ("texture", ctypes.c_int32),
                 ("roughness", ctypes.c_double), ("texture_b", ctypes.c_int32), ("texture_c", ctypes.c_int32),
-                ("texture_scale", ctypes.c_double), ("texture_param", ctypes.c_double)]
+                ("texture_scale", ctypes.c_double), ("texture_param", ctypes.c_double),
+                ("aim_center", ctypes.c_double * 3), ("aim_normal", ctypes.c_double * 3), ("aim_radius", ctypes.c_double),
+                ("aim_share", ctypes.c_double)]
 
 
 TEXTURE_NONE, TEXTURE_CHECKER, TEXTURE_NOISE, TEXTURE_RINGS, TEXTURE_TERRAIN, TEXTURE_BANDS, TEXTURE_RADIAL, \

@@ -195,6 +195,15 @@ class SceneBuilder:
         opt.texture_scale, opt.texture_param = float(scale), float(param)
         return o
 
+    def aim_guide(self, optics, center, normal, radius, share):
+        """Guide a Lambertian surface's scattering: `share` of its directions toward the disk of
+        `radius` at `center` facing `normal` (SurfaceOptics::sampleAim*)."""
+        o = self.optics[optics]
+        o.aim_center = (ctypes.c_double * 3)(*center)
+        o.aim_normal = (ctypes.c_double * 3)(*normal)
+        o.aim_radius, o.aim_share = float(radius), float(share)
+        return optics
+
     def dielectric(self, roughness=0.0):
         return self.optics_(A.SURF_DIELECTRIC, roughness=roughness)
 

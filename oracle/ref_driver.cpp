@@ -201,6 +201,13 @@ std::unique_ptr<RefScene> buildScene(const owec_scene_desc& d) {
             so.texture.scale = o.texture_scale;
             so.texture.param = o.texture_param;
         }
+        if (o.aim_share > 0) {
+            const Vec3 n{o.aim_normal[0], o.aim_normal[1], o.aim_normal[2]};
+            so.sampleAimCenter = {o.aim_center[0], o.aim_center[1], o.aim_center[2]};
+            so.sampleAimNormal = normalize(n);
+            so.sampleAimRadius = o.aim_radius;
+            so.sampleAimShare = o.aim_share;
+        }
         if (so.type == SurfaceType::Detector) so.detector = 0;
         // a diffuse measurement screen: the sensor's own boundary with Lambertian optics
         if (so.type == SurfaceType::Diffuse && d.detector.kind == OWEC_DETECTOR_SENSOR &&
