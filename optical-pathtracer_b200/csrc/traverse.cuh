@@ -114,7 +114,7 @@ template <> __device__ __forceinline__ double farWiden<double>() { return 4e-16;
 // The analytic boundary b's first acceptable crossing in (0, best); FP64 refinement when Rr = double.
 template <class R, class Rr, class T, bool Full>
 __device__ __forceinline__ bool analyticCandidate(const DeviceScene& sc, const RayQuery<T>& q, uint32_t b, T best, Rr& tOut,
-                                                  bool& frontOut) {
+                                                  bool& frontOut, float& cosOut) {
     const DBoundary& bd = sc.boundaries[b];
     const V3<Rr> lo = bd.toLocal.point(V3<Rr>(q.od));
     const V3<Rr> ld = bd.toLocal.vector(V3<Rr>(q.d));
@@ -140,6 +140,7 @@ __device__ __forceinline__ bool analyticCandidate(const DeviceScene& sc, const R
         if (!acceptCrossing<T, Full>(sc, qs, b, 0u, false, T(h.t), nw)) continue;
         tOut = h.t;
         frontOut = dot(q.d, nw) < T(0);
+        cosOut = float(fabs(dot(q.d, nw)));
         return true;
     }
     return false;
@@ -153,6 +154,7 @@ struct AnalyticResult {
     Rr t;
     bool ok;
     bool front;  // met from the boundary's front side
+    float cosAbs;  // |cos| between the ray and the surface normal there
 };
 template <class T, class R, class Rr, bool Full>
 __device__ __noinline__ AnalyticResult<Rr> analyticHit(const DeviceScene* scp, uint32_t b, V3<double> od, V3<T> d, T best,
@@ -169,7 +171,8 @@ __device__ __noinline__ AnalyticResult<Rr> analyticHit(const DeviceScene* scp, u
     AnalyticResult<Rr> r;
     r.t = Rr(0);
     r.front = false;
-    r.ok = analyticCandidate<R, Rr, T, Full>(*scp, q, b, best, r.t, r.front);
+    r.cosAbs = 1.f;
+    r.ok = analyticCandidate<R, Rr, T, Full>(*scp, q, b, best, r.t, r.front, r.cosAbs);
     return r;
 }
 
@@ -325,6 +328,7 @@ struct Traversal {
     V3<T> inv, oinv;
     ShearedRay<T> sh;
     T best;
+    T bestCos;            // contact-resolving instantiation: |cos| of the closest crossing's incidence
     HitRec hit;           // written when a crossing is accepted
     Stack st;
     uint32_t nodeBase, nodeBits;  // the current node group (as a stack entry)
@@ -341,6 +345,7 @@ struct Traversal {
         oinv = V3<T>(q.o.x * inv.x, q.o.y * inv.y, q.o.z * inv.z);
         sh = shearRay(q.d);
         best = q.tmax;
+        bestCos = T(1);
         found = false;
         sp = 0;
         st.init(stack, stride);
@@ -387,7 +392,7 @@ struct Traversal {
             NodeWords nd;
             loadNode(sc.nodes, node, nd);
             if (Count) ++nodeVisits;
-            const uint32_t mask = intersectChildren(nd, inv, oinv, T(0), Full ? best * (T(1) + tieWindow<T>()) : best);
+            const uint32_t mask = intersectChildren(nd, inv, oinv, T(0), Full ? tieLimit() : best);
             const uint32_t inner = nd.a.w >> 24;
             nodeBase = nd.b.x;
             nodeBits = permuteSlots(mask & inner, first) | (inner << 8);
@@ -404,15 +409,21 @@ struct Traversal {
         return kTraceRunning;
     }
 
-    // Whether boundary b's crossing at t, met from its front side when `front`, replaces the current
-    // closest (the contact-resolving instantiation; NearestCrossing::offer,
-    // src/owe/scene/world.cpp:515-550). Crossings of different boundaries within the tie window are
+    // How far beyond the closest crossing the contact-resolving traversal still looks: the tie
+    // window, widened by the closest crossing's grazing incidence (coincident faces' distances differ
+    // by their offsets' rounding over the cosine).
+    __device__ __forceinline__ T tieSpan(T c) const { return best * tieWindow<T>() / fmax(c, T(1e-3)); }
+    __device__ __forceinline__ T tieLimit() const { return best + tieSpan(bestCos); }
+
+    // Whether boundary b's crossing at t, met from its front side when `front` at incidence |cos| c,
+    // replaces the current closest (the contact-resolving instantiation; NearestCrossing::offer,
+    // src/owe/scene/world.cpp:515-550). Crossings of different boundaries within the tie span are
     // one contact: the one met from the ray's region wins, matter wins over a zero-thickness
     // readout, then the lower boundary index; two that both match leave the order undecided
     // (kHitAmbiguous). `flags` receives the winner's flags.
-    __device__ __forceinline__ bool winsContact(const DeviceScene& sc, uint32_t b, T t, bool front, uint32_t& flags) {
+    __device__ __forceinline__ bool winsContact(const DeviceScene& sc, uint32_t b, T t, bool front, T c, uint32_t& flags) {
         const uint32_t frontFlag = front ? kHitFront : 0u;
-        if (!found || t < best * (T(1) - tieWindow<T>()) || b == hit.boundary) {
+        if (!found || t < best - tieSpan(fmin(c, bestCos)) || b == hit.boundary) {
             flags = frontFlag;
             return !found || t < best;
         }
@@ -450,7 +461,7 @@ struct Traversal {
         uint32_t b, prim, kind;
         TriFetch<T>::get(sc, i, v0, v1, v2, b, prim, kind);
         // the contact-resolving instantiation looks a tie window beyond the closest so far
-        const T limit = Full ? best * (T(1) + tieWindow<T>()) : best;
+        const T limit = Full ? tieLimit() : best;
         uint32_t flags = 0;
         if (kind == kPrimTriangle) {
             const V3<T> a = v0 - q.o, bb = v1 - q.o, c = v2 - q.o;
@@ -464,7 +475,9 @@ struct Traversal {
                 return false;
             if (!acceptCrossing<T, Full>(sc, q, b, prim, true, t, n)) return false;
             if constexpr (Full) {
-                if (!winsContact(sc, b, t, dn < T(0), flags)) return false;
+                const T c = fabs(dn) / sqrt(dot(n, n));
+                if (!winsContact(sc, b, t, dn < T(0), c, flags)) return false;
+                bestCos = c;
             }
             best = t;
             hit.t = double(t);
@@ -473,7 +486,8 @@ struct Traversal {
             const AnalyticResult<Rr> ar = analyticHit<T, R, Rr, Full>(sc.self, b, q.od, q.d, limit, q.depB, q.region, q.errN);
             if (!ar.ok) return false;
             if constexpr (Full) {
-                if (!winsContact(sc, b, T(ar.t), ar.front, flags)) return false;
+                if (!winsContact(sc, b, T(ar.t), ar.front, T(ar.cosAbs), flags)) return false;
+                bestCos = T(ar.cosAbs);
             }
             best = T(ar.t);
             hit.t = double(ar.t);

@@ -37,8 +37,7 @@ def test_touching_blocks_and_thin_plates_like_the_reference(thickness):
             for key in st:
                 st[key] += gs[key]
     save_artifact(f"contacts_{thickness:g}", ref=np.array(runs_ref), gpu=np.array(runs_gpu))
-    # The reference's paths meet no inconsistent region. On the device a few in 10^4 still do (grazing
-    # crossings of the coincident faces, whose FP32 distances differ by more than the tie window):
+    # The reference's paths meet no inconsistent region. On the device about two in 10^4 still do:
     # the bound is one path in 10^3. Before contacts were resolved one path in ten did.
     assert ref_stats["inconsistencies"] == 0 and ref_stats["leaks"] == 0, ref_stats
     assert st["inconsistencies"] + st["leaks"] <= 1e-3 * st["paths"], st
