@@ -56,6 +56,59 @@ struct alignas(16) PathAux {
 };
 constexpr uint32_t kFlagSpecular = 1u, kFlagAlive = 2u;
 
+// Path state passes through the L2 once per kernel, far more of it than the L2 holds. Its loads and
+// stores are marked evict-first (ld.global.cs / st.global.cs), so that it does not displace the
+// BVH nodes and primitives, which every traversal kernel reads again.
+#ifndef OWEC_STREAM_STATE
+#define OWEC_STREAM_STATE 1
+#endif
+template <class T>
+__device__ __forceinline__ T loadStream(const T* p) {
+#if OWEC_STREAM_STATE
+    if constexpr (alignof(T) >= 16 && sizeof(T) % 16 == 0) {
+        constexpr int n = int(sizeof(T) / 16);
+        uint4 w[n];
+#pragma unroll
+        for (int k = 0; k < n; ++k) w[k] = __ldcs(reinterpret_cast<const uint4*>(p) + k);
+        T v;
+        memcpy(&v, w, sizeof(T));
+        return v;
+    } else {
+        static_assert(sizeof(T) % 8 == 0 && alignof(T) >= 8, "path state records are whole 8-byte words");
+        constexpr int n = int(sizeof(T) / 8);
+        unsigned long long w[n];
+#pragma unroll
+        for (int k = 0; k < n; ++k) w[k] = __ldcs(reinterpret_cast<const unsigned long long*>(p) + k);
+        T v;
+        memcpy(&v, w, sizeof(T));
+        return v;
+    }
+#else
+    return *p;
+#endif
+}
+template <class T>
+__device__ __forceinline__ void storeStream(T* p, const T& v) {
+#if OWEC_STREAM_STATE
+    if constexpr (alignof(T) >= 16 && sizeof(T) % 16 == 0) {
+        constexpr int n = int(sizeof(T) / 16);
+        uint4 w[n];
+        memcpy(w, &v, sizeof(T));
+#pragma unroll
+        for (int k = 0; k < n; ++k) __stcs(reinterpret_cast<uint4*>(p) + k, w[k]);
+    } else {
+        static_assert(sizeof(T) % 8 == 0 && alignof(T) >= 8, "path state records are whole 8-byte words");
+        constexpr int n = int(sizeof(T) / 8);
+        unsigned long long w[n];
+        memcpy(w, &v, sizeof(T));
+#pragma unroll
+        for (int k = 0; k < n; ++k) __stcs(reinterpret_cast<unsigned long long*>(p) + k, w[k]);
+    }
+#else
+    *p = v;
+#endif
+}
+
 // A pending next-event visibility query and its contribution if the segment is clear.
 template <class R>
 struct alignas(16) ShadowRay {

@@ -274,7 +274,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kIntersect(DeviceScene sc, PathBuffers<RT<
         const uint32_t k = refillLanes(!alive, fetch, n, exhausted);
         if (!alive && k < n) {
             path = q.active[cur][k];
-            const PathRay<R> ray = pb.ray[path];
+            const PathRay<R> ray = loadStream(pb.ray + path);
             RayQuery<R> rq;
             rq.od = rayOrigin(ray.o);
             rq.o = V3<R>(rq.od);
@@ -304,7 +304,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kIntersect(DeviceScene sc, PathBuffers<RT<
                 }
                 if (s != kTraceHit) { h.boundary = kNone; h.t = INFINITY; }
                 if (s == kTraceOverflow) h.boundary = kNone - 1u;  // a fault: the path ends
-                pb.hit[path] = h;
+                storeStream(pb.hit + path, h);
                 if (Count) countTraversal(sc.travCounters, nv, nt);
                 ++segments;
                 faults += s == kTraceOverflow;
@@ -361,7 +361,7 @@ __device__ void queueNee(const DeviceScene& sc, PathBuffers<RT<M>>& pb, Queues& 
     sr.path = pathIdx;
     sr.errN = errN;
     for (int k = 0; k < NW; ++k) sr.contrib[k] = contrib[k];
-    pb.shadow[slot] = sr;
+    storeStream(pb.shadow + slot, sr);
     q.shadow[slot] = slot;
 }
 
@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kMedium(DeviceSc
     const uint32_t n = q.counts[cur];
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const uint32_t i = q.active[cur][k];
-        const HitRec h = pb.hit[i];
+        const HitRec h = loadStream(pb.hit + i);
         {
             // A segment through a region without absorption or scattering that met a boundary has
             // no medium event (sampleMedium draws nothing and changes nothing): straight to the
@@ -388,9 +388,9 @@ __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kMedium(DeviceSc
                 continue;
             }
         }
-        PathRay<R> ray = pb.ray[i];
-        PathSpec<R> sp = pb.spec[i];
-        PathAux aux = pb.aux[i];
+        PathRay<R> ray = loadStream(pb.ray + i);
+        PathSpec<R> sp = loadStream(pb.spec + i);
+        PathAux aux = loadStream(pb.aux + i);
         Pcg32 rng{aux.rngState, (uint64_t(aux.stream) << 1u) | 1u};
         const bool fault = h.boundary == kNone - 1u;
         const bool found = h.boundary < kNone - 1u;
@@ -487,9 +487,9 @@ __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kMedium(DeviceSc
         if (cont) aux.depth += 1;
         if (!toSurface && !cont) aux.flags &= ~kFlagAlive;
         aux.rngState = rng.state;
-        pb.ray[i] = ray;
-        pb.spec[i] = sp;
-        pb.aux[i] = aux;
+        storeStream(pb.ray + i, ray);
+        storeStream(pb.spec + i, sp);
+        storeStream(pb.aux + i, aux);
         queueNee<M>(sc, pb, q, i, sp, betaNee, ls, fN, pdfS, R(1), sp3, ray.region, kNone, kNone, 0.f, neeValid);
         warpCount(&st->leaks, leak);
         // surface events on Lambertian, absorbing and detecting boundaries go to the lean kernel
@@ -522,10 +522,10 @@ __global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SH
     const uint32_t* queue = Simple ? q.surfaceSimple : q.surface;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const uint32_t i = queue[k];
-        PathRay<R> ray = pb.ray[i];
-        PathSpec<R> sp = pb.spec[i];
-        PathAux aux = pb.aux[i];
-        const HitRec h = pb.hit[i];
+        PathRay<R> ray = loadStream(pb.ray + i);
+        PathSpec<R> sp = loadStream(pb.spec + i);
+        PathAux aux = loadStream(pb.aux + i);
+        const HitRec h = loadStream(pb.hit + i);
         Pcg32 rng{aux.rngState, (uint64_t(aux.stream) << 1u) | 1u};
         const DBoundary& bd = sc.boundaries[h.boundary];
         const SurfacePoint<R> g = hitGeometry<R, Ro, Rr, Full>(sc, ray, h);
@@ -654,9 +654,9 @@ __global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SH
         if (cont) aux.depth += 1;
         else aux.flags &= ~kFlagAlive;
         aux.rngState = rng.state;
-        pb.ray[i] = ray;
-        pb.spec[i] = sp;
-        pb.aux[i] = aux;
+        storeStream(pb.ray + i, ray);
+        storeStream(pb.spec + i, sp);
+        storeStream(pb.aux + i, aux);
         queueNee<M>(sc, pb, q, i, sp, betaNee, ls, fN, pdfS, cosF, g.p, neeRegion, h.boundary, h.prim, errN, neeValid);
         warpCount(&st->inconsistencies, inconsistent);
         warpPush(q.active[nxt], &q.counts[nxt], cont, i);
@@ -693,7 +693,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
         bool begin = false;  // start a segment from rq
         RayQuery<R> rq;
         if (!alive && k < n) {
-            const ShadowRay<R> sr = pb.shadow[k];
+            const ShadowRay<R> sr = loadStream(pb.shadow + k);
             job = k;
             path = sr.path;
             for (int j = 0; j < NW; ++j) Tr[j] = R(1);
@@ -881,7 +881,7 @@ __global__ void __launch_bounds__(256) kShadowApply(DeviceScene sc, PathBuffers<
         uint8_t v = vis[k];
         bool clear = v == 1;
         if (clear) {
-            const ShadowRay<R> sr = pb.shadow[k];
+            const ShadowRay<R> sr = loadStream(pb.shadow + k);
             const bool finite = !isinf(sr.tmax);
             // Tracer::transmittance's one segment (transport.cpp:237-308): the medium it crosses
             R Tr[NW] = {R(1), R(1), R(1), R(1)};
