@@ -186,14 +186,36 @@ struct NodeWords {
     uint4 a, b, c, d, e;
 };
 
+// Read-only 16-byte load of a BVH word with the L2 eviction priority evict-last (a createpolicy cache
+// hint): every traversal rereads the nodes and primitives, while the path state that streams past
+// them is evict-first.
+#ifndef OWEC_BVH_KEEP
+#define OWEC_BVH_KEEP 1
+#endif
+__device__ __forceinline__ uint4 ldgKeep(const uint4* p) {
+#if defined(__CUDA_ARCH__) && OWEC_BVH_KEEP
+    uint64_t policy;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(policy));
+    uint4 v;
+    asm("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+        : "l"(p), "l"(policy));
+    return v;
+#elif defined(__CUDA_ARCH__)
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
+
 __device__ __forceinline__ void loadNode(const WideNode* nodes, uint32_t i, NodeWords& nd) {
 #if defined(__CUDA_ARCH__)
     const uint4* src = reinterpret_cast<const uint4*>(nodes + i);
-    nd.a = __ldg(src + 0);
-    nd.b = __ldg(src + 1);
-    nd.c = __ldg(src + 2);
-    nd.d = __ldg(src + 3);
-    nd.e = __ldg(src + 4);
+    nd.a = ldgKeep(src + 0);
+    nd.b = ldgKeep(src + 1);
+    nd.c = ldgKeep(src + 2);
+    nd.d = ldgKeep(src + 3);
+    nd.e = ldgKeep(src + 4);
 #else
     const uint4* src = reinterpret_cast<const uint4*>(nodes + i);
     nd.a = src[0]; nd.b = src[1]; nd.c = src[2]; nd.d = src[3]; nd.e = src[4];
@@ -258,10 +280,11 @@ __device__ __forceinline__ uint32_t intersectChildren(const NodeWords& nd, const
 
 __device__ __forceinline__ void loadPrim(const PrimRec* prims, uint32_t i, PrimRec& p) {
 #if defined(__CUDA_ARCH__)
-    const float4* src = reinterpret_cast<const float4*>(prims + i);
-    float4* dst = reinterpret_cast<float4*>(&p);
+    const uint4* src = reinterpret_cast<const uint4*>(prims + i);
+    uint4 w[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) dst[k] = __ldg(src + k);
+    for (int k = 0; k < 3; ++k) w[k] = ldgKeep(src + k);
+    memcpy(&p, w, sizeof(PrimRec));
 #else
     p = prims[i];
 #endif
