@@ -137,7 +137,7 @@ __device__ void queueConnection(const DeviceScene& sc, PathBuffers<RT<M>>& pb, Q
     sr.path = path;
     sr.errN = errN;
     for (int j = 0; j < NW; ++j) sr.contrib[j] = c[j];
-    pb.shadow[slot] = sr;
+    storeStream(pb.shadow + slot, sr);
     q.shadow[slot] = slot;
     film.pixel[slot] = k.pixel;
 }
@@ -329,10 +329,10 @@ __global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, Particl
     const bool observer = det.kind == OWEC_DETECTOR_OBSERVER;
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
         const uint32_t i = q.active[cur][e];
-        const HitRec h = pb.hit[i];
-        PathRay<R> ray = pb.ray[i];
-        PathSpec<R> sp = pb.spec[i];
-        PathAux aux = pb.aux[i];
+        const HitRec h = loadStream(pb.hit + i);
+        PathRay<R> ray = loadStream(pb.ray + i);
+        PathSpec<R> sp = loadStream(pb.spec + i);
+        PathAux aux = loadStream(pb.aux + i);
         Pcg32 rng{aux.rngState, (uint64_t(aux.stream) << 1u) | 1u};
         const int depth = int(aux.depth);
         // a connection goes out with the spectrum it was made with, before a dispersive interface
@@ -514,9 +514,9 @@ __global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, Particl
         if (cont) aux.depth += 1;
         else aux.flags &= ~kFlagAlive;
         aux.rngState = rng.state;
-        pb.ray[i] = ray;
-        pb.spec[i] = sp;
-        pb.aux[i] = aux;
+        storeStream(pb.ray + i, ray);
+        storeStream(pb.spec + i, sp);
+        storeStream(pb.aux + i, aux);
         warpCount(&st->leaks, leak);
         warpCount(&st->inconsistencies, inconsistent);
         warpCount(&st->faults, lost);
