@@ -367,6 +367,9 @@ def run_cuda(args):
     # end to end through the public API: a pass and the film read back to the host, every step
     e2e_steps = max(2, min(args.steps, 10))
     image = torch.empty((HEIGHT, WIDTH, 3), dtype=torch.float64, pin_memory=True).numpy()
+    for _ in range(2):  # untimed: the first resolve sets up its device and staging buffers
+        renderer.run_pass(1)
+        renderer.resolve(out=image)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     split = []
@@ -390,8 +393,10 @@ def run_cuda(args):
         hbm, peak_kind = peaks()
         q, nodes, prims = cnt[0], cnt[1], cnt[2]
         bytes_isec = nodes * NODE_BYTES + prims * PRIM_BYTES + q * RAY_STATE_BYTES
+        # algorithmic bytes of an average launch (from the counting pass's visit counts) over the
+        # average device time of the timed passes' intersect launches
         per_launch_bytes = bytes_isec / max(1, launches_prof)
-        per_launch_s = isec_prof / max(1, launches_prof)
+        per_launch_s = sum(isec) / max(1, launches)
         achieved = per_launch_bytes / per_launch_s / 1e9
         # DRAM traffic per launch: the ncu-measured bytes per query (profiles/) times this launch's queries
         traffic = None
