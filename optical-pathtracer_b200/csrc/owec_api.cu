@@ -1097,6 +1097,11 @@ PathBuffers<ModeR<M>> pathState(owec_ctx& c, uint32_t cap, Queues& q) {
                           reinterpret_cast<ShadowRay<R>*>(c.dShadow.get())};
 }
 
+// Blocks per SM of the grid-stride medium and surface kernels of the camera paths.
+#ifndef OWEC_SHADING_GRID
+#define OWEC_SHADING_GRID 8
+#endif
+
 template <int M>
 void runPass(owec_ctx& c, int spp) {
     using R = ModeR<M>;
@@ -1157,8 +1162,8 @@ void runPass(owec_ctx& c, int spp) {
             ++intersectLaunches;
             OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 1], s));
             checkLaunch();
-            launchMedium<M>(c.ds, pp, pb, q, cur, c.dStats.get(), grid, s);
-            launchSurface<M>(c.ds, pp, pb, q, cur, c.dStats.get(), grid, s);
+            launchMedium<M>(c.ds, pp, pb, q, cur, c.dStats.get(), c.numSMs * OWEC_SHADING_GRID, s);
+            launchSurface<M>(c.ds, pp, pb, q, cur, c.dStats.get(), c.numSMs * OWEC_SHADING_GRID, s);
             OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 2], s));
             launchShadow<M>(c.ds, pp, pb, q, c.dStats.get(), c.dCounts.get() + 5, c.dShadowVis.get(), grid, s);
             OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 3], s));
