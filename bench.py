@@ -251,7 +251,7 @@ def adjoint_study(device, n=256, bins=512, walks=1 << 24):
 
 def configs_study(device):
     """The other configurations' own rates: C1 (N-BK7 sphere on a floor under the sun, 256 x 256,
-    one uniform wavelength per path, depth 16) in paths/s over 64 one-sample passes, and C3 (the
+    one uniform wavelength per path, depth 16) in paths/s of one 64-spp pass, and C3 (the
     achromat imaging a point source onto a 1024 x 1024 detector, stochastic Fresnel branching with
     ghosts, depth 32) in walks/s over 2^24 walks."""
     import owe_cuda
@@ -261,11 +261,12 @@ def configs_study(device):
         c.build_bvh()
         c.set_settings(A.make_settings(seed=0, max_depth=16, rr_depth=4, wavelength_mode=A.WAVELENGTHS_UNIFORM1))
         c.run_pass(1)
-        seconds = 0.0
-        for _ in range(64):
-            c.run_pass(1)
-            seconds += c.last_pass_timing()[0]
-        out["c1_paths_per_s"] = 256 * 256 * 64 / seconds
+        c.reset_film()
+        # the configuration's own pass: 64 samples per pixel in one call, which batches 32 samples
+        # of the 256 x 256 film (2^21 paths) per wavefront batch
+        c.run_pass(64)
+        out["c1_paths_per_s"] = 256 * 256 * 64 / c.last_pass_timing()[0]
+        out["c1_pass_s"] = c.last_pass_timing()[0]
     sb, info = scenes.achromat_scene(film=1024)
     w = scenes.achromat_walk(info, seed=1, mode=A.WALK_STOCHASTIC, max_events=32)
     with owe_cuda.Context(device) as c:
@@ -307,9 +308,28 @@ def light_study(device, passes=8):
     return out
 
 
+def spawn_ranks(args):
+    """`--gpus N` without a launcher: starts N copies of this script, one per GPU, with RANK,
+    LOCAL_RANK, WORLD_SIZE and a loopback rendezvous set (what torch.distributed.run would set), and
+    returns the first non-zero exit status (0 when all ranks succeed)."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    procs = []
+    for r in range(args.gpus):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(args.gpus), LOCAL_WORLD_SIZE=str(args.gpus),
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, os.path.abspath(__file__)] + sys.argv[1:], env=env))
+    codes = [p.wait() for p in procs]
+    return next((c for c in codes if c != 0), 0)
+
+
 def run_cuda(args):
     import torch
     world, rank, local = dist_env()
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE is {world}: launch one process per GPU")
     torch.cuda.set_device(local)
     if world > 1:
         import torch.distributed as dist
@@ -373,8 +393,12 @@ def run_cuda(args):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     split = []
+    step_settings = renderer.settings
     for _ in range(e2e_steps):
         ta = time.perf_counter()
+        # the step's inputs: the render settings (seed, depths, modes) through the public API; the
+        # scene and its BVH stay resident in HBM from one step to the next
+        ctx.set_settings(step_settings)
         renderer.run_pass(1)
         tb = time.perf_counter()
         img = renderer.resolve(out=image)
@@ -382,6 +406,7 @@ def run_cuda(args):
     e2e_seconds = time.perf_counter() - t0
     e2e_value = n_pix * world * e2e_steps / e2e_seconds
     d2h = n_pix * 3 * 8  # the resolved XYZ image (Renderer::resolve), FP64
+    h2d = __import__("ctypes").sizeof(A.Settings)  # the settings record uploaded every step
 
     # the film over NCCL: the one exchange step of a multi-GPU render
     if world > 1:
@@ -441,10 +466,10 @@ def run_cuda(args):
             "clocks": clk,
             "cpu_baseline": {"value": cpu_rate, "unit": "particles/s" if light else "paths/s", "cores": cores, "kind": "reference",
                              "sample": sample},
-            "e2e": {"value": e2e_value, "unit": "particles/s" if light else "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
+            "e2e": {"value": e2e_value, "unit": "particles/s" if light else "paths/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "value_at_median_step": n_pix * world / statistics.median(a + b for a, b in split),
                     "steps": e2e_steps, "pass_ms": [round(1e3 * a, 2) for a, _ in split],
-                    "resolve_ms": [round(1e3 * b, 2) for _, b in split], "note": "pass + resolved image read back into pinned host memory per step through owe_cuda.Renderer"},
+                    "resolve_ms": [round(1e3 * b, 2) for _, b in split], "note": "per step through owe_cuda.Renderer: the settings record set, one pass, the resolved image read back into pinned host memory; the scene and BVH are uploaded once and stay resident in HBM"},
             "faults": stats1["device_faults"],
         }
         if not args.no_extras and world == 1 and not light:
@@ -487,6 +512,8 @@ def main():
     globals()["INTEGRATOR"] = args.integrator
     if args.impl == "reference":
         return run_reference(args)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return spawn_ranks(args)
     return run_cuda(args)
 
 

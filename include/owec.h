@@ -448,9 +448,9 @@ int owec_walk_adjoint(owec_ctx* ctx, const owec_walk_desc* walk, uint64_t first,
  * counters) is a fixed array in the library image, 10.5 MB on every GPU that loads the library,
  * so the walk film may have at most 512 x 512 bins and the heightfield at most 1048576 vertices;
  * larger calls return OWEC_E_INVALID. The scene must be uploaded and its BVH built, after the
- * settings, beforehand, since those steps allocate. The first call on a
- * device looks up the array's device address, which also loads it onto the device: make that
- * first call before any stream capture. Calls share the array, so two calls that overlap on the
+ * settings, beforehand, since those steps allocate. Every call looks up the array's device address
+ * (so a device reset between calls is harmless); the first call on a device also loads the array
+ * onto it: make that first call before any stream capture. Calls share the array, so two calls that overlap on the
  * GPU (from two threads, or two contexts on one device) race and corrupt each other's results.
  * Same arguments and result as owec_walk_adjoint. */
 int owec_walk_adjoint_noalloc(owec_ctx* ctx, const owec_walk_desc* walk, uint64_t first, uint64_t n,

@@ -997,6 +997,9 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
     c.hasScene = true;
     c.bvhDirty = true;
     c.prims64Ready = false;
+    // a new scene has no heightfield until owec_set_heightfield names one of its boundaries
+    c.hf.boundary = kNone;
+    c.hfVertices = 0;
     c.passCount = 0;
     c.dFilm.release();
     c.dComp.release();
@@ -1317,22 +1320,15 @@ static __device__ __align__(256) double gAdjointScratch[kNoAllocMaxBins + kNoAll
 
 namespace {
 
-// The device address of gAdjointScratch on `device`, which must be current. In host code the array's
-// name is only a host-side stand-in, so the address is asked of the runtime, once per device; that
-// first request also loads the array onto the device.
-constexpr int kMaxNoAllocDevices = 64;
-std::mutex gScratchMutex;
-double* gScratchAddress[kMaxNoAllocDevices] = {};
-
-double* adjointScratch(int device) {
-    require(device >= 0 && device < kMaxNoAllocDevices, "owec_walk_adjoint_noalloc: device index out of range");
-    std::lock_guard<std::mutex> lock(gScratchMutex);
-    if (!gScratchAddress[device]) {
-        void* p = nullptr;
-        OWEC_CUDA(cudaGetSymbolAddress(&p, gAdjointScratch));
-        gScratchAddress[device] = static_cast<double*>(p);
-    }
-    return gScratchAddress[device];
+// The device address of gAdjointScratch on the current device. In host code the array's name is only
+// a host-side stand-in, so the address is asked of the runtime. It is asked on every call, not kept:
+// a host application that resets the device (cudaDeviceReset) or tears its primary context down
+// gets the module loaded again at another address, and a kept pointer would then point at freed
+// memory. The first request on a device also loads the array onto it.
+double* adjointScratch() {
+    void* p = nullptr;
+    OWEC_CUDA(cudaGetSymbolAddress(&p, gAdjointScratch));
+    return static_cast<double*>(p);
 }
 
 }  // namespace
@@ -1829,7 +1825,7 @@ int owec_walk_adjoint_noalloc(owec_ctx* ctx, const owec_walk_desc* w, uint64_t f
                 "owec_build_bvh): that prepares the FP64 primitives",
                 OWEC_E_STATE);
         OWEC_CUDA(cudaSetDevice(ctx->device));
-        double* base = adjointScratch(ctx->device);
+        double* base = adjointScratch();
         double* dG = base;
         double* dDH = base + kNoAllocMaxBins;
         auto* st = reinterpret_cast<unsigned long long*>(base + kNoAllocMaxBins + kNoAllocMaxHeights);

@@ -54,6 +54,8 @@ class Context:
         self._desc = desc  # the pointed-to arrays must outlive the call only; kept for inspection
         _check(self.lib, self.lib.owec_upload_scene(self.handle, ctypes.byref(desc)), "owec_upload_scene")
         self.width, self.height = desc.detector.width, desc.detector.height
+        for stale in ("_hf_n", "_hf_heights", "_hf_boundary"):  # a new scene has no heightfield yet
+            self.__dict__.pop(stale, None)
 
     def build_bvh(self):
         _check(self.lib, self.lib.owec_build_bvh(self.handle), "owec_build_bvh")
@@ -151,11 +153,27 @@ class Context:
         _check(self.lib, self.lib.owec_set_heightfield(self.handle, boundary, len(h), base_z,
                                                        h.ctypes.data_as(A.c_double_p)), "owec_set_heightfield")
         self._hf_n = len(h)
+        self._hf_heights = h.copy()
+        self._hf_boundary = boundary
+
+    def _adjoint_args(self, desc, g, dheights=None):
+        """The loss gradient (one per walk bin) and the height-gradient accumulator (one per vertex)
+        as contiguous float64 vectors, checked against the sizes the library will read and write."""
+        if not hasattr(self, "_hf_n"):
+            raise RuntimeError("no heightfield set (set_heightfield)")
+        gg = np.ascontiguousarray(g, np.float64).ravel()
+        if gg.size != desc.width * desc.height:
+            raise ValueError(f"g has {gg.size} values; the walk film has {desc.width} x {desc.height} bins")
+        if dheights is None:
+            return gg, np.zeros(self._hf_n)
+        out = np.ascontiguousarray(dheights, np.float64).ravel().copy()
+        if out.size != self._hf_n:
+            raise ValueError(f"dheights has {out.size} values; the heightfield has {self._hf_n} vertices")
+        return gg, out
 
     def walk_adjoint(self, desc, first, n, g):
         """d(sum_b g_b bins_b) / d heights by path replay of walks first .. first + n - 1."""
-        gg = np.ascontiguousarray(g, np.float64).ravel()
-        out = np.zeros(self._hf_n)
+        gg, out = self._adjoint_args(desc, g)
         _check(self.lib, self.lib.owec_walk_adjoint(self.handle, ctypes.byref(desc), int(first), int(n),
                                                     gg.ctypes.data_as(A.c_double_p), out.ctypes.data_as(A.c_double_p)),
                "owec_walk_adjoint")
@@ -165,8 +183,7 @@ class Context:
         """walk_adjoint through owec_walk_adjoint_noalloc, which allocates no device memory: its
         scratch is a fixed array in the library (at most 512 x 512 bins, 2^20 vertices). The
         gradient is added to `dheights` (zeros when not given) and returned."""
-        gg = np.ascontiguousarray(g, np.float64).ravel()
-        out = np.zeros(self._hf_n) if dheights is None else np.ascontiguousarray(dheights, np.float64).ravel().copy()
+        gg, out = self._adjoint_args(desc, g, dheights)
         _check(self.lib, self.lib.owec_walk_adjoint_noalloc(self.handle, ctypes.byref(desc), int(first), int(n),
                                                             gg.ctypes.data_as(A.c_double_p),
                                                             out.ctypes.data_as(A.c_double_p)),

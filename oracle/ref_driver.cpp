@@ -459,8 +459,12 @@ int oweref_cast_rays(void* scene, uint64_t n, const double* o, const double* d, 
 // (hashCombine(seed, first + i), stream): its wavelength, its emission (Draw2), then the walk's own
 // draws. bins (width * height) receive the sum of the binned walks' throughput times their splat
 // weights; stats: [walks, binned, escaped, events].
-int oweref_walk(void* scene, const owec_walk_desc* w, uint64_t first, uint64_t n, int threads, double* bins,
-                uint64_t* stats) {
+namespace {
+
+// Tracer::walk for walks first .. first + n - 1 binned as owec_walk bins them; with a box (xmin, xmax,
+// ymin, ymax, zmin, zmax, world coordinates), only the walks whose emission point lies in it run.
+int walkRange(void* scene, const owec_walk_desc* w, uint64_t first, uint64_t n, int threads, double* bins,
+              uint64_t* stats, const double* box) {
     return guarded([&] {
         const RefScene& rs = *static_cast<const RefScene*>(scene);
         const World& world = rs.scene.world;
@@ -492,6 +496,9 @@ int oweref_walk(void* scene, const owec_walk_desc* w, uint64_t first, uint64_t n
                     o = o + (S * (2 * u.u1 - 1) + T * (2 * u.u2 - 1)) * w->extent;
                     d = axis;
                 }
+                if (box && !(o.x >= box[0] && o.x <= box[1] && o.y >= box[2] && o.y <= box[3] && o.z >= box[4] &&
+                             o.z <= box[5]))
+                    continue;
                 const PathRecord rec = tracer.walk(Ray{o, d}, rs.regionMap.at(w->region), lambda, mode, rng, w->max_events);
                 st[t][0]++;
                 st[t][3] += rec.v.size() - 1;
@@ -533,6 +540,22 @@ int oweref_walk(void* scene, const owec_walk_desc* w, uint64_t first, uint64_t n
             for (int t = 0; t < nt; ++t) stats[k] += st[size_t(t)][size_t(k)];
         }
     });
+}
+
+}  // namespace
+
+int oweref_walk(void* scene, const owec_walk_desc* w, uint64_t first, uint64_t n, int threads, double* bins,
+                uint64_t* stats) {
+    return walkRange(scene, w, first, n, threads, bins, stats, nullptr);
+}
+
+// The walks of first .. first + n - 1 whose emission point lies in box (xmin, xmax, ymin, ymax, zmin,
+// zmax, world coordinates), binned as oweref_walk bins them (raw throughput sums). A finite
+// difference of the binned film with common random numbers needs only the walks that can meet the
+// moved geometry: the others repeat the same arithmetic on both sides and cancel exactly.
+int oweref_walk_in_box(void* scene, const owec_walk_desc* w, uint64_t first, uint64_t n, const double* box,
+                       int threads, double* bins, uint64_t* stats) {
+    return walkRange(scene, w, first, n, threads, bins, stats, box);
 }
 
 // World-level facts the tests pin the restatement against: the light table (selection pdfs),

@@ -41,6 +41,8 @@ def ref_lib():
         lib.oweref_medium_index.argtypes = [P, ctypes.c_uint32, ctypes.c_double, A.c_double_p]
         lib.oweref_walk.argtypes = [P, ctypes.POINTER(A.WalkDesc), ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int,
                                     A.c_double_p, ctypes.POINTER(ctypes.c_uint64)]
+        lib.oweref_walk_in_box.argtypes = [P, ctypes.POINTER(A.WalkDesc), ctypes.c_uint64, ctypes.c_uint64, A.c_double_p,
+                                           ctypes.c_int, A.c_double_p, ctypes.POINTER(ctypes.c_uint64)]
         _ref = lib
     return _ref
 
@@ -112,6 +114,20 @@ class ReferenceEngine:
             raise RuntimeError(self.lib.oweref_last_error().decode())
         return normalise_walk_bins(desc, bins, n), {"walks": st[0], "binned": st[1], "escaped": st[2],
                                                     "events": st[3]}
+
+    def walk_in_box(self, desc, first, n, box, threads=0):
+        """The walks of first .. first + n - 1 whose emission point lies in box (xmin, xmax, ymin,
+        ymax, zmin, zmax, world coordinates): their binned throughput as raw sums (not normalised)
+        and the number of them that ran."""
+        nb = desc.width * desc.height
+        bins = np.zeros(nb)
+        st = (ctypes.c_uint64 * 4)()
+        b = np.ascontiguousarray(box, np.float64)
+        r = self.lib.oweref_walk_in_box(self.h, ctypes.byref(desc), first, n, b.ctypes.data_as(A.c_double_p), threads,
+                                        bins.ctypes.data_as(A.c_double_p), st)
+        if r != 0:
+            raise RuntimeError(self.lib.oweref_last_error().decode())
+        return bins.reshape(desc.height, desc.width), int(st[0])
 
     def info(self):
         pdfs = np.zeros(64)

@@ -75,3 +75,41 @@ def test_noalloc_adjoint_refuses_a_film_beyond_its_scratch():
         assert st == A.E_INVALID
         assert "512 x 512" in c.lib.owec_last_error().decode()
         assert not out.any()
+
+
+def _noalloc_status(c, w, nh):
+    g = np.zeros(w.width * w.height)
+    out = np.zeros(nh)
+    st = c.lib.owec_walk_adjoint_noalloc(c.handle, ctypes.byref(w), 0, 1024, g.ctypes.data_as(A.c_double_p),
+                                         out.ctypes.data_as(A.c_double_p))
+    return st, c.lib.owec_last_error().decode(), out
+
+
+def test_noalloc_adjoint_refuses_when_the_fp64_primitives_were_not_built():
+    # the BVH built under FP32 has no FP64 primitives; the mixed precision set afterwards would need
+    # them, and preparing them allocates: the call must refuse instead
+    sb, info = scenes.caustic_slab_scene(n=N, heights=_heights(), wall_bins=BINS)
+    with owe_cuda.Context() as c:
+        c.set_settings(A.make_settings(seed=0, precision=A.PRECISION_FP32))
+        c.upload(sb.desc())
+        c.build_bvh()
+        c.set_heightfield(info["heightfield"], info["thickness"], _heights())
+        c.set_settings(A.make_settings(seed=0, precision=A.PRECISION_MIXED))
+        st, msg, out = _noalloc_status(c, scenes.caustic_walk(info, seed=7), N * N)
+        assert st == A.E_STATE, msg
+        assert "FP64 primitives" in msg
+        assert not out.any()
+
+
+def test_noalloc_adjoint_refuses_a_new_scene_without_its_heightfield_and_bvh():
+    # uploading a scene discards the BVH and the heightfield of the previous one: building them
+    # allocates, so the call refuses until the caller has done that set-up
+    sb, info = scenes.caustic_slab_scene(n=N, heights=_heights(), wall_bins=BINS)
+    with owe_cuda.Context() as c:
+        c.upload(sb.desc())
+        c.build_bvh()
+        c.set_heightfield(info["heightfield"], info["thickness"], _heights())
+        c.upload(sb.desc())
+        st, msg, out = _noalloc_status(c, scenes.caustic_walk(info, seed=7), N * N)
+        assert st == A.E_STATE, msg
+        assert not out.any()
