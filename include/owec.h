@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define OWEC_ABI_VERSION 4
+#define OWEC_ABI_VERSION 5
 
 /* ------------------------------------------------------------------ status codes */
 #define OWEC_OK 0
@@ -455,6 +455,29 @@ int owec_walk_adjoint(owec_ctx* ctx, const owec_walk_desc* walk, uint64_t first,
  * Same arguments and result as owec_walk_adjoint. */
 int owec_walk_adjoint_noalloc(owec_ctx* ctx, const owec_walk_desc* walk, uint64_t first, uint64_t n,
                               const double* g, double* dheights);
+/* The path-replay adjoint of the camera film: the gradient of sum_p g[p] . film[p] with respect to the
+ * heights set by owec_set_heightfield, added into dheights (one per vertex). film is the resolved image
+ * (XYZ per pixel, owec_resolve) of the samples first_pass .. first_pass + spp - 1 of every pixel, as
+ * owec_set_pass_index(first_pass) followed by owec_pass(spp) after owec_reset_film renders it; g holds
+ * 3 doubles per pixel, row-major. Each camera path is regenerated from its stream and walked again with
+ * the forward pass's arithmetic, carrying the derivatives of its vertices, directions and throughput
+ * with respect to the heights of the heightfield triangles it crosses; nothing of the forward pass is
+ * stored. This is the backward half of the camera film's forward/backward pair (the forward half is
+ * owec_pass); the reference has no differentiable transport. replay_xyz (may be NULL) receives the
+ * replayed paths' mean XYZ per pixel, which equals the forward film of the same samples. Needs the
+ * path integrator and a scene without null boundaries (OWEC_E_UNSUPPORTED otherwise). */
+typedef struct owec_adjoint_stats {
+    uint64_t paths;       /* camera paths replayed */
+    uint64_t heightfield; /* of them, the paths that crossed the heightfield */
+    uint64_t dropped;     /* of those, the paths whose derivative was not followed (an event beyond the
+                           * adjoint's model: rough or conductor lobes, textures, shapes other than planes,
+                           * spheres and meshes, more than 12 heights): left out of the gradient */
+    uint64_t faults;      /* bounded loops that ran out */
+    double seconds;       /* device time of the replay */
+} owec_adjoint_stats;
+int owec_path_adjoint(owec_ctx* ctx, uint64_t first_pass, int spp, const double* g, double* dheights,
+                      double* replay_xyz, owec_adjoint_stats* stats);
+
 /* Device seconds of the last owec_walk and owec_walk_adjoint calls. */
 int owec_walk_timing(owec_ctx* ctx, double out[2]);
 

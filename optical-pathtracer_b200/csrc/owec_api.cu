@@ -17,6 +17,7 @@
 #include "owec.h"
 #include "particle.hpp"
 #include "spectral.cuh"
+#include "path_adjoint.hpp"
 #include "walk.hpp"
 #include "wavefront.hpp"
 
@@ -434,6 +435,7 @@ struct owec_ctx {
     // the heightfield the adjoint differentiates
     HeightfieldParams hf{kNone, nullptr, {0, 0, 1}};
     uint64_t hfVertices = 0;
+    double lastPathAdjointSeconds = 0;
     DBuf<uint32_t> dHfTris;
     struct MeshCopy {
         std::vector<double> verts;    // shape-frame vertices as uploaded
@@ -1850,6 +1852,72 @@ int owec_walk_adjoint_noalloc(owec_ctx* ctx, const owec_walk_desc* w, uint64_t f
         float ms = 0;
         OWEC_CUDA(cudaEventElapsedTime(&ms, ctx->passStart, ctx->passStop));
         ctx->lastAdjointSeconds = ms * 1e-3;
+    });
+}
+
+int owec_path_adjoint(owec_ctx* ctx, uint64_t first_pass, int spp, const double* g, double* dheights,
+                      double* replay_xyz, owec_adjoint_stats* stats) {
+    return guarded([&] {
+        require(ctx && g && dheights, "owec_path_adjoint: null argument");
+        require(spp > 0, "owec_path_adjoint: spp must be positive");
+        require(ctx->hasScene, "no scene uploaded", OWEC_E_STATE);
+        require(ctx->hf.boundary != kNone, "no heightfield set (owec_set_heightfield)", OWEC_E_STATE);
+        require(ctx->settings.integrator == OWEC_INTEGRATOR_PATH,
+                "owec_path_adjoint differentiates the path integrator's film", OWEC_E_UNSUPPORTED);
+        require(!ctx->hasNull, "owec_path_adjoint: scenes with null boundaries are not differentiated",
+                OWEC_E_UNSUPPORTED);
+        require(first_pass + uint64_t(spp) <= (1ull << 32), "owec_path_adjoint: the PCG32 stream index is 32 bits");
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        ensureReady(*ctx);
+        const uint32_t nPix = uint32_t(ctx->ds.det.width) * uint32_t(ctx->ds.det.height);
+        const size_t nh = ctx->hfVertices;
+        DBuf<double> dG(3 * size_t(nPix)), dDH(nh), dRep(replay_xyz ? 3 * size_t(nPix) : 0);
+        DBuf<unsigned long long> ctr(4);
+        OWEC_CUDA(cudaMemcpyAsync(dG.get(), g, 3 * size_t(nPix) * 8, cudaMemcpyHostToDevice, ctx->stream));
+        OWEC_CUDA(cudaMemsetAsync(dDH.get(), 0, nh * 8, ctx->stream));
+        OWEC_CUDA(cudaMemsetAsync(ctr.get(), 0, 4 * 8, ctx->stream));
+        if (replay_xyz) OWEC_CUDA(cudaMemsetAsync(dRep.get(), 0, dRep.bytes(), ctx->stream));
+        PassParams pp{};
+        pp.seed = ctx->settings.seed;
+        pp.maxDepth = ctx->settings.max_depth;
+        pp.rrDepth = ctx->settings.rr_depth;
+        pp.wavelengthMode = ctx->settings.wavelength_mode;
+        pp.lambdaMin = float(ctx->settings.lambda_min);
+        pp.lambdaMax = float(ctx->settings.lambda_max);
+        pp.fresnelFloor = float(std::min(0.49, std::max(0.0, ctx->settings.fresnel_floor)));
+        pp.nPixels = nPix;
+        pp.anyHitShadows = 1;
+        PathAdjointTargets t{dG.get(), 1.0 / double(spp), dDH.get(), replay_xyz ? dRep.get() : nullptr, ctr.get()};
+        // one launch replays up to 2^22 paths (whole samples of the film)
+        const uint32_t perBatch = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(spp), (1u << 22) / std::max(1u, nPix)));
+        OWEC_CUDA(cudaEventRecord(ctx->passStart, ctx->stream));
+        for (int done = 0; done < spp;) {
+            const uint32_t S = std::min<uint32_t>(perBatch, uint32_t(spp - done));
+            pp.nPaths = S * nPix;
+            pp.streamBase = uint32_t(first_pass + uint64_t(done));
+            launchPathAdjoint(ctx->settings.precision, ctx->ds, pp, ctx->hf, t, ctx->numSMs * 8, ctx->stream);
+            checkLaunch();
+            done += int(S);
+        }
+        OWEC_CUDA(cudaEventRecord(ctx->passStop, ctx->stream));
+        std::vector<double> h(nh);
+        unsigned long long counts[4];
+        OWEC_CUDA(cudaMemcpyAsync(h.data(), dDH.get(), nh * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        OWEC_CUDA(cudaMemcpyAsync(counts, ctr.get(), sizeof(counts), cudaMemcpyDeviceToHost, ctx->stream));
+        if (replay_xyz)
+            OWEC_CUDA(cudaMemcpyAsync(replay_xyz, dRep.get(), dRep.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
+        OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+        float ms = 0;
+        OWEC_CUDA(cudaEventElapsedTime(&ms, ctx->passStart, ctx->passStop));
+        ctx->lastPathAdjointSeconds = ms * 1e-3;
+        for (size_t i = 0; i < nh; ++i) dheights[i] += h[i];
+        if (stats) {
+            stats->paths = counts[0];
+            stats->heightfield = counts[1];
+            stats->dropped = counts[2];
+            stats->faults = counts[3];
+            stats->seconds = ms * 1e-3;
+        }
     });
 }
 

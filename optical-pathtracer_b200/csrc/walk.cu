@@ -13,6 +13,7 @@
 // (the hit point moves within its surface), of refraction and reflection, of the Fresnel weight,
 // of Beer-Lambert attenuation, and finally of the bilinear splat on the target. Nothing of the
 // forward pass is stored.
+#include "tangents.cuh"
 #include "transport.cuh"
 #include "walk.hpp"
 
@@ -75,24 +76,6 @@ struct Tangents {
     double dB[kSlots];
     bool valid;
 };
-
-// Unpolarised Fresnel reflectance and its derivative in cosThetaI (the function of
-// src/owe/core/shared/optics.hpp:42-54).
-__device__ void fresnelWithDerivative(double c, double eta, double& R, double& dRdc) {
-    double sgn = 1;
-    c = fmin(1.0, fmax(-1.0, c));
-    if (c < 0) { eta = 1 / eta; c = -c; sgn = -1; }
-    const double s2 = (1 - c * c) / (eta * eta);
-    if (s2 >= 1) { R = 1; dRdc = 0; return; }
-    const double ct = sqrt(fmax(0.0, 1 - s2));
-    const double dct = ct > 0 ? (c / (eta * eta)) / ct : 0;
-    const double a = eta * c - ct, b = eta * c + ct;
-    const double rp = a / b, drp = ((eta - dct) * b - a * (eta + dct)) / (b * b);
-    const double e = c - eta * ct, f = c + eta * ct;
-    const double rs = e / f, drs = ((1 - eta * dct) * f - e * (1 + eta * dct)) / (f * f);
-    R = (rp * rp + rs * rs) / 2;
-    dRdc = sgn * (rp * drp + rs * drs);
-}
 
 template <int M, bool ADJ, bool Full>
 __device__ void walkOne(const DeviceScene& sc, const WalkParams& P, uint64_t walkIndex, StackEntry* stack, int stride,

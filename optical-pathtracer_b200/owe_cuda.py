@@ -190,6 +190,29 @@ class Context:
                "owec_walk_adjoint_noalloc")
         return out
 
+    def path_adjoint(self, first_pass, spp, g, dheights=None, replay=False, with_stats=False):
+        """d(sum_p g_p . film_p) / d heights by path replay of the camera paths of samples first_pass
+        .. first_pass + spp - 1 (owec_path_adjoint). g: dLoss/dFilm, height x width x 3. Returns the
+        gradient (added to `dheights` when given); with with_stats, (gradient, stats dict, replayed
+        image or None)."""
+        if not hasattr(self, "_hf_n"):
+            raise RuntimeError("no heightfield set (set_heightfield)")
+        gg = np.ascontiguousarray(g, np.float64).ravel()
+        if gg.size != 3 * self.width * self.height:
+            raise ValueError(f"g has {gg.size} values; the film has {self.width} x {self.height} x 3")
+        out = np.zeros(self._hf_n) if dheights is None else np.ascontiguousarray(dheights, np.float64).ravel().copy()
+        if out.size != self._hf_n:
+            raise ValueError(f"dheights has {out.size} values; the heightfield has {self._hf_n} vertices")
+        rep = np.zeros(3 * self.width * self.height) if replay else None
+        st = A.AdjointStats()
+        _check(self.lib, self.lib.owec_path_adjoint(self.handle, int(first_pass), int(spp), gg.ctypes.data_as(A.c_double_p),
+                                                    out.ctypes.data_as(A.c_double_p),
+                                                    rep.ctypes.data_as(A.c_double_p) if replay else None,
+                                                    ctypes.byref(st)), "owec_path_adjoint")
+        if not with_stats:
+            return out
+        return out, st.as_dict(), (rep.reshape(self.height, self.width, 3) if replay else None)
+
     def walk_timing(self):
         out = (ctypes.c_double * 2)()
         _check(self.lib, self.lib.owec_walk_timing(self.handle, out), "owec_walk_timing")

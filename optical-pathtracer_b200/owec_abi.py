@@ -10,7 +10,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libowec.so")
 
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 OK = 0
 E_INVALID, E_CUDA, E_NOMEM, E_STATE, E_DEVICE_FAULT, E_UNSUPPORTED = -1, -2, -3, -4, -5, -6
@@ -145,6 +145,14 @@ class WalkStats(ctypes.Structure):
         return {name: int(getattr(self, name)) for name, _ in self._fields_}
 
 
+class AdjointStats(ctypes.Structure):
+    _fields_ = [("paths", ctypes.c_uint64), ("heightfield", ctypes.c_uint64), ("dropped", ctypes.c_uint64),
+                ("faults", ctypes.c_uint64), ("seconds", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("paths", ctypes.c_uint64), ("segments", ctypes.c_uint64), ("inconsistencies", ctypes.c_uint64),
                 ("leaks", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64), ("device_faults", ctypes.c_uint64)]
@@ -209,6 +217,8 @@ def load_library(path=LIB_PATH):
         "owec_walk_adjoint_noalloc": ([P, ctypes.POINTER(WalkDesc), ctypes.c_uint64, ctypes.c_uint64, c_double_p,
                                        c_double_p], ctypes.c_int),
         "owec_walk_timing": ([P, c_double_p], ctypes.c_int),
+        "owec_path_adjoint": ([P, ctypes.c_uint64, ctypes.c_int, c_double_p, c_double_p, c_double_p,
+                               ctypes.POINTER(AdjointStats)], ctypes.c_int),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(lib, name)
