@@ -249,6 +249,91 @@ def adjoint_study(device, n=256, bins=512, walks=1 << 24):
             "adjoint_over_forward": a / f, "forward_walks_per_s": walks / f}
 
 
+def c5_study(device, spp_timing=16, steps=0, spp_step=4, width=1920, height=1080):
+    """The large adjoint: the caustic room (a 1024 x 1024 heightfield PMMA panel, two displaced-sphere
+    props of 2^20 triangles each, fog with sigma_s 0.5 / m, sigma_a 0.05 / m, Henyey-Greenstein g 0.8,
+    one ceiling light), 1920 x 1080, depth 24. Device seconds of a forward pass (owec_pass) and of the
+    path-replay adjoint (owec_path_adjoint) over the same spp_timing samples, their ratio, the device
+    memory of each; then, when steps > 0, that many gradient-descent steps on the heights toward a
+    target film rendered at seeded target heights (spp_step samples per step for the film and an
+    independent replay for the gradient), reporting the loss before and after and the time per step."""
+    import torch
+    import owe_cuda
+    n = 1024
+    sb, info = scenes.caustic_room(width=width, height=height, panel_n=n)
+    desc = sb.desc()
+    settings = A.make_settings(seed=11, max_depth=24, rr_depth=6, wavelength_mode=A.WAVELENGTHS_HERO4)
+    out = {"film": f"{width}x{height}", "heightfield": f"{n}x{n}", "depth": 24, "spp": spp_timing}
+    free0, total = torch.cuda.mem_get_info(device)
+    with owe_cuda.Context(device) as c:
+        c.set_settings(settings)
+        c.upload(desc)
+        c.build_bvh()
+        c.set_heightfield(info["heightfield"], info["base_z"], np.zeros(n * n))
+        out["triangles"] = c.bvh_info()["triangles"]
+        c.run_pass(1)
+        c.path_adjoint(0, 1, np.zeros((height, width, 3)))  # warm-up: buffers, the replay's stacks
+        free1, _ = torch.cuda.mem_get_info(device)
+        c.reset_film()
+        c.set_pass_index(100)
+        c.run_pass(spp_timing)
+        fwd = c.last_pass_timing()[0]
+        img, _ = c.resolve(samples=False)
+        g = np.zeros_like(img)
+        g[..., 1] = 1.0 / img.size  # the gradient of the image's mean luminance
+        _, st, _ = c.path_adjoint(100, spp_timing, g, with_stats=True)
+        out.update({"forward_s": fwd, "adjoint_s": st["seconds"], "adjoint_over_forward": st["seconds"] / fwd,
+                    "forward_paths_per_s": width * height * spp_timing / fwd,
+                    "paths_met_heightfield": st["heightfield"] / max(1, st["paths"]),
+                    "dropped_of_those": st["dropped"] / max(1, st["heightfield"]), "faults": st["faults"],
+                    "context_bytes": int(free0 - free1), "adjoint_call_bytes": int(st["device_bytes"]),
+                    "device_total_bytes": int(total)})
+        if steps > 0:
+            rng = np.random.Generator(np.random.PCG64(5))
+            yy, xx = np.mgrid[0:n, 0:n] / (n - 1)
+            target_h = np.zeros((n, n))
+            for _ in range(8):
+                fx, fy, ph = rng.uniform(1, 4, 2).tolist() + [rng.uniform(0, 2 * np.pi)]
+                target_h += np.sin(np.pi * fx * xx + ph) * np.sin(np.pi * fy * yy)
+            target_h *= 4e-3 / np.abs(target_h).max()
+            target_h[0, :] = target_h[-1, :] = target_h[:, 0] = target_h[:, -1] = 0
+            c.set_heightfield(info["heightfield"], info["base_z"], target_h)
+            c.reset_film()
+            c.set_pass_index(1 << 20)
+            c.run_pass(64)
+            target, _ = c.resolve(samples=False)
+            h = np.zeros(n * n)
+            lr = None
+            losses, t_fwd, t_adj = [], 0.0, 0.0
+            for k in range(steps):
+                c.set_heightfield(info["heightfield"], info["base_z"], h)
+                c.reset_film()
+                c.set_pass_index(2 * k * spp_step)
+                c.run_pass(spp_step)
+                t_fwd += c.last_pass_timing()[0]
+                img, _ = c.resolve(samples=False)
+                diff = img - target
+                losses.append(float((diff ** 2).mean()))
+                # the gradient from an independent replay (other sample streams), so that the film's
+                # noise and the replay's do not correlate
+                grad, st, _ = c.path_adjoint((2 * k + 1) * spp_step, spp_step, 2 * diff / diff.size, with_stats=True)
+                t_adj += st["seconds"]
+                if lr is None:  # a first step of 0.1 mm on the largest gradient
+                    lr = 1e-4 / max(np.abs(grad).max(), 1e-30)
+                h = h - lr * grad
+                h = h.reshape(n, n)
+                h[0, :] = h[-1, :] = h[:, 0] = h[:, -1] = 0
+                h = h.ravel()
+            out["optimisation"] = {"steps": steps, "spp_per_step": spp_step, "loss_first": losses[0],
+                                   "loss_last": losses[-1], "loss_min": min(losses),
+                                   "loss_mean_first10": float(np.mean(losses[:10])),
+                                   "loss_mean_last10": float(np.mean(losses[-10:])),
+                                   "forward_s_per_step": t_fwd / steps, "adjoint_s_per_step": t_adj / steps,
+                                   "height_rmse_vs_target_first": float(np.sqrt((target_h ** 2).mean())),
+                                   "height_rmse_vs_target_last": float(np.sqrt(((h.reshape(n, n) - target_h) ** 2).mean()))}
+    return out
+
+
 def configs_study(device):
     """The other configurations' own rates: C1 (N-BK7 sphere on a floor under the sun, 256 x 256,
     one uniform wavelength per path, depth 16) in paths/s of one 64-spp pass, and C3 (the
@@ -503,6 +588,9 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=sorted(PRECISIONS),
                     help="mixed: FP32 camera-relative + selective FP64 (the product); fp64: the all-FP64 "
                          "instantiation of the same kernels it is compared with")
+    ap.add_argument("--c5", type=int, default=-1, metavar="STEPS",
+                    help="run only the large-adjoint study (caustic room at 1920x1080, depth 24) with STEPS "
+                         "gradient steps (0: timing and memory alone) and print its JSON")
     ap.add_argument("--integrator", default="path", choices=["path", "light"],
                     help="path: the headline camera-path integrator; light: particles from the emitters, "
                          "measured in particles/s on the same scene")
@@ -512,6 +600,11 @@ def main():
     globals()["INTEGRATOR"] = args.integrator
     if args.impl == "reference":
         return run_reference(args)
+    if args.c5 >= 0:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps({"c5_study": c5_study(0, steps=args.c5)}))
+        return 0
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         return spawn_ranks(args)
     return run_cuda(args)

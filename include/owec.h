@@ -459,13 +459,17 @@ int owec_walk_adjoint_noalloc(owec_ctx* ctx, const owec_walk_desc* walk, uint64_
  * heights set by owec_set_heightfield, added into dheights (one per vertex). film is the resolved image
  * (XYZ per pixel, owec_resolve) of the samples first_pass .. first_pass + spp - 1 of every pixel, as
  * owec_set_pass_index(first_pass) followed by owec_pass(spp) after owec_reset_film renders it; g holds
- * 3 doubles per pixel, row-major. Each camera path is regenerated from its stream and walked again with
- * the forward pass's arithmetic, carrying the derivatives of its vertices, directions and throughput
- * with respect to the heights of the heightfield triangles it crosses; nothing of the forward pass is
- * stored. This is the backward half of the camera film's forward/backward pair (the forward half is
- * owec_pass); the reference has no differentiable transport. replay_xyz (may be NULL) receives the
- * replayed paths' mean XYZ per pixel, which equals the forward film of the same samples. Needs the
- * path integrator and a scene without null boundaries (OWEC_E_UNSUPPORTED otherwise). */
+ * 3 doubles per pixel, row-major. The camera paths are regenerated from their streams and walked again
+ * with the forward pass's arithmetic, in two phases per batch: the wavefront kernels run them and stop
+ * each at its first surface event on the heightfield, keeping its state there (one checkpoint per path
+ * that reaches the heightfield), and a replay kernel resumes from those checkpoints, carrying the
+ * derivatives of the path's vertices, directions and throughput with respect to the heights of the
+ * heightfield triangles it crosses. This is the backward half of the camera film's forward/backward
+ * pair (the forward half is owec_pass); the reference has no differentiable transport. With
+ * replay_xyz (may be NULL) every path is instead replayed from its camera ray by the replay kernel,
+ * and replay_xyz receives their mean XYZ per pixel, which equals the forward film of the same
+ * samples. Needs the path integrator and a scene without null boundaries (OWEC_E_UNSUPPORTED
+ * otherwise). */
 typedef struct owec_adjoint_stats {
     uint64_t paths;       /* camera paths replayed */
     uint64_t heightfield; /* of them, the paths that crossed the heightfield */
@@ -473,9 +477,18 @@ typedef struct owec_adjoint_stats {
                            * adjoint's model: rough or conductor lobes, textures, shapes other than planes,
                            * spheres and meshes, more than 12 heights): left out of the gradient */
     uint64_t faults;      /* bounded loops that ran out */
-    double seconds;       /* device time of the replay */
+    double seconds;       /* device time of the call */
+    uint64_t device_bytes;/* device memory the call held beyond what the context held before it: its
+                           * buffers (loss gradient, height gradient, checkpoints, replayed film) and the
+                           * replay kernel's per-thread stacks */
 } owec_adjoint_stats;
-int owec_path_adjoint(owec_ctx* ctx, uint64_t first_pass, int spp, const double* g, double* dheights,
+/* flags: 0, the unbiased gradient of the expected film (sampling detached: the Fresnel branch and
+ * roulette probabilities and the drawn scattering directions held fixed, their weights' values
+ * differentiated); OWEC_ADJOINT_FIXED_DECISIONS, the derivative of the estimator at fixed random
+ * numbers (those probabilities and frames moving with the path), which central differences with
+ * common random numbers measure but which leaves out the branches' boundary terms. */
+#define OWEC_ADJOINT_FIXED_DECISIONS 1
+int owec_path_adjoint(owec_ctx* ctx, uint64_t first_pass, int spp, int flags, const double* g, double* dheights,
                       double* replay_xyz, owec_adjoint_stats* stats);
 
 /* Device seconds of the last owec_walk and owec_walk_adjoint calls. */

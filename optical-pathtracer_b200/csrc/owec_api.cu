@@ -1107,6 +1107,60 @@ PathBuffers<ModeR<M>> pathState(owec_ctx& c, uint32_t cap, Queues& q) {
 #define OWEC_SHADING_GRID 8
 #endif
 
+// The bounces of one batch of camera paths already generated into pb: intersect, medium, surface
+// and shadow kernels per bounce until the active queue is empty. The kernels read their queue
+// lengths on the device, so the bounces are queued without a look at the host: maxDepth + 1 of
+// them first (a path without null boundaries ends by then), then four at a time until the queue
+// is empty. The host waits once per batch, not once per bounce. With timed, CUDA events around the
+// intersect and shadow launches add their device seconds to travSeconds.
+template <int M>
+void runBounces(owec_ctx& c, const PassParams& pp, PathBuffers<ModeR<M>>& pb, Queues& q, StatCounters* st, int grid,
+                bool timed, double travSeconds[2], int& evUsed, int& intersectLaunches) {
+    cudaStream_t s = c.stream;
+    int cur = 0;
+    int nextCheck = pp.maxDepth + 1;
+    for (int bounce = 0; bounce < 4 * pp.maxDepth + 8; ++bounce) {
+        if (bounce == nextCheck) {
+            OWEC_CUDA(cudaMemcpyAsync(c.hostCounts, c.dCounts.get(), 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            OWEC_CUDA(cudaStreamSynchronize(s));
+            if (c.hostCounts[cur] == 0) break;
+            nextCheck = bounce + 4;
+        }
+        // the next-bounce queue and the per-bounce queues start empty
+        OWEC_CUDA(cudaMemsetAsync(c.dCounts.get() + (cur ^ 1), 0, sizeof(uint32_t), s));
+        OWEC_CUDA(cudaMemsetAsync(c.dCounts.get() + 2, 0, 5 * sizeof(uint32_t), s));  // + fetch counters, simple queue
+        if (timed && size_t(evUsed + 4) > c.travEvents.size())
+            for (int k = 0; k < 4; ++k) {
+                cudaEvent_t e;
+                OWEC_CUDA(cudaEventCreate(&e));
+                c.travEvents.push_back(e);
+            }
+        if (timed) OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed], s));
+        launchIntersect<M>(c.ds, pb, q, cur, st, c.dCounts.get() + 4, grid, s);
+        ++intersectLaunches;
+        if (timed) OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 1], s));
+        checkLaunch();
+        launchMedium<M>(c.ds, pp, pb, q, cur, st, c.numSMs * OWEC_SHADING_GRID, s);
+        launchSurface<M>(c.ds, pp, pb, q, cur, st, c.numSMs * OWEC_SHADING_GRID, s);
+        if (timed) OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 2], s));
+        launchShadow<M>(c.ds, pp, pb, q, st, c.dCounts.get() + 5, c.dShadowVis.get(), grid, s);
+        if (timed) OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 3], s));
+        checkLaunch();
+        if (timed) evUsed += 4;
+        OWEC_CUDA(cudaMemsetAsync(c.dCounts.get() + cur, 0, sizeof(uint32_t), s));
+        cur ^= 1;
+        if (timed && evUsed >= 256) {  // fold the timings in before reusing the events
+            OWEC_CUDA(cudaStreamSynchronize(s));
+            for (int e = 0; e < evUsed; e += 2) {
+                float ms = 0;
+                OWEC_CUDA(cudaEventElapsedTime(&ms, c.travEvents[e], c.travEvents[e + 1]));
+                travSeconds[(e >> 1) & 1] += ms * 1e-3;
+            }
+            evUsed = 0;
+        }
+    }
+}
+
 template <int M>
 void runPass(owec_ctx& c, int spp) {
     using R = ModeR<M>;
@@ -1140,52 +1194,7 @@ void runPass(owec_ctx& c, int spp) {
         OWEC_CUDA(cudaMemsetAsync(c.dCounts.get(), 0, 8 * sizeof(uint32_t), s));
         launchGenerate<M>(c.ds, pp, pb, q, c.dStats.get(), s);
         checkLaunch();
-        int cur = 0;
-        // The kernels read their queue lengths on the device, so the bounces are queued without a
-        // look at the host: maxDepth + 1 of them first (a path without null boundaries ends by
-        // then), then four at a time until the queue is empty. The host waits once per batch, not
-        // once per bounce.
-        int nextCheck = pp.maxDepth + 1;
-        for (int bounce = 0; bounce < 4 * pp.maxDepth + 8; ++bounce) {
-            if (bounce == nextCheck) {
-                OWEC_CUDA(cudaMemcpyAsync(c.hostCounts, c.dCounts.get(), 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-                OWEC_CUDA(cudaStreamSynchronize(s));
-                if (c.hostCounts[cur] == 0) break;
-                nextCheck = bounce + 4;
-            }
-            // the next-bounce queue and the per-bounce queues start empty
-            OWEC_CUDA(cudaMemsetAsync(c.dCounts.get() + (cur ^ 1), 0, sizeof(uint32_t), s));
-            OWEC_CUDA(cudaMemsetAsync(c.dCounts.get() + 2, 0, 5 * sizeof(uint32_t), s));  // + fetch counters, simple queue
-            if (size_t(evUsed + 4) > c.travEvents.size())
-                for (int k = 0; k < 4; ++k) {
-                    cudaEvent_t e;
-                    OWEC_CUDA(cudaEventCreate(&e));
-                    c.travEvents.push_back(e);
-                }
-            OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed], s));
-            launchIntersect<M>(c.ds, pb, q, cur, c.dStats.get(), c.dCounts.get() + 4, grid, s);
-            ++intersectLaunches;
-            OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 1], s));
-            checkLaunch();
-            launchMedium<M>(c.ds, pp, pb, q, cur, c.dStats.get(), c.numSMs * OWEC_SHADING_GRID, s);
-            launchSurface<M>(c.ds, pp, pb, q, cur, c.dStats.get(), c.numSMs * OWEC_SHADING_GRID, s);
-            OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 2], s));
-            launchShadow<M>(c.ds, pp, pb, q, c.dStats.get(), c.dCounts.get() + 5, c.dShadowVis.get(), grid, s);
-            OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 3], s));
-            checkLaunch();
-            evUsed += 4;
-            OWEC_CUDA(cudaMemsetAsync(c.dCounts.get() + cur, 0, sizeof(uint32_t), s));
-            cur ^= 1;
-            if (evUsed >= 256) {  // fold the timings in before reusing the events
-                OWEC_CUDA(cudaStreamSynchronize(s));
-                for (int e = 0; e < evUsed; e += 2) {
-                    float ms = 0;
-                    OWEC_CUDA(cudaEventElapsedTime(&ms, c.travEvents[e], c.travEvents[e + 1]));
-                    travSeconds[(e >> 1) & 1] += ms * 1e-3;
-                }
-                evUsed = 0;
-            }
-        }
+        runBounces<M>(c, pp, pb, q, c.dStats.get(), grid, true, travSeconds, evUsed, intersectLaunches);
         launchFilm<M>(c.ds, pp, pb, c.dFilm.get(), c.dComp.get(), c.dSamples.get(), S, s);
         checkLaunch();
         done += int(S);
@@ -1307,6 +1316,51 @@ void runParticles(owec_ctx& c, int spp) {
     c.lastIntersectLaunches = intersectLaunches;
     c.particles += double(total);
     c.passCount += uint64_t(spp);
+}
+
+// The camera-path adjoint in two phases per batch of paths: the wavefront runs the batch and stops
+// each path at its first surface event on the heightfield, leaving its state there (a checkpoint);
+// the derivative replay then resumes only those paths. Paths that never meet the heightfield carry
+// no derivative and so cost one forward pass's work and nothing more.
+// Returns the number of camera paths the first phase generated.
+template <int M>
+uint64_t runAdjointCheckpointed(owec_ctx& c, PassParams pp, uint64_t firstPass, int spp, const PathAdjointTargets& t,
+                                bool fixedDecisions) {
+    using R = ModeR<M>;
+    const uint32_t nPix = pp.nPixels;
+    const uint32_t target = std::max<uint32_t>(nPix, 1u << 21);
+    const uint32_t perBatch = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(spp), target / nPix));
+    const uint32_t cap = perBatch * nPix;
+    Queues q;
+    PathBuffers<R> pb = pathState<M>(c, cap, q);
+    // every path checkpoints at most once (it ends there)
+    DBuf<uint8_t> ckpt(size_t(cap) * pathCheckpointBytes(M));
+    DBuf<uint32_t> ckptCount(1);
+    DBuf<StatCounters> st(1);  // the phase's own counters: the context's transport statistics stay the forward's
+    OWEC_CUDA(cudaMemsetAsync(st.get(), 0, sizeof(StatCounters), c.stream));
+    pp.ckptBoundary = c.hf.boundary;
+    pp.ckptCount = ckptCount.get();
+    pp.ckpt = ckpt.get();
+    const int grid = c.numSMs * 8;
+    double unusedSeconds[2] = {0, 0};
+    int unusedEvents = 0, unusedLaunches = 0;
+    for (int done = 0; done < spp;) {
+        const uint32_t S = std::min<uint32_t>(perBatch, uint32_t(spp - done));
+        pp.nPaths = S * nPix;
+        pp.streamBase = uint32_t(firstPass + uint64_t(done));
+        OWEC_CUDA(cudaMemsetAsync(c.dCounts.get(), 0, 8 * sizeof(uint32_t), c.stream));
+        OWEC_CUDA(cudaMemsetAsync(ckptCount.get(), 0, sizeof(uint32_t), c.stream));
+        launchGenerate<M>(c.ds, pp, pb, q, st.get(), c.stream);
+        checkLaunch();
+        runBounces<M>(c, pp, pb, q, st.get(), grid, false, unusedSeconds, unusedEvents, unusedLaunches);
+        launchPathAdjoint(M, c.ds, pp, c.hf, t, fixedDecisions, ckpt.get(), ckptCount.get(), grid, c.stream);
+        checkLaunch();
+        done += int(S);
+    }
+    StatCounters hs{};
+    OWEC_CUDA(cudaMemcpyAsync(&hs, st.get(), sizeof(StatCounters), cudaMemcpyDeviceToHost, c.stream));
+    OWEC_CUDA(cudaStreamSynchronize(c.stream));
+    return hs.paths;
 }
 
 }  // namespace
@@ -1855,10 +1909,11 @@ int owec_walk_adjoint_noalloc(owec_ctx* ctx, const owec_walk_desc* w, uint64_t f
     });
 }
 
-int owec_path_adjoint(owec_ctx* ctx, uint64_t first_pass, int spp, const double* g, double* dheights,
+int owec_path_adjoint(owec_ctx* ctx, uint64_t first_pass, int spp, int flags, const double* g, double* dheights,
                       double* replay_xyz, owec_adjoint_stats* stats) {
     return guarded([&] {
         require(ctx && g && dheights, "owec_path_adjoint: null argument");
+        require((flags & ~OWEC_ADJOINT_FIXED_DECISIONS) == 0, "owec_path_adjoint: unknown flags");
         require(spp > 0, "owec_path_adjoint: spp must be positive");
         require(ctx->hasScene, "no scene uploaded", OWEC_E_STATE);
         require(ctx->hf.boundary != kNone, "no heightfield set (owec_set_heightfield)", OWEC_E_STATE);
@@ -1869,6 +1924,8 @@ int owec_path_adjoint(owec_ctx* ctx, uint64_t first_pass, int spp, const double*
         require(first_pass + uint64_t(spp) <= (1ull << 32), "owec_path_adjoint: the PCG32 stream index is 32 bits");
         OWEC_CUDA(cudaSetDevice(ctx->device));
         ensureReady(*ctx);
+        size_t freeBefore = 0, freeDuring = 0, total = 0;
+        OWEC_CUDA(cudaMemGetInfo(&freeBefore, &total));
         const uint32_t nPix = uint32_t(ctx->ds.det.width) * uint32_t(ctx->ds.det.height);
         const size_t nh = ctx->hfVertices;
         DBuf<double> dG(3 * size_t(nPix)), dDH(nh), dRep(replay_xyz ? 3 * size_t(nPix) : 0);
@@ -1888,18 +1945,32 @@ int owec_path_adjoint(owec_ctx* ctx, uint64_t first_pass, int spp, const double*
         pp.nPixels = nPix;
         pp.anyHitShadows = 1;
         PathAdjointTargets t{dG.get(), 1.0 / double(spp), dDH.get(), replay_xyz ? dRep.get() : nullptr, ctr.get()};
-        // one launch replays up to 2^22 paths (whole samples of the film)
-        const uint32_t perBatch = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(spp), (1u << 22) / std::max(1u, nPix)));
+        const bool fixed = (flags & OWEC_ADJOINT_FIXED_DECISIONS) != 0;
+        uint64_t cameraPaths = 0;  // the first phase's count (the replay kernel counts only what it walks)
         OWEC_CUDA(cudaEventRecord(ctx->passStart, ctx->stream));
-        for (int done = 0; done < spp;) {
-            const uint32_t S = std::min<uint32_t>(perBatch, uint32_t(spp - done));
-            pp.nPaths = S * nPix;
-            pp.streamBase = uint32_t(first_pass + uint64_t(done));
-            launchPathAdjoint(ctx->settings.precision, ctx->ds, pp, ctx->hf, t, ctx->numSMs * 8, ctx->stream);
-            checkLaunch();
-            done += int(S);
+        if (replay_xyz) {
+            // the replayed film needs every path: replay them all from the camera, up to 2^22 per
+            // launch (whole samples of the film)
+            const uint32_t perBatch = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(spp), (1u << 22) / std::max(1u, nPix)));
+            for (int done = 0; done < spp;) {
+                const uint32_t S = std::min<uint32_t>(perBatch, uint32_t(spp - done));
+                pp.nPaths = S * nPix;
+                pp.streamBase = uint32_t(first_pass + uint64_t(done));
+                launchPathAdjoint(ctx->settings.precision, ctx->ds, pp, ctx->hf, t, fixed, nullptr, nullptr,
+                                  ctx->numSMs * 8, ctx->stream);
+                checkLaunch();
+                done += int(S);
+            }
+        } else if (ctx->settings.precision == OWEC_PRECISION_FP64) {
+            cameraPaths = runAdjointCheckpointed<OWEC_PRECISION_FP64>(*ctx, pp, first_pass, spp, t, fixed);
+        } else if (ctx->settings.precision == OWEC_PRECISION_FP32) {
+            cameraPaths = runAdjointCheckpointed<OWEC_PRECISION_FP32>(*ctx, pp, first_pass, spp, t, fixed);
+        } else {
+            cameraPaths = runAdjointCheckpointed<OWEC_PRECISION_MIXED>(*ctx, pp, first_pass, spp, t, fixed);
         }
         OWEC_CUDA(cudaEventRecord(ctx->passStop, ctx->stream));
+        OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+        OWEC_CUDA(cudaMemGetInfo(&freeDuring, &total));  // the buffers and the kernels' stacks, still held
         std::vector<double> h(nh);
         unsigned long long counts[4];
         OWEC_CUDA(cudaMemcpyAsync(h.data(), dDH.get(), nh * 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1912,11 +1983,12 @@ int owec_path_adjoint(owec_ctx* ctx, uint64_t first_pass, int spp, const double*
         ctx->lastPathAdjointSeconds = ms * 1e-3;
         for (size_t i = 0; i < nh; ++i) dheights[i] += h[i];
         if (stats) {
-            stats->paths = counts[0];
+            stats->paths = replay_xyz ? counts[0] : cameraPaths;
             stats->heightfield = counts[1];
             stats->dropped = counts[2];
             stats->faults = counts[3];
             stats->seconds = ms * 1e-3;
+            stats->device_bytes = freeBefore > freeDuring ? uint64_t(freeBefore - freeDuring) : 0;
         }
     });
 }

@@ -19,6 +19,11 @@
 //     (1 - R) (ni/nt)^2 / (1 - pR) moves with R, the roulette's 1 / q does not;
 //   - refraction and reflection at the moved normal are differentiated (attached), and every hit
 //     point moves within its surface (implicit differentiation of the crossing).
+// With fixed decisions the branch and roulette probabilities and the Henyey-Greenstein frame move
+// with the path instead (attached): the result is then the derivative of the estimator at fixed
+// random numbers, which is what central differences with common random numbers measure, but it
+// leaves out the branches' boundary terms (a path switching from refraction to reflection as R
+// moves) and so is not the gradient of the expected film.
 // Each contribution (next-event estimates, emission and sky with MIS) is differentiated with respect
 // to the vertex's position, incident direction and pdf through dual numbers, and the derivative of
 // the path's hero radiance is summed per slot. At the end of the path the slots are weighted as the
@@ -66,6 +71,28 @@ __device__ __forceinline__ bool survivesQ(PathSpec<R>& sp, Pcg32& rng, double& q
     return true;
 }
 
+// The roulette's effect on the throughput derivatives: beta / q with q held fixed (the detached
+// convention), or with q = min(1, max beta) moving with the hero throughput b0 it was taken from
+// (the derivative of the estimator at fixed random numbers; the secondaries are dead whenever a path
+// carries derivatives, so the maximum is the hero's).
+__device__ __forceinline__ void rouletteTangents(double* dB, int n, double q, double b0, bool fixedDecisions) {
+    const bool moves = fixedDecisions && q < 1 && b0 > 0;
+    for (int k = 0; k < n; ++k) dB[k] = moves ? dB[k] / q - b0 * dB[k] / (q * q) : dB[k] / q;
+}
+
+// The derivative of a Henyey-Greenstein direction drawn about wo = -d (sampleHg's frame, the Duff et al.
+// basis of wo) when wo moves by dwo with the drawn angles held: the direction attached to the incident
+// one.
+__device__ V3<double> hgDirectionTangent(const V3<double>& wo, const V3<double>& wi, const V3<double>& dwo) {
+    const double sgn = copysign(1.0, wo.z);
+    const double a = -1 / (sgn + wo.z), da = a * a * dwo.z;
+    const double b = wo.x * wo.y * a, db = (dwo.x * wo.y + wo.x * dwo.y) * a + wo.x * wo.y * da;
+    const V3<double> b1(1 + sgn * wo.x * wo.x * a, sgn * b, -sgn * wo.x), b2(b, sgn + wo.y * wo.y * a, -wo.y);
+    const V3<double> db1(sgn * (2 * wo.x * dwo.x * a + wo.x * wo.x * da), sgn * db, -sgn * dwo.x);
+    const V3<double> db2(db, 2 * wo.y * dwo.y * a + wo.y * wo.y * da, -dwo.y);
+    return db1 * dot(wi, b1) + db2 * dot(wi, b2) + dwo * dot(wi, wo);
+}
+
 // The next-event estimate toward a point light sample y (normal nL, emitter area, selection pdf)
 // from a vertex at x, divided by the throughput: f * Le * cosF * w / pdfL * Tr as a dual in x (and in
 // the incident direction d for a medium vertex, through the phase function). Surface vertices:
@@ -101,6 +128,7 @@ struct AdjointParams {
     PassParams pp;
     HeightfieldParams hf;
     PathAdjointTargets t;
+    bool fixedDecisions;
 };
 
 // Adds slot k's derivative of a contribution c = beta * c', c' a dual in the vertex position (vars
@@ -172,46 +200,29 @@ __device__ bool neeClear(const DeviceScene& sc, const LightSampleD& ls, const V3
     return clear;
 }
 
+// One camera path from `ray`, `sp`, `aux`, `rng` on: from its camera ray (resume null), or from a
+// checkpoint at its first heightfield surface event (resume: that event's hit, whose segment's free
+// flight the forward pass has already taken).
 template <int M, bool Full>
-__device__ void adjointPath(const DeviceScene& sc, const AdjointParams& P, uint32_t i, StackEntry* stack, int stride) {
+__device__ void adjointPath(const DeviceScene& sc, const AdjointParams& P, PathRay<typename Mode<M>::R> ray,
+                            PathSpec<typename Mode<M>::R> sp, PathAux aux, Pcg32 rng, const HitRec* resume,
+                            StackEntry* stack, int stride) {
     using R = typename Mode<M>::R;
     using Ro = typename Mode<M>::Ro;
     using Rr = typename Mode<M>::Rr;
     const PassParams& pp = P.pp;
-    PathRay<R> ray;
-    PathSpec<R> sp;
-    PathAux aux;
-    Pcg32 rng;
-    if (!generateCameraPath<M>(sc, pp, i, ray, sp, aux, rng)) return;
     unsigned long long* ctr = P.t.counters;
     PathTangents tg;
     tg.n = 0;
     tg.valid = true;
     bool metHeightfield = false, fault = false;
     for (;;) {
-        // ---------------------------------------------------------------- closest hit (kIntersect)
-        RayQuery<R> rq;
-        rq.od = rayOrigin(ray.o);
-        rq.o = V3<R>(rq.od);
-        rq.d = rayDir(ray);
-        rq.tmax = R(INFINITY);
-        rq.depB = ray.depB;
-        rq.depP = ray.depP;
-        rq.region = ray.region;
-        rq.errN = R(ray.errN);
-        HitRec h;
-        h.boundary = kNone;
-        h.t = INFINITY;
-        h.flags = 0;
-        const int s = traceRay<R, Ro, Rr, false, Full>(sc, rq, stack, stride, h);
-        if (s != kTraceHit) { h.boundary = kNone; h.t = INFINITY; }
-        if (s == kTraceOverflow) { fault = true; break; }
-        const bool found = h.boundary < kNone - 1u;
         const V3<R> d = rayDir(ray);
         const V3<double> dd(d);
-        // ---------------------------------------------------------------- free flight (kMedium)
         const owec_medium med = sc.media[sc.regionMedium[ray.region]];
         const bool absorbs = mediumAbsorbs(med, sc), scatters = mediumScatters(med, sc);
+        HitRec h;
+        bool found;
         int event = 0;  // 0 pass, 1 scatter, 2 end
         double tS = 0;
         R beforeAbs = sp.beta[0], sigmaA0 = R(0);
@@ -221,38 +232,66 @@ __device__ void adjointPath(const DeviceScene& sc, const AdjointParams& P, uint3
         LightSampleD ls;
         R contrib[NW] = {R(0), R(0), R(0), R(0)};
         R Tr[NW];
-        if (found && !absorbs && !scatters) {
-            event = 0;
+        if (resume) {
+            // the checkpointed surface event: its segment's Beer-Lambert factor is already applied
+            h = *resume;
+            resume = nullptr;
+            found = true;
+            if (absorbs && !scatters) {
+                sigmaA0 = evalSpectrum(sc, med.absorption, R(sp.lambda[0]));
+                const R att = exp(-sigmaA0 * R(h.t));
+                beforeAbs = att > R(0) ? sp.beta[0] / att : R(0);
+            }
         } else {
-            const double seg = found ? h.t : INFINITY;
-            if (scatters) {
-                R sT[NW];
-                for (int j = 0; j < NW; ++j)
-                    sT[j] = evalSpectrum(sc, med.absorption, R(sp.lambda[j])) + evalSpectrum(sc, med.scattering, R(sp.lambda[j]));
-                tS = -log(1 - rng.uniform()) / double(sT[0]);
-                if (tS < seg) {
-                    const R pdf0 = sT[0] * exp(-sT[0] * R(tS));
-                    const R b0 = sp.beta[0];
+            // ------------------------------------------------------------ closest hit (kIntersect)
+            RayQuery<R> rq;
+            rq.od = rayOrigin(ray.o);
+            rq.o = V3<R>(rq.od);
+            rq.d = d;
+            rq.tmax = R(INFINITY);
+            rq.depB = ray.depB;
+            rq.depP = ray.depP;
+            rq.region = ray.region;
+            rq.errN = R(ray.errN);
+            h.boundary = kNone;
+            h.t = INFINITY;
+            h.flags = 0;
+            const int s = traceRay<R, Ro, Rr, false, Full>(sc, rq, stack, stride, h);
+            if (s != kTraceHit) { h.boundary = kNone; h.t = INFINITY; }
+            if (s == kTraceOverflow) { fault = true; break; }
+            found = h.boundary < kNone - 1u;
+            // ------------------------------------------------------------ free flight (kMedium)
+            if (!(found && !absorbs && !scatters)) {
+                const double seg = found ? h.t : INFINITY;
+                if (scatters) {
+                    R sT[NW];
                     for (int j = 0; j < NW; ++j)
-                        sp.beta[j] *= evalSpectrum(sc, med.scattering, R(sp.lambda[j])) * exp(-sT[j] * R(tS)) / pdf0;
-                    // the hero's weight sigma_s / sigma_t does not move with the heights
-                    const double w0 = b0 != R(0) ? double(sp.beta[0]) / double(b0) : 0.0;
-                    for (int k = 0; k < tg.n; ++k) tg.dB[k] *= w0;
-                    event = 1;
-                } else if (isinf(seg)) {
-                    event = 2;
-                } else {
-                    const R pass0 = exp(-sT[0] * R(seg));
-                    for (int j = 0; j < NW; ++j) sp.beta[j] *= exp(-sT[j] * R(seg)) / pass0;
-                }
-            } else if (absorbs) {
-                if (isinf(seg)) {
-                    event = 2;
-                } else {
-                    beforeAbs = sp.beta[0];
-                    sigmaA0 = evalSpectrum(sc, med.absorption, R(sp.lambda[0]));
-                    for (int j = 0; j < NW; ++j)
-                        sp.beta[j] *= exp(-evalSpectrum(sc, med.absorption, R(sp.lambda[j])) * R(seg));
+                        sT[j] = evalSpectrum(sc, med.absorption, R(sp.lambda[j])) + evalSpectrum(sc, med.scattering, R(sp.lambda[j]));
+                    tS = -log(1 - rng.uniform()) / double(sT[0]);
+                    if (tS < seg) {
+                        const R pdf0 = sT[0] * exp(-sT[0] * R(tS));
+                        const R b0 = sp.beta[0];
+                        for (int j = 0; j < NW; ++j)
+                            sp.beta[j] *= evalSpectrum(sc, med.scattering, R(sp.lambda[j])) * exp(-sT[j] * R(tS)) / pdf0;
+                        // the hero's weight sigma_s / sigma_t does not move with the heights
+                        const double w0 = b0 != R(0) ? double(sp.beta[0]) / double(b0) : 0.0;
+                        for (int k = 0; k < tg.n; ++k) tg.dB[k] *= w0;
+                        event = 1;
+                    } else if (isinf(seg)) {
+                        event = 2;
+                    } else {
+                        const R pass0 = exp(-sT[0] * R(seg));
+                        for (int j = 0; j < NW; ++j) sp.beta[j] *= exp(-sT[j] * R(seg)) / pass0;
+                    }
+                } else if (absorbs) {
+                    if (isinf(seg)) {
+                        event = 2;
+                    } else {
+                        beforeAbs = sp.beta[0];
+                        sigmaA0 = evalSpectrum(sc, med.absorption, R(sp.lambda[0]));
+                        for (int j = 0; j < NW; ++j)
+                            sp.beta[j] *= exp(-evalSpectrum(sc, med.absorption, R(sp.lambda[j])) * R(seg));
+                    }
                 }
             }
         }
@@ -301,7 +340,14 @@ __device__ void adjointPath(const DeviceScene& sc, const AdjointParams& P, uint3
             const Draw2<R> u(rng);
             V3<R> wi;
             aux.prevPdf = float(sampleHg(-d, R(med.g), u.u1, u.u2, wi));
-            if (tg.n > 0) {
+            if (tg.n > 0 && P.fixedDecisions) {
+                // the drawn angles stay: the direction turns with the incident one, weight 1
+                const V3<double> wo = -dd, w(wi);
+                for (int k = 0; k < tg.n; ++k) {
+                    st3(tg.dD[k], hgDirectionTangent(wo, w, -ld3(tg.dD[k])));
+                    tg.dPdf[k] = 0;
+                }
+            } else if (tg.n > 0) {
                 // the drawn direction stays; the phase at the moved incident direction weighs it
                 const V3<double> w(wi);
                 const double g = med.g, c = dot(-dd, w);
@@ -327,8 +373,9 @@ __device__ void adjointPath(const DeviceScene& sc, const AdjointParams& P, uint3
             ray.depP = kNone;
             ray.errN = 0.f;
             double q = 1;
+            const double b0 = double(sp.beta[0]);
             cont = int(aux.depth) < pp.rrDepth || survivesQ(sp, rng, q);
-            for (int k = 0; k < tg.n; ++k) tg.dB[k] /= q;
+            rouletteTangents(tg.dB, tg.n, q, b0, P.fixedDecisions);
         } else if (event == 0 && !found) {
             if (ray.region == 0) {
                 // skyMet (transport.cpp:401-417)
@@ -606,6 +653,10 @@ __device__ void adjointPath(const DeviceScene& sc, const AdjointParams& P, uint3
                             double Rf, dRdc;
                             fresnelWithDerivative(-dot(dd, n), eta, Rf, dRdc);
                             const double pR = double(fresnelBranchProbability(R(Rf), it.fresnelFloor));
+                            // dpR/dR: held (detached), or moving with R unless the floor clamps it
+                            const double fl = double(it.fresnelFloor);
+                            const double dpR = !P.fixedDecisions ? 0.0
+                                               : ((fl > 0 && Rf < 1 && (Rf < fl || Rf > 1 - fl)) ? 0.0 : 1.0);
                             const bool fr = dot(dd, n) < 0;
                             const double ni = fr ? double(it.nFront) : double(it.nBack);
                             const double nt = fr ? double(it.nBack) : double(it.nFront);
@@ -615,10 +666,11 @@ __device__ void adjointPath(const DeviceScene& sc, const AdjointParams& P, uint3
                                 V3<double> dOut;
                                 if (ss.transmitted) {
                                     const double radiance = sqr(ni / nt);
-                                    tg.dB[k] = tg.dB[k] * double(ss.weight) - beta0 * dRdc * dc / (1 - pR) * radiance;
+                                    tg.dB[k] = tg.dB[k] * double(ss.weight) -
+                                               beta0 * dRdc * dc * ((1 - pR) - (1 - Rf) * dpR) / ((1 - pR) * (1 - pR)) * radiance;
                                     dOut = refractTangent(dd, n, ni, nt, dDk, dnk);
                                 } else {
-                                    tg.dB[k] = tg.dB[k] * double(ss.weight) + beta0 * dRdc * dc / pR;
+                                    tg.dB[k] = tg.dB[k] * double(ss.weight) + beta0 * dRdc * dc * (pR - Rf * dpR) / (pR * pR);
                                     dOut = reflectTangent(dd, n, dDk, dnk);
                                 }
                                 st3(tg.dD[k], dOut);
@@ -664,8 +716,9 @@ __device__ void adjointPath(const DeviceScene& sc, const AdjointParams& P, uint3
                     ray.errN = errN;
                     scattered = true;
                     double q = 1;
+                    const double b0 = double(sp.beta[0]);
                     cont = !(int(aux.depth) >= pp.rrDepth && !survivesQ(sp, rng, q));
-                    for (int k = 0; k < tg.n; ++k) tg.dB[k] /= q;
+                    rouletteTangents(tg.dB, tg.n, q, b0, P.fixedDecisions);
                 }
             }
             (void)scattered;
@@ -674,7 +727,7 @@ __device__ void adjointPath(const DeviceScene& sc, const AdjointParams& P, uint3
         aux.depth += 1;
     }
     // ---------------------------------------------------------------- the film's weighting (kFilm)
-    const uint32_t pixel = i % pp.nPixels;
+    const uint32_t pixel = aux.pixel;
     const double inv = 1.0 / (NW * sc.cieYIntegral);
     double xyz[3] = {0, 0, 0};
     for (int k = 0; k < NW; ++k) {
@@ -704,29 +757,63 @@ __device__ void adjointPath(const DeviceScene& sc, const AdjointParams& P, uint3
         if (tg.acc[k] != 0) atomicAdd(P.t.dH + tg.vert[k], tg.acc[k] * gam);
 }
 
+// Full replay: every camera path of the batch from its camera ray.
 template <int M, bool Full>
 __global__ void __launch_bounds__(128) kPathAdjoint(DeviceScene sc, AdjointParams P) {
     extern __shared__ StackEntry stackMem[];
     StackEntry* stack = stackMem + threadIdx.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.pp.nPaths; i += gridDim.x * blockDim.x)
-        adjointPath<M, Full>(sc, P, i, stack, blockDim.x);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.pp.nPaths; i += gridDim.x * blockDim.x) {
+        PathRay<typename Mode<M>::R> ray;
+        PathSpec<typename Mode<M>::R> sp;
+        PathAux aux;
+        Pcg32 rng;
+        if (generateCameraPath<M>(sc, P.pp, i, ray, sp, aux, rng))
+            adjointPath<M, Full>(sc, P, ray, sp, aux, rng, nullptr, stack, blockDim.x);
+    }
+}
+
+// From the checkpoints the wavefront left at the paths' first heightfield surface events.
+template <int M, bool Full>
+__global__ void __launch_bounds__(128) kPathAdjointResume(DeviceScene sc, AdjointParams P,
+                                                          const PathCheckpoint<typename Mode<M>::R>* ckpt,
+                                                          const uint32_t* count) {
+    extern __shared__ StackEntry stackMem[];
+    StackEntry* stack = stackMem + threadIdx.x;
+    const uint32_t n = *count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const PathCheckpoint<typename Mode<M>::R> c = loadStream(ckpt + i);
+        const Pcg32 rng{c.aux.rngState, (uint64_t(c.aux.stream) << 1u) | 1u};
+        adjointPath<M, Full>(sc, P, c.ray, c.spec, c.aux, rng, &c.hit, stack, blockDim.x);
+    }
 }
 
 template <int M>
-void launchMode(const DeviceScene& sc, const AdjointParams& P, int grid, cudaStream_t s) {
+void launchMode(const DeviceScene& sc, const AdjointParams& P, const void* ckpt, const uint32_t* count, int grid,
+                cudaStream_t s) {
+    using C = PathCheckpoint<typename Mode<M>::R>;
     const size_t smem = traversalSharedBytes(128);
-    if (sc.fullFeatures) kPathAdjoint<M, true><<<grid, 128, smem, s>>>(sc, P);
-    else kPathAdjoint<M, false><<<grid, 128, smem, s>>>(sc, P);
+    if (ckpt) {
+        if (sc.fullFeatures) kPathAdjointResume<M, true><<<grid, 128, smem, s>>>(sc, P, static_cast<const C*>(ckpt), count);
+        else kPathAdjointResume<M, false><<<grid, 128, smem, s>>>(sc, P, static_cast<const C*>(ckpt), count);
+    } else {
+        if (sc.fullFeatures) kPathAdjoint<M, true><<<grid, 128, smem, s>>>(sc, P);
+        else kPathAdjoint<M, false><<<grid, 128, smem, s>>>(sc, P);
+    }
 }
 
 }  // namespace
 
+size_t pathCheckpointBytes(int mode) {
+    return mode == OWEC_PRECISION_FP64 ? sizeof(PathCheckpoint<double>) : sizeof(PathCheckpoint<float>);
+}
+
 void launchPathAdjoint(int mode, const DeviceScene& sc, const PassParams& pp, const HeightfieldParams& hf,
-                       const PathAdjointTargets& t, int grid, cudaStream_t s) {
-    AdjointParams P{pp, hf, t};
-    if (mode == OWEC_PRECISION_FP64) launchMode<OWEC_PRECISION_FP64>(sc, P, grid, s);
-    else if (mode == OWEC_PRECISION_FP32) launchMode<OWEC_PRECISION_FP32>(sc, P, grid, s);
-    else launchMode<OWEC_PRECISION_MIXED>(sc, P, grid, s);
+                       const PathAdjointTargets& t, bool fixedDecisions, const void* ckpt, const uint32_t* ckptCount,
+                       int grid, cudaStream_t s) {
+    AdjointParams P{pp, hf, t, fixedDecisions};
+    if (mode == OWEC_PRECISION_FP64) launchMode<OWEC_PRECISION_FP64>(sc, P, ckpt, ckptCount, grid, s);
+    else if (mode == OWEC_PRECISION_FP32) launchMode<OWEC_PRECISION_FP32>(sc, P, ckpt, ckptCount, grid, s);
+    else launchMode<OWEC_PRECISION_MIXED>(sc, P, ckpt, ckptCount, grid, s);
 }
 
 }  // namespace owec

@@ -156,6 +156,21 @@ struct PassParams {
     uint32_t nPaths;         // paths in this batch: nPixels * samples
     uint32_t streamBase;     // PCG32 stream of the batch's first sample
     int32_t anyHitShadows;   // 1: no null boundaries, shadow rays stop at the first crossing
+    // The adjoint's first phase: a path about to meet boundary ckptBoundary (kNone: never) stops there
+    // and leaves its state as a PathCheckpoint (slot from ckptCount) for the derivative replay.
+    uint32_t ckptBoundary = kNone;
+    uint32_t* ckptCount = nullptr;
+    void* ckpt = nullptr;
+};
+
+// A path's state at the surface event where it first meets the heightfield: what kSurface would
+// load for it (after the free flight of the segment), and the hit.
+template <class R>
+struct alignas(16) PathCheckpoint {
+    PathRay<R> ray;
+    PathSpec<R> spec;
+    PathAux aux;
+    HitRec hit;
 };
 
 }  // namespace owec

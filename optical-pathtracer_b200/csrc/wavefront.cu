@@ -208,6 +208,15 @@ __device__ void queueNee(const DeviceScene& sc, PathBuffers<RT<M>>& pb, Queues& 
 }
 
 // ------------------------------------------------------------------ medium
+// The adjoint's first phase: the path's state at its surface event on the checkpoint boundary, for
+// the derivative replay to take over from; the path itself ends here.
+template <int M>
+__device__ __forceinline__ void checkpointPath(const PassParams& pp, const PathRay<RT<M>>& ray, const PathSpec<RT<M>>& sp,
+                                               const PathAux& aux, const HitRec& h) {
+    const uint32_t slot = atomicAdd(pp.ckptCount, 1u);
+    storeStream(reinterpret_cast<PathCheckpoint<RT<M>>*>(pp.ckpt) + slot, PathCheckpoint<RT<M>>{ray, sp, aux, h});
+}
+
 template <int M>
 __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kMedium(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
                                                int cur, StatCounters* st) {
@@ -223,6 +232,10 @@ __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kMedium(DeviceSc
             // surface queues, without reading or writing the rest of the path's state.
             const owec_medium& m0 = sc.media[sc.regionMedium[pb.ray[i].region]];
             if (h.boundary < kNone - 1u && !mediumAbsorbs(m0, sc) && !mediumScatters(m0, sc)) {
+                if (h.boundary == pp.ckptBoundary) {
+                    checkpointPath<M>(pp, loadStream(pb.ray + i), loadStream(pb.spec + i), loadStream(pb.aux + i), h);
+                    continue;
+                }
                 const int32_t ot = sc.optics[sc.boundaries[h.boundary].optics].type;
                 const bool simple = ot == OWEC_SURF_DIFFUSE || ot == OWEC_SURF_ABSORBER || ot == OWEC_SURF_DETECTOR;
                 warpPush(q.surface, &q.counts[2], !simple, i);
@@ -334,6 +347,10 @@ __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kMedium(DeviceSc
         storeStream(pb.aux + i, aux);
         queueNee<M>(sc, pb, q, i, sp, betaNee, ls, fN, pdfS, R(1), sp3, ray.region, kNone, kNone, 0.f, neeValid);
         warpCount(&st->leaks, leak);
+        if (toSurface && h.boundary == pp.ckptBoundary) {
+            checkpointPath<M>(pp, ray, sp, aux, h);
+            toSurface = false;
+        }
         // surface events on Lambertian, absorbing and detecting boundaries go to the lean kernel
         bool simple = false;
         if (toSurface) {

@@ -52,26 +52,29 @@ class WalkFilm(torch.autograd.Function):
 
 class CameraFilm(torch.autograd.Function):
     """image(heights): the resolved camera film (height x width x 3, XYZ) of `spp` samples per pixel
-    from sample stream `first_pass` on, as a function of the heightfield's heights."""
+    from sample stream `first_pass` on, as a function of the heightfield's heights. The backward pass
+    is the gradient of the expected film, or with fixed_decisions the derivative of this film's
+    estimator at its own random numbers (what central differences with common random numbers
+    measure)."""
 
     @staticmethod
-    def forward(ctx, heights, context, boundary, base_z, first_pass, spp):
+    def forward(ctx, heights, context, boundary, base_z, first_pass, spp, fixed_decisions):
         h = heights.detach().cpu().numpy().astype(np.float64).ravel()
         _ensure_heights(context, boundary, base_z, h)
         context.reset_film()
         context.set_pass_index(first_pass)
         context.run_pass(spp)
         img, _ = context.resolve(samples=False)
-        ctx.args = (context, boundary, base_z, first_pass, spp, h, heights.shape)
+        ctx.args = (context, boundary, base_z, first_pass, spp, fixed_decisions, h, heights.shape)
         return torch.from_numpy(np.array(img)).to(heights.dtype)
 
     @staticmethod
     def backward(ctx, grad_img):
-        context, boundary, base_z, first_pass, spp, h, shape = ctx.args
+        context, boundary, base_z, first_pass, spp, fixed, h, shape = ctx.args
         _ensure_heights(context, boundary, base_z, h)
         g = grad_img.detach().cpu().numpy().astype(np.float64)
-        dh = context.path_adjoint(first_pass, spp, g)
-        return torch.from_numpy(dh.reshape(shape)).to(grad_img.dtype), None, None, None, None, None
+        dh = context.path_adjoint(first_pass, spp, g, fixed_decisions=fixed)
+        return torch.from_numpy(dh.reshape(shape)).to(grad_img.dtype), None, None, None, None, None, None
 
 
 def walk_film(heights, context, boundary, base_z, desc, first, n):
@@ -79,6 +82,6 @@ def walk_film(heights, context, boundary, base_z, desc, first, n):
     return WalkFilm.apply(heights, context, boundary, base_z, desc, first, n)
 
 
-def camera_film(heights, context, boundary, base_z, first_pass, spp):
+def camera_film(heights, context, boundary, base_z, first_pass, spp, fixed_decisions=False):
     """The camera film as a differentiable function of `heights` (a float64 tensor)."""
-    return CameraFilm.apply(heights, context, boundary, base_z, first_pass, spp)
+    return CameraFilm.apply(heights, context, boundary, base_z, first_pass, spp, fixed_decisions)

@@ -190,11 +190,13 @@ class Context:
                "owec_walk_adjoint_noalloc")
         return out
 
-    def path_adjoint(self, first_pass, spp, g, dheights=None, replay=False, with_stats=False):
+    def path_adjoint(self, first_pass, spp, g, dheights=None, replay=False, with_stats=False, fixed_decisions=False):
         """d(sum_p g_p . film_p) / d heights by path replay of the camera paths of samples first_pass
         .. first_pass + spp - 1 (owec_path_adjoint). g: dLoss/dFilm, height x width x 3. Returns the
         gradient (added to `dheights` when given); with with_stats, (gradient, stats dict, replayed
-        image or None)."""
+        image or None). replay: every path replayed from its camera ray and the replayed image
+        returned. fixed_decisions: the derivative at fixed random numbers (what central differences
+        with common random numbers measure) instead of the gradient of the expected film."""
         if not hasattr(self, "_hf_n"):
             raise RuntimeError("no heightfield set (set_heightfield)")
         gg = np.ascontiguousarray(g, np.float64).ravel()
@@ -205,7 +207,8 @@ class Context:
             raise ValueError(f"dheights has {out.size} values; the heightfield has {self._hf_n} vertices")
         rep = np.zeros(3 * self.width * self.height) if replay else None
         st = A.AdjointStats()
-        _check(self.lib, self.lib.owec_path_adjoint(self.handle, int(first_pass), int(spp), gg.ctypes.data_as(A.c_double_p),
+        flags = A.ADJOINT_FIXED_DECISIONS if fixed_decisions else 0
+        _check(self.lib, self.lib.owec_path_adjoint(self.handle, int(first_pass), int(spp), flags, gg.ctypes.data_as(A.c_double_p),
                                                     out.ctypes.data_as(A.c_double_p),
                                                     rep.ctypes.data_as(A.c_double_p) if replay else None,
                                                     ctypes.byref(st)), "owec_path_adjoint")

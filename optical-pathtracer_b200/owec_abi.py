@@ -25,6 +25,7 @@ SKY_NONE, SKY_UNIFORM, SKY_GRADIENT = 0, 1, 2
 DETECTOR_OBSERVER, DETECTOR_SENSOR = 0, 1
 WAVELENGTHS_HERO4, WAVELENGTHS_UNIFORM1 = 0, 1
 PRECISION_MIXED, PRECISION_FP32, PRECISION_FP64 = 0, 1, 2
+ADJOINT_FIXED_DECISIONS = 1
 REGION_OUTSIDE = 0xFFFFFFFF
 KNONE = 0xFFFFFFFE  # the reference's kNone: "no boundary"
 
@@ -147,7 +148,7 @@ class WalkStats(ctypes.Structure):
 
 class AdjointStats(ctypes.Structure):
     _fields_ = [("paths", ctypes.c_uint64), ("heightfield", ctypes.c_uint64), ("dropped", ctypes.c_uint64),
-                ("faults", ctypes.c_uint64), ("seconds", ctypes.c_double)]
+                ("faults", ctypes.c_uint64), ("seconds", ctypes.c_double), ("device_bytes", ctypes.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -217,7 +218,7 @@ def load_library(path=LIB_PATH):
         "owec_walk_adjoint_noalloc": ([P, ctypes.POINTER(WalkDesc), ctypes.c_uint64, ctypes.c_uint64, c_double_p,
                                        c_double_p], ctypes.c_int),
         "owec_walk_timing": ([P, c_double_p], ctypes.c_int),
-        "owec_path_adjoint": ([P, ctypes.c_uint64, ctypes.c_int, c_double_p, c_double_p, c_double_p,
+        "owec_path_adjoint": ([P, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, c_double_p, c_double_p, c_double_p,
                                ctypes.POINTER(AdjointStats)], ctypes.c_int),
     }
     for name, (args, res) in sigs.items():

@@ -565,6 +565,78 @@ def fog_room(width=64, height=48, n_lon=128, n_lat=64, panel_n=16, sigma_s=0.5, 
     return sb
 
 
+def heightfield_panel(sb, n, heights, half, thickness, offset, inside):
+    """A closed slab of `inside`'s medium whose top face is an n x n heightfield over
+    [-half, half]^2 at z = thickness + heights, bottom at z = 0, moved by `offset`; both faces smooth
+    dielectric boundaries with the ambient region outside. Returns (heightfield boundary, base z of
+    its heights in its frame)."""
+    h = np.asarray(heights, np.float64).reshape(n, n)
+    off = np.asarray(offset, float)
+    glass = sb.dielectric()
+    top_v, top_t = heightfield_grid(n, n, half, half, thickness, h)
+    hf = sb.boundary(A.SHAPE_MESH, [], pose(), 0, inside, glass, -1, sb.mesh(np.asarray(top_v) + off, top_t))
+    rest_v, rest_t = slab_rest(n, n, half, half, lambda i, j: thickness + h[j, i])
+    sb.boundary(A.SHAPE_MESH, [], pose(), 0, inside, glass, -1, sb.mesh(np.asarray(rest_v) + off, rest_t))
+    return hf, thickness + off[2]
+
+
+def refraction_panel(n=16, heights=None, width=32, height=32, size=0.2, thickness=0.02, elevation=0.3,
+                     fog=None, sky=0.05, lamp=20.0):
+    """The camera-path adjoint's check scene: a PMMA panel whose top face is an n x n heightfield,
+    held `elevation` above a Lambertian floor and seen from 4 m above by a narrow pinhole, so that the
+    image is the floor seen through the refracting heights. A rectangular lamp standing low at the
+    side lights the floor beneath the panel with a strong falloff; a dim uniform sky lights the rest.
+    fog = (sigma_s, sigma_a, g) fills the ambient region with a homogeneous medium."""
+    sb = SceneBuilder()
+    if fog is not None:
+        sb.region_medium[0] = sb._medium(A.INDEX_CONSTANT, (1.0,), absorption=sb.spectrum_constant(fog[1]),
+                                         scattering=sb.spectrum_constant(fog[0]), g=fog[2])
+    pmma = sb.medium_sellmeier(*PMMA, rel_air=False)
+    inside = sb.region(pmma)
+    h = np.zeros((n, n)) if heights is None else np.asarray(heights, np.float64).reshape(n, n)
+    hf, base_z = heightfield_panel(sb, n, h, size / 2, thickness, (0.0, 0.0, elevation), inside)
+    sb.sheet(2.0, 2.0, pose(), sb.diffuse(0.7))
+    light = sb.emission(sb.spectrum_constant(lamp))
+    sb.sheet(0.1, 0.15, pose(rotate_to((0, 0, 1), (1, 0, 0)), (-0.5, 0.0, 0.15)), sb.absorber(), emission=light)
+    if sky > 0:
+        sb.uniform_sky(sky)
+    sb.observer(width, height, (0.0, 0.0, 4.0), (0.0, 0.0, 0.0), up=(0, 1, 0), fov_y_deg=2.5)
+    return sb, {"heightfield": hf, "base_z": base_z, "n": n, "half": size / 2}
+
+
+def caustic_room(width=1920, height=1080, n_lon=1024, n_lat=512, panel_n=1024, heights=None, sigma_s=0.5,
+                 sigma_a=0.05, g=0.8, seed=3, panel_half=0.4, panel_thickness=0.05):
+    """The large-adjoint configuration: the closed Lambertian box of bvh_stress_room filled with a
+    homogeneous medium (scattering sigma_s, absorption sigma_a per metre, Henyey-Greenstein g), two
+    displaced-sphere props of n_lon x n_lat each (2^21 triangles at 1024 x 512), a PMMA panel whose
+    top face is a panel_n x panel_n heightfield (heights 0 unless given) standing in the camera's view,
+    and one area light on the ceiling; 1920 x 1080 pinhole camera."""
+    sb = SceneBuilder()
+    fog = sb._medium(A.INDEX_CONSTANT, (1.0,), absorption=sb.spectrum_constant(sigma_a),
+                     scattering=sb.spectrum_constant(sigma_s), g=g)
+    sb.region_medium[0] = fog
+    opaque = sb.medium_opaque()
+    for k, (c, r) in enumerate((((-1.2, 0.8, 0.9), 0.7), ((1.4, 1.2, 0.7), 0.55))):
+        verts, tris = uv_sphere(n_lon, n_lat, radius=r, seed=seed + k)
+        sb.mesh_body(verts, tris, opaque, sb.diffuse(0.6), xf=translate(*c))
+    pmma = sb.medium_sellmeier(*PMMA, rel_air=False)
+    inside = sb.region(pmma)
+    h = np.zeros((panel_n, panel_n)) if heights is None else np.asarray(heights, np.float64).reshape(panel_n, panel_n)
+    hf, base_z = heightfield_panel(sb, panel_n, h, panel_half, panel_thickness, (0.3, -0.6, 0.5), inside)
+    wall = sb.diffuse(0.7)
+    w = 3.0
+    sb.sheet(w, w, pose(), wall)
+    sb.sheet(w, w, pose(rotate_to((0, 0, 1), (0, 0, -1)), (0, 0, 4.0)), wall)
+    sb.sheet(2.0, w, pose(rotate_to((0, 0, 1), (1, 0, 0)), (-w, 0, 2.0)), wall)
+    sb.sheet(2.0, w, pose(rotate_to((0, 0, 1), (-1, 0, 0)), (w, 0, 2.0)), wall)
+    sb.sheet(w, 2.0, pose(rotate_to((0, 0, 1), (0, -1, 0)), (0, w, 2.0)), wall)
+    sb.sheet(w, 2.0, pose(rotate_to((0, 0, 1), (0, 1, 0)), (0, -w, 2.0)), wall)
+    lamp = sb.emission(sb.spectrum_constant(8.0))
+    sb.sheet(0.8, 0.8, pose(rotate_to((0, 0, 1), (0, 0, -1)), (0.0, 0.0, 3.98)), sb.absorber(), emission=lamp)
+    sb.observer(width, height, (0.3, -2.7, 1.6), (0.2, -0.2, 0.6), fov_y_deg=50.0)
+    return sb, {"heightfield": hf, "base_z": base_z, "n": panel_n, "half": panel_half}
+
+
 def furnace_sphere(rho, width=16, height=16):
     """Inside a closed diffuse sphere of albedo rho emitting Le = 1 inward: L = Le / (1 - rho)
     (tests/test_backends.cpp:349-378)."""
@@ -734,6 +806,56 @@ def touching_glass(width=48, height=36, thickness=0.2, gap=0.0):
     sb.sun((0.35, -0.3, 0.9), 2.0e4)
     sb.uniform_sky(0.3)
     sb.observer(width, height, (0.2, -2.8, 1.9), (0.0, -0.2, 0.25), fov_y_deg=40.0)
+    return sb
+
+
+GALLERY = ("cauchy", "tabulated", "gold", "rough_gold", "rough_glass")
+
+
+def materials_gallery(width=48, height=36, fog_box=True, sun=True, objects=GALLERY):
+    """The optics the configurations do not use, side by side on a Lambertian floor before a wall,
+    under a rectangular lamp (and the sun): spheres of Cauchy glass and of glass with a tabulated
+    index (both dispersive), a smooth and a rough gold conductor (tabulated n + ik), a rough N-BK7
+    dielectric (`objects` picks some; one alone fills the view). With fog_box, a box of scattering fog
+    bounded by null boundaries stands between the camera and the spheres, so that camera paths cross
+    null boundaries and next-event shadow rays walk through them (Tracer::transmittance,
+    src/owe/transport/transport.cpp:237-321)."""
+    sb = SceneBuilder()
+    sb.sheet(3.0, 3.0, pose(), sb.diffuse(0.6))
+    sb.sheet(3.0, 1.5, pose(rotate_to((0, 0, 1), (0, -1, 0)), (0.0, 1.2, 1.5)), sb.diffuse(0.5))
+    lam = np.linspace(380.0, 780.0, 11)
+    gold_n = sb.spectrum_tabulated([400, 500, 600, 700, 780], [1.47, 0.97, 0.25, 0.16, 0.17])
+    gold_k = sb.spectrum_tabulated([400, 500, 600, 700, 780], [1.95, 1.87, 2.98, 3.95, 4.70])
+    opaque = sb.medium_opaque()
+    places = {"cauchy": (-1.2, 0.2, 0.3), "tabulated": (-0.4, 0.2, 0.3), "gold": (0.4, 0.2, 0.3),
+              "rough_gold": (1.2, 0.2, 0.3), "rough_glass": (0.0, -0.5, 0.25)}
+    for name in objects:
+        c = places[name]
+        if name == "cauchy":
+            sb.sphere_body(0.3, c, sb._medium(A.INDEX_CAUCHY, (1.5046, 0.00420, 0.0)), sb.dielectric())
+        elif name == "tabulated":
+            table = sb.spectrum_tabulated(lam, 1.60 + 0.0135 / (lam / 1000) ** 2)
+            sb.sphere_body(0.3, c, sb._medium(A.INDEX_TABULATED, index_table=table), sb.dielectric())
+        elif name == "gold":
+            sb.sphere_body(0.3, c, opaque, sb.optics_(A.SURF_CONDUCTOR, cond_n=gold_n, cond_k=gold_k))
+        elif name == "rough_gold":
+            sb.sphere_body(0.3, c, opaque, sb.optics_(A.SURF_CONDUCTOR, roughness=0.25, cond_n=gold_n, cond_k=gold_k))
+        else:
+            sb.sphere_body(0.25, c, sb.medium_sellmeier(*NBK7, rel_air=True), sb.dielectric(roughness=0.2))
+    if fog_box:
+        fog = sb._medium(A.INDEX_CONSTANT, (1.0,), absorption=sb.spectrum_constant(0.2),
+                         scattering=sb.spectrum_constant(1.5), g=0.3)
+        v, t = box_mesh((-1.8, -1.6, 0.05), (1.8, -1.0, 1.1))
+        sb.boundary(A.SHAPE_MESH, [], pose(), 0, sb.region(fog), sb.optics_(A.SURF_NULL), -1, sb.mesh(v, t))
+    lamp = sb.emission(sb.spectrum_constant(6.0))
+    sb.sheet(0.6, 0.4, pose(rotate_to((0, 0, 1), (0, 0, -1)), (0.3, -0.3, 2.6)), sb.absorber(), emission=lamp)
+    if sun:
+        sb.sun((-0.4, -0.5, 0.75), 1.0e4)
+    if len(objects) == 1:
+        c = places[objects[0]]
+        sb.observer(width, height, (c[0], c[1] - 1.6, c[2] + 0.5), c, fov_y_deg=24.0)
+    else:
+        sb.observer(width, height, (0.0, -3.6, 1.3), (0.0, 0.0, 0.35), fov_y_deg=42.0)
     return sb
 
 
@@ -924,18 +1046,24 @@ def slab_rest(nx, ny, half_x, half_y, top_z_edges):
     watertight. top_z_edges(i, j) gives the top z at edge vertex (i, j). Faces point outward."""
     x = np.linspace(-half_x, half_x, nx)
     y = np.linspace(-half_y, half_y, ny)
-    verts, tris = [], []
+    # bottom as a grid with the same edge vertices (no T-junctions with the sides), facing -z: one
+    # quad (x_i, y_j), (x_i, y_j+1), (x_i+1, y_j+1), (x_i+1, y_j) per cell, four vertices each
+    I, J = np.meshgrid(np.arange(nx - 1), np.arange(ny - 1))
+    I, J = I.ravel(), J.ravel()
+    zeros = np.zeros(len(I))
+    q = np.stack([np.stack([x[I], y[J], zeros], 1), np.stack([x[I], y[J + 1], zeros], 1),
+                  np.stack([x[I + 1], y[J + 1], zeros], 1), np.stack([x[I + 1], y[J], zeros], 1)], 1)
+    verts = [q.reshape(-1, 3)]
+    base = 4 * np.arange(len(I), dtype=np.int64)
+    tris = [np.stack([np.stack([base, base + 1, base + 2], 1), np.stack([base, base + 2, base + 3], 1)], 1).reshape(-1, 3)]
+    side_v, side_t = [], []
 
     def quad(a, b, c, d):  # counter-clockwise seen from outside
-        base = len(verts)
-        verts.extend([a, b, c, d])
-        tris.append((base, base + 1, base + 2))
-        tris.append((base, base + 2, base + 3))
+        k = len(side_v)
+        side_v.extend([a, b, c, d])
+        side_t.append((k, k + 1, k + 2))
+        side_t.append((k, k + 2, k + 3))
 
-    # bottom as a grid with the same edge vertices (no T-junctions with the sides), facing -z
-    for j in range(ny - 1):
-        for i in range(nx - 1):
-            quad((x[i], y[j], 0.0), (x[i], y[j + 1], 0.0), (x[i + 1], y[j + 1], 0.0), (x[i + 1], y[j], 0.0))
     for i in range(nx - 1):  # side y = -half (normal -y) and y = +half (normal +y)
         quad((x[i], y[0], 0.0), (x[i + 1], y[0], 0.0), (x[i + 1], y[0], top_z_edges(i + 1, 0)), (x[i], y[0], top_z_edges(i, 0)))
         quad((x[i + 1], y[-1], 0.0), (x[i], y[-1], 0.0), (x[i], y[-1], top_z_edges(i, ny - 1)),
@@ -944,7 +1072,10 @@ def slab_rest(nx, ny, half_x, half_y, top_z_edges):
         quad((x[0], y[j + 1], 0.0), (x[0], y[j], 0.0), (x[0], y[j], top_z_edges(0, j)), (x[0], y[j + 1], top_z_edges(0, j + 1)))
         quad((x[-1], y[j], 0.0), (x[-1], y[j + 1], 0.0), (x[-1], y[j + 1], top_z_edges(nx - 1, j + 1)),
              (x[-1], y[j], top_z_edges(nx - 1, j)))
-    return np.array(verts), np.array(tris, np.uint32)
+    off = len(verts[0])
+    verts.append(np.array(side_v, float))
+    tris.append(np.array(side_t, np.int64) + off)
+    return np.concatenate(verts), np.concatenate(tris).astype(np.uint32)
 
 
 def caustic_slab_scene(n=256, heights=None, wall_bins=512, wall_half=0.075, size=0.1, thickness=0.01,

@@ -44,9 +44,9 @@ def test_c2_ten_million_rays_match_world_intersect():
              "within_1e-6": float(np.mean(rel <= 1e-6)), "rel_max": float(rel.max())}
     save_artifact("c2_ray_cast_stats", **{k: np.array(v) for k, v in stats.items()})
     assert ties.sum() <= 1e-4 * n, stats
-    # FP32 geometry: the distance agrees to 1e-6 for all but grazing hits
-    assert stats["within_1e-6"] >= 0.999, stats
-    assert stats["rel_max"] < 1e-3, stats
+    # the traversal finds the triangle in FP32; the distance is then recomputed from the FP64
+    # vertices: every hit on the reference's own triangle agrees to 1e-6 relative
+    assert stats["rel_max"] <= 1e-6, stats
 
 
 def test_c1_film_at_4096_spp_matches_the_reference_streams():

@@ -19,9 +19,9 @@ from oracle_ref import ReferenceEngine, block_z_test
 
 pytestmark = pytest.mark.gpu
 
-# Mixed precision: FP32 triangles and directions, FP64 origins. A distance's relative error is a few
-# FP32 ulps of the coordinates over the distance, amplified by 1/cos at grazing incidence; the bound
-# holds for 99.9 % of the hits, and every hit stays within 1e-3.
+# Mixed precision: FP32 triangles and directions, FP64 origins; a triangle hit's distance is
+# recomputed from the FP64 vertices, an analytic one refined in FP64. Every hit's distance agrees
+# with World::intersect's to this relative tolerance.
 T_REL_TOL = 1e-6
 
 
@@ -54,8 +54,8 @@ def test_cast_rays_match_world_intersect_on_displaced_sphere():
     assert frac < 1e-3, f"{frac:.2e} of rays hit another primitive"
     hit = same & (rb != A.KNONE)
     rel = np.abs(gt[hit] - rt[hit]) / np.maximum(rt[hit], 1e-9)
-    assert np.quantile(rel, 0.999) < 10 * T_REL_TOL, f"99.9 % relative t error {np.quantile(rel, 0.999):.2e}"
-    assert np.median(rel) < T_REL_TOL and np.max(rel) < 1e-3
+    # distances recomputed from the FP64 vertices once the FP32 traversal has found the triangle
+    assert np.max(rel) <= T_REL_TOL, f"max relative t error {np.max(rel):.2e}"
 
 
 def test_cast_rays_hit_analytic_shapes_like_the_reference():
@@ -101,9 +101,10 @@ def _glass_settings(seed):
     return A.make_settings(seed=seed, max_depth=16, rr_depth=4, wavelength_mode=A.WAVELENGTHS_UNIFORM1)
 
 
-def test_glass_sphere_agrees_with_reference_statistically():
+@pytest.mark.parametrize("precision", [A.PRECISION_MIXED, A.PRECISION_FP64, A.PRECISION_FP32])
+def test_glass_sphere_agrees_with_reference_statistically(precision):
     """The plain-method workload at 48 x 48: block z-test over independent seeds against the
-    reference's FP64 transport (compareRenderers)."""
+    reference's FP64 transport (compareRenderers), for each precision instantiation."""
     desc = scenes.glass_sphere_on_floor(48, 48).desc()
     ref = ReferenceEngine(desc)
     runs_ref, runs_gpu = [], []
@@ -111,31 +112,38 @@ def test_glass_sphere_agrees_with_reference_statistically():
         for k in range(8):
             img, st = ref.render(_glass_settings(1000 + k), 64)
             runs_ref.append(img)
-            c.set_settings(_glass_settings(2000 + k))
+            s = _glass_settings(2000 + k)
+            s.precision = precision
+            c.set_settings(s)
             c.reset_film()
             c.run_pass(64)
             runs_gpu.append(c.resolve()[0])
             assert st["leaks"] == 0
         assert c.stats()["device_faults"] == 0
-    save_artifact("glass_sphere_runs", ref=np.array(runs_ref), gpu=np.array(runs_gpu))
+    save_artifact(f"glass_sphere_runs_{precision}", ref=np.array(runs_ref), gpu=np.array(runs_gpu))
     ok, rep = block_z_test(runs_ref, runs_gpu)
     assert ok, rep
 
 
-def test_one_sample_paths_follow_the_reference_paths():
+@pytest.mark.parametrize("precision,agree", [(A.PRECISION_MIXED, 0.97), (A.PRECISION_FP64, 0.995),
+                                             (A.PRECISION_FP32, 0.9)])
+def test_one_sample_paths_follow_the_reference_paths(precision, agree):
     """With one-sample passes both draw from the stream (hashCombine(seed, pixel), pass): most
-    device paths make every decision the CPU path makes and return the same value."""
+    device paths make every decision the CPU path makes and return the same value. The all-FP64
+    instantiation follows nearly every path; plain FP32 (origins rounded after every event, roots
+    and distances in FP32) turns more decisions the other way."""
     desc = scenes.glass_sphere_on_floor(64, 64).desc()
     ref = ReferenceEngine(desc)
     s = _glass_settings(5)
+    s.precision = precision
     img_ref, _ = ref.render(s, 1, passes=1)
     with _ctx(desc, s) as c:
         c.run_pass(1)
         img_gpu = c.resolve()[0]
-    save_artifact("one_sample_paths", ref=img_ref, gpu=img_gpu)
+    save_artifact(f"one_sample_paths_{precision}", ref=img_ref, gpu=img_gpu)
     a, b = img_ref[:, :, 1].ravel(), img_gpu[:, :, 1].ravel()
     close = np.abs(a - b) <= 1e-4 * np.maximum(np.abs(a), 1e-3)
-    assert close.mean() > 0.97, f"only {close.mean():.3f} of paths agree"
+    assert close.mean() > agree, f"only {close.mean():.3f} of paths agree"
 
 
 def test_hero_wavelength_render_agrees_with_reference_backend():
