@@ -39,6 +39,10 @@ METRIC = "spectral paths/s"
 WORKLOAD = "bvh_stress_room: 2^20-tri displaced UV sphere in a Lambertian box, 1 area light, 1920x1080, hero-4 spectral, depth 12"
 NODE_BYTES, PRIM_BYTES = 80, 48
 RAY_STATE_BYTES = 4 + 64 + 24  # queue index, the path's ray record, the hit record written
+# Arithmetic per visit, counted from the traversal's source: a wide node tests its 8 child boxes
+# (per box 6 FMA-form plane distances = 12 flops, 6 min/max = 6, entry/exit compares = 6: 24), a
+# triangle the shear-space watertight test and the plane distance (about 40).
+NODE_FLOPS, PRIM_FLOPS = 8 * 24, 40
 
 
 def peaks():
@@ -191,35 +195,65 @@ def run_reference(args):
     return 0
 
 
-def precision_study(device, width=480, height=270, spp=16, ref_spp=256):
-    """The metric's RMSE half: the same workload at a reduced film, FP64 kernels at ref_spp as the
-    oracle image, then the mixed and the all-FP64 instantiations at spp on the same sample streams.
-    Returns their RMSEs against the oracle (over pixels and XYZ), their paths/s, and the speed-up
-    of mixed over FP64 at that (equal) RMSE."""
-    import owe_cuda
-    desc = scenes.bvh_stress_room(width, height).desc()
+def rel_mse(img, ref):
+    """The reference's relative MSE (docs/BENCHMARKS.md): mean((img - ref)^2 / (ref^2 + 0.01 mean(ref)^2))
+    over pixels and XYZ channels."""
+    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 0.01 * np.mean(ref) ** 2)))
 
-    def render(precision, seed, n):
+
+def precision_study(device, ref_rows=16, ref_spp=1024, spp=16, bias_spp=256):
+    """The metric's RMSE half on the bench's own workload at 1920 x 1080: each precision
+    instantiation (FP32 + selective FP64, plain FP32, all FP64) against the reference engine's FP64
+    CPU transport (oracle/_ref), which renders ref_rows rows through the middle of the frame at
+    ref_spp samples per pixel (another seed). Per mode: paths/s of a one-sample pass; relMSE of a
+    `spp` render over the band; seconds to a relMSE of 1e-3 (seconds per sample x spp x relMSE /
+    1e-3, as relMSE falls as 1 / spp for an unbiased estimator); the bias (mean signed error over the
+    band's pixels at bias_spp, relative to the reference's mean, with its standard error); the
+    transport statistics. speedup_at_equal_relmse: FP64's seconds to that relMSE over the mode's."""
+    import owe_cuda
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_ref import ReferenceEngine  # the FP64 oracle image, not a timed leg
+    desc = scenes.bvh_stress_room(WIDTH, HEIGHT).desc()
+    r0 = HEIGHT // 2 - ref_rows // 2
+    t0 = time.perf_counter()
+    ref_img, ref_st = ReferenceEngine(desc).render(
+        A.make_settings(seed=1000, max_depth=MAX_DEPTH, rr_depth=RR_DEPTH, wavelength_mode=A.WAVELENGTHS_HERO4), 1,
+        passes=ref_spp, pixel_begin=r0 * WIDTH, pixel_end=(r0 + ref_rows) * WIDTH)
+    ref_band = ref_img[r0:r0 + ref_rows]
+    out = {"film": f"{WIDTH}x{HEIGHT}", "oracle": f"reference engine FP64 CPU transport, rows {r0}-{r0 + ref_rows - 1}, "
+           f"{ref_spp} spp, other seed ({time.perf_counter() - t0:.0f} s)", "spp": spp, "bias_spp": bias_spp,
+           "target_relmse": 1e-3}
+    for name, prec in (("mixed", A.PRECISION_MIXED), ("fp32", A.PRECISION_FP32), ("fp64", A.PRECISION_FP64)):
         with owe_cuda.Context(device) as c:
             c.upload(desc)
             c.build_bvh()
-            c.set_settings(A.make_settings(seed=seed, max_depth=MAX_DEPTH, rr_depth=RR_DEPTH,
-                                           wavelength_mode=A.WAVELENGTHS_HERO4, precision=precision))
-            c.run_pass(1)  # warm-up: the FP64 primitives, the path buffers
-            c.reset_film()
-            seconds = 0.0
-            for _ in range(n):
+            c.set_settings(A.make_settings(seed=7, max_depth=MAX_DEPTH, rr_depth=RR_DEPTH,
+                                           wavelength_mode=A.WAVELENGTHS_HERO4, precision=prec))
+            c.run_pass(1)  # warm-up: the mode's primitives and path buffers
+            secs = []
+            for _ in range(3):
                 c.run_pass(1)
-                seconds += c.last_pass_timing()[0]
-            return c.resolve()[0], width * height * n / seconds
-
-    oracle, _ = render(A.PRECISION_FP64, 1000, ref_spp)
-    out = {"film": f"{width}x{height}", "spp": spp, "oracle": f"fp64 kernels, {ref_spp} spp, other seed"}
-    for name, prec in (("mixed", A.PRECISION_MIXED), ("fp64", A.PRECISION_FP64)):
-        img, rate = render(prec, 7, spp)
-        out[name] = {"rmse": float(np.sqrt(np.mean((img - oracle) ** 2))), "paths_per_s": rate}
-    out["rmse_ratio_mixed_over_fp64"] = out["mixed"]["rmse"] / out["fp64"]["rmse"]
-    out["speedup_at_equal_rmse"] = out["mixed"]["paths_per_s"] / out["fp64"]["paths_per_s"]
+                secs.append(c.last_pass_timing()[0])
+            sec_per_spp = min(secs)
+            c.reset_film()
+            c.run_pass(spp)
+            img = c.resolve()[0][r0:r0 + ref_rows]
+            rm = rel_mse(img, ref_band)
+            c.reset_film()
+            c.set_pass_index(1 << 16)
+            c.run_pass(bias_spp)
+            img_b = c.resolve()[0][r0:r0 + ref_rows]
+            st = c.stats()
+        diff = (img_b - ref_band)[..., 1].ravel()
+        mean_ref = float(ref_band[..., 1].mean())
+        out[name] = {"paths_per_s": WIDTH * HEIGHT / sec_per_spp, "relmse": rm,
+                     "seconds_to_target": sec_per_spp * spp * rm / 1e-3,
+                     "bias": float(diff.mean()) / mean_ref, "bias_se": float(diff.std() / np.sqrt(diff.size)) / mean_ref,
+                     "inconsistencies_per_path": st["inconsistencies"] / max(1, st["paths"]),
+                     "leaks_per_path": st["leaks"] / max(1, st["paths"]), "faults": st["device_faults"]}
+    for name in ("mixed", "fp32"):
+        out[name]["speedup_at_equal_relmse"] = out["fp64"]["seconds_to_target"] / out[name]["seconds_to_target"]
+    out["reference_leaks"] = ref_st["leaks"]
     return out
 
 
@@ -516,6 +550,22 @@ def run_cuda(args):
         except (OSError, KeyError, ValueError):
             pass
         clk = clocks.summary()
+        # the device's FP32 FMA rate and L2 read bandwidth, probed after the timed region
+        probe = ctx.device_peaks()
+        fp32_peak = probe["fp32_flops"] / 1e12
+        l2_peak = probe["l2_read_bytes_per_s"] / 1e9
+        flops_per_launch = (nodes * NODE_FLOPS + prims * PRIM_FLOPS) / max(1, launches_prof)
+        fp32_achieved = flops_per_launch / per_launch_s / 1e12
+        issue = None
+        try:
+            with open(os.path.join(ROOT, "profiles", "kIntersect_issue.json")) as f:
+                issue = json.load(f)["issue_active"]
+        except (OSError, KeyError, ValueError):
+            pass
+        terms = {"hbm": achieved / hbm, "l2": achieved / l2_peak, "fp32": fp32_achieved / fp32_peak}
+        if issue is not None:
+            terms["issue"] = issue
+        bound = max(terms, key=terms.get)
         cpu_rate, cores, sample = (None, None, "skipped")
         if INTEGRATOR == "light":
             sample = "none: the reference has no CPU light integrator"
@@ -545,6 +595,14 @@ def run_cuda(args):
             "shadow_share": sum(shadow) / sum(times),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_kind": peak_kind, "traffic": traffic, "kernel": "kIntersect",
+                         "binding_term": bound,
+                         "terms": {k: round(v, 4) for k, v in terms.items()},
+                         "term_sources": {"hbm": f"algorithmic bytes / launch time vs {peak_kind} copy bandwidth",
+                                          "l2": f"the same bytes vs the probed L2 read bandwidth ({l2_peak:.0f} GB/s)",
+                                          "fp32": f"{NODE_FLOPS} flops per node visit + {PRIM_FLOPS} per primitive test "
+                                                  f"vs the probed FP32 FMA rate ({fp32_peak:.1f} TFLOP/s)",
+                                          "issue": "ncu issue-active fraction of the kernel (profiles/kIntersect_issue.json)"},
+                         "fp32_tflops": fp32_achieved, "fp64_peak_tflops": probe["fp64_flops"] / 1e12,
                          "bytes_per_launch": per_launch_bytes,
                          "per_query": {"nodes": nodes / max(1, q), "prims": prims / max(1, q)},
                          "queries_per_pass": q, "launches_per_pass": launches_prof},

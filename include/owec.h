@@ -491,6 +491,14 @@ typedef struct owec_adjoint_stats {
 int owec_path_adjoint(owec_ctx* ctx, uint64_t first_pass, int spp, int flags, const double* g, double* dheights,
                       double* replay_xyz, owec_adjoint_stats* stats);
 
+/* Throughput probes of the opened device, for rooflines that no driver-measured peak covers: out[0] the
+ * FP32 and out[1] the FP64 fused multiply-add rate (flop/s, eight independent chains per thread on
+ * every multiprocessor), out[2] the L2 read bandwidth (bytes/s, 128-bit loads that bypass L1 over a
+ * buffer a quarter of the L2's size, read repeatedly). Each is one CUDA-event-timed kernel after a
+ * warm-up; the call allocates a scratch buffer of a quarter of the L2 for the last. No counterpart
+ * in the reference. */
+int owec_device_peaks(owec_ctx* ctx, double out[3]);
+
 /* Device seconds of the last owec_walk and owec_walk_adjoint calls. */
 int owec_walk_timing(owec_ctx* ctx, double out[2]);
 

@@ -18,6 +18,7 @@
 #include "particle.hpp"
 #include "spectral.cuh"
 #include "path_adjoint.hpp"
+#include "peaks.hpp"
 #include "walk.hpp"
 #include "wavefront.hpp"
 
@@ -1322,10 +1323,11 @@ void runParticles(owec_ctx& c, int spp) {
 // each path at its first surface event on the heightfield, leaving its state there (a checkpoint);
 // the derivative replay then resumes only those paths. Paths that never meet the heightfield carry
 // no derivative and so cost one forward pass's work and nothing more.
-// Returns the number of camera paths the first phase generated.
+// Returns the number of camera paths the first phase generated; freeDuring receives the device's free
+// memory while the phases' buffers are still held.
 template <int M>
 uint64_t runAdjointCheckpointed(owec_ctx& c, PassParams pp, uint64_t firstPass, int spp, const PathAdjointTargets& t,
-                                bool fixedDecisions) {
+                                bool fixedDecisions, size_t& freeDuring) {
     using R = ModeR<M>;
     const uint32_t nPix = pp.nPixels;
     const uint32_t target = std::max<uint32_t>(nPix, 1u << 21);
@@ -1360,6 +1362,8 @@ uint64_t runAdjointCheckpointed(owec_ctx& c, PassParams pp, uint64_t firstPass, 
     StatCounters hs{};
     OWEC_CUDA(cudaMemcpyAsync(&hs, st.get(), sizeof(StatCounters), cudaMemcpyDeviceToHost, c.stream));
     OWEC_CUDA(cudaStreamSynchronize(c.stream));
+    size_t total = 0;
+    OWEC_CUDA(cudaMemGetInfo(&freeDuring, &total));
     return hs.paths;
 }
 
@@ -1962,15 +1966,15 @@ int owec_path_adjoint(owec_ctx* ctx, uint64_t first_pass, int spp, int flags, co
                 done += int(S);
             }
         } else if (ctx->settings.precision == OWEC_PRECISION_FP64) {
-            cameraPaths = runAdjointCheckpointed<OWEC_PRECISION_FP64>(*ctx, pp, first_pass, spp, t, fixed);
+            cameraPaths = runAdjointCheckpointed<OWEC_PRECISION_FP64>(*ctx, pp, first_pass, spp, t, fixed, freeDuring);
         } else if (ctx->settings.precision == OWEC_PRECISION_FP32) {
-            cameraPaths = runAdjointCheckpointed<OWEC_PRECISION_FP32>(*ctx, pp, first_pass, spp, t, fixed);
+            cameraPaths = runAdjointCheckpointed<OWEC_PRECISION_FP32>(*ctx, pp, first_pass, spp, t, fixed, freeDuring);
         } else {
-            cameraPaths = runAdjointCheckpointed<OWEC_PRECISION_MIXED>(*ctx, pp, first_pass, spp, t, fixed);
+            cameraPaths = runAdjointCheckpointed<OWEC_PRECISION_MIXED>(*ctx, pp, first_pass, spp, t, fixed, freeDuring);
         }
         OWEC_CUDA(cudaEventRecord(ctx->passStop, ctx->stream));
         OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
-        OWEC_CUDA(cudaMemGetInfo(&freeDuring, &total));  // the buffers and the kernels' stacks, still held
+        if (replay_xyz) OWEC_CUDA(cudaMemGetInfo(&freeDuring, &total));  // the buffers and the kernel's stacks, held
         std::vector<double> h(nh);
         unsigned long long counts[4];
         OWEC_CUDA(cudaMemcpyAsync(h.data(), dDH.get(), nh * 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1990,6 +1994,16 @@ int owec_path_adjoint(owec_ctx* ctx, uint64_t first_pass, int spp, int flags, co
             stats->seconds = ms * 1e-3;
             stats->device_bytes = freeBefore > freeDuring ? uint64_t(freeBefore - freeDuring) : 0;
         }
+    });
+}
+
+int owec_device_peaks(owec_ctx* ctx, double out[3]) {
+    return guarded([&] {
+        require(ctx && out, "owec_device_peaks: null argument");
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        int l2 = 0;
+        OWEC_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, ctx->device));
+        measurePeaks(ctx->numSMs, size_t(l2), ctx->stream, out);
     });
 }
 

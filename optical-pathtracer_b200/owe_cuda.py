@@ -216,6 +216,13 @@ class Context:
             return out
         return out, st.as_dict(), (rep.reshape(self.height, self.width, 3) if replay else None)
 
+    def device_peaks(self):
+        """{"fp32_flops", "fp64_flops", "l2_read_bytes_per_s"}: the device's FMA rates and L2 read
+        bandwidth, measured by owec_device_peaks."""
+        out = (ctypes.c_double * 3)()
+        _check(self.lib, self.lib.owec_device_peaks(self.handle, out), "owec_device_peaks")
+        return {"fp32_flops": out[0], "fp64_flops": out[1], "l2_read_bytes_per_s": out[2]}
+
     def walk_timing(self):
         out = (ctypes.c_double * 2)()
         _check(self.lib, self.lib.owec_walk_timing(self.handle, out), "owec_walk_timing")

@@ -218,6 +218,7 @@ def load_library(path=LIB_PATH):
         "owec_walk_adjoint_noalloc": ([P, ctypes.POINTER(WalkDesc), ctypes.c_uint64, ctypes.c_uint64, c_double_p,
                                        c_double_p], ctypes.c_int),
         "owec_walk_timing": ([P, c_double_p], ctypes.c_int),
+        "owec_device_peaks": ([P, c_double_p], ctypes.c_int),
         "owec_path_adjoint": ([P, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, c_double_p, c_double_p, c_double_p,
                                ctypes.POINTER(AdjointStats)], ctypes.c_int),
     }

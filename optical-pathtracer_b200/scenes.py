@@ -637,6 +637,27 @@ def caustic_room(width=1920, height=1080, n_lon=1024, n_lat=512, panel_n=1024, h
     return sb, {"heightfield": hf, "base_z": base_z, "n": panel_n, "half": panel_half}
 
 
+def reflected_moonlight(width=16, height=16):
+    """The reference's conformance check of light reflected by a distant body (tests/test_backends.cpp:
+    69-97): a white two-sided Lambertian floor lit only by a full-phase Lambertian moon (albedo 0.3,
+    radius 1e6 m, 1e9 m overhead) under a sun shining up from below (radiance 1e5), the floor's
+    scattering guided toward the moon's disk (Scene::indirectGuide: half the samples, radius x 1.001);
+    a narrow pinhole looks at the floor. Expected luminance (2/3) 0.3 E_sun (1e6 / 1e9)^2 / pi."""
+    sb = SceneBuilder()
+    white = sb.diffuse(1.0)
+    sb.aim_guide(white, (0.0, 0.0, 1e9), (0.0, 0.0, -1.0), 1e6 * 1.001, 0.5)
+    sb.sheet(4.0, 4.0, pose(), white, disk=True)
+    sb.sphere_body(1e6, (0.0, 0.0, 1e9), sb.medium_opaque(), sb.diffuse(0.3))
+    sb.sun((0.0, 0.0, -1.0), 1e5)
+    sb.observer(width, height, (0.0, -1.0, 1.0), (0.0, 0.0, 0.0), fov_y_deg=0.01)
+    return sb
+
+
+def reflected_moonlight_expected(angular_radius=math.radians(0.2665)):
+    solar = 1e5 * math.pi * math.sin(angular_radius) ** 2
+    return (2.0 / 3.0) * 0.3 * solar * (1e6 / 1e9) ** 2 / math.pi
+
+
 def furnace_sphere(rho, width=16, height=16):
     """Inside a closed diffuse sphere of albedo rho emitting Le = 1 inward: L = Le / (1 - rho)
     (tests/test_backends.cpp:349-378)."""

@@ -195,3 +195,20 @@ def test_switching_precision_in_one_context_matches_a_fresh_context(integrator):
         c.run_pass(700)
         fresh = c.resolve()[0]
     assert np.array_equal(switched, fresh)
+
+
+@pytest.mark.parametrize("precision", [A.PRECISION_MIXED, A.PRECISION_FP64])
+def test_reflected_moonlight_matches_the_analytic_answer(precision):
+    """The reference's conformance check of a distant reflector (tests/test_backends.cpp:69-97): a
+    floor lit only by a full-phase Lambertian moon 1e9 m away, within 1.5 % of (2/3) rho E_sun
+    (R / d)^2 / pi, with no inconsistent regions and no leaks."""
+    desc = scenes.reflected_moonlight().desc()
+    s = A.make_settings(seed=1, precision=precision)
+    with _ctx(desc, s) as c:
+        c.run_pass(2048)
+        img = c.resolve()[0]
+        st = c.stats()
+    expected = scenes.reflected_moonlight_expected()
+    measured = float(img[:, :, 1].mean())
+    assert abs(measured / expected - 1) < 0.015, (measured, expected, st)
+    assert st["inconsistencies"] == 0 and st["leaks"] == 0 and st["device_faults"] == 0, st
