@@ -265,13 +265,16 @@ OWEC_HD int classicCrossings(const DBoundary& b, const V3<Rr>& o, const V3<Rr>& 
     const double* P = b.params;
     switch (b.shape) {
         case OWEC_SHAPE_SPHERE: {
+            // Sphere roots in the refinement's precision: a ray leaving a large sphere (a moon, a
+            // planet, a dome) has |o| near R, where FP32 loses c = |o|^2 - R^2 entirely, and a root
+            // the refinement cannot pull back within its window would survive as a false crossing.
             const Rr Rad = Rr(P[0]);
-            R t0, t1;
-            if (!sphereRoots(V3<R>(o), V3<R>(d), R(P[0]), t0, t1)) return 0;
-            const R ts[2] = {t0, t1};
+            Rr t0, t1;
+            if (!sphereRoots(o, d, Rad, t0, t1)) return 0;
+            const Rr ts[2] = {t0, t1};
             for (int i = 0; i < 2; ++i) {
                 Rr tr;
-                if (!refinedRootIn<R, Rr>(kQuadSphere, Rad * Rad, Rr(0), o, d, Rr(ts[i]), tmin, tmax, tr)) continue;
+                if (!refinedRootIn<Rr, Rr>(kQuadSphere, Rad * Rad, Rr(0), o, d, ts[i], tmin, tmax, tr)) continue;
                 const V3<Rr> p = o + d * tr;
                 out.add({tr, p, normalize(p / Rad)});
             }
@@ -632,20 +635,20 @@ OWEC_HD int fullCrossings(const DBoundary& b, const double* data, const V3<Rr>& 
     out.n = 0;
     const double* P = b.params;
     switch (b.shape) {
-        case OWEC_SHAPE_SPHERE: {
+        case OWEC_SHAPE_SPHERE: {  // roots in the refinement's precision, as classicCrossings
             const Rr Rad = Rr(P[0]);
-            R t0, t1;
-            if (!sphereRoots(V3<R>(o), V3<R>(d), R(P[0]), t0, t1)) return 0;
-            quadricHits<R, Rr>(kQuadSphere, Rad * Rad, Rr(0), Rr(0), o, d, t0, t1, tmin, tmax,
-                               [](const V3<Rr>&) { return true; }, [&](const V3<Rr>& p) { return normalize(p / Rad); },
-                               out);
+            Rr t0, t1;
+            if (!sphereRoots(o, d, Rad, t0, t1)) return 0;
+            quadricHits<Rr, Rr>(kQuadSphere, Rad * Rad, Rr(0), Rr(0), o, d, t0, t1, tmin, tmax,
+                                [](const V3<Rr>&) { return true; }, [&](const V3<Rr>& p) { return normalize(p / Rad); },
+                                out);
             break;
         }
         case OWEC_SHAPE_DOME: {
             const Rr Rad = Rr(P[0]), az = Rr(P[1]), w = Rr(P[2]), top = Rr(P[3]);
-            R t0, t1;
-            if (!sphereRoots(V3<R>(o), V3<R>(d), R(P[0]), t0, t1)) return 0;
-            quadricHits<R, Rr>(kQuadSphere, Rad * Rad, Rr(0), Rr(0), o, d, t0, t1, tmin, tmax,
+            Rr t0, t1;
+            if (!sphereRoots(o, d, Rad, t0, t1)) return 0;
+            quadricHits<Rr, Rr>(kQuadSphere, Rad * Rad, Rr(0), Rr(0), o, d, t0, t1, tmin, tmax,
                                [&](const V3<Rr>& p) { return domeSolid(Rad, az, w, top, p); },
                                [](const V3<Rr>& p) { return normalize(p); }, out);
             break;

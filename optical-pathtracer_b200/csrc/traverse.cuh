@@ -433,12 +433,9 @@ struct Traversal {
     }
 
     // How far beyond the closest crossing the contact-resolving traversal still looks: the tie
-    // window relative to the distance plus the anchor's own error (coincident faces through the
-    // anchor lie at distance zero, where a relative window closes), widened by the closest
-    // crossing's grazing incidence (coincident faces' distances differ by their offsets' rounding
-    // over the cosine). NearestCrossing::offer's tie, |t - best| <= the candidates' error,
-    // src/owe/scene/world.cpp:527.
-    __device__ __forceinline__ T tieSpan(T c) const { return (best * tieWindow<T>() + q.errN) / fmax(c, T(1e-3)); }
+    // window, widened by the closest crossing's grazing incidence (coincident faces' distances differ
+    // by their offsets' rounding over the cosine).
+    __device__ __forceinline__ T tieSpan(T c) const { return best * tieWindow<T>() / fmax(c, T(1e-3)); }
     __device__ __forceinline__ T tieLimit() const { return best + tieSpan(bestCos); }
 
     // Whether boundary b's crossing at t, met from its front side when `front` at incidence |cos| c,
@@ -500,26 +497,22 @@ struct Traversal {
                   t < limit))
                 return false;
             if (!acceptCrossing<T, Full>(sc, q, b, prim, true, t, n)) return false;
-            // a crossing just behind the anchor is offered at distance zero, as the reference offers
-            // max(0, t) (World::intersect, src/owe/scene/world.cpp:564)
-            const T tc = Full ? fmax(t, T(0)) : t;
             if constexpr (Full) {
                 const T c = fabs(dn) / sqrt(dot(n, n));
-                if (!winsContact(sc, b, tc, dn < T(0), c, flags)) return false;
+                if (!winsContact(sc, b, t, dn < T(0), c, flags)) return false;
                 bestCos = c;
             }
-            best = tc;
+            best = t;
             hit.t = double(t);
             hit.prim = prim;
         } else {
             const AnalyticResult<Rr> ar = analyticHit<T, R, Rr, Full>(sc.self, b, q.od, q.d, limit, q.depB, q.region, q.errN);
             if (!ar.ok) return false;
-            const T tc = Full ? fmax(T(ar.t), T(0)) : T(ar.t);
             if constexpr (Full) {
-                if (!winsContact(sc, b, tc, ar.front, T(ar.cosAbs), flags)) return false;
+                if (!winsContact(sc, b, T(ar.t), ar.front, T(ar.cosAbs), flags)) return false;
                 bestCos = T(ar.cosAbs);
             }
-            best = tc;
+            best = T(ar.t);
             hit.t = double(ar.t);
             hit.prim = 0;
         }

@@ -83,7 +83,7 @@ def test_gallery_agrees_with_reference_statistically(fog_box, precision):
     assert st["device_faults"] == 0
     # plain FP32 rounds every origin to FP32, which now and then puts a path on the wrong side of a
     # sphere: a leak; the product's modes must have none
-    assert st["leaks"] <= (1e-5 * st["paths"] if precision == A.PRECISION_FP32 else 0), st
+    assert st["leaks"] <= (1e-4 * st["paths"] if precision == A.PRECISION_FP32 else 0), st
     save_artifact(f"gallery_runs_{fog_box}_{precision}", ref=np.array(runs_ref), gpu=np.array(runs_gpu))
     ok, rep = block_z_test(runs_ref, runs_gpu)
     assert ok, rep
