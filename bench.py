@@ -317,6 +317,7 @@ def c5_study(device, spp_timing=16, steps=0, spp_step=4, width=1920, height=1080
         g[..., 1] = 1.0 / img.size  # the gradient of the image's mean luminance
         _, st, _ = c.path_adjoint(100, spp_timing, g, with_stats=True)
         out.update({"forward_s": fwd, "adjoint_s": st["seconds"], "adjoint_over_forward": st["seconds"] / fwd,
+                    "adjoint_replay_s": st["replay_seconds"],
                     "forward_paths_per_s": width * height * spp_timing / fwd,
                     "paths_met_heightfield": st["heightfield"] / max(1, st["paths"]),
                     "dropped_of_those": st["dropped"] / max(1, st["heightfield"]), "faults": st["faults"],
@@ -527,10 +528,10 @@ def run_cuda(args):
     d2h = n_pix * 3 * 8  # the resolved XYZ image (Renderer::resolve), FP64
     h2d = __import__("ctypes").sizeof(A.Settings)  # the settings record uploaded every step
 
-    # the film over NCCL: the one exchange step of a multi-GPU render
+    # the film over NCCL, device to device: the one exchange step of a multi-GPU render
     if world > 1:
-        film = torch.from_numpy(np.ascontiguousarray(img)).to(f"cuda:{local}")
-        torch.distributed.all_reduce(film)
+        import distributed
+        distributed.reduce_film_device(ctx)
         torch.cuda.synchronize()
 
     if rank == 0:

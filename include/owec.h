@@ -343,6 +343,11 @@ int owec_resolve(owec_ctx* ctx, double* xyz, double* samples);
  * sums are the particle splats over width x height and the samples spp summed over the passes, so
  * that sums / samples is the resolved image there too. */
 int owec_read_film(owec_ctx* ctx, double* xyz_sums, double* samples);
+/* owec_read_film into device memory of the context's device (xyz_sums_dev: 3 doubles per pixel,
+ * samples_dev: 1 per pixel; either may be NULL): the film's sums stay on the device, for a
+ * device-side all-reduce of the ranks' films (NCCL). Path integrator only. No counterpart in the
+ * reference. */
+int owec_read_film_device(owec_ctx* ctx, double* xyz_sums_dev, double* samples_dev);
 /* Sets the index of the next pass's first sample stream (the pass index of owec_pass): each rank
  * of a multi-GPU render starts its share of the streams there, so that the ranks together draw
  * exactly the streams one device would. */
@@ -481,6 +486,8 @@ typedef struct owec_adjoint_stats {
     uint64_t device_bytes;/* device memory the call held beyond what the context held before it: its
                            * buffers (loss gradient, height gradient, checkpoints, replayed film) and the
                            * replay kernel's per-thread stacks */
+    double replay_seconds;/* of seconds, the device time of the derivative replay alone (the rest is the
+                           * wavefront phase that runs the paths to their first heightfield crossing) */
 } owec_adjoint_stats;
 /* flags: 0, the unbiased gradient of the expected film (sampling detached: the Fresnel branch and
  * roulette probabilities and the drawn scattering directions held fixed, their weights' values

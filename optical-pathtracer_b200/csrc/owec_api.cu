@@ -1327,7 +1327,7 @@ void runParticles(owec_ctx& c, int spp) {
 // memory while the phases' buffers are still held.
 template <int M>
 uint64_t runAdjointCheckpointed(owec_ctx& c, PassParams pp, uint64_t firstPass, int spp, const PathAdjointTargets& t,
-                                bool fixedDecisions, size_t& freeDuring) {
+                                bool fixedDecisions, size_t& freeDuring, double& replaySeconds) {
     using R = ModeR<M>;
     const uint32_t nPix = pp.nPixels;
     const uint32_t target = std::max<uint32_t>(nPix, 1u << 21);
@@ -1346,6 +1346,9 @@ uint64_t runAdjointCheckpointed(owec_ctx& c, PassParams pp, uint64_t firstPass, 
     const int grid = c.numSMs * 8;
     double unusedSeconds[2] = {0, 0};
     int unusedEvents = 0, unusedLaunches = 0;
+    cudaEvent_t replayStart, replayStop;
+    OWEC_CUDA(cudaEventCreate(&replayStart));
+    OWEC_CUDA(cudaEventCreate(&replayStop));
     for (int done = 0; done < spp;) {
         const uint32_t S = std::min<uint32_t>(perBatch, uint32_t(spp - done));
         pp.nPaths = S * nPix;
@@ -1355,10 +1358,18 @@ uint64_t runAdjointCheckpointed(owec_ctx& c, PassParams pp, uint64_t firstPass, 
         launchGenerate<M>(c.ds, pp, pb, q, st.get(), c.stream);
         checkLaunch();
         runBounces<M>(c, pp, pb, q, st.get(), grid, false, unusedSeconds, unusedEvents, unusedLaunches);
+        OWEC_CUDA(cudaEventRecord(replayStart, c.stream));
         launchPathAdjoint(M, c.ds, pp, c.hf, t, fixedDecisions, ckpt.get(), ckptCount.get(), grid, c.stream);
         checkLaunch();
+        OWEC_CUDA(cudaEventRecord(replayStop, c.stream));
+        OWEC_CUDA(cudaEventSynchronize(replayStop));
+        float ms = 0;
+        OWEC_CUDA(cudaEventElapsedTime(&ms, replayStart, replayStop));
+        replaySeconds += ms * 1e-3;
         done += int(S);
     }
+    cudaEventDestroy(replayStart);
+    cudaEventDestroy(replayStop);
     StatCounters hs{};
     OWEC_CUDA(cudaMemcpyAsync(&hs, st.get(), sizeof(StatCounters), cudaMemcpyDeviceToHost, c.stream));
     OWEC_CUDA(cudaStreamSynchronize(c.stream));
@@ -1589,6 +1600,25 @@ int owec_read_film(owec_ctx* ctx, double* xyz_sums, double* samples) {
             OWEC_CUDA(cudaMemcpyAsync(samples, ctx->dSamples.get(), np * 8, cudaMemcpyDeviceToHost, ctx->stream));
             OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
         }
+    });
+}
+
+int owec_read_film_device(owec_ctx* ctx, double* xyz_sums_dev, double* samples_dev) {
+    return guarded([&] {
+        require(ctx != nullptr, "owec_read_film_device: null context");
+        require(ctx->hasScene, "no scene uploaded", OWEC_E_STATE);
+        require(ctx->settings.integrator == OWEC_INTEGRATOR_PATH,
+                "owec_read_film_device reads the path integrator's film", OWEC_E_UNSUPPORTED);
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        ensureFilm(*ctx);
+        const size_t np = size_t(ctx->ds.det.width) * ctx->ds.det.height;
+        if (xyz_sums_dev) {
+            launchFoldFilm(ctx->dFilm.get(), ctx->dComp.get(), xyz_sums_dev, 3 * np, ctx->stream);
+            checkLaunch();
+        }
+        if (samples_dev)
+            OWEC_CUDA(cudaMemcpyAsync(samples_dev, ctx->dSamples.get(), np * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
     });
 }
 
@@ -1951,6 +1981,7 @@ int owec_path_adjoint(owec_ctx* ctx, uint64_t first_pass, int spp, int flags, co
         PathAdjointTargets t{dG.get(), 1.0 / double(spp), dDH.get(), replay_xyz ? dRep.get() : nullptr, ctr.get()};
         const bool fixed = (flags & OWEC_ADJOINT_FIXED_DECISIONS) != 0;
         uint64_t cameraPaths = 0;  // the first phase's count (the replay kernel counts only what it walks)
+        double replaySeconds = 0;
         OWEC_CUDA(cudaEventRecord(ctx->passStart, ctx->stream));
         if (replay_xyz) {
             // the replayed film needs every path: replay them all from the camera, up to 2^22 per
@@ -1966,11 +1997,14 @@ int owec_path_adjoint(owec_ctx* ctx, uint64_t first_pass, int spp, int flags, co
                 done += int(S);
             }
         } else if (ctx->settings.precision == OWEC_PRECISION_FP64) {
-            cameraPaths = runAdjointCheckpointed<OWEC_PRECISION_FP64>(*ctx, pp, first_pass, spp, t, fixed, freeDuring);
+            cameraPaths = runAdjointCheckpointed<OWEC_PRECISION_FP64>(*ctx, pp, first_pass, spp, t, fixed, freeDuring,
+                                                                      replaySeconds);
         } else if (ctx->settings.precision == OWEC_PRECISION_FP32) {
-            cameraPaths = runAdjointCheckpointed<OWEC_PRECISION_FP32>(*ctx, pp, first_pass, spp, t, fixed, freeDuring);
+            cameraPaths = runAdjointCheckpointed<OWEC_PRECISION_FP32>(*ctx, pp, first_pass, spp, t, fixed, freeDuring,
+                                                                      replaySeconds);
         } else {
-            cameraPaths = runAdjointCheckpointed<OWEC_PRECISION_MIXED>(*ctx, pp, first_pass, spp, t, fixed, freeDuring);
+            cameraPaths = runAdjointCheckpointed<OWEC_PRECISION_MIXED>(*ctx, pp, first_pass, spp, t, fixed, freeDuring,
+                                                                      replaySeconds);
         }
         OWEC_CUDA(cudaEventRecord(ctx->passStop, ctx->stream));
         OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -1993,6 +2027,7 @@ int owec_path_adjoint(owec_ctx* ctx, uint64_t first_pass, int spp, int flags, co
             stats->faults = counts[3];
             stats->seconds = ms * 1e-3;
             stats->device_bytes = freeBefore > freeDuring ? uint64_t(freeBefore - freeDuring) : 0;
+            stats->replay_seconds = replay_xyz ? ms * 1e-3 : replaySeconds;
         }
     });
 }

@@ -812,6 +812,12 @@ __global__ void __launch_bounds__(256) kFilm(DeviceScene sc, PassParams pp, Path
     samples[pixel] += samplesPerPixel;
 }
 
+// The film's compensated sums as plain sums (sum - compensation), for a device-side reduction.
+__global__ void __launch_bounds__(256) kFoldFilm(const double* film, const double* comp, double* out, size_t n) {
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        out[i] = film[i] - comp[i];
+}
+
 // ------------------------------------------------------------------ ray casts
 template <int M, bool Full>
 __global__ void __launch_bounds__(128) kCastRays(DeviceScene sc, uint64_t n, const double* o, const double* d,
@@ -976,6 +982,10 @@ void launchConnect(const DeviceScene& sc, const PassParams& pp, const PathBuffer
                    StatCounters* st, uint32_t* fetch, uint8_t* vis, const SplatTarget& film, int grid, cudaStream_t s) {
     shadowKernels<M, true>(sc, pp, pb, q, st, fetch, vis, film, grid, s);
 }
+void launchFoldFilm(const double* film, const double* comp, double* out, size_t n, cudaStream_t s) {
+    kFoldFilm<<<int(std::min<size_t>((n + 255) / 256, 4096)), 256, 0, s>>>(film, comp, out, n);
+}
+
 template <int M>
 void launchFilm(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, double* film, double* comp,
                 double* samples, uint32_t spp, cudaStream_t s) {

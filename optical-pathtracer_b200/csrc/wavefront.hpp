@@ -35,6 +35,8 @@ void launchConnect(const DeviceScene&, const PassParams&, const PathBuffers<Mode
                    uint32_t* fetch, uint8_t* vis, const SplatTarget& film, int grid, cudaStream_t);
 void launchResolve(const double* film, const double* comp, const double* samples, uint32_t nPixels, double* xyz,
                    cudaStream_t);
+// out[i] = film[i] - comp[i] (the compensated sums as plain sums), n values, on stream s.
+void launchFoldFilm(const double* film, const double* comp, double* out, size_t n, cudaStream_t s);
 template <int M>
 void launchFilm(const DeviceScene&, const PassParams&, const PathBuffers<ModeR<M>>&, double* film, double* comp,
                 double* samples, uint32_t spp, cudaStream_t);

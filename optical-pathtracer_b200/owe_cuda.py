@@ -97,6 +97,12 @@ class Context:
                                                  cnt.ctypes.data_as(A.c_double_p)), "owec_read_film")
         return sums.reshape(self.height, self.width, 3), cnt.reshape(self.height, self.width)
 
+    def read_film_device(self, sums_ptr, samples_ptr):
+        """owec_read_film_device: the film's XYZ sums (3 doubles per pixel) and samples per pixel
+        into device buffers at the given addresses (0: skipped), e.g. torch CUDA tensors' data_ptr()."""
+        _check(self.lib, self.lib.owec_read_film_device(self.handle, ctypes.c_void_p(sums_ptr or None),
+                                                        ctypes.c_void_p(samples_ptr or None)), "owec_read_film_device")
+
     def set_pass_index(self, index):
         """The sample stream the next pass starts at."""
         _check(self.lib, self.lib.owec_set_pass_index(self.handle, int(index)), "owec_set_pass_index")

@@ -148,7 +148,8 @@ class WalkStats(ctypes.Structure):
 
 class AdjointStats(ctypes.Structure):
     _fields_ = [("paths", ctypes.c_uint64), ("heightfield", ctypes.c_uint64), ("dropped", ctypes.c_uint64),
-                ("faults", ctypes.c_uint64), ("seconds", ctypes.c_double), ("device_bytes", ctypes.c_uint64)]
+                ("faults", ctypes.c_uint64), ("seconds", ctypes.c_double), ("device_bytes", ctypes.c_uint64),
+                ("replay_seconds", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -200,6 +201,7 @@ def load_library(path=LIB_PATH):
         "owec_pass": ([P, ctypes.c_int], ctypes.c_int),
         "owec_resolve": ([P, c_double_p, c_double_p], ctypes.c_int),
         "owec_read_film": ([P, c_double_p, c_double_p], ctypes.c_int),
+        "owec_read_film_device": ([P, P, P], ctypes.c_int),
         "owec_set_pass_index": ([P, ctypes.c_uint64], ctypes.c_int),
         "owec_reset_film": ([P], ctypes.c_int),
         "owec_read_stats": ([P, ctypes.POINTER(Stats)], ctypes.c_int),

@@ -23,6 +23,7 @@
 #include "owe/backends/cpu/cpu_backend.hpp"
 #include "owe/core/parallel.hpp"
 #include "owe/scene/builders.hpp"
+#include "owe/scene/prescription.hpp"
 #include "owe/scene/scene.hpp"
 #include "owe/transport/transport.hpp"
 #include "owec.h"
@@ -569,6 +570,39 @@ int oweref_scene_info(void* scene, double* light_pdfs, int max_lights, int* n_li
         for (int i = 0; i < std::min(max_lights, *n_lights); ++i) light_pdfs[i] = w.lightSelectPdf(size_t(i));
         *scene_radius = w.sceneRadius();
         *detector_region = rs.scene.detectors[0]->region;
+    });
+}
+
+// The reference's paraxial analysis (paraxialAnalysis, src/owe/scene/prescription.cpp) of a
+// sequence of n spherical surfaces (radii, m; Inf: flat) with thicknesses n - 1 (m) between them
+// and Sellmeier glasses after each of the first n - 1 surfaces (3 B and 3 C coefficients per glass,
+// relative to air), in air: the image distance behind the last vertex of an on-axis object
+// object_distance in front of the first, at lambda (nm).
+int oweref_paraxial_image_distance(int n, const double* radii, const double* thickness, const double* sellmeier,
+                                   double object_distance, double lambda, double* image_distance) {
+    return guarded([&] {
+        Prescription p;
+        p.objectDistance = object_distance;
+        p.wavelength = lambda;
+        for (int i = 0; i < n; ++i) {
+            PrescriptionSurface s;
+            s.R = radii[i];
+            s.t = i + 1 < n ? thickness[i] : 0.0;
+            s.medium = i + 1 < n ? "glass" + std::to_string(i) : "air";
+            s.sd = 0.0125;
+            p.surfaces.push_back(s);
+        }
+        const IndexFn catalog = catalogIndex();
+        const IndexFn index = [&](const std::string& medium, double l) {
+            if (medium.rfind("glass", 0) != 0) return catalog(medium, l);
+            const int g = std::stoi(medium.substr(5));
+            const double* c = sellmeier + 6 * g;
+            const double um2 = (l * 1e-3) * (l * 1e-3);
+            double n2 = 1;
+            for (int k = 0; k < 3; ++k) n2 += c[k] * um2 / (um2 - c[3 + k]);
+            return std::sqrt(n2) * catalog("air", l);
+        };
+        *image_distance = paraxialAnalysis(p, lambda, index).imageDistance;
     });
 }
 

@@ -43,6 +43,8 @@ def ref_lib():
                                     A.c_double_p, ctypes.POINTER(ctypes.c_uint64)]
         lib.oweref_walk_in_box.argtypes = [P, ctypes.POINTER(A.WalkDesc), ctypes.c_uint64, ctypes.c_uint64, A.c_double_p,
                                            ctypes.c_int, A.c_double_p, ctypes.POINTER(ctypes.c_uint64)]
+        lib.oweref_paraxial_image_distance.argtypes = [ctypes.c_int, A.c_double_p, A.c_double_p, A.c_double_p,
+                                                       ctypes.c_double, ctypes.c_double, A.c_double_p]
         _ref = lib
     return _ref
 
@@ -144,6 +146,22 @@ class ReferenceEngine:
         v = ctypes.c_double()
         self.lib.oweref_medium_index(self.h, region, lam, ctypes.byref(v))
         return v.value
+
+
+def paraxial_image_distance(radii, thickness, glasses, object_distance, wavelength):
+    """The reference's paraxialAnalysis: image distance behind the last vertex for spherical surfaces
+    `radii` (m), `thickness` between them (m) and Sellmeier `glasses` ((B1, B2, B3), (C1, C2, C3))
+    after each surface but the last, relative to air, in air."""
+    lib = ref_lib()
+    r = np.ascontiguousarray(radii, np.float64)
+    t = np.ascontiguousarray(thickness, np.float64)
+    c = np.ascontiguousarray([v for B, C in glasses for v in list(B) + list(C)], np.float64)
+    out = ctypes.c_double()
+    st = lib.oweref_paraxial_image_distance(len(r), r.ctypes.data_as(A.c_double_p), t.ctypes.data_as(A.c_double_p),
+                                            c.ctypes.data_as(A.c_double_p), object_distance, wavelength, ctypes.byref(out))
+    if st != 0:
+        raise RuntimeError(lib.oweref_last_error().decode())
+    return out.value
 
 
 def normalise_walk_bins(desc, bins, n):

@@ -85,3 +85,49 @@ def test_two_gloo_ranks_reproduce_one_device_film(tmp_path):
     assert list(s0) + list(s1) == list(range(total))
     assert np.array_equal(m0, m1)
     assert np.allclose(m0, expect, rtol=1e-13, atol=1e-13)
+
+
+class FakeAdjointContext:
+    """The adjoint calls of distributed.walk_gradient / path_gradient on a known function: the
+    gradient of a block of walks or samples is the mean over them of a per-index vector, as the
+    library normalises by the walks (samples) of its own call."""
+
+    _hf_n = 9
+
+    @staticmethod
+    def _g(k):
+        return np.sin(0.3 * k + np.arange(9))
+
+    def walk_adjoint(self, desc, first, n, g):
+        return sum(self._g(k) for k in range(first, first + n)) / n * float(np.sum(g))
+
+    def path_adjoint(self, first_pass, spp, g):
+        return sum(self._g(k) for k in range(first_pass, first_pass + spp)) / spp * float(np.sum(g))
+
+
+def _grad_rank(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        c = FakeAdjointContext()
+        g = np.full(4, 0.5)
+        np.save(os.path.join(out, f"walk{rank}.npy"), D.walk_gradient(c, None, 13, g))
+        np.save(os.path.join(out, f"path{rank}.npy"), D.path_gradient(c, 7, g, first_pass=3))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_reproduce_one_device_gradient(tmp_path):
+    c = FakeAdjointContext()
+    g = np.full(4, 0.5)
+    walk1 = c.walk_adjoint(None, 0, 13, g)
+    path1 = c.path_adjoint(3, 7, g)
+    port = _free_port()
+    mp.start_processes(_grad_rank, args=(2, port, str(tmp_path)), nprocs=2, join=True, start_method="spawn")
+    for name, one in (("walk", walk1), ("path", path1)):
+        a, b = np.load(tmp_path / f"{name}0.npy"), np.load(tmp_path / f"{name}1.npy")
+        assert np.array_equal(a, b)
+        assert np.allclose(a, one, rtol=1e-13, atol=1e-13)

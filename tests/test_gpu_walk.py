@@ -74,3 +74,51 @@ def test_walk_film_is_deterministic_across_batch_splits():
     a, _ = _walk_gpu(desc, w, 300_000, chunk=300_000)
     b, _ = _walk_gpu(desc, w, 300_000, chunk=70_000)
     assert np.array_equal(a, b)
+
+
+def _spot(bins, half):
+    """Centroid (x, y) and RMS radius about it of a binned spot, in metres on the detector."""
+    n = bins.shape[0]
+    w = bins / bins.sum()
+    c = (np.arange(n) + 0.5) / n * 2 * half - half
+    X, Y = np.meshgrid(c, -c)
+    cx, cy = (w * X).sum(), (w * Y).sum()
+    return cx, cy, math.sqrt((w * ((X - cx) ** 2 + (Y - cy) ** 2)).sum())
+
+
+def test_c3_lens_at_its_configuration():
+    """C3 as configured: the cemented achromat imaging a point source 10 m away onto a 1024 x 1024
+    detector placed at the paraxial focus the reference's own paraxial analysis gives
+    (paraxialAnalysis, as tests/test_instruments.cpp:249 places it); 10^9 walks over 380-780 nm,
+    Monte-Carlo Fresnel branching with ghosts, depth 32. The spot diagram (centroid, RMS radius) of
+    the 10^9 walks against the reference's Tracer::walk over a subsample, and the image error of the
+    same 2^22 walks (common random numbers) bin for bin."""
+    from oracle_ref import paraxial_image_distance
+    sb, info = scenes.achromat_scene(film=1024, half_size=2.5e-4)
+    wl = 587.5618
+    back = paraxial_image_distance([0.0615, -0.0446, -0.129], [0.006, 0.0025], [scenes.NBK7, scenes.SF5], 10.0, wl)
+    assert abs(0.0085 + back - info["z_focus"]) < 1e-9  # the detector where the reference puts the focus
+    desc = sb.desc()
+    w = scenes.achromat_walk(info, seed=5, max_events=32)
+    sub = 1 << 22
+    ref_bins, ref_st = ReferenceEngine(desc).walk(w, 0, sub)
+    with owe_cuda.Context() as c:
+        c.upload(desc)
+        c.build_bvh()
+        c.walk(w, 0, sub)
+        same, st = c.walk_resolve()
+        c.walk_reset()
+        total = 10 ** 9
+        for first in range(0, total, 1 << 27):
+            c.walk(w, first, min(1 << 27, total - first))
+        full, st_full = c.walk_resolve()
+    assert st["faults"] == 0 and st_full["faults"] == 0 and st_full["walks"] == total
+    # the same walks: the same image, up to landing points that rounding moves across a bin edge
+    assert np.abs(same - ref_bins).sum() <= 0.01 * ref_bins.sum(), np.abs(same - ref_bins).sum() / ref_bins.sum()
+    half = info["half"]
+    rx, ry, rr = _spot(ref_bins, half)
+    gx, gy, gr = _spot(full, half)
+    bin_size = 2 * half / 1024
+    assert abs(gx - rx) < 0.25 * bin_size and abs(gy - ry) < 0.25 * bin_size, (gx, rx, gy, ry)
+    assert abs(gr / rr - 1) < 0.02, (gr, rr)
+    assert abs(full.sum() / ref_bins.sum() - 1) < 0.005
