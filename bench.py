@@ -283,14 +283,12 @@ def adjoint_study(device, n=256, bins=512, walks=1 << 24):
             "adjoint_over_forward": a / f, "forward_walks_per_s": walks / f}
 
 
-def c5_study(device, spp_timing=16, steps=0, spp_step=4, width=1920, height=1080):
+def c5_study(device, spp_timing=1024, steps=0, spp_step=8, width=1920, height=1080):
     """The large adjoint: the caustic room (a 1024 x 1024 heightfield PMMA panel, two displaced-sphere
     props of 2^20 triangles each, fog with sigma_s 0.5 / m, sigma_a 0.05 / m, Henyey-Greenstein g 0.8,
     one ceiling light), 1920 x 1080, depth 24. Device seconds of a forward pass (owec_pass) and of the
     path-replay adjoint (owec_path_adjoint) over the same spp_timing samples, their ratio, the device
-    memory of each; then, when steps > 0, that many gradient-descent steps on the heights toward a
-    target film rendered at seeded target heights (spp_step samples per step for the film and an
-    independent replay for the gradient), reporting the loss before and after and the time per step."""
+    memory of each; then, when steps > 0, that many Adam steps toward a target film (c5_optimise)."""
     import torch
     import owe_cuda
     n = 1024
@@ -324,49 +322,86 @@ def c5_study(device, spp_timing=16, steps=0, spp_step=4, width=1920, height=1080
                     "context_bytes": int(free0 - free1), "adjoint_call_bytes": int(st["device_bytes"]),
                     "device_total_bytes": int(total)})
         if steps > 0:
-            rng = np.random.Generator(np.random.PCG64(5))
-            yy, xx = np.mgrid[0:n, 0:n] / (n - 1)
-            target_h = np.zeros((n, n))
-            for _ in range(8):
-                fx, fy, ph = rng.uniform(1, 4, 2).tolist() + [rng.uniform(0, 2 * np.pi)]
-                target_h += np.sin(np.pi * fx * xx + ph) * np.sin(np.pi * fy * yy)
-            target_h *= 4e-3 / np.abs(target_h).max()
-            target_h[0, :] = target_h[-1, :] = target_h[:, 0] = target_h[:, -1] = 0
-            c.set_heightfield(info["heightfield"], info["base_z"], target_h)
-            c.reset_film()
-            c.set_pass_index(1 << 20)
-            c.run_pass(64)
-            target, _ = c.resolve(samples=False)
-            h = np.zeros(n * n)
-            lr = None
-            losses, t_fwd, t_adj = [], 0.0, 0.0
-            for k in range(steps):
-                c.set_heightfield(info["heightfield"], info["base_z"], h)
-                c.reset_film()
-                c.set_pass_index(2 * k * spp_step)
-                c.run_pass(spp_step)
-                t_fwd += c.last_pass_timing()[0]
-                img, _ = c.resolve(samples=False)
-                diff = img - target
-                losses.append(float((diff ** 2).mean()))
-                # the gradient from an independent replay (other sample streams), so that the film's
-                # noise and the replay's do not correlate
-                grad, st, _ = c.path_adjoint((2 * k + 1) * spp_step, spp_step, 2 * diff / diff.size, with_stats=True)
-                t_adj += st["seconds"]
-                if lr is None:  # a first step of 0.1 mm on the largest gradient
-                    lr = 1e-4 / max(np.abs(grad).max(), 1e-30)
-                h = h - lr * grad
-                h = h.reshape(n, n)
-                h[0, :] = h[-1, :] = h[:, 0] = h[:, -1] = 0
-                h = h.ravel()
-            out["optimisation"] = {"steps": steps, "spp_per_step": spp_step, "loss_first": losses[0],
-                                   "loss_last": losses[-1], "loss_min": min(losses),
-                                   "loss_mean_first10": float(np.mean(losses[:10])),
-                                   "loss_mean_last10": float(np.mean(losses[-10:])),
-                                   "forward_s_per_step": t_fwd / steps, "adjoint_s_per_step": t_adj / steps,
-                                   "height_rmse_vs_target_first": float(np.sqrt((target_h ** 2).mean())),
-                                   "height_rmse_vs_target_last": float(np.sqrt(((h.reshape(n, n) - target_h) ** 2).mean()))}
+            out["optimisation"] = c5_optimise(c, info, n, steps, spp_step, width, height)
     return out
+
+
+def _bilinear(n, m):
+    """The n x m matrix that samples a piecewise-linear function through m evenly spaced control
+    values at n evenly spaced points (both ends included)."""
+    x = np.linspace(0.0, m - 1.0, n)
+    return np.maximum(0.0, 1.0 - np.abs(x[:, None] - np.arange(m)[None, :]))
+
+
+def c5_optimise(c, info, n, steps, spp_step, width, height, m=12, block=16, lr=2e-4):
+    """Heightfield optimisation on the caustic room through owe_autograd.camera_film: the heights are
+    a bilinear surface through an m x m grid of control heights (its outer ring held at zero, so the
+    panel's rim stays flat), the target film is rendered at 64 spp at seeded target control heights,
+    the loss is the mean squared difference of the two films averaged over block x block pixel
+    tiles, and Adam steps the control heights (step size decaying tenfold over the run) with a
+    gradient from an independent replay each step.
+    The loss at 64 spp is measured before and after, beside the same loss between two independent
+    64-spp renders at the target heights (the noise floor)."""
+    import torch
+    import torch.nn.functional as F
+    import owe_autograd
+    hf, base_z = info["heightfield"], info["base_z"]
+    W = torch.from_numpy(_bilinear(n, m))
+    rng = np.random.Generator(np.random.PCG64(5))
+    u = np.linspace(0.0, 1.0, m)
+    ct = np.zeros((m, m))
+    for _ in range(4):
+        fx, fy, px, py = rng.uniform(0.5, 2.0, 2).tolist() + rng.uniform(0, 2 * np.pi, 2).tolist()
+        ct += np.outer(np.sin(np.pi * fy * u + py), np.sin(np.pi * fx * u + px))
+    ct[0, :] = ct[-1, :] = ct[:, 0] = ct[:, -1] = 0
+    ct *= 4e-3 / np.abs(ct).max()
+    ct = torch.from_numpy(ct)
+    mask = torch.zeros(m, m, dtype=torch.float64)
+    mask[1:-1, 1:-1] = 1
+    hc = height // block * block
+    wc = width // block * block
+
+    def heights(ctrl):
+        return (W @ (ctrl * mask) @ W.T).reshape(-1)
+
+    def tiles(img):
+        x = img[:hc, :wc].permute(2, 0, 1).unsqueeze(0)
+        return F.avg_pool2d(x, block)
+
+    def render(ctrl, first, spp):
+        with torch.no_grad():
+            return owe_autograd.camera_film(heights(ctrl), c, hf, base_z, first, spp)
+
+    target = tiles(render(ct, 1 << 24, 64))
+    def loss64(ctrl, first):
+        return float(((tiles(render(ctrl, first, 64)) - target) ** 2).mean())
+
+    ctrl = torch.zeros(m, m, dtype=torch.float64, requires_grad=True)
+    opt = torch.optim.Adam([ctrl], lr=lr)
+    decay = torch.optim.lr_scheduler.ExponentialLR(opt, gamma=0.1 ** (1.0 / steps))  # to lr / 10 at the end
+    res = {"steps": steps, "spp_per_step": spp_step, "control_grid": f"{m}x{m} (outer ring fixed at 0)",
+           "loss": f"mean squared XYZ difference of {block}x{block}-pixel tile means", "adam_lr_m": lr,
+           "loss64_noise_floor": loss64(ct, 1 << 25), "loss64_first": loss64(ctrl.detach(), 1 << 26)}
+    losses, t_fwd, t_adj, rmse = [], 0.0, 0.0, []
+    for k in range(steps):
+        opt.zero_grad()
+        img = owe_autograd.camera_film(heights(ctrl), c, hf, base_z, 2 * k * spp_step, spp_step,
+                                       adjoint_pass=(2 * k + 1) * spp_step)
+        t_fwd += c.last_pass_timing()[0]
+        loss = ((tiles(img) - target) ** 2).mean()
+        loss.backward()
+        t_adj += c.last_path_adjoint_seconds()
+        opt.step()
+        decay.step()
+        losses.append(float(loss.detach()))
+        rmse.append(float(torch.sqrt((((ctrl.detach() - ct) * mask) ** 2).sum() / mask.sum())))
+    res.update({"loss64_last": loss64(ctrl.detach(), 1 << 26), "loss_first": losses[0], "loss_last": losses[-1],
+                "loss_mean_first10": float(np.mean(losses[:10])), "loss_mean_last10": float(np.mean(losses[-10:])),
+                "forward_s_per_step": t_fwd / steps, "adjoint_s_per_step": t_adj / steps,
+                "control_rmse_vs_target_first": float(torch.sqrt((ct ** 2).sum() / mask.sum())),
+                "control_rmse_vs_target_last": rmse[-1],
+                "control_rmse_every_20": [round(r, 7) for r in rmse[19::20]]})
+    return res
 
 
 def configs_study(device):
@@ -650,6 +685,9 @@ def main():
     ap.add_argument("--c5", type=int, default=-1, metavar="STEPS",
                     help="run only the large-adjoint study (caustic room at 1920x1080, depth 24) with STEPS "
                          "gradient steps (0: timing and memory alone) and print its JSON")
+    ap.add_argument("--c5-spp", type=int, default=1024,
+                    help="samples per pixel of the large-adjoint study's timed forward pass and adjoint")
+    ap.add_argument("--c5-step-spp", type=int, default=8, help="samples per pixel of each optimisation step")
     ap.add_argument("--integrator", default="path", choices=["path", "light"],
                     help="path: the headline camera-path integrator; light: particles from the emitters, "
                          "measured in particles/s on the same scene")
@@ -662,7 +700,7 @@ def main():
     if args.c5 >= 0:
         import torch
         torch.cuda.set_device(0)
-        print(json.dumps({"c5_study": c5_study(0, steps=args.c5)}))
+        print(json.dumps({"c5_study": c5_study(0, spp_timing=args.c5_spp, steps=args.c5, spp_step=args.c5_step_spp)}))
         return 0
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         return spawn_ranks(args)

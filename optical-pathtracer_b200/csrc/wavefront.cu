@@ -772,44 +772,90 @@ __global__ void __launch_bounds__(256) kShadowApply(DeviceScene sc, PathBuffers<
 }
 
 // ------------------------------------------------------------------ film
-// Folds the batch's samples of every pixel into the film in sample order: XYZ of each path
-// (Wavelengths::toXYZ of L * weight, wavelengths.hpp:71-84), skipping non-finite estimates as
-// CpuRenderer::pass does, with compensated (Kahan) FP64 sums.
+// XYZ of one path (Wavelengths::toXYZ of L * weight, wavelengths.hpp:71-84); false for a path that
+// adds nothing: no estimate, or a non-finite one, which CpuRenderer::pass skips.
+template <int M>
+__device__ __forceinline__ bool pathXYZ(const DeviceScene& sc, const PathBuffers<RT<M>>& pb, uint32_t i, double v[3]) {
+    using R = RT<M>;
+    const PathAux aux = pb.aux[i];
+    if (!(aux.weight > 0.f)) return false;
+    const PathSpec<R> sp = pb.spec[i];
+    const double inv = 1.0 / (NW * sc.cieYIntegral);
+    double x = 0, y = 0, z = 0;
+    for (int k = 0; k < NW; ++k) {
+        const double Lk = double(sp.L[k]) * double(aux.weight);
+        if (sp.pdf[k] == 0.f || Lk == 0) continue;
+        const double w = Lk / double(sp.pdf[k]) * inv;
+        const double l = double(sp.lambda[k]);
+        x += w * cieX(l);
+        y += w * cieY(l);
+        z += w * cieZ(l);
+    }
+    if (!isfinite(x + y + z)) return false;
+    v[0] = x;
+    v[1] = y;
+    v[2] = z;
+    return true;
+}
+
+// One compensated (Kahan) addition.
+__device__ __forceinline__ void kahanAdd(double& s, double& c, double v) {
+    const double yv = v - c;
+    const double t = s + yv;
+    c = (t - s) - yv;
+    s = t;
+}
+
+// Folds the batch's samples of every pixel into the film in sample order, with compensated FP64
+// sums as CpuRenderer::pass keeps them; one thread per pixel (films with many pixels).
 template <int M>
 __global__ void __launch_bounds__(256) kFilm(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, double* film,
                                              double* comp, double* samples, uint32_t samplesPerPixel) {
-    using R = RT<M>;
     const uint32_t pixel = blockIdx.x * blockDim.x + threadIdx.x;
     if (pixel >= pp.nPixels) return;
     double s[3], c[3];
     for (int ch = 0; ch < 3; ++ch) { s[ch] = film[3 * pixel + ch]; c[ch] = comp[3 * pixel + ch]; }
-    const double inv = 1.0 / (NW * sc.cieYIntegral);
     for (uint32_t sub = 0; sub < samplesPerPixel; ++sub) {
-        const uint32_t i = sub * pp.nPixels + pixel;
-        const PathAux aux = pb.aux[i];
-        if (!(aux.weight > 0.f)) continue;
-        const PathSpec<R> sp = pb.spec[i];
-        double x = 0, y = 0, z = 0;
-        for (int k = 0; k < NW; ++k) {
-            const double Lk = double(sp.L[k]) * double(aux.weight);
-            if (sp.pdf[k] == 0.f || Lk == 0) continue;
-            const double w = Lk / double(sp.pdf[k]) * inv;
-            const double l = double(sp.lambda[k]);
-            x += w * cieX(l);
-            y += w * cieY(l);
-            z += w * cieZ(l);
-        }
-        if (!isfinite(x + y + z)) continue;
-        const double v[3] = {x, y, z};
-        for (int ch = 0; ch < 3; ++ch) {
-            const double yv = v[ch] - c[ch];
-            const double t = s[ch] + yv;
-            c[ch] = (t - s[ch]) - yv;
-            s[ch] = t;
-        }
+        double v[3];
+        if (!pathXYZ<M>(sc, pb, sub * pp.nPixels + pixel, v)) continue;
+        for (int ch = 0; ch < 3; ++ch) kahanAdd(s[ch], c[ch], v[ch]);
     }
     for (int ch = 0; ch < 3; ++ch) { film[3 * pixel + ch] = s[ch]; comp[3 * pixel + ch] = c[ch]; }
     samples[pixel] += samplesPerPixel;
+}
+
+// The same fold for films of few pixels and many samples per pixel: one block per pixel. Its
+// threads turn 256 consecutive samples into XYZ at a time; three lanes, one per channel, then add
+// them to the compensated sums in sample order, so the film is kFilm's to the bit.
+constexpr int kFilmChunk = 256;
+
+template <int M>
+__global__ void __launch_bounds__(kFilmChunk) kFilmPerPixel(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb,
+                                                            double* film, double* comp, double* samples,
+                                                            uint32_t samplesPerPixel) {
+    __shared__ double xyz[3][kFilmChunk];
+    __shared__ uint8_t keep[kFilmChunk];
+    const uint32_t pixel = blockIdx.x;
+    const int ch = threadIdx.x;  // the folding lanes
+    double s = 0, c = 0;
+    if (ch < 3) { s = film[3 * pixel + ch]; c = comp[3 * pixel + ch]; }
+    for (uint32_t base = 0; base < samplesPerPixel; base += kFilmChunk) {
+        const uint32_t sub = base + threadIdx.x;
+        double v[3];
+        const bool ok = sub < samplesPerPixel && pathXYZ<M>(sc, pb, sub * pp.nPixels + pixel, v);
+        keep[threadIdx.x] = ok;
+        if (ok)
+            for (int k = 0; k < 3; ++k) xyz[k][threadIdx.x] = v[k];
+        __syncthreads();
+        if (ch < 3) {
+            const int n = int(umin(uint32_t(kFilmChunk), samplesPerPixel - base));
+            for (int j = 0; j < n; ++j)
+                if (keep[j]) kahanAdd(s, c, xyz[ch][j]);
+        }
+        __syncthreads();
+    }
+    if (ch < 3) { film[3 * pixel + ch] = s; comp[3 * pixel + ch] = c; }
+    if (threadIdx.x == 0) samples[pixel] += samplesPerPixel;
 }
 
 // The film's compensated sums as plain sums (sum - compensation), for a device-side reduction.
@@ -989,7 +1035,12 @@ void launchFoldFilm(const double* film, const double* comp, double* out, size_t 
 template <int M>
 void launchFilm(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, double* film, double* comp,
                 double* samples, uint32_t spp, cudaStream_t s) {
-    kFilm<M><<<(pp.nPixels + 255) / 256, 256, 0, s>>>(sc, pp, pb, film, comp, samples, spp);
+    // a thread per pixel fills the GPU from 148 x 256 pixels on; below that, with many samples per
+    // pixel, the serial loop over a pixel's samples is the kernel's length
+    if (pp.nPixels < 148u * 256u && spp >= 64)
+        kFilmPerPixel<M><<<pp.nPixels, kFilmChunk, 0, s>>>(sc, pp, pb, film, comp, samples, spp);
+    else
+        kFilm<M><<<(pp.nPixels + 255) / 256, 256, 0, s>>>(sc, pp, pb, film, comp, samples, spp);
 }
 template <int M>
 void launchCastRays(const DeviceScene& sc, uint64_t n, const double* o, const double* d, uint32_t* b, uint32_t* p,

@@ -10,8 +10,8 @@ The C ABI exposes each differentiable measurement as a forward call and a backwa
 Here each pair becomes one torch.autograd.Function of the heightfield's heights, so that a loss
 written in torch differentiates through the renderer with loss.backward(). The functions run on the
 CPU side of torch: heights, films and gradients are float64 tensors on the host, copied through
-the C ABI; the device work is the library's. These wrappers exist for the tests; an optimiser loop
-calls the C ABI directly.
+the C ABI; the device work is the library's. The heightfield optimisation of the large camera
+configuration (bench.py --c5) runs through camera_film.
 """
 import numpy as np
 import torch
@@ -55,17 +55,20 @@ class CameraFilm(torch.autograd.Function):
     from sample stream `first_pass` on, as a function of the heightfield's heights. The backward pass
     is the gradient of the expected film, or with fixed_decisions the derivative of this film's
     estimator at its own random numbers (what central differences with common random numbers
-    measure)."""
+    measure). The backward pass replays the forward pass's sample streams unless adjoint_pass names
+    another block of spp streams: an optimiser of a loss that is not linear in the film wants that,
+    since the film's noise and the gradient's noise then do not correlate."""
 
     @staticmethod
-    def forward(ctx, heights, context, boundary, base_z, first_pass, spp, fixed_decisions):
+    def forward(ctx, heights, context, boundary, base_z, first_pass, spp, fixed_decisions, adjoint_pass=None):
         h = heights.detach().cpu().numpy().astype(np.float64).ravel()
         _ensure_heights(context, boundary, base_z, h)
         context.reset_film()
         context.set_pass_index(first_pass)
         context.run_pass(spp)
         img, _ = context.resolve(samples=False)
-        ctx.args = (context, boundary, base_z, first_pass, spp, fixed_decisions, h, heights.shape)
+        replay = first_pass if adjoint_pass is None else adjoint_pass
+        ctx.args = (context, boundary, base_z, replay, spp, fixed_decisions, h, heights.shape)
         return torch.from_numpy(np.array(img)).to(heights.dtype)
 
     @staticmethod
@@ -74,7 +77,7 @@ class CameraFilm(torch.autograd.Function):
         _ensure_heights(context, boundary, base_z, h)
         g = grad_img.detach().cpu().numpy().astype(np.float64)
         dh = context.path_adjoint(first_pass, spp, g, fixed_decisions=fixed)
-        return torch.from_numpy(dh.reshape(shape)).to(grad_img.dtype), None, None, None, None, None, None
+        return torch.from_numpy(dh.reshape(shape)).to(grad_img.dtype), None, None, None, None, None, None, None
 
 
 def walk_film(heights, context, boundary, base_z, desc, first, n):
@@ -82,6 +85,6 @@ def walk_film(heights, context, boundary, base_z, desc, first, n):
     return WalkFilm.apply(heights, context, boundary, base_z, desc, first, n)
 
 
-def camera_film(heights, context, boundary, base_z, first_pass, spp, fixed_decisions=False):
+def camera_film(heights, context, boundary, base_z, first_pass, spp, fixed_decisions=False, adjoint_pass=None):
     """The camera film as a differentiable function of `heights` (a float64 tensor)."""
-    return CameraFilm.apply(heights, context, boundary, base_z, first_pass, spp, fixed_decisions)
+    return CameraFilm.apply(heights, context, boundary, base_z, first_pass, spp, fixed_decisions, adjoint_pass)

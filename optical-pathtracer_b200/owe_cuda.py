@@ -218,9 +218,14 @@ class Context:
                                                     out.ctypes.data_as(A.c_double_p),
                                                     rep.ctypes.data_as(A.c_double_p) if replay else None,
                                                     ctypes.byref(st)), "owec_path_adjoint")
+        self._last_adjoint = st.as_dict()
         if not with_stats:
             return out
-        return out, st.as_dict(), (rep.reshape(self.height, self.width, 3) if replay else None)
+        return out, self._last_adjoint, (rep.reshape(self.height, self.width, 3) if replay else None)
+
+    def last_path_adjoint_seconds(self):
+        """Device seconds of the last path_adjoint call (both phases)."""
+        return self._last_adjoint["seconds"]
 
     def device_peaks(self):
         """{"fp32_flops", "fp64_flops", "l2_read_bytes_per_s"}: the device's FMA rates and L2 read

@@ -610,7 +610,9 @@ def caustic_room(width=1920, height=1080, n_lon=1024, n_lat=512, panel_n=1024, h
     homogeneous medium (scattering sigma_s, absorption sigma_a per metre, Henyey-Greenstein g), two
     displaced-sphere props of n_lon x n_lat each (2^21 triangles at 1024 x 512), a PMMA panel whose
     top face is a panel_n x panel_n heightfield (heights 0 unless given) standing in the camera's view,
-    and one area light on the ceiling; 1920 x 1080 pinhole camera."""
+    one area light on the ceiling and a small lamp standing low beside the panel, whose steep falloff
+    across the floor beneath the panel is what the camera sees move when the heights refract it;
+    1920 x 1080 pinhole camera."""
     sb = SceneBuilder()
     fog = sb._medium(A.INDEX_CONSTANT, (1.0,), absorption=sb.spectrum_constant(sigma_a),
                      scattering=sb.spectrum_constant(sigma_s), g=g)
@@ -633,6 +635,8 @@ def caustic_room(width=1920, height=1080, n_lon=1024, n_lat=512, panel_n=1024, h
     sb.sheet(w, 2.0, pose(rotate_to((0, 0, 1), (0, 1, 0)), (0, -w, 2.0)), wall)
     lamp = sb.emission(sb.spectrum_constant(8.0))
     sb.sheet(0.8, 0.8, pose(rotate_to((0, 0, 1), (0, 0, -1)), (0.0, 0.0, 3.98)), sb.absorber(), emission=lamp)
+    side = sb.emission(sb.spectrum_constant(40.0))
+    sb.sheet(0.15, 0.2, pose(rotate_to((0, 0, 1), (1, 0, 0)), (-0.45, -0.6, 0.15)), sb.absorber(), emission=side)
     sb.observer(width, height, (0.3, -2.7, 1.6), (0.2, -0.2, 0.6), fov_y_deg=50.0)
     return sb, {"heightfield": hf, "base_z": base_z, "n": panel_n, "half": panel_half}
 

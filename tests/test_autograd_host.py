@@ -54,3 +54,38 @@ def test_backward_restores_the_heights_of_its_forward():
     assert np.array_equal(c._hf_heights, np.zeros(4))
     f1.sum().backward()
     assert np.array_equal(c._hf_heights, h1.detach().numpy())
+
+
+class LinearCameraContext(LinearContext):
+    """The camera-film calls, with film = M @ heights (one channel) and a record of the sample
+    streams each call used."""
+
+    def reset_film(self):
+        pass
+
+    def set_pass_index(self, first):
+        self.first = first
+
+    def run_pass(self, spp):
+        self.forward_streams = (self.first, spp)
+        self._film = self.M @ self._hf_heights
+
+    def resolve(self, samples=False):
+        return self._film.reshape(-1, 1, 1).repeat(3, axis=2), None
+
+    def path_adjoint(self, first_pass, spp, g, fixed_decisions=False):
+        self.adjoint_streams = (first_pass, spp, fixed_decisions)
+        return self.M.T @ np.asarray(g)[:, 0, 1]
+
+
+def test_camera_film_replays_the_streams_it_is_given():
+    c = LinearCameraContext(6, 9)
+    h = torch.tensor(np.linspace(-1, 1, 6), dtype=torch.float64, requires_grad=True)
+    film = owe_autograd.camera_film(h, c, 2, 0.0, 40, 8)
+    film[:, 0, 1].sum().backward()
+    assert c.forward_streams == (40, 8) and c.adjoint_streams == (40, 8, False)
+    assert np.allclose(h.grad.numpy(), c.M.T @ np.ones(9), rtol=1e-12)
+    h.grad = None
+    film = owe_autograd.camera_film(h, c, 2, 0.0, 40, 8, adjoint_pass=48)
+    film[:, 0, 1].sum().backward()
+    assert c.forward_streams == (40, 8) and c.adjoint_streams == (48, 8, False)

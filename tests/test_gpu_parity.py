@@ -178,6 +178,22 @@ def test_film_is_deterministic_and_passes_accumulate():
     assert np.array_equal(a, b), "a pass split into sub-passes must give the same film, bit for bit"
 
 
+def test_small_film_folds_many_samples_like_one_sample_passes():
+    """A 16 x 16 film of 300 samples per pixel in one pass (the block-per-pixel fold) equals the same
+    samples in ten passes of 30 (the thread-per-pixel fold), bit for bit."""
+    desc = scenes.glass_sphere_on_floor(16, 16).desc()
+    s = _glass_settings(12)
+    with _ctx(desc, s) as c:
+        c.run_pass(300)
+        a, n = c.resolve()
+        c.reset_film()
+        for _ in range(10):
+            c.run_pass(30)
+        b, n2 = c.resolve()
+    assert np.array_equal(n, n2) and n.max() == 300
+    assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("integrator", ["path", "light"])
 def test_switching_precision_in_one_context_matches_a_fresh_context(integrator):
     """The path state is sized per precision mode: an FP64 pass after a mixed one in the same
