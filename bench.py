@@ -36,7 +36,9 @@ import scenes  # noqa: E402
 WIDTH, HEIGHT = 1920, 1080
 MAX_DEPTH, RR_DEPTH = 12, 6
 METRIC = "spectral paths/s"
-WORKLOAD = "bvh_stress_room: 2^20-tri displaced UV sphere in a Lambertian box, 1 area light, 1920x1080, hero-4 spectral, depth 12"
+def workload():
+    return (f"bvh_stress_room: 2^20-tri displaced UV sphere in a Lambertian box, 1 area light, {WIDTH}x{HEIGHT}, "
+            "hero-4 spectral, depth 12")
 NODE_BYTES, PRIM_BYTES = 80, 48
 RAY_STATE_BYTES = 4 + 64 + 24  # queue index, the path's ray record, the hit record written
 # Arithmetic per visit, counted from the traversal's source: a wide node tests its 8 child boxes
@@ -148,7 +150,7 @@ def cpu_reference_rate(desc, seconds_target=12.0, threads=0):
     _, st = ref.render(s, 1, pixel_begin=r0 * WIDTH, pixel_end=(r0 + rows) * WIDTH, threads=threads)
     dt = time.perf_counter() - t0
     n_threads = threads if threads > 0 else os.cpu_count()
-    return st["paths"] / dt, n_threads, f"{rows} centre rows of the 1920x1080 frame at 1 spp ({st['paths']} paths, {dt:.1f} s)"
+    return st["paths"] / dt, n_threads, f"{rows} centre rows of the {WIDTH}x{HEIGHT} frame at 1 spp ({st['paths']} paths, {dt:.1f} s)"
 
 
 def run_reference(args):
@@ -183,12 +185,12 @@ def run_reference(args):
     dt = time.perf_counter() - t0
     rate = paths / dt
     cores = os.cpu_count()
-    sample = f"{rows} centre rows of the 1920x1080 frame at 1 spp per step"
+    sample = f"{rows} centre rows of the {WIDTH}x{HEIGHT} frame at 1 spp per step"
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": rate, "unit": "paths/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "rows_per_step": rows},
+        "config": {"workload": workload(), "rows_per_step": rows},
         "cpu_baseline": {"value": rate, "unit": "paths/s", "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": rate, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
@@ -333,13 +335,31 @@ def _bilinear(n, m):
     return np.maximum(0.0, 1.0 - np.abs(x[:, None] - np.arange(m)[None, :]))
 
 
-def c5_optimise(c, info, n, steps, spp_step, width, height, m=12, block=16, lr=2e-4):
+def _screen_box(points, eye, look_at, up, fov_y_deg, width, height):
+    """Pixel bounds (x0, x1, y0, y1) of world points seen by the pinhole observer (IdealObserver's
+    image plane: x to the right, y down)."""
+    eye, f = np.asarray(eye, float), np.asarray(look_at, float) - np.asarray(eye, float)
+    f /= np.linalg.norm(f)
+    r = np.cross(f, np.asarray(up, float))
+    r /= np.linalg.norm(r)
+    u = np.cross(r, f)
+    ty = np.tan(np.radians(fov_y_deg) / 2)
+    tx = ty * width / height
+    v = np.asarray(points, float) - eye
+    px = (v @ r / (v @ f) / tx + 1) * width / 2
+    py = (1 - v @ u / (v @ f) / ty) * height / 2
+    return px.min(), px.max(), py.min(), py.max()
+
+
+def c5_optimise(c, info, n, steps, spp_step, width, height, m=8, block=16, lr=2e-4):
     """Heightfield optimisation on the caustic room through owe_autograd.camera_film: the heights are
     a bilinear surface through an m x m grid of control heights (its outer ring held at zero, so the
     panel's rim stays flat), the target film is rendered at 64 spp at seeded target control heights,
     the loss is the mean squared difference of the two films averaged over block x block pixel
-    tiles, and Adam steps the control heights (step size decaying tenfold over the run) with a
-    gradient from an independent replay each step.
+    tiles that show the panel (its outline projected to the screen, a tile wider on each side; the
+    rest of the film does not depend on the heights and would add only its noise), and Adam steps
+    the control heights (step size decaying tenfold over the run) with a gradient from an
+    independent replay each step.
     The loss at 64 spp is measured before and after, beside the same loss between two independent
     64-spp renders at the target heights (the noise floor)."""
     import torch
@@ -360,13 +380,19 @@ def c5_optimise(c, info, n, steps, spp_step, width, height, m=12, block=16, lr=2
     mask[1:-1, 1:-1] = 1
     hc = height // block * block
     wc = width // block * block
+    cx, cy, cz = info["centre"]
+    half, thick = info["half"], info["thickness"]
+    corners = [(cx + sx * half, cy + sy * half, cz + dz) for sx in (-1, 1) for sy in (-1, 1) for dz in (0.0, thick)]
+    x0, x1, y0, y1 = _screen_box(corners, *info["view"], width, height)
+    tx0, ty0 = max(0, int(x0 // block) - 1), max(0, int(y0 // block) - 1)
+    tx1, ty1 = min(wc // block, int(x1 // block) + 2), min(hc // block, int(y1 // block) + 2)
 
     def heights(ctrl):
         return (W @ (ctrl * mask) @ W.T).reshape(-1)
 
     def tiles(img):
         x = img[:hc, :wc].permute(2, 0, 1).unsqueeze(0)
-        return F.avg_pool2d(x, block)
+        return F.avg_pool2d(x, block)[..., ty0:ty1, tx0:tx1]
 
     def render(ctrl, first, spp):
         with torch.no_grad():
@@ -380,7 +406,8 @@ def c5_optimise(c, info, n, steps, spp_step, width, height, m=12, block=16, lr=2
     opt = torch.optim.Adam([ctrl], lr=lr)
     decay = torch.optim.lr_scheduler.ExponentialLR(opt, gamma=0.1 ** (1.0 / steps))  # to lr / 10 at the end
     res = {"steps": steps, "spp_per_step": spp_step, "control_grid": f"{m}x{m} (outer ring fixed at 0)",
-           "loss": f"mean squared XYZ difference of {block}x{block}-pixel tile means", "adam_lr_m": lr,
+           "loss": f"mean squared XYZ difference of {block}x{block}-pixel tile means over the panel's "
+                   f"{tx1 - tx0}x{ty1 - ty0} tiles", "adam_lr_m": lr,
            "loss64_noise_floor": loss64(ct, 1 << 25), "loss64_first": loss64(ctrl.detach(), 1 << 26)}
     losses, t_fwd, t_adj, rmse = [], 0.0, 0.0, []
     for k in range(steps):
@@ -505,6 +532,7 @@ def run_cuda(args):
     # algorithmic traffic of a pass (counting pass, untimed)
     ctx.trace_counters(1)
     ctx.run_pass(1)
+    launch_queries = ctx.trace_launch_queries()
     cnt = ctx.trace_counters(0)
     _, isec_prof, _, launches_prof = ctx.last_pass_timing()
 
@@ -617,7 +645,7 @@ def run_cuda(args):
             "warmup": args.warmup, "ms_per_step": 1e3 * device_seconds / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": {"mixed": "f32+f64", "fp32": "f32", "fp64": "f64"}[PRECISION], "data": "synthetic",
-            "config": {"workload": WORKLOAD + (", light integrator (particles)" if light else ""),
+            "config": {"workload": workload() + (", light integrator (particles)" if light else ""),
                        "paths_per_step": n_pix, "triangles": info["triangles"],
                        "precision": {"mixed": "fp32 camera-relative + selective fp64", "fp32": "plain fp32",
                                      "fp64": "all fp64"}[PRECISION], "l2": "flushed between steps (512 MB write)",
@@ -641,7 +669,8 @@ def run_cuda(args):
                          "fp32_tflops": fp32_achieved, "fp64_peak_tflops": probe["fp64_flops"] / 1e12,
                          "bytes_per_launch": per_launch_bytes,
                          "per_query": {"nodes": nodes / max(1, q), "prims": prims / max(1, q)},
-                         "queries_per_pass": q, "launches_per_pass": launches_prof},
+                         "queries_per_pass": q, "launches_per_pass": launches_prof,
+                         "queries_per_launch": launch_queries},
             "clocks": clk,
             "cpu_baseline": {"value": cpu_rate, "unit": "particles/s" if light else "paths/s", "cores": cores, "kind": "reference",
                              "sample": sample},

@@ -376,6 +376,11 @@ int owec_cast_rays_device(owec_ctx* ctx, uint64_t n, const float* origins_dev, c
  * tested, shadow queries, their nodes, their primitives] counted while enabled. Counting adds
  * atomics to the traversal kernels: never enable it in a timed pass. */
 int owec_trace_counters(owec_ctx* ctx, int enable, uint64_t out[6]);
+/* The closest-hit queries of each closest-hit kernel launch, in launch order, of the camera passes
+ * run since counting was last enabled (owec_trace_counters with enable = 1), up to 256 launches:
+ * out[0 .. min(capacity, *count) - 1]; *count = the launches logged. For dividing a profiler's
+ * per-launch counters by the work each launch did. */
+int owec_trace_launch_queries(owec_ctx* ctx, uint64_t* out, int capacity, int* count);
 /* The camera-relative origin the device geometry is stored against (world = stored + origin). */
 int owec_scene_origin(owec_ctx* ctx, double origin[3]);
 

@@ -429,6 +429,10 @@ struct owec_ctx {
     DBuf<uint32_t> dShadowPixel;  // light integrator: the pixel of each queued connection
     DBuf<StatCounters> dStats;
     DBuf<unsigned long long> dTravCounters;
+    // while counting: the query counter after each closest-hit launch of the last pass
+    static constexpr int kLaunchLog = 256;
+    DBuf<unsigned long long> dLaunchQueries;
+    int launchQueryCount = 0;
     uint32_t capacity = 0;
     double lastPassSeconds = 0, lastIntersectSeconds = 0, lastShadowSeconds = 0, lastIntersectLaunches = 0;
     uint32_t* hostCounts = nullptr;  // pinned
@@ -1139,6 +1143,9 @@ void runBounces(owec_ctx& c, const PassParams& pp, PathBuffers<ModeR<M>>& pb, Qu
         if (timed) OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed], s));
         launchIntersect<M>(c.ds, pb, q, cur, st, c.dCounts.get() + 4, grid, s);
         ++intersectLaunches;
+        if (c.ds.travCounters && c.launchQueryCount < owec_ctx::kLaunchLog)
+            OWEC_CUDA(cudaMemcpyAsync(c.dLaunchQueries.get() + c.launchQueryCount++, c.ds.travCounters,
+                                      sizeof(unsigned long long), cudaMemcpyDeviceToDevice, s));
         if (timed) OWEC_CUDA(cudaEventRecord(c.travEvents[evUsed + 1], s));
         checkLaunch();
         launchMedium<M>(c.ds, pp, pb, q, cur, st, c.numSMs * OWEC_SHADING_GRID, s);
@@ -1734,10 +1741,28 @@ int owec_trace_counters(owec_ctx* ctx, int enable, uint64_t out[6]) {
         if (enable) {
             OWEC_CUDA(cudaMemsetAsync(ctx->dTravCounters.get(), 0, 6 * sizeof(unsigned long long), ctx->stream));
             OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+            ctx->dLaunchQueries.reserve(owec_ctx::kLaunchLog);
+            ctx->launchQueryCount = 0;
             ctx->ds.travCounters = ctx->dTravCounters.get();
         } else {
             ctx->ds.travCounters = nullptr;
         }
+    });
+}
+
+int owec_trace_launch_queries(owec_ctx* ctx, uint64_t* out, int capacity, int* count) {
+    return guarded([&] {
+        require(ctx != nullptr && count != nullptr, "owec_trace_launch_queries: null argument");
+        require(capacity >= 0 && (out != nullptr || capacity == 0), "owec_trace_launch_queries: no output array");
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        const int n = std::min(capacity, ctx->launchQueryCount);
+        *count = ctx->launchQueryCount;
+        if (n == 0) return;
+        std::vector<unsigned long long> h(static_cast<size_t>(n));
+        OWEC_CUDA(cudaMemcpyAsync(h.data(), ctx->dLaunchQueries.get(), size_t(n) * sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+        OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (int k = 0; k < n; ++k) out[k] = h[size_t(k)] - (k ? h[size_t(k - 1)] : 0ull);
     });
 }
 

@@ -140,6 +140,15 @@ class Context:
         _check(self.lib, self.lib.owec_trace_counters(self.handle, int(enable), out), "owec_trace_counters")
         return [int(v) for v in out]
 
+    def trace_launch_queries(self):
+        """The closest-hit queries of each closest-hit launch of the passes run since counting was
+        enabled (owec_trace_launch_queries), in launch order."""
+        out = (ctypes.c_uint64 * 256)()
+        n = ctypes.c_int()
+        _check(self.lib, self.lib.owec_trace_launch_queries(self.handle, out, 256, ctypes.byref(n)),
+               "owec_trace_launch_queries")
+        return [int(out[k]) for k in range(min(256, n.value))]
+
     def walk(self, desc, first, n):
         """n forward light walks (walk indices first .. first + n - 1) binned on desc.target."""
         self._walk_shape = (desc.height, desc.width)

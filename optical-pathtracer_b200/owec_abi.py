@@ -211,6 +211,8 @@ def load_library(path=LIB_PATH):
         "owec_cast_rays_device": ([P, ctypes.c_uint64, P, P, P, P, P, c_double_p], ctypes.c_int),
         "owec_scene_origin": ([P, c_double_p], ctypes.c_int),
         "owec_trace_counters": ([P, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+        "owec_trace_launch_queries": ([P, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
+                                      ctypes.c_int),
         "owec_walk": ([P, ctypes.POINTER(WalkDesc), ctypes.c_uint64, ctypes.c_uint64], ctypes.c_int),
         "owec_walk_resolve": ([P, c_double_p, ctypes.POINTER(WalkStats)], ctypes.c_int),
         "owec_walk_reset": ([P], ctypes.c_int),

@@ -638,7 +638,8 @@ def caustic_room(width=1920, height=1080, n_lon=1024, n_lat=512, panel_n=1024, h
     side = sb.emission(sb.spectrum_constant(40.0))
     sb.sheet(0.15, 0.2, pose(rotate_to((0, 0, 1), (1, 0, 0)), (-0.45, -0.6, 0.15)), sb.absorber(), emission=side)
     sb.observer(width, height, (0.3, -2.7, 1.6), (0.2, -0.2, 0.6), fov_y_deg=50.0)
-    return sb, {"heightfield": hf, "base_z": base_z, "n": panel_n, "half": panel_half}
+    return sb, {"heightfield": hf, "base_z": base_z, "n": panel_n, "half": panel_half, "centre": (0.3, -0.6, 0.5),
+                "thickness": panel_thickness, "view": ((0.3, -2.7, 1.6), (0.2, -0.2, 0.6), (0, 0, 1), 50.0)}
 
 
 def reflected_moonlight(width=16, height=16):
