@@ -381,6 +381,16 @@ int owec_trace_counters(owec_ctx* ctx, int enable, uint64_t out[6]);
  * out[0 .. min(capacity, *count) - 1]; *count = the launches logged. For dividing a profiler's
  * per-launch counters by the work each launch did. */
 int owec_trace_launch_queries(owec_ctx* ctx, uint64_t* out, int capacity, int* count);
+/* A log of the crossings whose met region differs from the ray's (TransportStats::inconsistencies),
+ * for scenes with contacts (touching bodies, thin plates): capacity > 0 records up to that many
+ * (at most 2^20) from the next pass on, 0 stops. Each record is 16 doubles: boundary, triangle,
+ * hit flags (1 met from the front, 2 undecided contact), the ray's region, the region met, the
+ * boundary and triangle the ray left, the path's depth, the distance, the camera-relative origin
+ * (3), the direction (3) and the anchor's error. Scenes without contacts record nothing. */
+int owec_inconsistency_log(owec_ctx* ctx, int capacity);
+/* Copies min(capacity, *count) records into out (16 doubles each); *count = the crossings logged
+ * since the log was enabled (it may exceed the log's capacity). */
+int owec_read_inconsistency_log(owec_ctx* ctx, double* out, int capacity, int* count);
 /* The camera-relative origin the device geometry is stored against (world = stored + origin). */
 int owec_scene_origin(owec_ctx* ctx, double origin[3]);
 

@@ -127,6 +127,12 @@ struct DeviceScene {
     // When set: [0] closest-hit queries, [1] wide nodes visited, [2] primitives tested, [3] shadow
     // queries, [4] their nodes, [5] their primitives (the algorithmic traffic of a pass).
     unsigned long long* travCounters;
+    // When set (owec_inconsistency_log): the contact-resolving surface kernel records up to
+    // eventLogCap crossings that met a region other than the ray's, kEventRecord doubles each.
+    double* eventLog;
+    uint32_t* eventLogCount;
+    uint32_t eventLogCap;
 };
+constexpr int kEventRecord = 16;
 
 }  // namespace owec

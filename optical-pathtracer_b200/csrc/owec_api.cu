@@ -433,6 +433,10 @@ struct owec_ctx {
     static constexpr int kLaunchLog = 256;
     DBuf<unsigned long long> dLaunchQueries;
     int launchQueryCount = 0;
+    // the inconsistent-crossing log (owec_inconsistency_log)
+    DBuf<double> dEventLog;
+    DBuf<uint32_t> dEventLogCount;
+    uint32_t eventLogCap = 0;
     uint32_t capacity = 0;
     double lastPassSeconds = 0, lastIntersectSeconds = 0, lastShadowSeconds = 0, lastIntersectLaunches = 0;
     uint32_t* hostCounts = nullptr;  // pinned
@@ -948,6 +952,11 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
 
     DeviceScene& ds = c.ds;
     ds = DeviceScene{};
+    if (c.eventLogCap > 0) {  // an enabled event log outlasts a scene upload
+        ds.eventLog = c.dEventLog.get();
+        ds.eventLogCount = c.dEventLogCount.get();
+        ds.eventLogCap = c.eventLogCap;
+    }
     ds.spectra = c.dSpectra.get();
     ds.table = c.dTable.get();
     ds.media = c.dMedia.get();
@@ -1763,6 +1772,46 @@ int owec_trace_launch_queries(owec_ctx* ctx, uint64_t* out, int capacity, int* c
                                   cudaMemcpyDeviceToHost, ctx->stream));
         OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
         for (int k = 0; k < n; ++k) out[k] = h[size_t(k)] - (k ? h[size_t(k - 1)] : 0ull);
+    });
+}
+
+int owec_inconsistency_log(owec_ctx* ctx, int capacity) {
+    return guarded([&] {
+        require(ctx != nullptr, "owec_inconsistency_log: null context");
+        require(capacity >= 0 && capacity <= (1 << 20), "owec_inconsistency_log: capacity out of range [0, 2^20]");
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        if (capacity > 0) {
+            ctx->dEventLog.reserve(size_t(capacity) * kEventRecord);
+            ctx->dEventLogCount.reserve(1);
+            OWEC_CUDA(cudaMemsetAsync(ctx->dEventLogCount.get(), 0, sizeof(uint32_t), ctx->stream));
+            OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+            ctx->ds.eventLog = ctx->dEventLog.get();
+            ctx->ds.eventLogCount = ctx->dEventLogCount.get();
+        } else {
+            ctx->ds.eventLog = nullptr;
+            ctx->ds.eventLogCount = nullptr;
+        }
+        ctx->eventLogCap = uint32_t(capacity);
+        ctx->ds.eventLogCap = uint32_t(capacity);
+    });
+}
+
+int owec_read_inconsistency_log(owec_ctx* ctx, double* out, int capacity, int* count) {
+    return guarded([&] {
+        require(ctx != nullptr && count != nullptr, "owec_read_inconsistency_log: null argument");
+        require(capacity >= 0 && (out != nullptr || capacity == 0), "owec_read_inconsistency_log: no output array");
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        *count = 0;
+        if (ctx->eventLogCap == 0) return;
+        uint32_t n = 0;
+        OWEC_CUDA(cudaMemcpyAsync(&n, ctx->dEventLogCount.get(), sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+        OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+        *count = int(std::min<uint32_t>(n, uint32_t(INT32_MAX)));
+        const size_t k = std::min<size_t>({size_t(capacity), size_t(n), size_t(ctx->eventLogCap)});
+        if (k == 0) return;
+        OWEC_CUDA(cudaMemcpyAsync(out, ctx->dEventLog.get(), k * kEventRecord * sizeof(double), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+        OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
     });
 }
 

@@ -352,6 +352,7 @@ struct Traversal {
     ShearedRay<T> sh;
     T best;
     T bestCos;            // contact-resolving instantiation: |cos| of the closest crossing's incidence
+    double bestD;         // and its distance in the refinement's precision
     HitRec hit;           // written when a crossing is accepted
     Stack st;
     uint32_t nodeBase, nodeBits;  // the current node group (as a stack entry)
@@ -369,6 +370,7 @@ struct Traversal {
         sh = shearRay(q.d);
         best = q.tmax;
         bestCos = T(1);
+        bestD = double(q.tmax);
         found = false;
         sp = 0;
         st.init(stack, stride);
@@ -444,11 +446,17 @@ struct Traversal {
     // one contact: the one met from the ray's region wins, matter wins over a zero-thickness
     // readout, then the lower boundary index; two that both match leave the order undecided
     // (kHitAmbiguous). `flags` receives the winner's flags.
-    __device__ __forceinline__ bool winsContact(const DeviceScene& sc, uint32_t b, T t, bool front, T c, uint32_t& flags) {
+    __device__ __forceinline__ bool winsContact(const DeviceScene& sc, uint32_t b, T t, double tD, bool front, T c,
+                                                uint32_t& flags) {
         const uint32_t frontFlag = front ? kHitFront : 0u;
-        if (!found || t < best - tieSpan(fmin(c, bestCos)) || b == hit.boundary) {
+        const T span = tieSpan(fmin(c, bestCos));
+        if (!found || t < best - span || b == hit.boundary) {
             flags = frontFlag;
-            return !found || t < best;
+            if (!found) return true;
+            // two crossings of one boundary within the span (the faces of a plate thinner than the
+            // FP32 distances resolve) go in the order of their refined distances
+            if (b == hit.boundary && fabs(t - best) <= span) return tD < bestD;
+            return t < best;
         }
         const bool hinted = q.region != kNone;
         auto incident = [&](uint32_t bb, bool fr) {
@@ -478,6 +486,21 @@ struct Traversal {
         return true;
     }
 
+    // The distance of triangle slot i's crossing from its FP64 vertices and the FP64 origin when the
+    // traversal runs in FP32 and refines in FP64 (the value the closest hit is later refined to); t
+    // itself otherwise, or when the two disagree beyond the refinement's reach.
+    __device__ __forceinline__ double refinedTriangleT(const DeviceScene& sc, uint32_t i, T t) const {
+        if constexpr (sizeof(T) == sizeof(float) && sizeof(Rr) == sizeof(double)) {
+            const PrimRec64& p = sc.prims64[i];
+            const V3<double> v0(p.v0[0], p.v0[1], p.v0[2]), v1(p.v1[0], p.v1[1], p.v1[2]), v2(p.v2[0], p.v2[1], p.v2[2]);
+            const V3<double> n = triangleNormal(v0, v1, v2);
+            const double tD = dot(v0 - q.od, n) / dot(V3<double>(q.d), n);
+            return fabs(tD - double(t)) <= 1e-3 * (1 + fabs(double(t))) ? tD : double(t);
+        } else {
+            return double(t);
+        }
+    }
+
     // Tests primitive slot i; true when its crossing was accepted as the new closest.
     __device__ __forceinline__ bool testPrim(const DeviceScene& sc, uint32_t i) {
         V3<T> v0, v1, v2;
@@ -499,8 +522,10 @@ struct Traversal {
             if (!acceptCrossing<T, Full>(sc, q, b, prim, true, t, n)) return false;
             if constexpr (Full) {
                 const T c = fabs(dn) / sqrt(dot(n, n));
-                if (!winsContact(sc, b, t, dn < T(0), c, flags)) return false;
+                const double tD = refinedTriangleT(sc, i, t);
+                if (!winsContact(sc, b, t, tD, dn < T(0), c, flags)) return false;
                 bestCos = c;
+                bestD = tD;
             }
             best = t;
             hit.t = double(t);
@@ -509,8 +534,9 @@ struct Traversal {
             const AnalyticResult<Rr> ar = analyticHit<T, R, Rr, Full>(sc.self, b, q.od, q.d, limit, q.depB, q.region, q.errN);
             if (!ar.ok) return false;
             if constexpr (Full) {
-                if (!winsContact(sc, b, T(ar.t), ar.front, T(ar.cosAbs), flags)) return false;
+                if (!winsContact(sc, b, T(ar.t), double(ar.t), ar.front, T(ar.cosAbs), flags)) return false;
                 bestCos = T(ar.cosAbs);
+                bestD = double(ar.t);
             }
             best = T(ar.t);
             hit.t = double(ar.t);

@@ -370,6 +370,20 @@ __global__ void __launch_bounds__(128, OWEC_SHADING_MIN_BLOCKS) kMedium(DeviceSc
 #ifndef OWEC_SIMPLE_MIN_BLOCKS
 #define OWEC_SIMPLE_MIN_BLOCKS 4
 #endif
+// One inconsistent crossing into the scene's event log: the boundary, triangle and hit flags, the
+// ray's region and the region its crossing met, the boundary and triangle the ray left, the path's
+// depth, the distance, the ray's camera-relative origin and direction, and its anchor error.
+template <class R>
+__device__ __noinline__ void logInconsistency(const DeviceScene& sc, const PathRay<R>& ray, const HitRec& h, uint32_t inc,
+                                              uint32_t depth) {
+    const uint32_t k = atomicAdd(sc.eventLogCount, 1u);
+    if (k >= sc.eventLogCap) return;
+    const double rec[kEventRecord] = {double(h.boundary), double(h.prim), double(h.flags), double(ray.region), double(inc),
+                                      double(ray.depB), double(ray.depP), double(depth), h.t, ray.o[0], ray.o[1], ray.o[2],
+                                      double(ray.d[0]), double(ray.d[1]), double(ray.d[2]), double(ray.errN)};
+    for (int j = 0; j < kEventRecord; ++j) sc.eventLog[size_t(k) * kEventRecord + j] = rec[j];
+}
+
 template <int M, bool Simple, bool Full>
 __global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SHADING_MIN_BLOCKS) kSurface(DeviceScene sc, PassParams pp, PathBuffers<RT<M>> pb, Queues q,
                                                 int cur, StatCounters* st) {
@@ -396,6 +410,9 @@ __global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SH
         // an undecided contact counts as inconsistent and ends the path (transport.cpp:503)
         const bool ambiguous = Full && (h.flags & kHitAmbiguous);
         const bool inconsistent = inc != ray.region || ambiguous;
+        if constexpr (Full) {
+            if (inconsistent && sc.eventLog) logInconsistency(sc, ray, h, inc, aux.depth);
+        }
         ray.region = inc;
         aux.lastBoundary = h.boundary;
         const bool specular = aux.flags & kFlagSpecular;

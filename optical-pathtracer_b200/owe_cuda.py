@@ -149,6 +149,23 @@ class Context:
                "owec_trace_launch_queries")
         return [int(out[k]) for k in range(min(256, n.value))]
 
+    INCONSISTENCY_FIELDS = ("boundary", "prim", "flags", "region", "met", "dep_boundary", "dep_prim", "depth", "t",
+                            "ox", "oy", "oz", "dx", "dy", "dz", "err_n")
+
+    def inconsistency_log(self, capacity):
+        """Record up to `capacity` crossings that meet a region other than the ray's (0 stops)."""
+        _check(self.lib, self.lib.owec_inconsistency_log(self.handle, int(capacity)), "owec_inconsistency_log")
+        self._event_cap = int(capacity)
+
+    def read_inconsistency_log(self):
+        """(records as an n x 16 array, fields INCONSISTENCY_FIELDS; crossings logged in all)."""
+        cap = getattr(self, "_event_cap", 0)
+        out = np.zeros((max(cap, 1), 16))
+        n = ctypes.c_int()
+        _check(self.lib, self.lib.owec_read_inconsistency_log(self.handle, out.ctypes.data_as(A.c_double_p), cap,
+                                                              ctypes.byref(n)), "owec_read_inconsistency_log")
+        return out[:min(cap, n.value)], n.value
+
     def walk(self, desc, first, n):
         """n forward light walks (walk indices first .. first + n - 1) binned on desc.target."""
         self._walk_shape = (desc.height, desc.width)

@@ -185,10 +185,11 @@ def block_z_test(runs_a, runs_b, block=6):
         by, bx = (h + block - 1) // block, (w + block - 1) // block
         out = np.zeros((by, bx, 3))
         cnt = np.zeros((by, bx, 1))
-        for y in range(h):
-            for x in range(w):
-                out[y // block, x // block] += img[y, x]
-                cnt[y // block, x // block] += 1
+        yi = (np.arange(h) // block)[:, None]
+        xi = (np.arange(w) // block)[None, :]
+        cell = (yi * bx + xi).ravel()
+        np.add.at(out.reshape(-1, 3), cell, img.reshape(-1, 3))
+        np.add.at(cnt.reshape(-1, 1), cell, 1.0)
         return (out / np.maximum(cnt, 1)).ravel()
 
     def mean_se(xs):
