@@ -434,10 +434,38 @@ struct Traversal {
         return kTraceRunning;
     }
 
-    // How far beyond the closest crossing the contact-resolving traversal still looks: the tie
-    // window, widened by the closest crossing's grazing incidence (coincident faces' distances differ
-    // by their offsets' rounding over the cosine).
-    __device__ __forceinline__ T tieSpan(T c) const { return best * tieWindow<T>() / fmax(c, T(1e-3)); }
+    // Contact decisions compare FP64 distances where the instantiation has them: the FP64 one, and
+    // FP32 traversal with FP64 refinement (triangles' distances from their FP64 vertices and the FP64
+    // origin, analytic roots refined in FP64). Plain FP32 compares its own distances.
+    static constexpr bool kExactTies = sizeof(T) == sizeof(double) || sizeof(Rr) == sizeof(double);
+
+    // The magnitude of the coordinates a crossing's distance is computed from (origin and hit point).
+    __device__ __forceinline__ double coordScale() const {
+        return fmax(fmax(fabs(q.od.x), fabs(q.od.y)), fabs(q.od.z)) + fmin(bestD, 1e30);
+    }
+
+    // The tie window of two crossings' distances: coincident faces' distances differ by the rounding
+    // of their offsets over the cosine of incidence. With FP64 distances, the reference's contact
+    // error, 64 ulps of the coordinates' magnitude (contactError, src/owe/core/math.hpp:15,
+    // NearestCrossing::offer, src/owe/scene/world.cpp:526); plain FP32 keeps a relative window.
+    __device__ __forceinline__ double tieSpanD(T c) const {
+        if constexpr (kExactTies) return 64 * 2.220446049250313e-16 * fmax(coordScale(), 1e-3) / fmax(double(c), 1e-3);
+        else return bestD * double(tieWindow<T>()) / fmax(double(c), 1e-3);
+    }
+
+    // How far beyond the closest crossing the contact-resolving traversal still looks (node culling
+    // and the crossings it admits): the tie window in the traversal's precision, and with FP64
+    // decisions at least the FP64 window plus, for FP32 traversal, its distances' own rounding (a few
+    // ulps of the coordinates' magnitude), so that every near tie reaches the FP64 test.
+    __device__ __forceinline__ T tieSpan(T c) const {
+        T s = best * tieWindow<T>();
+        if constexpr (kExactTies) {
+            const T scale = T(fmax(coordScale(), 1e-3));
+            s += T(64 * 2.220446049250313e-16) * scale;
+            if constexpr (sizeof(T) == sizeof(float)) s += T(1e-6) * scale;
+        }
+        return s / fmax(c, T(1e-3));
+    }
     __device__ __forceinline__ T tieLimit() const { return best + tieSpan(bestCos); }
 
     // Whether boundary b's crossing at t, met from its front side when `front` at incidence |cos| c,
@@ -446,17 +474,13 @@ struct Traversal {
     // one contact: the one met from the ray's region wins, matter wins over a zero-thickness
     // readout, then the lower boundary index; two that both match leave the order undecided
     // (kHitAmbiguous). `flags` receives the winner's flags.
-    __device__ __forceinline__ bool winsContact(const DeviceScene& sc, uint32_t b, T t, double tD, bool front, T c,
+    __device__ __forceinline__ bool winsContact(const DeviceScene& sc, uint32_t b, double tD, bool front, T c,
                                                 uint32_t& flags) {
         const uint32_t frontFlag = front ? kHitFront : 0u;
-        const T span = tieSpan(fmin(c, bestCos));
-        if (!found || t < best - span || b == hit.boundary) {
+        // outside the tie window, or two crossings of one boundary: the nearer one
+        if (!found || b == hit.boundary || !(fabs(tD - bestD) <= tieSpanD(fmin(c, bestCos)))) {
             flags = frontFlag;
-            if (!found) return true;
-            // two crossings of one boundary within the span (the faces of a plate thinner than the
-            // FP32 distances resolve) go in the order of their refined distances
-            if (b == hit.boundary && fabs(t - best) <= span) return tD < bestD;
-            return t < best;
+            return !found || tD < bestD;
         }
         const bool hinted = q.region != kNone;
         auto incident = [&](uint32_t bb, bool fr) {
@@ -523,7 +547,7 @@ struct Traversal {
             if constexpr (Full) {
                 const T c = fabs(dn) / sqrt(dot(n, n));
                 const double tD = refinedTriangleT(sc, i, t);
-                if (!winsContact(sc, b, t, tD, dn < T(0), c, flags)) return false;
+                if (!winsContact(sc, b, tD, dn < T(0), c, flags)) return false;
                 bestCos = c;
                 bestD = tD;
             }
@@ -534,7 +558,7 @@ struct Traversal {
             const AnalyticResult<Rr> ar = analyticHit<T, R, Rr, Full>(sc.self, b, q.od, q.d, limit, q.depB, q.region, q.errN);
             if (!ar.ok) return false;
             if constexpr (Full) {
-                if (!winsContact(sc, b, T(ar.t), double(ar.t), ar.front, T(ar.cosAbs), flags)) return false;
+                if (!winsContact(sc, b, double(ar.t), ar.front, T(ar.cosAbs), flags)) return false;
                 bestCos = T(ar.cosAbs);
                 bestD = double(ar.t);
             }

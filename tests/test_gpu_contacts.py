@@ -37,10 +37,59 @@ def test_touching_blocks_and_thin_plates_like_the_reference(thickness):
             for key in st:
                 st[key] += gs[key]
     save_artifact(f"contacts_{thickness:g}", ref=np.array(runs_ref), gpu=np.array(runs_gpu))
-    # The reference's paths meet no inconsistent region. On the device about two in 10^4 still do:
-    # the bound is one path in 10^3. Before contacts were resolved one path in ten did.
+    # The reference's paths meet no inconsistent region. On the device in mixed precision about one
+    # in 10^6 still does (a crossing whose FP32 distance the traversal culled before the FP64 tie
+    # test saw it): the bound is one in 10^5. Before contacts were resolved one path in ten did;
+    # with ties decided on FP32 distances, about one in 7000.
     assert ref_stats["inconsistencies"] == 0 and ref_stats["leaks"] == 0, ref_stats
-    assert st["inconsistencies"] + st["leaks"] <= 1e-3 * st["paths"], st
+    assert st["inconsistencies"] + st["leaks"] <= 1e-5 * st["paths"], st
     assert st["device_faults"] == 0, st
     ok, rep = block_z_test(runs_ref, runs_gpu)
     assert ok, rep
+
+
+@pytest.mark.parametrize("gap", [0.0, 1e-3])
+def test_fp64_contacts_meet_no_inconsistent_region(gap):
+    """With FP64 distances and the reference's contact window the device's paths meet no inconsistent
+    region on touching blocks standing on the floor, for plates of 0.2 m, 0.1 mm and 1 um."""
+    for thickness in (0.2, 1e-4, 1e-6):
+        desc = scenes.touching_glass(thickness=thickness, gap=gap).desc()
+        with owe_cuda.Context() as c:
+            c.upload(desc)
+            c.build_bvh()
+            c.set_settings(A.make_settings(seed=20, max_depth=24, precision=A.PRECISION_FP64))
+            c.reset_film()
+            c.run_pass(512)
+            st = c.stats()
+        assert st["inconsistencies"] == 0 and st["leaks"] == 0 and st["device_faults"] == 0, (thickness, st)
+
+
+def test_inconsistency_log_records_what_the_statistics_count():
+    """owec_inconsistency_log on overlapping blocks (the second block starts 0.1 inside the first, so
+    a ray inside the first meets the second's face from a region that face does not bound): the
+    log's count equals the transport statistics' inconsistencies, each record names a boundary and
+    regions of the scene, a positive distance and a met region other than the ray's; once stopped,
+    the log records nothing."""
+    desc = scenes.touching_glass(gap=-0.1).desc()
+    with owe_cuda.Context() as c:
+        c.upload(desc)
+        c.build_bvh()
+        c.set_settings(A.make_settings(seed=3, max_depth=24))
+        c.inconsistency_log(1 << 16)
+        c.reset_film()
+        c.run_pass(64)
+        rec, n = c.read_inconsistency_log()
+        st = c.stats()
+        assert n == st["inconsistencies"] and n > 0, (n, st)
+        assert len(rec) == min(n, 1 << 16)
+        F = owe_cuda.Context.INCONSISTENCY_FIELDS
+        for r in rec:
+            r = dict(zip(F, r))
+            assert 0 <= r["boundary"] < desc.n_boundaries, r
+            assert 0 <= r["region"] < desc.n_regions and 0 <= r["met"] < desc.n_regions, r
+            assert r["t"] > 0 and (r["met"] != r["region"] or int(r["flags"]) & 2), r
+        c.inconsistency_log(0)
+        c.reset_film()
+        c.run_pass(16)
+        rec2, n2 = c.read_inconsistency_log()
+        assert n2 == 0 and len(rec2) == 0
