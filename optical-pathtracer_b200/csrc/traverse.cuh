@@ -441,7 +441,7 @@ struct Traversal {
 
     // The magnitude of the coordinates a crossing's distance is computed from (origin and hit point).
     __device__ __forceinline__ double coordScale() const {
-        return fmax(fmax(fabs(q.od.x), fabs(q.od.y)), fabs(q.od.z)) + fmin(bestD, 1e30);
+        return fmax(fmax(fabs(q.od.x), fabs(q.od.y)), fabs(q.od.z)) + fmin(fabs(bestD), 1e30);
     }
 
     // The tie window of two crossings' distances: coincident faces' distances differ by the rounding
@@ -450,7 +450,7 @@ struct Traversal {
     // NearestCrossing::offer, src/owe/scene/world.cpp:526); plain FP32 keeps a relative window.
     __device__ __forceinline__ double tieSpanD(T c) const {
         if constexpr (kExactTies) return 64 * 2.220446049250313e-16 * fmax(coordScale(), 1e-3) / fmax(double(c), 1e-3);
-        else return bestD * double(tieWindow<T>()) / fmax(double(c), 1e-3);
+        else return fabs(bestD) * double(tieWindow<T>()) / fmax(double(c), 1e-3);
     }
 
     // How far beyond the closest crossing the contact-resolving traversal still looks (node culling
@@ -458,7 +458,8 @@ struct Traversal {
     // decisions at least the FP64 window plus, for FP32 traversal, its distances' own rounding (a few
     // ulps of the coordinates' magnitude), so that every near tie reaches the FP64 test.
     __device__ __forceinline__ T tieSpan(T c) const {
-        T s = best * tieWindow<T>();
+        // |best|: a crossing just behind the anchor (a contact through it) may be the closest
+        T s = fabs(best) * tieWindow<T>();
         if constexpr (kExactTies) {
             const T scale = T(fmax(coordScale(), 1e-3));
             s += T(64 * 2.220446049250313e-16) * scale;
