@@ -337,6 +337,15 @@ int owec_pass(owec_ctx* ctx, int spp);
  * With OWEC_INTEGRATOR_LIGHT the image is the particle splats over the particles emitted
  * (GpuRenderer::resolve, gpu_renderer_film.cpp:17-21) and `samples` is spp summed over the passes. */
 int owec_resolve(owec_ctx* ctx, double* xyz, double* samples);
+/* owec_resolve without the wait: the image of the passes run so far is formed on the device at once
+ * (later passes do not change it) and copied into xyz / samples by a second stream while the caller
+ * runs the next passes; owec_resolve_wait returns when every copy started has landed. The buffers
+ * must stay valid until then and be page-locked for the copy to overlap (cudaHostAlloc). Two images
+ * are kept on the device, so a render loop can start a resolve after every pass: a call waits for
+ * the copy it would overwrite, started two calls before (in such a loop it ended during the pass in
+ * between). No counterpart in the reference, whose Renderer::resolve returns the image. */
+int owec_resolve_async(owec_ctx* ctx, double* xyz, double* samples);
+int owec_resolve_wait(owec_ctx* ctx);
 /* The film as sums: the compensated per-pixel XYZ sums (3 doubles, row-major) and the samples per
  * pixel, which the ranks of a multi-GPU render add up before dividing. No counterpart in the
  * reference, which renders on one device. Either pointer may be NULL. With OWEC_INTEGRATOR_LIGHT the

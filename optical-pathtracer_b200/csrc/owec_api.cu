@@ -421,6 +421,12 @@ struct owec_ctx {
     uint64_t passCount = 0;  // samples per pixel accumulated (the PCG32 stream of the next sample)
     DBuf<double> dFilm, dComp, dSamples;
     DBuf<double> dResolved;  // owec_resolve's per-pixel XYZ, read back in one copy
+    // owec_resolve_async: two device images (XYZ, then samples) that a copy stream reads back while
+    // later passes run, each read-back ordered after its image by an event
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t resolvedEv[2] = {nullptr, nullptr};
+    DBuf<double> dResolvedAsync[2];
+    int asyncSlot = 0;
     DBuf<unsigned long long> dSplat;  // the light integrator's film: fixed-point splat sums
     double particles = 0;             // particles emitted into it
     DBuf<uint8_t> dPathRay, dPathSpec, dPathAux, dHit, dShadow;
@@ -1461,6 +1467,11 @@ int owec_close(owec_ctx* ctx) {
     return guarded([&] {
         cudaSetDevice(ctx->device);
         cudaStreamSynchronize(ctx->stream);
+        if (ctx->copyStream) {
+            cudaStreamSynchronize(ctx->copyStream);
+            for (int k = 0; k < 2; ++k) cudaEventDestroy(ctx->resolvedEv[k]);
+            cudaStreamDestroy(ctx->copyStream);
+        }
         for (cudaEvent_t e : ctx->travEvents) cudaEventDestroy(e);
         cudaEventDestroy(ctx->passStart);
         cudaEventDestroy(ctx->passStop);
@@ -1583,6 +1594,54 @@ int owec_resolve(owec_ctx* ctx, double* xyz, double* samples) {
         if (samples)
             OWEC_CUDA(cudaMemcpyAsync(samples, ctx->dSamples.get(), np * 8, cudaMemcpyDeviceToHost, ctx->stream));
         OWEC_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int owec_resolve_async(owec_ctx* ctx, double* xyz, double* samples) {
+    return guarded([&] {
+        require(ctx != nullptr, "owec_resolve_async: null context");
+        require(ctx->hasScene, "no scene uploaded", OWEC_E_STATE);
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        ensureFilm(*ctx);
+        if (!ctx->copyStream) {
+            OWEC_CUDA(cudaStreamCreateWithFlags(&ctx->copyStream, cudaStreamNonBlocking));
+            for (int k = 0; k < 2; ++k) OWEC_CUDA(cudaEventCreateWithFlags(&ctx->resolvedEv[k], cudaEventDisableTiming));
+        }
+        const size_t np = size_t(ctx->ds.det.width) * ctx->ds.det.height;
+        const int slot = ctx->asyncSlot;
+        ctx->asyncSlot ^= 1;
+        DBuf<double>& img = ctx->dResolvedAsync[slot];
+        // the slot's previous read-back (two calls ago) must end before its image is overwritten or
+        // resized; in a render loop it ended during the pass since
+        OWEC_CUDA(cudaStreamSynchronize(ctx->copyStream));
+        img.reserve(4 * np);
+        const bool light = ctx->settings.integrator == OWEC_INTEGRATOR_LIGHT;
+        if (xyz) {
+            if (light)
+                launchResolveSplats(ctx->dSplat.get(), uint32_t(np), ctx->particles > 0 ? 1.0 / ctx->particles : 0.0,
+                                    img.get(), ctx->stream);
+            else
+                launchResolve(ctx->dFilm.get(), ctx->dComp.get(), ctx->dSamples.get(), uint32_t(np), img.get(), ctx->stream);
+            checkLaunch();
+        }
+        if (samples && !light)
+            OWEC_CUDA(cudaMemcpyAsync(img.get() + 3 * np, ctx->dSamples.get(), np * 8, cudaMemcpyDeviceToDevice,
+                                      ctx->stream));
+        if (samples && light) std::fill(samples, samples + np, ctx->particles / double(np));
+        // the read-back waits for the image, not for the passes queued after it
+        OWEC_CUDA(cudaEventRecord(ctx->resolvedEv[slot], ctx->stream));
+        OWEC_CUDA(cudaStreamWaitEvent(ctx->copyStream, ctx->resolvedEv[slot], 0));
+        if (xyz) OWEC_CUDA(cudaMemcpyAsync(xyz, img.get(), 3 * np * 8, cudaMemcpyDeviceToHost, ctx->copyStream));
+        if (samples && !light)
+            OWEC_CUDA(cudaMemcpyAsync(samples, img.get() + 3 * np, np * 8, cudaMemcpyDeviceToHost, ctx->copyStream));
+    });
+}
+
+int owec_resolve_wait(owec_ctx* ctx) {
+    return guarded([&] {
+        require(ctx != nullptr, "owec_resolve_wait: null context");
+        OWEC_CUDA(cudaSetDevice(ctx->device));
+        if (ctx->copyStream) OWEC_CUDA(cudaStreamSynchronize(ctx->copyStream));
     });
 }
 

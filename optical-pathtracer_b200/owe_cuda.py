@@ -88,6 +88,23 @@ class Context:
                                                cnt.ctypes.data_as(A.c_double_p) if samples else None), "owec_resolve")
         return xyz.reshape(self.height, self.width, 3), (cnt.reshape(self.height, self.width) if samples else None)
 
+    def resolve_async(self, out, samples=None):
+        """Starts the resolve of the passes run so far into `out` (a C-contiguous float64 array of
+        height x width x 3, page-locked for the copy to overlap later passes) and `samples` (height x
+        width, or None) without waiting (owec_resolve_async); resolve_wait() waits for the copies.
+        The arrays must stay alive until then."""
+        n = self.width * self.height
+        if not (out.dtype == np.float64 and out.flags.c_contiguous and out.size == 3 * n):
+            raise ValueError("resolve_async: out must be a C-contiguous float64 array of height x width x 3")
+        if samples is not None and not (samples.dtype == np.float64 and samples.flags.c_contiguous and samples.size == n):
+            raise ValueError("resolve_async: samples must be a C-contiguous float64 array of height x width")
+        _check(self.lib, self.lib.owec_resolve_async(self.handle, out.ctypes.data_as(A.c_double_p),
+                                                     samples.ctypes.data_as(A.c_double_p) if samples is not None else None),
+               "owec_resolve_async")
+
+    def resolve_wait(self):
+        _check(self.lib, self.lib.owec_resolve_wait(self.handle), "owec_resolve_wait")
+
     def read_film(self):
         """(compensated XYZ sums (height, width, 3), samples per pixel (height, width))."""
         n = self.width * self.height
@@ -312,6 +329,14 @@ class Renderer:
         """Per-pixel mean XYZ, shape (height, width, 3) (Renderer::resolve), written into `out` when
         given."""
         return self.ctx.resolve(samples=False, out=out)[0]
+
+    def resolve_async(self, out):
+        """Renderer::resolve into `out` (page-locked, height x width x 3 float64) without waiting: the
+        copy overlaps the passes run next; resolve_wait() waits for it."""
+        self.ctx.resolve_async(out)
+
+    def resolve_wait(self):
+        self.ctx.resolve_wait()
 
     def passes(self):
         return self._passes

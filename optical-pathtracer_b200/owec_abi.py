@@ -214,6 +214,8 @@ def load_library(path=LIB_PATH):
         "owec_trace_launch_queries": ([P, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
                                       ctypes.c_int),
         "owec_inconsistency_log": ([P, ctypes.c_int], ctypes.c_int),
+        "owec_resolve_async": ([P, c_double_p, c_double_p], ctypes.c_int),
+        "owec_resolve_wait": ([P], ctypes.c_int),
         "owec_read_inconsistency_log": ([P, c_double_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
         "owec_walk": ([P, ctypes.POINTER(WalkDesc), ctypes.c_uint64, ctypes.c_uint64], ctypes.c_int),
         "owec_walk_resolve": ([P, c_double_p, ctypes.POINTER(WalkStats)], ctypes.c_int),

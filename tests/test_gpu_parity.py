@@ -178,6 +178,33 @@ def test_film_is_deterministic_and_passes_accumulate():
     assert np.array_equal(a, b), "a pass split into sub-passes must give the same film, bit for bit"
 
 
+@pytest.mark.parametrize("integrator", [A.INTEGRATOR_PATH, A.INTEGRATOR_LIGHT])
+def test_resolve_async_in_a_render_loop_matches_resolve(integrator):
+    """owec_resolve_async after every pass of a loop, each image into its own page-locked buffer
+    while the next passes run: every image equals the synchronous resolve of the same passes, bit
+    for bit, and so do the sample counts."""
+    import torch
+    desc = scenes.lamp_over_floor(64, 48).desc()
+    s = A.make_settings(seed=31, integrator=integrator)
+    sync_imgs, sync_cnts = [], []
+    with _ctx(desc, s) as c:
+        for _ in range(5):
+            c.run_pass(2)
+            img, cnt = c.resolve()
+            sync_imgs.append(img.copy())
+            sync_cnts.append(cnt.copy())
+    outs = [torch.empty((48, 64, 3), dtype=torch.float64, pin_memory=True).numpy() for _ in range(5)]
+    cnts = [torch.empty((48, 64), dtype=torch.float64, pin_memory=True).numpy() for _ in range(5)]
+    with _ctx(desc, s) as c:
+        for k in range(5):
+            c.run_pass(2)
+            c.resolve_async(outs[k], cnts[k])
+        c.resolve_wait()
+    for k in range(5):
+        assert np.array_equal(outs[k], sync_imgs[k]), k
+        assert np.array_equal(cnts[k], sync_cnts[k]), k
+
+
 def test_small_film_folds_many_samples_like_one_sample_passes():
     """A 16 x 16 film of 300 samples per pixel in one pass (the block-per-pixel fold) equals the same
     samples in ten passes of 30 (the thread-per-pixel fold), bit for bit."""
