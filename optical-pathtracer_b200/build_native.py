@@ -65,10 +65,14 @@ def build(verbose=True, ptxas_info=False):
         msg = "\n".join(" ".join(c) + "\n" + out for c, out in failed)
         raise RuntimeError("CUDA compilation failed:\n" + msg)
     if jobs or not os.path.exists(LIB):
-        cmd = [nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs
+        # linked under another name and renamed over the library in one step, so that a process
+        # loading it (or a copy of the tree) never sees a partly written file
+        tmp = LIB + ".partial"
+        cmd = [nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+        os.replace(tmp, LIB)
     return LIB
 
 

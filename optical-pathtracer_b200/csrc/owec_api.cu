@@ -1034,7 +1034,19 @@ void ensurePrims64(owec_ctx& c);
 
 void buildBvh(owec_ctx& c) {
     require(c.hasScene, "no scene uploaded", OWEC_E_STATE);
-    require(c.nPrims > 0, "the scene has no boundaries");
+    if (c.nPrims == 0) {
+        // nothing to meet (a sky or a sun alone): no tree, and every traversal misses at once
+        // (Traversal::run returns before it reads a node when the tree is empty)
+        c.nNodes = 0;
+        c.ds.nodes = nullptr;
+        c.ds.prims = nullptr;
+        c.ds.prims64 = nullptr;
+        c.ds.nNodes = 0;
+        c.ds.nPrims = 0;
+        c.bvhDirty = false;
+        c.prims64Ready = true;
+        return;
+    }
     c.nNodes = buildWideBvh(c.dPrimLo.get(), c.dPrimHi.get(), c.nPrims, c.scratch, c.dNodes, c.dLeafOrder, c.stream);
     c.dPrims.reserve(c.nPrims);
     launchMaterialize(c.dLeafOrder.get(), c.nPrims, c.dTri.get(), nullptr, c.dPrims.get(), nullptr, c.stream);
@@ -1050,7 +1062,7 @@ void buildBvh(owec_ctx& c) {
 }
 
 void ensurePrims64(owec_ctx& c) {
-    if (c.prims64Ready) return;
+    if (c.prims64Ready || c.nPrims == 0) return;
     c.dTri64.upload(c.tri64.data(), c.tri64.size(), c.stream);
     c.dPrims64.reserve(c.nPrims);
     launchMaterialize(c.dLeafOrder.get(), c.nPrims, c.dTri.get(), c.dTri64.get(), c.dPrims.get(), c.dPrims64.get(),
