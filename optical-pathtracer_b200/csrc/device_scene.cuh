@@ -103,6 +103,8 @@ struct DeviceScene {
     const DBoundary* boundaries;
     const DLight* lights;
     const double* shapeData;  // the shapes' data, addressed by DBoundary::dataOffset
+    int32_t simpleOptics;     // 1: every boundary Lambertian, absorbing or detecting, no null boundary,
+                              // no region's medium absorbs or scatters (the particles' lean event kernel)
     int32_t fullFeatures;     // 1: shapes beyond spheres, conic sags, plain apertures and cylinders, or
                               // textured materials (the kernels' Full instantiations)
     uint32_t nRegions, nBoundaries, nLights, nMedia;

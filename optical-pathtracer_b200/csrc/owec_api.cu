@@ -986,6 +986,21 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
     // is the FP32 anchor error over the scene's extent
     c.contacts = hasContacts(d, 1e-5 * std::max(2 * sceneRadius, 1e-3));
     if (c.contacts) ds.fullFeatures = 1;
+    {
+        auto participates = [&](int32_t spectrum) {
+            return spectrum >= 0 && !(d.spectra[spectrum].kind == OWEC_SPEC_CONSTANT && d.spectra[spectrum].a == 0.0);
+        };
+        bool simple = !c.hasNull && !ds.fullFeatures;
+        for (uint32_t i = 0; i < d.n_boundaries && simple; ++i) {
+            const int32_t t = d.optics[d.boundaries[i].optics].type;
+            simple = t == OWEC_SURF_DIFFUSE || t == OWEC_SURF_ABSORBER || t == OWEC_SURF_DETECTOR;
+        }
+        for (uint32_t r = 0; r < d.n_regions && simple; ++r) {
+            const owec_medium& m = d.media[d.region_medium[r]];
+            simple = !participates(m.absorption) && !participates(m.scattering);
+        }
+        ds.simpleOptics = simple ? 1 : 0;
+    }
     ds.nRegions = d.n_regions;
     ds.nBoundaries = d.n_boundaries;
     ds.nLights = uint32_t(c.lights.size());

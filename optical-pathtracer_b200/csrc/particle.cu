@@ -317,9 +317,12 @@ __global__ void __launch_bounds__(128) kEmit(DeviceScene sc, ParticleParams P, P
 // connection at a scattering event), escape, the boundary (null crossing, sensor record,
 // absorption), the connection of a non-delta surface vertex and the importance-transport
 // scattering sample with roulette (traceParticle's loop body, particle.slang:365-426).
-template <int M, bool Full>
-__global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, ParticleParams P, PathBuffers<RT<M>> pb,
-                                                         Queues q, int cur, StatCounters* st, SplatTarget film) {
+// Lean: the instantiation for scenes of Lambertian, absorbing and detecting boundaries in regions
+// without participating media (DeviceScene::simpleOptics): the medium events, null boundaries and
+// the other lobes fold away, and with them the registers they hold.
+template <int M, bool Full, bool Lean>
+__global__ void __launch_bounds__(128, Lean ? 4 : 3) kParticleEvent(DeviceScene sc, ParticleParams P, PathBuffers<RT<M>> pb,
+                                                                   Queues q, int cur, StatCounters* st, SplatTarget film) {
     using R = RT<M>;
     using Ro = typename Mode<M>::Ro;
     using Rr = typename Mode<M>::Rr;
@@ -355,7 +358,8 @@ __global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, Particl
             const double seg = found ? h.t : INFINITY;
             int event = 0;  // 0 pass, 1 scatter, 2 end
             double tS = 0;
-            if (mediumScatters(med, sc)) {
+            if (Lean) {
+            } else if (mediumScatters(med, sc)) {
                 R sT[NW];
                 for (int j = 0; j < NW; ++j)
                     sT[j] = evalSpectrum(sc, med.absorption, R(sp.lambda[j])) + evalSpectrum(sc, med.scattering, R(sp.lambda[j]));
@@ -377,7 +381,7 @@ __global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, Particl
                     for (int j = 0; j < NW; ++j)
                         sp.beta[j] *= exp(-evalSpectrum(sc, med.absorption, R(sp.lambda[j])) * R(seg));
             }
-            if (event == 1) {
+            if (!Lean && event == 1) {
                 // a scattering event in the medium: its connection, then Henyey-Greenstein
                 const V3<double> x = plainPoint<M>(o + V3<double>(d) * tS);
                 if (observer && linkObserver(sc, P, x, rng, k)) {
@@ -418,7 +422,7 @@ __global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, Particl
                 const V3<double> gp = plainPoint<M>(g.p);
                 const float errG = anchorError<R>(g.p);
                 if (ambiguous) {
-                } else if (op.type == OWEC_SURF_NULL) {
+                } else if (!Lean && op.type == OWEC_SURF_NULL) {
                     ray.region = other;
                     ray.o[0] = gp.x; ray.o[1] = gp.y; ray.o[2] = gp.z;
                     ray.depB = h.boundary;
@@ -448,15 +452,15 @@ __global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, Particl
                     if (op.type != OWEC_SURF_DETECTOR && op.type != OWEC_SURF_ABSORBER) {
                         V3<double> texW;
                         const V3<double>* tex = hitTexture<Full>(sc, bd, g.pLocal, g.nLocal, texW);
-                        const Interface<R> it = makeInterface(sc, bd, g.n, R(sp.lambda[0]), R(P.fresnelFloor), tex);
-                        if (observer && !isDeltaOptics<R>(op) && linkObserver(sc, P, gp, rng, k)) {
+                        const Interface<R> it = makeInterface<R, Lean>(sc, bd, g.n, R(sp.lambda[0]), R(P.fresnelFloor), tex);
+                        if (observer && (Lean || !isDeltaOptics<R>(op)) && linkObserver(sc, P, gp, rng, k)) {
                             const V3<R> wo(k.dir);
                             bool any = false;
                             for (int j = 0; j < NW; ++j) {
                                 if (sp.beta[j] == R(0)) continue;
                                 R pdf;
                                 const Interface<R> itj =
-                                    j == 0 ? it : makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor), tex);
+                                    j == 0 ? it : makeInterface<R, Lean>(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor), tex);
                                 value[j] = sp.beta[j] * evalScatter(sc, itj, d, wo, false, pdf);
                                 any = any || value[j] != R(0);
                             }
@@ -472,7 +476,7 @@ __global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, Particl
                             }
                         }
                         if (depth < P.maxDepth) {
-                            if (op.type == OWEC_SURF_DIELECTRIC) {  // terminateIfDispersive (transport.cpp:216-225)
+                            if (!Lean && op.type == OWEC_SURF_DIELECTRIC) {  // terminateIfDispersive (transport.cpp:216-225)
                                 for (int j = 1; j < NW; ++j) {
                                     if (sp.pdf[j] == 0.f) continue;
                                     if (isDispersive(it, makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor), tex))) {
@@ -489,7 +493,7 @@ __global__ void __launch_bounds__(128, 3) kParticleEvent(DeviceScene sc, Particl
                                 sp.beta[0] *= ss.weight;
                                 for (int j = 1; j < NW; ++j) {
                                     if (sp.pdf[j] == 0.f) continue;
-                                    const Interface<R> itj = makeInterface(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor), tex);
+                                    const Interface<R> itj = makeInterface<R, Lean>(sc, bd, g.n, R(sp.lambda[j]), R(P.fresnelFloor), tex);
                                     sp.beta[j] *= secondaryScatterWeight(sc, itj, d, ss, false);
                                 }
                                 if (ss.transmitted) ray.region = other;
@@ -545,8 +549,9 @@ void launchEmit(const DeviceScene& sc, const ParticleParams& P, const PathBuffer
 template <int M>
 void launchParticleEvent(const DeviceScene& sc, const ParticleParams& P, const PathBuffers<ModeR<M>>& pb,
                          const Queues& q, int cur, StatCounters* st, const SplatTarget& film, int grid, cudaStream_t s) {
-    if (sc.fullFeatures) kParticleEvent<M, true><<<grid, 128, 0, s>>>(sc, P, pb, q, cur, st, film);
-    else kParticleEvent<M, false><<<grid, 128, 0, s>>>(sc, P, pb, q, cur, st, film);
+    if (sc.fullFeatures) kParticleEvent<M, true, false><<<grid, 128, 0, s>>>(sc, P, pb, q, cur, st, film);
+    else if (sc.simpleOptics) kParticleEvent<M, false, true><<<grid, 128, 0, s>>>(sc, P, pb, q, cur, st, film);
+    else kParticleEvent<M, false, false><<<grid, 128, 0, s>>>(sc, P, pb, q, cur, st, film);
 }
 void launchResolveSplats(const unsigned long long* splat, uint32_t nPixels, double scale, double* xyz, cudaStream_t s) {
     kResolveSplats<<<(3 * nPixels + 255) / 256, 256, 0, s>>>(splat, nPixels, scale, xyz);
