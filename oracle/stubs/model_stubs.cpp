@@ -22,7 +22,7 @@ bool isGltf(const std::string& path) {
 }  // namespace
 
 MeshData loadGltf(const std::string& path, double) {
-    throw std::runtime_error("glTF models are not available in this build (no glTF decoder): " + path);
+    throw std::runtime_error("glTF models are not available in the oracle's build of the engine (no glTF decoder): " + path);
 }
 
 MeshData loadModel(const std::string& path, double scale) {
@@ -32,7 +32,7 @@ MeshData loadModel(const std::string& path, double scale) {
 
 MeshData selectParts(const MeshData& m, const std::vector<std::string>& names) {
     if (names.empty()) return m;
-    throw std::runtime_error("selecting named model parts needs the glTF decoder, absent in this build");
+    throw std::runtime_error("selecting named model parts needs the glTF decoder, absent from the oracle's build of the engine");
 }
 
 }  // namespace owe

@@ -1,6 +1,6 @@
 """The oracle itself (CPU): the reference engine built from its own sources drives the same scene
 descriptions the CUDA backend takes, and reproduces the reference's own known answers. These pin
-the harness before it judges the GPU."""
+the harness before it checks the GPU."""
 import math
 
 import numpy as np
@@ -12,7 +12,7 @@ from oracle_ref import ReferenceEngine
 
 
 def test_driver_pass_equals_the_reference_cpu_backend_bit_for_bit():
-    """The driver's pass loop (hero-4 wavelengths) is CpuRenderer::pass: identical films."""
+    """ref_driver.cpp's pass loop (hero-4 wavelengths) is CpuRenderer::pass: identical films."""
     desc = scenes.glass_sphere_on_floor(24, 24).desc()
     ref = ReferenceEngine(desc)
     s = A.make_settings(seed=3, max_depth=16, rr_depth=4)
