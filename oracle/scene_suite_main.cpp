@@ -1,0 +1,84 @@
+// Scene suite (test infrastructure): every scene file given on the command line, loaded by the
+// reference engine's own loader (src/owe/loader/scene_loader.hpp, built from its sources), rendered
+// on its `cpu` backend and on the `cuda` backend (the registry with cudaBackend() added, as in the
+// conformance build), and compared by the reference's own statistics (compareRenderers,
+// src/owe/backends/compare.cpp) at a reduced film size. The scenes are the reference's `scenes/`
+// and `benchmarks/` (the `owe bench` suites, benchmarks/suites.json).
+//
+// One line per scene and detector:
+//   LOAD-FAILED <file>: <why>            the reference itself cannot load it here (missing assets)
+//   REFUSED <file> <detector>: <why>     the cuda backend refuses a feature of the scene
+//   ok|FAIL <file> <detector>: <report>  the comparison (consistent() of ComparisonReport)
+// Exits 1 when any comparison fails, 0 otherwise.
+//
+// Usage: owe_scene_suite [--width W] [--spp S] [--runs R] [--all-detectors] FILE...
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <exception>
+#include <string>
+#include <vector>
+
+#include "owe/backends/compare.hpp"
+#include "owe/backends/registry.hpp"
+#include "owe/loader/scene_loader.hpp"
+
+using namespace owe;
+
+int main(int argc, char** argv) {
+    int width = 64, spp = 8, runs = 6;
+    bool allDetectors = false;
+    std::vector<std::string> files;
+    for (int i = 1; i < argc; ++i) {
+        const std::string a = argv[i];
+        if (a == "--width" && i + 1 < argc) width = std::atoi(argv[++i]);
+        else if (a == "--spp" && i + 1 < argc) spp = std::atoi(argv[++i]);
+        else if (a == "--runs" && i + 1 < argc) runs = std::atoi(argv[++i]);
+        else if (a == "--all-detectors") allDetectors = true;
+        else files.push_back(a);
+    }
+    int failures = 0;
+    for (const std::string& file : files) {
+        Scene sc;
+        try {
+            sc = loadScene(file);
+        } catch (const std::exception& e) {
+            std::printf("LOAD-FAILED %s: %s\n", file.c_str(), e.what());
+            std::fflush(stdout);
+            continue;
+        }
+        const int nd = allDetectors ? int(sc.detectors.size()) : std::min<int>(1, int(sc.detectors.size()));
+        if (nd == 0) {
+            std::printf("LOAD-FAILED %s: no detector\n", file.c_str());
+            continue;
+        }
+        for (int di = 0; di < nd; ++di) {
+            Detector& det = *sc.detectors[size_t(di)];
+            // the same measurement on a coarser film: the detector's aspect kept
+            const int w0 = det.width, h0 = det.height;
+            det.width = std::min(width, w0);
+            det.height = std::max(1, int(std::lround(double(h0) * det.width / std::max(1, w0))));
+            RenderSettings a = sc.settingsFor(di), b = a;
+            a.backend = "cpu";
+            b.backend = "cuda";
+            adaptToBackend(a);
+            adaptToBackend(b);
+            b.integrator = a.integrator;  // the one both implement: the comparison is like for like
+            try {
+                const ComparisonReport r = compareRenderers(sc, di, a, b, spp, runs, 4);
+                const bool ok = r.consistent();
+                if (!ok) ++failures;
+                std::printf("%s %s %s (%dx%d, %s): zImage %.2f, blocks over 4 sigma %d of %d, chi2/test %.2f, "
+                            "mean Y cpu %.6g cuda %.6g, %.2f s / %.2f s\n",
+                            ok ? "ok  " : "FAIL", file.c_str(), det.name.c_str(), det.width, det.height,
+                            a.integrator.c_str(), r.zImage, r.over4, r.tests, r.chi2PerTest, r.meanA, r.meanB,
+                            r.secondsA, r.secondsB);
+            } catch (const std::exception& e) {
+                std::printf("REFUSED %s %s: %s\n", file.c_str(), det.name.c_str(), e.what());
+            }
+            std::fflush(stdout);
+        }
+    }
+    return failures ? 1 : 0;
+}
