@@ -25,7 +25,7 @@ def test_reference_scene_files_render_alike_on_cuda():
     files = sorted(os.path.relpath(p, HERE) for pattern in ("scenes/*.owe", "scenes/*/*.owe", "benchmarks/*.owe",
                                                               "benchmarks/*/*.owe")
                    for p in glob.glob(os.path.join(HERE, pattern)))
-    r = subprocess.run([BIN, "--all-detectors"] + files, cwd=HERE, capture_output=True, text=True, timeout=1500)
+    r = subprocess.run([BIN, "--all-detectors", "--spp", "16", "--runs", "8"] + files, cwd=HERE, capture_output=True, text=True, timeout=1500)
     print(r.stdout)
     lines = r.stdout.splitlines()
     fails = [l for l in lines if l.startswith("FAIL")]
