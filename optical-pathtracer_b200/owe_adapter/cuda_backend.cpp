@@ -6,9 +6,10 @@
 // rule allows it core/, scene/, render/ and backends/cuda/ (not transport/). It flattens the world
 // model into owec_scene_desc: media, regions, optics, emitters, boundaries with their rigid frames
 // and shape data, the sun and sky, and the detector. Scenes using features the CUDA backend does not
-// implement (image textures and maps, environment maps, stained glass) are refused with
+// implement (image albedo textures, environment maps, stained glass) are refused with
 // std::runtime_error, as Backend::createRenderer does for unsupported settings
-// (src/owe/render/backend.hpp:44).
+// (src/owe/render/backend.hpp:44); the material maps only the reference GPU renderer applies
+// (relief, roughness maps, normal and roughness images) are left out, as its CPU transport leaves them.
 #include <cmath>
 #include <cstring>
 #include <initializer_list>
@@ -126,9 +127,12 @@ std::unique_ptr<Flat> flatten(const Scene& sc, int detectorIndex) {
     }
     for (const Region& r : w.regions()) f->regionMedium.push_back(r.medium);
     for (const SurfaceOptics& so : w.optics()) {
-        if (so.texture.kind == Texture::Kind::Image || !so.roughnessMap.empty() || so.reliefDepth != 0 ||
-            so.normalImage.image || so.roughnessImage.image)
-            throw std::runtime_error("material '" + so.name + "' uses image textures or maps, which the cuda backend does not render");
+        // A surface relief, roughness maps and normal or roughness images are the reference GPU
+        // renderer's alone (SurfaceOptics, src/owe/scene/world.hpp:88-100): the CPU transport, which
+        // this backend follows, renders such a material without them, and so does this backend. An
+        // image albedo texture the CPU transport does render; this backend does not.
+        if (so.texture.kind == Texture::Kind::Image)
+            throw std::runtime_error("material '" + so.name + "' uses an image texture, which the cuda backend does not render");
         if (so.type == SurfaceType::StainedGlass) throw std::runtime_error("stained glass is not rendered by the cuda backend");
         owec_optics o{};
         o.type = int32_t(so.type);

@@ -76,6 +76,8 @@ class Context:
         """(per-pixel mean XYZ (height, width, 3), per-pixel sample counts or None). `out`: a
         C-contiguous float64 array of height x width x 3 values to write the image into (pinned
         host memory reads back fastest)."""
+        if not hasattr(self, "width"):
+            raise RuntimeError("owec_resolve: no scene uploaded")
         n = self.width * self.height
         if out is not None:
             if not (out.dtype == np.float64 and out.flags.c_contiguous and out.size == 3 * n):

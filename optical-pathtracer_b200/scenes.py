@@ -642,6 +642,22 @@ def caustic_room(width=1920, height=1080, n_lon=1024, n_lat=512, panel_n=1024, h
                 "thickness": panel_thickness, "view": ((0.3, -2.7, 1.6), (0.2, -0.2, 0.6), (0, 0, 1), 50.0)}
 
 
+def planetary_ground(width=64, height=64, radius=6371000.0):
+    """The reference's planetary-surface regression (benchmarks/regressions/planetary_ground.owe):
+    the ground is a sphere of the Earth's radius whose top lies 0.2 m below the origin, a 5 cm marker
+    sphere stands near the origin, the sun at 45 degrees elevation behind the camera and a dim
+    uniform sky; a pinhole looks down at the marker. A ray leaving the ground starts |o| = R from the
+    sphere's centre, where single precision cannot tell the surface from a metre off it."""
+    sb = SceneBuilder()
+    sb.uniform_sky(0.1)
+    sb.sun((0.0, -math.sqrt(0.5), math.sqrt(0.5)), 1.0e4)
+    opaque = sb.medium_opaque()
+    sb.sphere_body(radius, (0.0, 0.0, -radius - 0.2), opaque, sb.diffuse(0.3))
+    sb.sphere_body(0.05, (0.0, 0.0, 0.05), opaque, sb.diffuse(0.4))
+    sb.observer(width, height, (0.0, -0.7, 0.4), (0.0, 0.0, -0.1), fov_y_deg=35.0)
+    return sb
+
+
 def reflected_moonlight(width=16, height=16):
     """The reference's conformance check of light reflected by a distant body (tests/test_backends.cpp:
     69-97): a white two-sided Lambertian floor lit only by a full-phase Lambertian moon (albedo 0.3,
