@@ -123,6 +123,75 @@ OWEC_HD bool sphereRoots(const V3<T>& o, const V3<T>& d, T R, T& t0, T& t1) {
     return true;
 }
 
+// Double-double numbers (hi + lo, |lo| at most half an ulp of hi) built from the error-free
+// transformations: Knuth's two-sum for a sum, the fused multiply-add for the error of a product.
+struct DDouble {
+    double hi, lo;
+};
+OWEC_HD DDouble ddTwoSum(double a, double b) {
+    const double s = a + b, v = s - a;
+    return {s, (a - (s - v)) + (b - v)};
+}
+OWEC_HD DDouble ddAdd(const DDouble& a, const DDouble& b) {
+    const DDouble s = ddTwoSum(a.hi, b.hi);
+    return ddTwoSum(s.hi, s.lo + a.lo + b.lo);
+}
+OWEC_HD DDouble ddMul(const DDouble& a, const DDouble& b) {
+    const double p = a.hi * b.hi;
+    return ddTwoSum(p, fma(a.hi, b.hi, -p) + (a.hi * b.lo + a.lo * b.hi));
+}
+OWEC_HD DDouble ddNeg(const DDouble& a) { return {-a.hi, -a.lo}; }
+OWEC_HD double ddValue(const DDouble& a) { return a.hi + a.lo; }
+
+// Whether a ray from od lies near boundary b's sphere against the sphere's size (a planet's surface
+// under the camera): there |od - c|^2 - R^2 cancels to nothing in FP64 once od - c is rounded, and
+// the reference solves the quadratic in double-double arithmetic (needsNearSphere, intersectNearSphere,
+// src/owe/scene/world.cpp:404-438). The same switch.
+OWEC_HD bool nearSphere(const DBoundary& b, const V3<double>& od) {
+    if (b.shape != OWEC_SHAPE_SPHERE) return false;
+    const double R = b.params[0];
+    const V3<double> c(b.toWorld.m[3], b.toWorld.m[7], b.toWorld.m[11]);
+    return R > 4096 * fmax(1e-9, fabs(length(od - c) - R));
+}
+
+// The sphere's crossings in (tmin, tmax) for such a ray, in the world frame (a sphere's roots do not
+// depend on its frame's rotation): od - c exact as a double-double, the quadratic's coefficients in
+// double-double, the roots in the numerically stable form. Points and normals in the sphere's local
+// frame, as classicCrossings gives them (the normal from the exact od - c; the point converted from
+// the world point od + t d).
+OWEC_HD int nearSphereCrossings(const DBoundary& b, const V3<double>& od, const V3<double>& d, double tmin,
+                                       double tmax, AHits<double>& out) {
+    out.n = 0;
+    const double R = b.params[0];
+    const double o[3] = {od.x, od.y, od.z}, dv[3] = {d.x, d.y, d.z};
+    const double c[3] = {b.toWorld.m[3], b.toWorld.m[7], b.toWorld.m[11]};
+    DDouble rel[3], A{0, 0}, B{0, 0}, C{0, 0};
+    for (int k = 0; k < 3; ++k) {
+        rel[k] = ddTwoSum(o[k], -c[k]);
+        A = ddAdd(A, ddMul({dv[k], 0}, {dv[k], 0}));
+        B = ddAdd(B, ddMul(rel[k], {dv[k], 0}));
+        C = ddAdd(C, ddMul(rel[k], rel[k]));
+    }
+    C = ddAdd(C, ddNeg(ddMul({R, 0}, {R, 0})));
+    const double disc = ddValue(ddAdd(ddMul(B, B), ddNeg(ddMul(A, C))));
+    if (!(disc >= 0)) return 0;
+    const double bv = ddValue(B), av = ddValue(A);
+    const double q = -bv - copysign(sqrt(disc), bv);
+    double t0 = q / av, t1 = q != 0 ? ddValue(C) / q : t0;
+    if (t0 > t1) { const double tmp = t0; t0 = t1; t1 = tmp; }
+    const double ts[2] = {t0, t1};
+    for (int i = 0; i < 2; ++i) {
+        const double t = ts[i];
+        if (!(t > tmin && t < tmax) || (i == 1 && t1 == t0)) continue;
+        V3<double> nw;
+        nw.x = ddValue(ddAdd(rel[0], ddMul({dv[0], 0}, {t, 0}))) / R;
+        nw.y = ddValue(ddAdd(rel[1], ddMul({dv[1], 0}, {t, 0}))) / R;
+        nw.z = ddValue(ddAdd(rel[2], ddMul({dv[2], 0}, {t, 0}))) / R;
+        out.add({t, b.toLocal.point(od + d * t), normalize(b.toLocal.vector(nw))});
+    }
+    return out.n;
+}
+
 template <class T>
 OWEC_HD bool cylinderRoots(const V3<T>& o, const V3<T>& d, T R, T& t0, T& t1) {
     t0 = t1 = T(0);

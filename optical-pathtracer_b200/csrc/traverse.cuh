@@ -127,9 +127,19 @@ __device__ __forceinline__ bool analyticCandidate(const DeviceScene& sc, const R
     int n;
     // contacts: another surface through the anchor may lie just behind it (world.cpp:473-476); such
     // roots must lie within the rounding of the origin along the surface normal (checked below)
-    if constexpr (Full)
-        n = analyticCrossings<R, Rr, true>(bd, sc.shapeData + bd.dataOffset, lo, ld, -Rr(64) * Rr(q.errN), Rr(best),
-                                           b == q.depB, hits, Rr(qs.errN), Rr(q.errN));
+    const Rr tLow = Full ? -Rr(64) * Rr(q.errN) : Rr(0);
+    bool solved = false;
+    if constexpr (sizeof(Rr) == sizeof(double)) {
+        // a ray near a sphere far larger than its distance from it: the double-double solve
+        if (nearSphere(bd, q.od)) {
+            n = nearSphereCrossings(bd, q.od, V3<double>(q.d), tLow, double(best), hits);
+            solved = true;
+        }
+    }
+    if (solved) {
+    } else if constexpr (Full)
+        n = analyticCrossings<R, Rr, true>(bd, sc.shapeData + bd.dataOffset, lo, ld, tLow, Rr(best), b == q.depB, hits,
+                                           Rr(qs.errN), Rr(q.errN));
     else n = analyticCrossings<R, Rr, false>(bd, nullptr, lo, ld, Rr(0), Rr(best), false, hits);
 #pragma unroll
     for (int i = 0; i < 2; ++i) {

@@ -11,7 +11,11 @@
 //   ok|FAIL <file> <detector>: <report>  the comparison (consistent() of ComparisonReport)
 // Exits 1 when any comparison fails, 0 otherwise.
 //
-// Usage: owe_scene_suite [--width W] [--spp S] [--runs R] [--all-detectors] FILE...
+// With --same-streams N, each scene and detector is rendered instead on both backends from the same
+// seed, N one-sample passes, and the pixels whose images differ beyond 1e-4 relative are listed
+// (one-sample paths that make different decisions): for locating a difference the statistics find.
+//
+// Usage: owe_scene_suite [--width W] [--spp S] [--runs R] [--all-detectors] [--same-streams N] FILE...
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -26,9 +30,35 @@
 
 using namespace owe;
 
+namespace {
+
+Image renderOn(const std::string& name, const Scene& sc, int di, RenderSettings rs, int passes) {
+    rs.backend = name;
+    auto r = backend(name).createRenderer(sc, di, rs);
+    for (int k = 0; k < passes; ++k) r->runPass(1);
+    return r->resolve();
+}
+
+void sameStreams(const std::string& file, const Scene& sc, int di, const RenderSettings& rs, int passes) {
+    const Image a = renderOn("cpu", sc, di, rs, passes), b = renderOn("cuda", sc, di, rs, passes);
+    int differ = 0, listed = 0;
+    const int n = a.width * a.height;
+    for (int i = 0; i < n; ++i) {
+        const double ya = a.xyz[3 * size_t(i) + 1], yb = b.xyz[3 * size_t(i) + 1];
+        if (std::fabs(ya - yb) <= 1e-4 * std::max(std::fabs(ya), 1e-3)) continue;
+        ++differ;
+        if (listed++ < 12) std::printf("  pixel (%d, %d): cpu %.6g cuda %.6g\n", i % a.width, i / a.width, ya, yb);
+    }
+    std::printf("SAME-STREAMS %s %s: %d passes, %d of %d pixels differ, mean Y cpu %.6g cuda %.6g\n", file.c_str(),
+                sc.detectors[size_t(di)]->name.c_str(), passes, differ, n, a.meanY(), b.meanY());
+}
+
+}  // namespace
+
 int main(int argc, char** argv) {
     int width = 64, spp = 8, runs = 6;
     bool allDetectors = false;
+    int sameStreamPasses = 0;
     std::vector<std::string> files;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
@@ -36,6 +66,7 @@ int main(int argc, char** argv) {
         else if (a == "--spp" && i + 1 < argc) spp = std::atoi(argv[++i]);
         else if (a == "--runs" && i + 1 < argc) runs = std::atoi(argv[++i]);
         else if (a == "--all-detectors") allDetectors = true;
+        else if (a == "--same-streams" && i + 1 < argc) sameStreamPasses = std::atoi(argv[++i]);
         else files.push_back(a);
     }
     int failures = 0;
@@ -65,6 +96,15 @@ int main(int argc, char** argv) {
             adaptToBackend(a);
             adaptToBackend(b);
             b.integrator = a.integrator;  // the one both implement: the comparison is like for like
+            if (sameStreamPasses > 0) {
+                try {
+                    sameStreams(file, sc, di, a, sameStreamPasses);
+                } catch (const std::exception& e) {
+                    std::printf("REFUSED %s %s: %s\n", file.c_str(), det.name.c_str(), e.what());
+                }
+                std::fflush(stdout);
+                continue;
+            }
             try {
                 const ComparisonReport r = compareRenderers(sc, di, a, b, spp, runs, 4);
                 const bool ok = r.consistent();

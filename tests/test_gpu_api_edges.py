@@ -66,8 +66,8 @@ def test_no_samples_and_no_rays_are_no_ops():
 
 
 def test_rays_that_meet_nothing():
-    """Rays from inside the room pointing out through its open side, and rays far outside pointing
-    away: no boundary, infinite distance."""
+    """Rays far above the scene pointing away from it: no boundary (0xFFFFFFFE, the reference's
+    kNone), infinite distance."""
     desc = scenes.lamp_over_floor(8, 6).desc()
     rng = np.random.default_rng(3)
     o = rng.uniform(-1, 1, size=(1000, 3)) + np.array([0.0, 0.0, 50.0])
@@ -76,7 +76,7 @@ def test_rays_that_meet_nothing():
         c.upload(desc)
         c.build_bvh()
         b, p, t = c.cast_rays(o, d)
-    assert np.all(b == 0xFFFFFFFF) and np.all(np.isinf(t))
+    assert np.all(b == 0xFFFFFFFE) and np.all(np.isinf(t))
 
 
 def test_one_pixel_film():

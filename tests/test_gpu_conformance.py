@@ -65,7 +65,11 @@ def test_reference_conformance_suite_passes_on_cuda():
     res = parse(text)
     assert res, text[-2000:]
     ran_on_cuda = [t for t, v in res.items() if "cuda" in v["backends"]]
-    cuda_failures = {t: v["failures"]["cuda"] for t, v in res.items() if "cuda" in v["failures"]}
+    # a missing model file met while a listed case runs a backend's turn is the data's failure, not
+    # the backend's
+    data_error = ("OBJ file has no faces", "cannot read image", "cannot open")
+    cuda_failures = {t: v["failures"]["cuda"] for t, v in res.items() if "cuda" in v["failures"]
+                     and not (t in MISSING_DATA and all(any(e in l for e in data_error) for l in v["failures"]["cuda"]))}
     other = {t: v["failures"] for t, v in res.items() if v["status"] == "FAIL" and t not in MISSING_DATA
              and "cuda" not in v["failures"]}
     assert not cuda_failures, cuda_failures

@@ -255,3 +255,30 @@ def test_reflected_moonlight_matches_the_analytic_answer(precision):
     measured = float(img[:, :, 1].mean())
     assert abs(measured / expected - 1) < 0.015, (measured, expected, st)
     assert st["inconsistencies"] == 0 and st["leaks"] == 0 and st["device_faults"] == 0, st
+
+
+@pytest.mark.parametrize("precision", [A.PRECISION_MIXED, A.PRECISION_FP64])
+def test_planetary_ground_follows_the_reference(precision):
+    """The reference's planetary-surface regression (benchmarks/regressions/planetary_ground.owe): the
+    ground is a sphere of the Earth's radius, so a ray leaving it starts 6.4e6 m from the sphere's
+    centre, where |o - c|^2 - R^2 cancels in FP64 and the reference switches to its double-double
+    solve (intersectNearSphere). One-sample paths make the reference's decisions, 64-spp films on the
+    same streams agree, and no path meets an inconsistent region."""
+    desc = scenes.planetary_ground().desc()
+    ref = ReferenceEngine(desc)
+    s = A.make_settings(seed=7, max_depth=8, precision=precision)
+    one_ref, _ = ref.render(s, 1, passes=1)
+    many_ref, st_ref = ref.render(s, 1, passes=64)
+    with _ctx(desc, s) as c:
+        c.run_pass(1)
+        one = c.resolve()[0]
+        c.reset_film()
+        c.run_pass(64)
+        many = c.resolve()[0]
+        st = c.stats()
+    a, b = one_ref[..., 1], one[..., 1]
+    close = np.abs(a - b) <= 1e-4 * np.maximum(np.abs(a), 1e-3)
+    assert close.mean() > 0.99, close.mean()
+    assert abs(many[..., 1].mean() / many_ref[..., 1].mean() - 1) < 2e-3
+    assert st["inconsistencies"] == 0 and st["leaks"] == 0 and st["device_faults"] == 0, st
+    assert st_ref["inconsistencies"] == 0
