@@ -128,6 +128,9 @@ int main(int argc, char** argv) {
             const int w0 = det.width, h0 = det.height;
             det.width = std::min(width, w0);
             det.height = std::max(1, int(std::lround(double(h0) * det.width / std::max(1, w0))));
+            // the detector's derived quantities (an observer's field of view across, its frame) follow
+            // the new film, as when the scene was built
+            det.prepare(sc.world);
             RenderSettings a = sc.settingsFor(di), b = a;
             a.backend = "cpu";
             b.backend = "cuda";
