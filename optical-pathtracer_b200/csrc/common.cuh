@@ -8,8 +8,12 @@
 
 #if defined(__CUDACC__)
 #define OWEC_HD __host__ __device__ __forceinline__
+// Out of line on the device: a rarely taken branch whose registers would otherwise count against the
+// hot loop around it.
+#define OWEC_HD_COLD __host__ __device__ __noinline__ inline
 #else
 #define OWEC_HD inline
+#define OWEC_HD_COLD inline
 #endif
 
 namespace owec {

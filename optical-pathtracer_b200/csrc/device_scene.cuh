@@ -105,8 +105,9 @@ struct DeviceScene {
     const double* shapeData;  // the shapes' data, addressed by DBoundary::dataOffset
     int32_t simpleOptics;     // 1: every boundary Lambertian, absorbing or detecting, no null boundary,
                               // no region's medium absorbs or scatters (the particles' lean event kernel)
-    int32_t fullFeatures;     // 1: shapes beyond spheres, conic sags, plain apertures and cylinders, or
-                              // textured materials (the kernels' Full instantiations)
+    int32_t fullFeatures;     // 1: shapes beyond spheres, conic sags, plain apertures and cylinders, a
+                              // planet-sized sphere, contacts or textured materials (the kernels' Full
+                              // instantiations)
     uint32_t nRegions, nBoundaries, nLights, nMedia;
     const WideNode* nodes;
     const PrimRec* prims;

@@ -979,6 +979,10 @@ void uploadScene(owec_ctx& c, const owec_scene_desc& d) {
             b.shape == OWEC_SHAPE_DOME || b.shape == OWEC_SHAPE_WAVES || (b.shape == OWEC_SHAPE_SAG && b.data_count > 0) ||
             (b.shape == OWEC_SHAPE_PLANE && int(b.params[0]) == OWEC_APERTURE_DISK_HOLE))
             ds.fullFeatures = 1;
+        // a sphere of planetary size (the reference's scenes have 1.7e6 m and more; their lab-sized
+        // spheres stay under 50): rays near it take the double-double solve, in the Full instantiation
+        // only, so that the lean traversal's registers stay those of a scene without one
+        if (b.shape == OWEC_SHAPE_SPHERE && b.params[0] >= kNearSphereMinRadius) ds.fullFeatures = 1;
     }
     for (uint32_t i = 0; i < d.n_optics; ++i)
         if (d.optics[i].texture != OWEC_TEXTURE_NONE || d.optics[i].aim_share > 0) ds.fullFeatures = 1;

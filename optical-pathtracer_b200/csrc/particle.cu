@@ -134,6 +134,7 @@ __device__ void queueConnection(const DeviceScene& sc, PathBuffers<RT<M>>& pb, Q
     sr.endRegion = sc.det.region;
     sr.depB = depB;
     sr.depP = depP;
+    sr.endB = kNone;
     sr.path = path;
     sr.errN = errN;
     for (int j = 0; j < NW; ++j) sr.contrib[j] = c[j];

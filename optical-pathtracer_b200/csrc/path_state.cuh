@@ -118,10 +118,12 @@ struct alignas(16) ShadowRay {
     uint32_t region;      // region the segment starts in
     uint32_t endRegion;   // region it must arrive in (kNone: the ambient region for the sun)
     uint32_t depB, depP;
+    uint32_t endB;        // the light's boundary (kNone: the sun, or an eye the ray connects to)
     uint32_t path;
     float errN;
     float contrib[4];     // beta * f * Le * cos * w / pdf, before transmittance
 };
+static_assert(sizeof(ShadowRay<float>) == 96, "a mixed-precision shadow record stays six 16-byte words");
 
 struct Queues {
     uint32_t* active[2];

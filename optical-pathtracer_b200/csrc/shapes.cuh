@@ -146,9 +146,12 @@ OWEC_HD double ddValue(const DDouble& a) { return a.hi + a.lo; }
 // Whether a ray from od lies near boundary b's sphere against the sphere's size (a planet's surface
 // under the camera): there |od - c|^2 - R^2 cancels to nothing in FP64 once od - c is rounded, and
 // the reference solves the quadratic in double-double arithmetic (needsNearSphere, intersectNearSphere,
-// src/owe/scene/world.cpp:404-438). The same switch.
+// src/owe/scene/world.cpp:404-438). The same switch, for spheres of kNearSphereMinRadius and more:
+// for smaller ones the FP64 roots of a ray leaving the sphere stay within the refined departure
+// window, and a scene with a larger one runs the Full instantiations, the only ones that ask.
+constexpr double kNearSphereMinRadius = 64.0;
 OWEC_HD bool nearSphere(const DBoundary& b, const V3<double>& od) {
-    if (b.shape != OWEC_SHAPE_SPHERE) return false;
+    if (b.shape != OWEC_SHAPE_SPHERE || !(b.params[0] >= kNearSphereMinRadius)) return false;
     const double R = b.params[0];
     const V3<double> c(b.toWorld.m[3], b.toWorld.m[7], b.toWorld.m[11]);
     return R > 4096 * fmax(1e-9, fabs(length(od - c) - R));
@@ -158,10 +161,10 @@ OWEC_HD bool nearSphere(const DBoundary& b, const V3<double>& od) {
 // depend on its frame's rotation): od - c exact as a double-double, the quadratic's coefficients in
 // double-double, the roots in the numerically stable form. Points and normals in the sphere's local
 // frame, as classicCrossings gives them (the normal from the exact od - c; the point converted from
-// the world point od + t d).
-OWEC_HD int nearSphereCrossings(const DBoundary& b, const V3<double>& od, const V3<double>& d, double tmin,
-                                       double tmax, AHits<double>& out) {
-    out.n = 0;
+// the world point od + t d). Out of line, its result by value: the callers' own hits stay in registers.
+OWEC_HD_COLD AHits<double> nearSphereCrossings(const DBoundary& b, V3<double> od, V3<double> d, double tmin,
+                                               double tmax) {
+    AHits<double> out;
     const double R = b.params[0];
     const double o[3] = {od.x, od.y, od.z}, dv[3] = {d.x, d.y, d.z};
     const double c[3] = {b.toWorld.m[3], b.toWorld.m[7], b.toWorld.m[11]};
@@ -174,7 +177,7 @@ OWEC_HD int nearSphereCrossings(const DBoundary& b, const V3<double>& od, const 
     }
     C = ddAdd(C, ddNeg(ddMul({R, 0}, {R, 0})));
     const double disc = ddValue(ddAdd(ddMul(B, B), ddNeg(ddMul(A, C))));
-    if (!(disc >= 0)) return 0;
+    if (!(disc >= 0)) return out;
     const double bv = ddValue(B), av = ddValue(A);
     const double q = -bv - copysign(sqrt(disc), bv);
     double t0 = q / av, t1 = q != 0 ? ddValue(C) / q : t0;
@@ -189,7 +192,7 @@ OWEC_HD int nearSphereCrossings(const DBoundary& b, const V3<double>& od, const 
         nw.z = ddValue(ddAdd(rel[2], ddMul({dv[2], 0}, {t, 0}))) / R;
         out.add({t, b.toLocal.point(od + d * t), normalize(b.toLocal.vector(nw))});
     }
-    return out.n;
+    return out;
 }
 
 template <class T>

@@ -100,13 +100,13 @@ __device__ SurfacePoint<R> hitGeometry(const DeviceScene& sc, const PathRay<R>& 
         sp.nLocal = bd.toLocal.vector(V3<double>(sp.n));
         return sp;
     }
-    if constexpr (sizeof(Rr) == sizeof(double)) {
+    if constexpr (Full && sizeof(Rr) == sizeof(double)) {
         // a hit on a sphere far larger than the ray's distance from it (a planet's surface): the
         // double-double solve, and the point on the ray in the world frame, where it keeps its digits
         if (nearSphere(bd, od)) {
-            AHits<double> hits;
             const double t = h.t, slack = 1e-6 * (1 + fabs(t));
-            const int n = nearSphereCrossings(bd, od, V3<double>(d), 0.0, t + slack, hits);
+            const AHits<double> hits = nearSphereCrossings(bd, od, V3<double>(d), 0.0, t + slack);
+            const int n = hits.n;
             if (n > 0) {
                 const AHit<double>& hb = (n == 2 && fabs(hits.h1.t - t) < fabs(hits.h0.t - t)) ? hits.h1 : hits.h0;
                 sp.p = od + V3<double>(d) * hb.t;

@@ -129,10 +129,11 @@ __device__ __forceinline__ bool analyticCandidate(const DeviceScene& sc, const R
     // roots must lie within the rounding of the origin along the surface normal (checked below)
     const Rr tLow = Full ? -Rr(64) * Rr(q.errN) : Rr(0);
     bool solved = false;
-    if constexpr (sizeof(Rr) == sizeof(double)) {
-        // a ray near a sphere far larger than its distance from it: the double-double solve
+    if constexpr (Full && sizeof(Rr) == sizeof(double)) {
+        // a ray near a planet-sized sphere: the double-double solve
         if (nearSphere(bd, q.od)) {
-            n = nearSphereCrossings(bd, q.od, V3<double>(q.d), tLow, double(best), hits);
+            hits = nearSphereCrossings(bd, q.od, V3<double>(q.d), tLow, double(best));
+            n = hits.n;
             solved = true;
         }
     }
@@ -427,7 +428,7 @@ struct Traversal {
             NodeWords nd;
             loadNode(sc.nodes, node, nd);
             if (Count) ++nodeVisits;
-            const uint32_t mask = intersectChildren(nd, inv, oinv, T(0), Full ? tieLimit() : best);
+            const uint32_t mask = intersectChildren(nd, inv, oinv, T(0), (Full && !AnyHit) ? tieLimit() : best);
             const uint32_t inner = nd.a.w >> 24;
             nodeBase = nd.b.x;
             nodeBits = permuteSlots(mask & inner, first) | (inner << 8);
@@ -541,8 +542,10 @@ struct Traversal {
         V3<T> v0, v1, v2;
         uint32_t b, prim, kind;
         TriFetch<T>::get(sc, i, v0, v1, v2, b, prim, kind);
-        // the contact-resolving instantiation looks a tie window beyond the closest so far
-        const T limit = Full ? tieLimit() : best;
+        // the contact-resolving instantiation looks a tie window beyond the closest so far; a query for
+        // any crossing asks only about (0, tmax): the window there reached the light's own surface
+        // past the end of a shadow ray (4e-6 of its length short of it) whenever it was wider
+        const T limit = (Full && !AnyHit) ? tieLimit() : best;
         uint32_t flags = 0;
         if (kind == kPrimTriangle) {
             const V3<T> a = v0 - q.o, bb = v1 - q.o, c = v2 - q.o;

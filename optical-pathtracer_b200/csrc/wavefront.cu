@@ -200,6 +200,7 @@ __device__ void queueNee(const DeviceScene& sc, PathBuffers<RT<M>>& pb, Queues& 
     sr.endRegion = ls.boundary == kNone ? 0u : ls.region;
     sr.depB = depB;
     sr.depP = depP;
+    sr.endB = ls.boundary;
     sr.path = pathIdx;
     sr.errN = errN;
     for (int k = 0; k < NW; ++k) sr.contrib[k] = contrib[k];
@@ -545,6 +546,14 @@ __global__ void __launch_bounds__(128, Simple ? OWEC_SIMPLE_MIN_BLOCKS : OWEC_SH
 // media it crosses, and it must arrive in the region on the light's emitting side (the ambient
 // region for the sun). AnyHit: the scene has no null boundaries, so the first crossing blocks.
 //
+// Where a finite light lies: a scene without contacts has no other matter within the FP32 anchor
+// error of a light's surface, so a segment that stops that far short of the light point (4e-6 of
+// its length, plus the origin's error) passes its own face and misses nothing. With contacts (the
+// Full instantiation) matter may lie that close: the segment is walked to the light point and a
+// little past it, and a crossing clears it only when it is the light's own face there or lies
+// beyond the light point, as the reference's visibility endpoint decides (Tracer::transmittance
+// with an Endpoint, transport.cpp:237-284; an emitter is an analytic shape, one face).
+//
 // Persistent like kIntersect: a lane's job is one shadow ray, walked segment by segment through
 // null boundaries; its traversal advances a few visits per round and a finished lane takes the
 // next job. Splat: the rays are the light integrator's connections to the eye, whose
@@ -559,9 +568,11 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
     StackEntry* stack = stackMem + threadIdx.x;
     const uint32_t n = q.counts[3];
     Traversal<R, Ro, Rr, AnyHit, SharedStack, Count, Full> tr;
+    // the light point's identity decides (the Full instantiation's next-event rays)
+    constexpr bool kEndpoint = Full && !Splat && !AnyHit;
     R Tr[NW];
     double remaining = 0;
-    uint32_t job = 0, path = 0, region = 0, guard = 0, rays = 0, faults = 0;
+    uint32_t job = 0, path = 0, region = 0, guard = 0, rays = 0, faults = 0, endB = kNone;
     float errN0 = 0.f;
     bool alive = false, exhausted = false;
     for (;;) {
@@ -577,6 +588,7 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
             remaining = sr.tmax;
             guard = 0;
             errN0 = sr.errN;
+            endB = sr.endB;
             rq.od = rayOrigin(sr.o);
             rq.o = V3<R>(rq.od);
             rq.d = V3<R>(sr.d[0], sr.d[1], sr.d[2]);
@@ -627,6 +639,11 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
                         outcome = (!finite && region != 0) ? 2 : 1;
                     } else if (AnyHit) {
                         outcome = 2;
+                    } else if (kEndpoint && finite &&
+                               (h.t > remaining ||
+                                (h.boundary == endB && !(h.flags & kHitAmbiguous) &&
+                                 fabs(h.t - remaining) <= 4e-6 * remaining + double(errN0) + 1e-9))) {
+                        outcome = 1;  // the light's own face at the light point, or matter beyond it
                     } else {
                         const DBoundary& bd = sc.boundaries[h.boundary];
                         if (sc.optics[bd.optics].type != OWEC_SURF_NULL || (Full && (h.flags & kHitAmbiguous))) {
@@ -658,9 +675,13 @@ __global__ void OWEC_TRAVERSAL_BOUNDS kShadow(DeviceScene sc, PassParams pp, Pat
             }
         }
         if (begin) {
-            // the next segment, stopping short of the light's own surface
-            const double tq = finite ? remaining - (4e-6 * remaining + double(errN0) + 1e-9) : INFINITY;
-            if (guard >= 256 || (finite && tq <= 0)) {
+            // the next segment: short of the light's own surface, or with the light point's identity
+            // a little past it
+            const double w = 4e-6 * remaining + double(errN0) + 1e-9;
+            const double tq = finite ? (kEndpoint ? remaining + w : remaining - w) : INFINITY;
+            if (guard >= 256) {
+                outcome = 2;  // an exhausted walk is no evidence that the rest is clear (transport.cpp:283)
+            } else if (finite && tq <= 0) {
                 outcome = 1;
             } else {
                 rq.tmax = R(tq);
@@ -1016,7 +1037,9 @@ template <int M, bool Splat, bool Count, bool Full>
 void shadowKernelsOf(const DeviceScene& sc, const PassParams& pp, const PathBuffers<RT<M>>& pb, const Queues& q,
                      StatCounters* st, uint32_t* fetch, uint8_t* vis, const SplatTarget& film, int grid, cudaStream_t s) {
     const size_t smem = traversalSharedBytes(128);
-    if (pp.anyHitShadows) {
+    // next-event rays of a scene with contacts take the ordered walk, where the light point's
+    // identity decides what lies at its end
+    if (pp.anyHitShadows && !(Full && !Splat)) {
         kShadowVis<M, Count, Full><<<grid, 128, smem, s>>>(sc, pb, q, vis, fetch);
         kShadowApply<M, Splat><<<grid, 256, 0, s>>>(sc, pb, q, vis, st, film);
     } else {

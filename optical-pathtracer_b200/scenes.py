@@ -658,6 +658,22 @@ def planetary_ground(width=64, height=64, radius=6371000.0):
     return sb
 
 
+def far_nee_visibility(blocker="blocked", width=16, height=16):
+    """The reference's far next-event regression (benchmarks/regressions/far_nee_visibility.owe): a
+    white 0.4 m receiver at the origin lit only by a 0.1 m emitting sheet (radiance 1e12) 1e6 m
+    overhead, facing down, and a black 0.4 m screen 5 cm below the emitter that blocks all of its
+    light. blocker = "side" moves the screen 1 m aside, "beyond" to 5 cm above the emitter: both
+    leave the receiver lit alike. A segment shortened by a fraction of its length skips the 5 cm."""
+    sb = SceneBuilder()
+    down = np.diag([1.0, -1.0, -1.0])  # a half turn about x: the sheet's front faces down
+    sb.sheet(0.2, 0.2, pose(), sb.diffuse(0.8))
+    sb.sheet(0.05, 0.05, pose(down, (0.0, 0.0, 1.0e6)), sb.absorber(), sb.emission(sb.spectrum_constant(1.0e12)))
+    at = {"blocked": (0.0, 0.0, 1.0e6 - 0.05), "side": (1.0, 0.0, 1.0e6 - 0.05), "beyond": (0.0, 0.0, 1.0e6 + 0.05)}
+    sb.sheet(0.2, 0.2, pose(down, at[blocker]), sb.absorber())
+    sb.observer(width, height, (0.0, -0.1, 0.3), (0.0, 0.0, 0.0), fov_y_deg=20.0)
+    return sb
+
+
 def reflected_moonlight(width=16, height=16):
     """The reference's conformance check of light reflected by a distant body (tests/test_backends.cpp:
     69-97): a white two-sided Lambertian floor lit only by a full-phase Lambertian moon (albedo 0.3,

@@ -282,3 +282,52 @@ def test_planetary_ground_follows_the_reference(precision):
     assert abs(many[..., 1].mean() / many_ref[..., 1].mean() - 1) < 2e-3
     assert st["inconsistencies"] == 0 and st["leaks"] == 0 and st["device_faults"] == 0, st
     assert st_ref["inconsistencies"] == 0
+
+
+@pytest.mark.parametrize("precision", [A.PRECISION_MIXED, A.PRECISION_FP64])
+def test_a_screen_just_before_a_far_light_blocks_it(precision):
+    """The reference's far next-event regression (benchmarks/regressions/far_nee_visibility.owe,
+    tests/test_far_visibility.cpp): a screen 5 cm before a light 1e6 m away blocks all of its light,
+    so the film is exactly black; moved aside or behind the light, the same paths see the light and
+    give the same film, which the reference's on the same streams matches."""
+    s = A.make_settings(seed=11, max_depth=2, precision=precision)
+    films = {}
+    for where in ("blocked", "side", "beyond"):
+        with _ctx(scenes.far_nee_visibility(where).desc(), s) as c:
+            c.run_pass(64)
+            films[where] = c.resolve()[0]
+            st = c.stats()
+        assert st["inconsistencies"] == 0 and st["leaks"] == 0 and st["device_faults"] == 0, (where, st)
+    assert not films["blocked"].any()
+    assert films["side"][..., 1].mean() > 0
+    assert np.array_equal(films["side"], films["beyond"])
+    ref, _ = ReferenceEngine(scenes.far_nee_visibility("side").desc()).render(s, 1, passes=64)
+    assert abs(films["side"][..., 1].mean() / ref[..., 1].mean() - 1) < 2e-3
+
+
+@pytest.mark.parametrize("precision", [A.PRECISION_MIXED, A.PRECISION_FP64])
+def test_lamp_in_a_full_feature_scene_follows_the_reference(precision):
+    """The lamp over the floor with an absorbing sphere of 1e6 m far below the floor, out of every
+    path's way but for those that leave the floor's edge: a sphere that size sends the scene to the
+    Full instantiations. Their shadow queries stop at the shadow ray's end, short of the lamp: a
+    window past it would find the lamp's own surface and darken the floor. One-sample paths make the
+    reference's decisions and the 64-spp films agree."""
+    sb = scenes.lamp_over_floor(24, 18)
+    sb.sphere_body(1.0e6, (0.0, 0.0, -1.0e7), sb.medium_opaque(), sb.absorber())
+    desc = sb.desc()
+    ref = ReferenceEngine(desc)
+    s = A.make_settings(seed=5, max_depth=8, precision=precision)
+    one_ref, _ = ref.render(s, 1, passes=1)
+    many_ref, _ = ref.render(s, 1, passes=64)
+    with _ctx(desc, s) as c:
+        c.run_pass(1)
+        one = c.resolve()[0]
+        c.reset_film()
+        c.run_pass(64)
+        many = c.resolve()[0]
+        st = c.stats()
+    a, b = one_ref[..., 1], one[..., 1]
+    close = np.abs(a - b) <= 1e-4 * np.maximum(np.abs(a), 1e-3)
+    assert close.mean() > 0.99, close.mean()
+    assert abs(many[..., 1].mean() / many_ref[..., 1].mean() - 1) < 2e-3
+    assert st["inconsistencies"] == 0 and st["leaks"] == 0 and st["device_faults"] == 0, st
