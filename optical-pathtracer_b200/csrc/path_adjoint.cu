@@ -150,8 +150,10 @@ __device__ __forceinline__ void gather(PathTangents& tg, double beta, const Dual
 }
 
 // The visibility and transmittance of a next-event sample (kShadowVis and kShadowApply: any-hit
-// visibility short of the light, the medium's Beer-Lambert factor, the arrival regions). Returns
-// whether the segment is clear; Tr receives the transmittance per wavelength.
+// visibility short of the light, the medium's Beer-Lambert factor, the arrival regions; in the Full
+// instantiation kShadow's decision at a finite light: the closest crossing up to a little past the
+// light point, which clears the segment when it is the light's own face there or lies beyond it).
+// Returns whether the segment is clear; Tr receives the transmittance per wavelength.
 template <int M, bool Full>
 __device__ bool neeClear(const DeviceScene& sc, const LightSampleD& ls, const V3<double>& p, uint32_t region,
                          uint32_t depB, uint32_t depP, float errN, const float lambda[NW], typename Mode<M>::R Tr[NW],
@@ -161,7 +163,9 @@ __device__ bool neeClear(const DeviceScene& sc, const LightSampleD& ls, const V3
     using Rr = typename Mode<M>::Rr;
     const bool finite = !isinf(ls.dist);
     bool clear = true;
-    const double tq = finite ? ls.dist - (4e-6 * ls.dist + double(errN) + 1e-9) : INFINITY;
+    const double w = 4e-6 * ls.dist + double(errN) + 1e-9;
+    constexpr bool kEndpoint = Full;  // the light point's identity decides, as in the forward pass
+    const double tq = finite ? (kEndpoint ? ls.dist + w : ls.dist - w) : INFINITY;
     if (!(finite && tq <= 0)) {
         RayQuery<R> sq;
         V3<double> so = p;
@@ -178,12 +182,22 @@ __device__ bool neeClear(const DeviceScene& sc, const LightSampleD& ls, const V3
         sh.boundary = kNone;
         sh.t = INFINITY;
         sh.flags = 0;
-        const int vs = traceRay<R, Ro, Rr, true, Full>(sc, sq, stack, stride, sh);
-        if (vs == kTraceOverflow) {
-            fault = true;
-            return false;
+        if (kEndpoint && finite) {
+            const int vs = traceRay<R, Ro, Rr, false, Full>(sc, sq, stack, stride, sh);
+            if (vs == kTraceOverflow) {
+                fault = true;
+                return false;
+            }
+            clear = vs != kTraceHit || sh.t > ls.dist ||
+                    (sh.boundary == ls.boundary && !(sh.flags & kHitAmbiguous) && fabs(sh.t - ls.dist) <= w);
+        } else {
+            const int vs = traceRay<R, Ro, Rr, true, Full>(sc, sq, stack, stride, sh);
+            if (vs == kTraceOverflow) {
+                fault = true;
+                return false;
+            }
+            clear = vs != kTraceHit;
         }
-        clear = vs != kTraceHit;
     }
     for (int j = 0; j < NW; ++j) Tr[j] = R(1);
     const owec_medium& nm = sc.media[sc.regionMedium[region]];
