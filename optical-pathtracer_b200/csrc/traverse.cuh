@@ -87,11 +87,14 @@ __device__ __forceinline__ T behindWindow(const V3<T>& o) {
 }
 
 // The acceptance rule of a candidate crossing at distance t with (unnormalised) normal n. Near the
-// anchor the departed boundary is excluded, and a crossing counts only if it is met from the ray's
-// region. Contacts (the contact-resolving instantiation): of a departed mesh only the departed
-// triangle is excluded, so the far face of a plate thinner than the anchor's error is still met
-// (World::intersect's mesh departure, src/owe/scene/world.cpp:463-471; MeshShape::intersect).
-template <class T, bool Contacts = false>
+// anchor a departed analytic boundary is excluded, and a crossing counts only if it is met from the
+// ray's region. Of a departed mesh only the departed triangle is excluded (World::intersect's mesh
+// departure, src/owe/scene/world.cpp:463-471, and MeshShape::intersect's same-face test,
+// src/owe/scene/mesh.cpp:85): another of its triangles near the anchor counts when it is met from
+// the ray's region (the neighbour across a concave edge, which excluded let the ray into the body)
+// and not otherwise (a coplanar neighbour, met from behind: the root excludedRoot skips,
+// world.cpp:497-503); the far face of a plate thinner than the anchor's error is met the same way.
+template <class T>
 __device__ __forceinline__ bool acceptCrossing(const DeviceScene& sc, const RayQuery<T>& q, uint32_t b, uint32_t prim, bool mesh, T t,
                             const V3<T>& n) {
     if (mesh && b == q.depB && prim == q.depP) return false;
@@ -99,7 +102,7 @@ __device__ __forceinline__ bool acceptCrossing(const DeviceScene& sc, const RayQ
     const T nl = sqrt(dot(n, n));
     const bool near = fabs(t * dn) <= q.errN * nl;
     if (!near) return true;
-    if (b == q.depB && !(Contacts && mesh)) return false;
+    if (b == q.depB && !mesh) return false;
     if (q.region == kNone) return true;
     const DBoundary& bd = sc.boundaries[b];
     const uint32_t incident = dn < T(0) ? bd.front : bd.back;
@@ -148,7 +151,7 @@ __device__ __forceinline__ bool analyticCandidate(const DeviceScene& sc, const R
         const AHit<Rr>& h = hits.get(i);
         const V3<T> nw = V3<T>(bd.toWorld.vector(h.n));
         if (Full && !(h.t > Rr(0)) && (b == q.depB || !(fabs(T(h.t) * dot(q.d, nw)) <= behindWindow(q.o)))) continue;
-        if (!acceptCrossing<T, Full>(sc, qs, b, 0u, false, T(h.t), nw)) continue;
+        if (!acceptCrossing<T>(sc, qs, b, 0u, false, T(h.t), nw)) continue;
         tOut = h.t;
         frontOut = dot(q.d, nw) < T(0);
         cosOut = float(fabs(dot(q.d, nw)));
@@ -557,7 +560,7 @@ struct Traversal {
             if (!((Full ? t > T(0) || (b != q.depB && fabs(t * dn) <= behindWindow(q.o) * sqrt(dot(n, n))) : t > T(0)) &&
                   t < limit))
                 return false;
-            if (!acceptCrossing<T, Full>(sc, q, b, prim, true, t, n)) return false;
+            if (!acceptCrossing<T>(sc, q, b, prim, true, t, n)) return false;
             if constexpr (Full) {
                 const T c = fabs(dn) / sqrt(dot(n, n));
                 const double tD = refinedTriangleT(sc, i, t);
