@@ -37,10 +37,11 @@ def test_touching_blocks_and_thin_plates_like_the_reference(thickness):
             for key in st:
                 st[key] += gs[key]
     save_artifact(f"contacts_{thickness:g}", ref=np.array(runs_ref), gpu=np.array(runs_gpu))
-    # The reference's paths meet no inconsistent region. On the device in mixed precision about one
-    # in 10^6 still does (a crossing whose FP32 distance the traversal culled before the FP64 tie
-    # test saw it): the bound is one in 10^5. Before contacts were resolved one path in ten did;
-    # with ties decided on FP32 distances, about one in 7000.
+    # The reference's paths meet no inconsistent region. On the device in mixed precision none of
+    # 5.3 M paths did in the last count (16 seeds on each plate); the bound keeps a margin of one in
+    # 10^5 for a crossing whose FP32 distance the traversal might cull before the FP64 tie test sees
+    # it. Before contacts were resolved one path in ten met one; with ties decided on FP32 distances,
+    # about one in 7000; with FP64 ties, about one in 10^6.
     assert ref_stats["inconsistencies"] == 0 and ref_stats["leaks"] == 0, ref_stats
     assert st["inconsistencies"] + st["leaks"] <= 1e-5 * st["paths"], st
     assert st["device_faults"] == 0, st
