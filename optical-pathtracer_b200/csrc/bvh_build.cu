@@ -1,6 +1,7 @@
 // Device construction of the 8-wide quantised BVH.
 //
-//  1. 63-bit Morton codes of the primitives' box centres (21 bits per axis in the centres' bounds);
+//  1. 63-bit Morton codes of the primitives' box centres (21 bits per axis in the centres' bounds),
+//     the 64th bit set for a primitive larger than an eighth of the scene;
 //  2. a radix sort of (code, primitive) pairs (CUB);
 //  3. the binary radix tree over the sorted codes, one thread per inner node (Karras 2012), every
 //     node covering a contiguous range of sorted primitives;
@@ -78,14 +79,22 @@ __global__ void kMorton(const float4* lo, const float4* hi, uint32_t n, const in
     const float mx[3] = {orderedToFloat(bi[3]), orderedToFloat(bi[4]), orderedToFloat(bi[5])};
     const float4 a = lo[i], b = hi[i];
     const float c[3] = {0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z)};
+    const float size[3] = {b.x - a.x, b.y - a.y, b.z - a.z};
     uint64_t code = 0;
+    float sceneExt = 0.f, primExt = 0.f;
     for (int k = 0; k < 3; ++k) {
         const float ext = mx[k] - mn[k];
         float u = ext > 0.f ? (c[k] - mn[k]) / ext : 0.5f;
         u = fminf(fmaxf(u, 0.f), 1.f);
         const uint64_t q = uint64_t(fminf(u * 2097152.0f, 2097151.0f));
         code |= spread21(q) << (2 - k);
+        sceneExt = fmaxf(sceneExt, ext);
+        primExt = fmaxf(primExt, size[k]);
     }
+    // A primitive larger than an eighth of the scene (a wall, a floor, a lamp beside a finely
+    // tessellated body) sorts after all the others: the tree's root split separates the two sets,
+    // so no subtree of small primitives takes a wall's box.
+    if (primExt > 0.125f * sceneExt) code |= 1ull << 63;
     keys[i] = code;
     vals[i] = i;
 }
@@ -339,9 +348,9 @@ uint32_t buildWideBvh(const float4* primLo, const float4* primHi, uint32_t n, Bv
     size_t tempBytes = 0;
     cub::DoubleBuffer<uint64_t> dk(s.keys.get(), s.keysAlt.get());
     cub::DoubleBuffer<uint32_t> dv(s.vals.get(), s.valsAlt.get());
-    OWEC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, dk, dv, int(n), 0, 63, stream));
+    OWEC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, dk, dv, int(n), 0, 64, stream));
     s.cubTemp.reserve(tempBytes);
-    OWEC_CUDA(cub::DeviceRadixSort::SortPairs(s.cubTemp.get(), tempBytes, dk, dv, int(n), 0, 63, stream));
+    OWEC_CUDA(cub::DeviceRadixSort::SortPairs(s.cubTemp.get(), tempBytes, dk, dv, int(n), 0, 64, stream));
     const uint64_t* keys = dk.Current();
     const uint32_t* vals = dv.Current();
 
