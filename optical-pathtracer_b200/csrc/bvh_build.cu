@@ -29,6 +29,10 @@ namespace owec {
 namespace {
 
 constexpr uint32_t kLeafMax = 3;
+// The size, against the scene's, from which a primitive counts as large (sorted after the others).
+#ifndef OWEC_LARGE_PRIMITIVE
+#define OWEC_LARGE_PRIMITIVE 0.125f
+#endif
 constexpr uint32_t kNoParent = 0xFFFFFFFFu;
 
 __device__ __forceinline__ uint64_t spread21(uint64_t v) {
@@ -94,7 +98,7 @@ __global__ void kMorton(const float4* lo, const float4* hi, uint32_t n, const in
     // A primitive larger than an eighth of the scene (a wall, a floor, a lamp beside a finely
     // tessellated body) sorts after all the others: the tree's root split separates the two sets,
     // so no subtree of small primitives takes a wall's box.
-    if (primExt > 0.125f * sceneExt) code |= 1ull << 63;
+    if (primExt > OWEC_LARGE_PRIMITIVE * sceneExt) code |= 1ull << 63;
     keys[i] = code;
     vals[i] = i;
 }
